@@ -1,0 +1,315 @@
+"""Throughput of the FIT leap-frog wake stepper on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload lossy_256|cavity_40] [--dtype float64|float32]
+
+A step is one wakesolve step over the whole grid: Gaussian beam current on
+the beam line, capture of the 3x3 Ez window around the test line, H
+half-step and E half-step (one fused kernel launch).  Default workload:
+256x256x512 cells (33.5 M) FP64, lossy-wall cavity with pipe, 10-cell PML at
+both z ends (``wakis_b200.workloads.lossy_256``).  The state (4 x 805 MB
+ping-pong buffers) is far larger than L2, so no L2 flush is needed.
+
+value  = cells x steps / device time of the K timed steps (CUDA events,
+         max over ranks), in Gcell-steps/s, whole job.
+e2e    = the same through SolverFIT3D.run_with_io: every step copies the
+         beam-line current host->device and the captured Ez window
+         device->host (pinned buffers), wall clock around the K steps.
+Multi-GPU (torchrun): every rank runs an independent replica of the
+workload (weak scaling, no data-path collective); NCCL only carries the
+barrier and the max of the timings.
+
+--impl reference times the CPU oracle (a restatement of upstream's scipy
+solver) on the host cores with all threads, on a bounded sample of the
+workload (same geometry at 128x128x256), rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = {"float64": 96, "float32": 48}
+METRIC = "Gcell-steps/s"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic(workload, dtype):
+    """DRAM bytes per launch of the step kernel from the committed ncu
+    summary (profiles/traffic.json), if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(f"{workload}:{dtype}")
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    Q = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 8 or (self.uuid and self.uuid not in c[0]):
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax.append(float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    """CPU oracle on the host cores: Gcell-steps/s of upstream's scipy
+    algorithm on a bounded sample (same geometry, 128x128x256)."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    from oracle import fit as ofit
+    from wakis_b200 import workloads
+    sample = (128, 128, 256)
+    sp = workloads.spec(args.workload)
+    g0 = ofit.Grid(*workloads.BOUNDS, *sample)
+    m = workloads.cavity_mask(g0.x, g0.y, g0.z)
+    g = ofit.Grid(*workloads.BOUNDS, *sample, solids={"cavity": m}, materials={"cavity": "vacuum"})
+    so = ofit.Solver(g, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
+                     dtype=np.dtype(args.dtype).type, n_pml=sp["n_pml"])
+    cores = os.cpu_count() or 1
+    so.set_threads(cores)
+    beam = ofit.Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
+    for n in range(args.warmup):
+        beam.update(so, n * so.dt)
+        so.one_step()
+    t0 = time.perf_counter()
+    for n in range(args.warmup, args.warmup + args.steps):
+        beam.update(so, n * so.dt)
+        so.one_step()
+    t = time.perf_counter() - t0
+    value = so.N * args.steps / t / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.dtype == "float64" else "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.workload, "cells": int(np.prod(sp["shape"])),
+                       "sample_cells": so.N},
+            "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores,
+                             "kind": "port",
+                             "sample": f"oracle (scipy CSR, {cores} threads) on the "
+                                       f"{args.workload} geometry at 128x128x256, "
+                                       f"{args.steps} steps with beam"},
+            "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args, budget_s=20.0):
+    """Single-thread oracle on a bounded sample (rank 0, N=1 only)."""
+    from oracle import fit as ofit
+    from wakis_b200 import workloads
+    sample = (96, 96, 192)
+    sp = workloads.spec(args.workload)
+    g0 = ofit.Grid(*workloads.BOUNDS, *sample)
+    m = workloads.cavity_mask(g0.x, g0.y, g0.z)
+    g = ofit.Grid(*workloads.BOUNDS, *sample, solids={"cavity": m}, materials={"cavity": "vacuum"})
+    so = ofit.Solver(g, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
+                     dtype=np.dtype(args.dtype).type, n_pml=sp["n_pml"])
+    beam = ofit.Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
+    beam.update(so, 0.0)
+    so.one_step()
+    n, t0 = 0, time.perf_counter()
+    while True:
+        n += 1
+        beam.update(so, n * so.dt)
+        so.one_step()
+        if time.perf_counter() - t0 > budget_s / 2 or n >= 50:
+            break
+    t = time.perf_counter() - t0
+    return {"value": so.N * n / t / 1e9, "unit": "Gcell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"oracle (scipy CSR, 1 thread) on the {args.workload} geometry at "
+                      f"96x96x192, {n} steps with beam"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="lossy_256")
+    ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default=None,
+                    help="override the grid, e.g. 128x128x256 (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    sp = workloads.spec(args.workload)
+    dtype = np.dtype(args.dtype).type
+    shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else None
+    g, w, s = workloads.build_b200(args.workload, dtype=dtype, shape=shape)
+    N = s.N
+    bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
+              ).params(s)
+    ixt = int(np.abs(s.x - w.xtest).argmin())
+    iyt = int(np.abs(s.y - w.ytest).argmin())
+    total = args.warmup + args.steps
+    hist = torch.zeros((9, s.Nz, total), dtype=s._E[0].dtype, device=dev)
+    cap = (hist, ixt - 1, iyt - 1, 3, 3)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    # warm-up (includes the first-step ghost zeroing)
+    s._advance(args.warmup, 0, beam=bp, capture=cap)
+    torch.cuda.synchronize()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clk = Clocks(uuid)
+    time.sleep(0.3)
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(st)
+    s._advance(args.steps, args.warmup, beam=bp, capture=cap)
+    e1.record(st)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    t_dev = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
+    ms = float(t_dev.item())
+    launches = args.steps  # one fused step kernel per step
+
+    # end to end through the public API: per-step H2D line current, D2H window
+    prof = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
+    lines = np.stack([(prof.q * prof.v * prof.profile(s, n * s.dt) / s.dx[bp[0]] / s.dy[bp[1]])
+                      for n in range(total, total + args.steps)]).astype(dtype)
+    jz = torch.from_numpy(lines).pin_memory()
+    ez = torch.empty((args.steps, 9, s.Nz), dtype=s._E[0].dtype).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.run_with_io(jz, ez, step0=total)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    clocks = clk.stop()
+    t_e = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+    t_e2e = float(t_e.item())
+
+    if rank == 0:
+        value = N * args.steps * ws / (ms / 1e3) / 1e9
+        bpc = BYTES_PER_CELL[args.dtype]
+        achieved = bpc * N / (ms / 1e3 / args.steps) / 1e9
+        peak, src = _peaks()
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.dtype == "float64" else "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "cells": N, "grid": [s.Nx, s.Ny, s.Nz],
+                       "parallelism": f"replicas{ws}" if ws > 1 else "single",
+                       "l2": "state 4x%.0f MB > L2, no flush" % (3 * N * np.dtype(dtype).itemsize / 1e6),
+                       "step": "fused beam + Ez 3x3 capture + H and E half-steps"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": src,
+                         "bytes_per_cell_step": bpc,
+                         "traffic": _traffic(args.workload, args.dtype)},
+            "e2e": {"value": N * args.steps * ws / t_e2e / 1e9, "unit": "Gcell-steps/s",
+                    "h2d_bytes_per_step": int(jz[0].numel() * jz.element_size()),
+                    "d2h_bytes_per_step": int(ez[0].numel() * ez.element_size())},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

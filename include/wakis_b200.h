@@ -1,0 +1,194 @@
+/*
+ * wakis_b200 -- C ABI of the B200 (sm_100a) FIT leap-frog stepper and wake
+ * integration.
+ *
+ * Every entry point takes plain pointers and sizes (device pointers for
+ * field data, host pointers for descriptors), returns 0 on success, a
+ * positive WK_E_* code for an argument error detected on the host, or a
+ * negative value -(cudaError_t) for a CUDA error.  wk_last_error() returns a
+ * thread-local message for the last failure.  No entry point allocates or
+ * frees device memory: the caller (the Python host, through PyTorch) owns
+ * every buffer.  All work is enqueued on the given stream (a cudaStream_t
+ * passed as void*; NULL = legacy default stream) and is asynchronous.
+ *
+ * Field layout (same as upstream wakis/field.py:57-76,139-190): a field is a
+ * flat array of 3*N elements, N = Nx*Ny*Nz, holding the x, y and z component
+ * blocks; inside a block n = i + j*Nx + k*Nx*Ny.
+ */
+#ifndef WAKIS_B200_H
+#define WAKIS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WK_ABI_VERSION 1
+
+#define WK_OK 0
+#define WK_E_NULL 1      /* required pointer is NULL                     */
+#define WK_E_SHAPE 2     /* non-positive or too large dimension          */
+#define WK_E_DTYPE 3     /* unsupported dtype / id width                 */
+#define WK_E_ALIGN 4     /* pointer not aligned to its element size      */
+#define WK_E_RANGE 5     /* index (beam line, capture window) off-grid   */
+#define WK_E_MODE 6      /* inconsistent mode flags                      */
+
+#define WK_F64 0
+#define WK_F32 1
+
+/* J source used by the E half-step (upstream computes E += dt*(B*H - ieps*J)
+ * with J the stored current, solverFIT3D.py:492-503). */
+#define WK_J_ZERO 0      /* J = 0 everywhere except the beam line           */
+#define WK_J_SIGMA_E 1   /* J = sigma * E_old (the value upstream stored at
+                            the end of the previous step), beam line aside  */
+#define WK_J_ARRAY 2     /* J read from `J`; with use_conductivity the
+                            kernel also writes J = sigma * E_new back       */
+
+/*
+ * Geometry, coefficients and state of one FIT grid.  Field-type arrays
+ * (E, H, J, metrics, material table) hold `dtype` elements.
+ *
+ * Metric tables (values as upstream's diagonal matrices hold them after the
+ * boundary folding of wakis/boundaries.py:35-181, cast to dtype):
+ *   L{x,y,z}[Nx|Ny|Nz], tL{x,y,z}[Nx|Ny|Nz]    primal / dual edge lengths
+ *   iAx[j + k*Ny], iAy[i + k*Nx], iAz[i + j*Nx] inverse primal face areas
+ *   itAx, itAy, itAz (same indexing)           inverse dual face areas
+ * Materials: mat_id[n] (id_bytes = 1, 2 or 4 per cell) indexes
+ *   mat_table[9*id + {0,1,2}] = ieps (x,y,z), {3,4,5} = imu, {6,7,8} = sigma.
+ * Boundary faces, order x-lo, x-hi, y-lo, y-hi, z-lo, z-hi:
+ *   pec_face[f] = 0 masks the tangential E columns of the curl on face f
+ *   (C <- C*Dbc, boundaries.py:72-110); pmc_face[f] = 0 masks the tangential
+ *   H rows (C <- Dbc*C, boundaries.py:112-150).  has_pec / has_pmc say
+ *   whether the mask exists at all.  h_sum_desc = 1 sums the four terms of
+ *   an H row in descending column order (the row order scipy leaves in
+ *   the assembled H operator when exactly one of the two masks exists).
+ */
+typedef struct wk_fit_desc {
+  int Nx, Ny, Nz;
+  int dtype;               /* WK_F64 or WK_F32                               */
+  void* E[2];              /* ping-pong state buffers, 3N each; E[par] live  */
+  void* H[2];
+  int par;                 /* index of the live buffers                      */
+  void* J;                 /* 3N, used for WK_J_ARRAY                        */
+  int j_mode;
+  int use_conductivity;
+  const void* mat_id;
+  int id_bytes;
+  const void* mat_table;
+  int n_mat;
+  const void *Lx, *Ly, *Lz, *tLx, *tLy, *tLz;
+  const void *iAx, *iAy, *iAz, *itAx, *itAy, *itAz;
+  int pec_face[6];
+  int pmc_face[6];
+  int has_pec, has_pmc;
+  int h_sum_desc;
+  double dt;               /* solver time step (exact in dtype)              */
+  int dt_is_f32;           /* upstream dt is a float32 scalar               */
+  /* Gaussian beam on the z line (ixs, iys), wakis/sources.py:76-110:
+   * Jz(k) = ((q*v) * c0*exp(-(s-s0)^2/two_sig2) / dx_s) / dy_s,
+   * s = zc[k] - v*t, t = step*dt.                                         */
+  int beam_on;
+  int ixs, iys;
+  double b_qv, b_v, b_s0, b_c0, b_two_sig2, b_dx, b_dy;
+  const double* zc;        /* Nz cell-centre z coordinates                   */
+  /* Host-supplied line current instead of the Gaussian: with line_on, the
+   * Jz of line (ixs, iys) at step s is line[(s - line_step0) * Nz + k]
+   * (dtype elements, line_nsteps rows).                                     */
+  int line_on;
+  long long line_step0, line_nsteps;
+  const void* line;
+  /* Ez window capture before each step (wakis/routines.py:419-440):
+   * cap[((a*cap_nj + b)*Nz + k)*cap_nt + (step - cap_step0)]
+   *     = Ez(cap_i0+a, cap_j0+b, k)
+   * Every step run must satisfy cap_step0 <= step < cap_step0 + cap_nt (and
+   * line_step0 <= step < line_step0 + line_nsteps with line_on); the step
+   * entry points return WK_E_RANGE otherwise.                               */
+  int cap_on;
+  int cap_i0, cap_j0, cap_ni, cap_nj;
+  long long cap_nt, cap_step0;
+  void* cap;               /* dtype elements                                 */
+  int* status;             /* device status word (0 = ok), may be NULL       */
+} wk_fit_desc;
+
+/* ABI version (WK_ABI_VERSION). */
+int wk_version(void);
+
+/* Thread-local message for the last non-zero return. */
+const char* wk_last_error(void);
+
+/*
+ * Zero the ghost entries of the live E and H buffers before the first step.
+ * Replaces SolverFIT3D._set_ghosts_to_0 (wakis/solverFIT3D.py:820-840).
+ */
+int wk_zero_ghosts(const wk_fit_desc* d, void* stream);
+
+/*
+ * Advance `n_steps` leap-frog steps starting at global step index `step0`:
+ * for each step, (beam line J, Ez capture,) H <- H - dt*A*E, then
+ * E <- E + dt*(B*H - ieps*J) and, with WK_J_ARRAY and use_conductivity,
+ * J <- sigma*E.  Reads the buffers E[par], H[par] and leaves the result in
+ * E[par ^ (n_steps & 1)], H[par ^ (n_steps & 1)] (the caller flips `par`).
+ * Replaces SolverFIT3D._one_step (wakis/solverFIT3D.py:482-503) together with
+ * Beam.update (wakis/sources.py:76-110) and the per-step Ez save of
+ * RoutinesMixin.wakesolve (wakis/routines.py:435-445).
+ */
+int wk_fit_step(const wk_fit_desc* d, int n_steps, long long step0, void* stream);
+
+/*
+ * Same update with the two half-steps as separate in-place kernels (H pass,
+ * then E pass); the state stays in E[par], H[par].  Reference schedule used
+ * to cross-check the fused kernel of wk_fit_step.
+ */
+int wk_fit_step_split(const wk_fit_desc* d, int n_steps, long long step0, void* stream);
+
+/*
+ * Materialise J = sigma*E_live (dtype) into `J` (3N).  Replaces the
+ * J.fromarray(sigma*E) of wakis/solverFIT3D.py:502-503 for callers that read
+ * J between steps.
+ */
+int wk_sigma_e(const wk_fit_desc* d, void* J, void* stream);
+
+/*
+ * Longitudinal wake potential, calc_long_WP_3d / calc_long_WP
+ * (wakis/wakeSolver.py:310-420, 422-554), for n_win transverse positions
+ * processed in order w = 0..n_win-1:
+ *   acc = carry ? WP_3d[w-1][n] : 0          (carry-over of upstream 485/536)
+ *   for k: it = (long)((((z[k]+s[n])/v - zmin/v) - t0 + ti)/dt)
+ *          (counter-moving: (((z[nz-1-k]-s[n])/(-v) - zmax/(-v)) - t0) + ti)
+ *          if it < nt: acc += Ez(w, k_src, t_index[it]) * coef_k
+ *   WP_3d[w][n] = acc / qnorm
+ * Ez history: hist[(w_src*Nzh + kz)*hist_nt + t] (dtype hist_dtype), with
+ * w_src = win_map[w], kz = k + k_off (reversed index for counter-moving),
+ * t = key_order[it] (upstream sorts the '#%05d' keys as strings).
+ * coef_k = dz[k] (counter-moving: -dz[k]).  All double except hist.
+ */
+int wk_wake_potential(const void* hist, int hist_dtype, long long hist_nt, int Nzh,
+                      const int* win_map, int n_win, int carry,
+                      const double* z, const double* dz, int nz, int k_off,
+                      const double* s, int ns, const long long* key_order, long long nt,
+                      double v, double zmin, double zmax, double t0, double ti, double dt,
+                      double qnorm, int counter_moving, double* WP3d, void* stream);
+
+/*
+ * Transverse wake potential by Panofsky-Wenzel (wakis/wakeSolver.py:556-612):
+ *   int_w[n] = (sum_{m<n} WP3d[w][m]) * ds  (numpy pairwise summation order)
+ *   WPx[n] = -(int_{+1,0}[n] - int_{-1,0}[n]) / dxsum
+ *   WPy[n] = -(int_{0,+1}[n] - int_{0,-1}[n]) / dysum
+ * WP3d holds the 3x3 positions, w = (i+1)*3 + (j+1).
+ */
+int wk_trans_wake(const double* WP3d, int ns, double ds, double dxsum, double dysum,
+                  double* WPx, double* WPy, void* stream);
+
+/*
+ * Zero-padded DFT bins X[m] = sum_{n<len} x[n] * exp(-2*pi*i*m*n/N) for
+ * m = 0..nbins-1 (the bins 0 <= f < fmax of np.fft.fft(x, n=N) kept by
+ * calc_long_Z / calc_trans_Z, wakis/wakeSolver.py:679-766), for `nsig`
+ * real signals of length `len` stored back to back.  out is complex
+ * (re, im interleaved), out[(sig*nbins + m)*2 + {0,1}].
+ */
+int wk_dft_bins(const double* x, int nsig, long long len, long long N, int nbins,
+                double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WAKIS_B200_H */

@@ -1,0 +1,135 @@
+"""Generate the golden fixtures under tests/golden/ from the upstream Wakis
+package (pure Python, loaded through ``refshim``).
+
+Run on a machine that has the upstream source tree (default
+``/root/reference``, override with ``WAKIS_UPSTREAM``):
+
+    python tests/golden/make_golden.py
+
+Outputs (all small, committed):
+
+* ``upstream_test001.npz``  regression vectors of upstream
+  ``tests/test_001_pec_cubic_cavity.py`` (WP[::50], Z[::20], cumsum targets
+  and tolerances), extracted from that file's source with ``ast``.
+* ``step_cases.npz``  fields E, H, J after a few ``one_step`` calls of the
+  upstream solver on tiny grids, for a matrix of boundary conditions,
+  materials and dtypes, from seeded random initial fields, with a Gaussian
+  beam driving Jz.
+* ``wake_cases.npz``  WP, WP_3d, WPx, WPy, Z, Zx, Zy, f, s of upstream
+  ``wakesolve`` + ``WakeSolver.solve`` on small cavities.
+
+The case definitions live in ``tests/cases.py`` so that the tests rebuild the
+same inputs without the upstream package.
+"""
+
+import ast
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import refshim  # noqa: E402
+import cases  # noqa: E402
+
+
+def upstream_test001():
+    path = os.path.join(refshim.UPSTREAM, "tests", "test_001_pec_cubic_cavity.py")
+    tree = ast.parse(open(path).read())
+    vals = {}
+    for node in ast.walk(tree):
+        if isinstance(node, ast.Assign) and len(node.targets) == 1:
+            t = node.targets[0]
+            if isinstance(t, ast.Name) and t.id in ("WP", "Z"):
+                call = node.value
+                arr = ast.literal_eval(call.args[0])
+                vals[t.id] = np.array(arr[0] if isinstance(arr, tuple) else arr)
+    # cumsum targets: pytest.approx(<value>, <rel>) calls
+    approx = []
+    for node in ast.walk(tree):
+        if (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute)
+                and node.func.attr == "approx"):
+            approx.append([ast.literal_eval(a) for a in node.args])
+    assert len(approx) == 2 and "WP" in vals and "Z" in vals
+    np.savez(os.path.join(HERE, "upstream_test001.npz"), WP=vals["WP"], Z=vals["Z"],
+             WP_cumsum=approx[0][0], WP_cumsum_rel=approx[0][1],
+             Z_cumsum=approx[1][0], Z_cumsum_rel=approx[1][1],
+             WP_tol=50e-6, Z_tol=50e-5)
+    print("upstream_test001.npz:", len(vals["WP"]), "WP samples,", len(vals["Z"]), "Z samples")
+
+
+def step_cases(wakis):
+    out = {}
+    meta = []
+    for idx, c in enumerate(cases.STEP_CASES):
+        g = wakis.GridFIT3D(*c["bounds"], *c["shape"], verbose=0)
+        masks = cases.step_masks(c)
+        use_stl = bool(c["solids"])
+        if use_stl:
+            refshim.inject_solids(g, {k: masks[k] for k in c["solids"]}, c["solids"])
+        try:
+            s = wakis.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                                  dtype=np.dtype(c["dtype"]).type, bg=c["bg"],
+                                  n_pml=c["n_pml"], use_stl=use_stl, use_sibc=False)
+        except ValueError as e:
+            meta.append({"index": idx, "error": "ValueError", "msg": str(e)})
+            continue
+        E0, H0 = cases.initial_fields(c, s.N)
+        s.E.fromarray(E0.copy())
+        s.H.fromarray(H0.copy())
+        beam = wakis.sources.Beam(**c["beam"]) if c["beam"] else None
+        for n in range(c["steps"]):
+            if beam is not None:
+                beam.update(s, n * s.dt)
+            s.one_step()
+        for f in "EHJ":
+            out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+        for f in ("ieps", "imu", "sigma"):
+            out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+        out[f"c{idx}_dt"] = np.array(s.dt)
+        meta.append({"index": idx, "use_conductivity": bool(s.use_conductivity)})
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "step_cases.npz"), **out)
+    print("step_cases.npz:", len(cases.STEP_CASES), "cases")
+
+
+def wake_cases(wakis):
+    out = {}
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            for idx, c in enumerate(cases.WAKE_CASES):
+                g = wakis.GridFIT3D(*c["bounds"], *c["shape"], verbose=0)
+                m = cases.wake_mask(c, g.x, g.y, g.z)
+                refshim.inject_solids(g, {"cav": m}, {"cav": c["material"]})
+                w = wakis.WakeSolver(save=False, verbose=0, **c["wake"])
+                s = wakis.SolverFIT3D(g, w, bc_low=c["bc_low"], bc_high=c["bc_high"],
+                                      use_stl=True, bg=c["bg"], verbose=0,
+                                      dtype=np.dtype(c["dtype"]).type)
+                s.wakesolve(wakelength=c["wakelength"], compute_plane=c["compute_plane"])
+                names = ["s", "WP", "Z", "f", "lambdas", "lambdaf"]
+                if c["compute_plane"] == "both":
+                    names += ["WP_3d", "WPx", "WPy", "Zx", "Zy"]
+                for n in names:
+                    out[f"c{idx}_{n}"] = np.asarray(getattr(w, n))
+                out[f"c{idx}_Nt"] = np.array(s.Nt)
+                out[f"c{idx}_dt"] = np.array(s.dt)
+                out[f"c{idx}_Ez"] = s.E.toarray()[2 * s.N:].copy()
+        finally:
+            os.chdir(cwd)
+    np.savez_compressed(os.path.join(HERE, "wake_cases.npz"), **out)
+    print("wake_cases.npz:", len(cases.WAKE_CASES), "cases")
+
+
+if __name__ == "__main__":
+    wakis = refshim.install()
+    upstream_test001()
+    step_cases(wakis)
+    wake_cases(wakis)

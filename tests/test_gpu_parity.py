@@ -1,0 +1,186 @@
+"""Device parity: the wakis_b200 kernels (through the C ABI) against the
+oracle and the upstream fixtures.
+
+Tolerances: FP64 fields after N steps within 1e-12 relative (max-abs error
+over max-abs value, per field); wake potentials and impedances within 1e-10
+relative in the same sense.  Runs that involve no exponential (no beam) are
+required to be value-for-value identical to the oracle, which itself equals
+upstream value for value (tests/test_oracle.py); with the fused beam the
+only difference is CUDA's exp() against numpy's on the beam line.
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import cases  # noqa: E402
+from helpers import (b200_step_case, b200_wake_case, oracle_step_case,  # noqa: E402
+                     oracle_wake_case, rel_err)
+from oracle import fit as ofit  # noqa: E402
+from oracle import wake as owake  # noqa: E402
+
+FIELD_TOL = 1e-12
+WAKE_TOL = 1e-10
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _valid(idx):
+    try:
+        oracle_step_case(cases.STEP_CASES[idx])
+        return True
+    except ValueError:
+        return False
+
+
+VALID = [i for i in range(len(cases.STEP_CASES)) if _valid(i)]
+
+
+@pytest.mark.parametrize("split", [False, True])
+@pytest.mark.parametrize("idx", VALID)
+def test_steps_without_beam_are_exact(idx, split):
+    c = cases.STEP_CASES[idx]
+    o = oracle_step_case(c)
+    s = b200_step_case(c)
+    assert s.dt == o.dt
+    E0, H0 = cases.initial_fields(c, o.N)
+    o.E[:], o.H[:] = E0, H0
+    s.E.fromarray(E0)
+    s.H.fromarray(H0)
+    for _ in range(c["steps"]):
+        o.one_step()
+    s._advance(c["steps"], 0, split=split)
+    assert np.array_equal(s.E.numpy(), o.E)
+    assert np.array_equal(s.H.numpy(), o.H)
+    assert np.array_equal(s.J.numpy(), o.J)
+
+
+@pytest.mark.parametrize("idx", VALID)
+def test_steps_with_fused_beam_match_upstream(idx, golden_dir):
+    g = np.load(os.path.join(golden_dir, "step_cases.npz"))
+    c = cases.STEP_CASES[idx]
+    s = b200_step_case(c)
+    E0, H0 = cases.initial_fields(c, s.N)
+    s.E.fromarray(E0)
+    s.H.fromarray(H0)
+    from wakis_b200.sources import Beam
+    bp = Beam(**c["beam"]).params(s)
+    s._advance(c["steps"], 0, beam=bp)
+    tol = FIELD_TOL if c["dtype"] == "float64" else 1e-5
+    for f in "EHJ":
+        ref = g[f"c{idx}_{f}"]
+        got = getattr(s, f).numpy()
+        assert rel_err(got, ref) <= tol, (f, rel_err(got, ref))
+
+
+def test_generic_beam_path_matches_fused():
+    c = cases.STEP_CASES[2]   # conductive, PEC
+    from wakis_b200.sources import Beam
+    a = b200_step_case(c)
+    b = b200_step_case(c)
+    bm = Beam(**c["beam"])
+    bp = Beam(**c["beam"]).params(a)
+    for n in range(4):
+        a._advance(1, n, beam=bp)
+        bm.update(b, n * b.dt)
+        b.one_step()
+    assert rel_err(a.E.numpy(), b.E.numpy()) <= FIELD_TOL
+    assert rel_err(a.J.numpy(), b.J.numpy()) <= FIELD_TOL
+
+
+@pytest.mark.parametrize("idx", range(len(cases.WAKE_CASES)))
+def test_wakesolve_matches_upstream(idx, golden_dir):
+    g = np.load(os.path.join(golden_dir, "wake_cases.npz"))
+    c = cases.WAKE_CASES[idx]
+    s, w = b200_wake_case(c)
+    s.wakesolve(wakelength=c["wakelength"], compute_plane=c["compute_plane"])
+    assert s.Nt == int(g[f"c{idx}_Nt"])
+    assert np.array_equal(w.s, g[f"c{idx}_s"]) and np.array_equal(w.f, g[f"c{idx}_f"])
+    names = ["WP", "Z", "lambdaf"]
+    if c["compute_plane"] == "both":
+        names += ["WP_3d", "WPx", "WPy", "Zx", "Zy"]
+    tol = WAKE_TOL if c["dtype"] == "float64" else 1e-5
+    for n in names:
+        assert rel_err(getattr(w, n), g[f"c{idx}_{n}"]) <= tol, (n, rel_err(getattr(w, n),
+                                                                           g[f"c{idx}_{n}"]))
+    assert rel_err(s.E.numpy()[2 * s.N:], g[f"c{idx}_Ez"]) <= (FIELD_TOL if c["dtype"] ==
+                                                               "float64" else 1e-5)
+
+
+def test_wake_kernels_exact_on_oracle_history():
+    """Fed the oracle's own Ez history, the wake-potential and transverse
+    kernels reproduce the oracle value for value (same order of every sum)."""
+    c = cases.WAKE_CASES[0]
+    so, wo = oracle_wake_case(c)
+    owake.wakesolve(so, wo, c["wakelength"])
+    s, w = b200_wake_case(c)
+    keys = sorted(wo.hist)
+    Nt = len(keys)
+    hist = np.zeros((9, s.Nz, Nt))
+    for n in range(Nt):
+        hist[:, :, n] = wo.hist["#" + str(n).zfill(5)].reshape(9, s.Nz)
+    w.xf, w.yf, w.zf, w.t = wo.xf, wo.yf, wo.zf, wo.t
+    w.dx, w.dy, w.dz = wo.dx, wo.dy, wo.dz
+    w.wakelength = c["wakelength"]
+    w.set_history(torch.as_tensor(hist, device="cuda"), Nt)
+    w.solve("both")
+    assert np.array_equal(w.WP_3d, wo.WP_3d)
+    assert np.array_equal(w.WPx, wo.WPx) and np.array_equal(w.WPy, wo.WPy)
+    assert rel_err(w.Z, wo.Z) <= 1e-12 and rel_err(w.Zx, wo.Zx) <= 1e-12
+
+
+def _test001_mask(x, y, z):
+    from wakis_b200 import geometry
+    shp = geometry.Box(-0.025, 0.025, -0.025, 0.025, -0.015, 0.015, tol=1e-12) | \
+        geometry.Box(-0.0075, 0.0075, -0.0075, 0.0075, -1.0, 1.0, tol=1e-12)
+    return geometry.cell_mask(shp, x, y, z)
+
+
+def test_upstream_test001_regression_vectors(golden_dir):
+    """Upstream tests/test_001_pec_cubic_cavity.py on the device (float32,
+    50x50x150, 5184 steps) against its regression vectors and tolerances."""
+    import wakis_b200 as wb
+    gold = np.load(os.path.join(golden_dir, "upstream_test001.npz"))
+    g = wb.GridFIT3D(-0.025, 0.025, -0.025, 0.025, -0.05, 0.05, 50, 50, 150, verbose=0)
+    g.add_solid("cavity", _test001_mask(g.x, g.y, g.z), "vacuum")
+    w = wb.WakeSolver(q=1e-9, sigmaz=18.5e-3, beta=1.0, save=False, skip_cells=12, verbose=0)
+    s = wb.SolverFIT3D(g, w, bc_low=["pec"] * 3, bc_high=["pec"] * 3, use_stl=True, bg="pec",
+                       dtype=np.float32, verbose=0)
+    s.wakesolve(wakelength=1.0)
+    assert s.Nt == 5184
+    tol = float(gold["WP_tol"])
+    assert np.allclose(w.WP[::50], gold["WP"], rtol=tol, atol=tol)
+    assert np.cumsum(np.abs(w.WP))[-1] == pytest.approx(float(gold["WP_cumsum"]),
+                                                        float(gold["WP_cumsum_rel"]))
+    tz = float(gold["Z_tol"])
+    for fn in (np.abs, np.real, np.imag):
+        assert np.allclose(fn(w.Z)[::20], fn(gold["Z"]), rtol=tz, atol=tz)
+
+
+def test_cavity_40_wakesolve_matches_oracle():
+    """The 40x40x80 FP64 PEC cavity workload end to end (1896 steps)."""
+    from wakis_b200 import workloads
+    gb, wb_, sb = workloads.build_b200("cavity_40", dtype=np.float64)
+    sp = workloads.spec("cavity_40")
+    m = workloads.cavity_mask(gb.x, gb.y, gb.z)
+    go = ofit.Grid(*workloads.BOUNDS, *sp["shape"], solids={"cavity": m},
+                   materials={"cavity": "vacuum"})
+    wo = owake.WakeOracle(**sp["wake"])
+    so = ofit.Solver(go, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
+                     dtype=np.float64, wake_fmax=wo.fmax)
+    owake.wakesolve(so, wo, sp["wakelength"])
+    sb.wakesolve(wakelength=sp["wakelength"])
+    assert sb.Nt == so.Nt == 1896
+    for f in "EH":
+        assert rel_err(getattr(sb, f).numpy(), getattr(so, f)) <= FIELD_TOL, f
+    for n in ("WP", "WP_3d", "WPx", "WPy", "Z", "Zx", "Zy"):
+        assert rel_err(getattr(wb_, n), getattr(wo, n)) <= WAKE_TOL, n

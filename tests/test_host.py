@@ -1,0 +1,120 @@
+"""Host logic on the CPU: compact coefficients against the oracle's dense
+material fields and sparse operators, the kernels' update formula (numpy
+emulation) against the oracle's mat-vec step, geometry masks."""
+
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import cases
+import stencil_emulator as emu
+from helpers import oracle_step_case
+from wakis_b200 import coefficients, geometry
+from wakis_b200.gridFIT3D import GridFIT3D
+
+
+def _coef(c):
+    g = GridFIT3D(*c["bounds"], *c["shape"], verbose=0)
+    if c["solids"]:
+        masks = cases.step_masks(c)
+        for k, mat in c["solids"].items():
+            g.add_solid(k, masks[k], mat)
+    return coefficients.build(g, c["bc_low"], c["bc_high"], dtype=np.dtype(c["dtype"]).type,
+                              bg=c["bg"], use_stl=bool(c["solids"]), use_sibc=False,
+                              n_pml=c["n_pml"])
+
+
+def _valid_cases():
+    out = []
+    for i, c in enumerate(cases.STEP_CASES):
+        try:
+            oracle_step_case(c)
+        except ValueError:
+            continue
+        out.append(i)
+    return out
+
+
+VALID = _valid_cases()
+
+
+@pytest.mark.parametrize("idx", VALID)
+def test_coefficients_match_oracle(idx):
+    c = cases.STEP_CASES[idx]
+    o = oracle_step_case(c)
+    k = _coef(c)
+    assert k.dt == o.dt and type(k.dt) is type(o.dt)
+    ie, im, sg = coefficients.dense_materials(k)
+    assert np.array_equal(ie, o.ieps) and np.array_equal(im, o.imu)
+    assert np.array_equal(sg, o.sigma)
+    assert k.use_conductivity == o.use_conductivity
+    assert k.h_sum_desc == ((o.pec_mask is not None) + (o.pmc_mask is not None) == 1)
+
+
+@pytest.mark.parametrize("idx", VALID)
+def test_emulated_step_is_bitwise_equal_to_oracle(idx):
+    c = cases.STEP_CASES[idx]
+    o = oracle_step_case(c)
+    k = _coef(c)
+    E0, H0 = cases.initial_fields(c, o.N)
+    o.E[:], o.H[:] = E0, H0
+    o.zero_ghosts()
+    E, H = o.E.copy(), o.H.copy()
+    J = np.zeros_like(E)
+    o.step_0 = False
+    for _ in range(3):
+        Jin = o.J.copy()
+        o.one_step()
+        Hn = emu.h_update(k, E, H, k.dt)
+        assert np.array_equal(Hn, o.H)
+        En = emu.e_update(k, E, Hn, Jin, k.dt)
+        assert np.array_equal(En, o.E)
+        E, H = En, Hn
+
+
+def test_abc_views_reference_semantics_documented():
+    # both-ends ABC on one axis makes upstream drop the low-face snapshot;
+    # the flags still fold the high-face metric copy (boundaries.py:152-181)
+    pec, pmc, has_pec, has_pmc = coefficients.boundary_flags(["pec", "pec", "abc"],
+                                                             ["pec", "pec", "abc"])
+    assert pec == [0, 0, 0, 0, 1, 1] and has_pec and not has_pmc
+
+
+def _cube_stl(path, lo, hi):
+    # 12 triangles of an axis-aligned box, ASCII STL
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]])
+    faces = [(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4),
+             (1, 2, 6), (1, 6, 5), (2, 3, 7), (2, 7, 6), (3, 0, 4), (3, 4, 7)]
+    with open(path, "w") as f:
+        f.write("solid box\n")
+        for a, b, cc in faces:
+            f.write(" facet normal 0 0 0\n  outer loop\n")
+            for p in (a, b, cc):
+                f.write("   vertex %.9e %.9e %.9e\n" % tuple(v[p]))
+            f.write("  endloop\n endfacet\n")
+        f.write("endsolid box\n")
+
+
+def test_stl_voxeliser_matches_analytic_box():
+    x = np.linspace(-0.01, 0.01, 21)
+    y = np.linspace(-0.01, 0.01, 17)
+    z = np.linspace(-0.02, 0.02, 33)
+    lo, hi = (-0.0043, -0.0051, -0.0077), (0.0061, 0.0037, 0.0093)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "box.stl")
+        _cube_stl(p, lo, hi)
+        m_stl = geometry.cell_mask(geometry.STLSolid(p), x, y, z)
+    m_box = geometry.cell_mask(geometry.Box(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]), x, y, z)
+    assert m_stl.sum() > 0 and np.array_equal(m_stl, m_box)
+
+
+def test_surface_mask_marks_both_sides_of_interface():
+    m = np.zeros((6, 6, 6), bool)
+    m[2:4, 2:4, 2:4] = True
+    s = geometry.surface_mask(m)
+    assert s[2, 2, 2] and s[1, 2, 2] and not s[0, 0, 0]

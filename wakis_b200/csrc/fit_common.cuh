@@ -1,0 +1,242 @@
+// Shared device code of the FIT leap-frog kernels.
+//
+// The update reproduces upstream's sparse products term by term
+// (wakis/solverFIT3D.py:312-322,482-503):
+//   H_r -= sum_c fl(fl(dt * fl(fl(iA_r*imu_r) * L_c)) * E_c) * s_rc
+//   E_r += dt * (sum_c fl(fl(fl(ieps_r*itA_r) * tL_c) * H_c) * s_rc - ieps_r*J_r)
+// with s_rc = +-1 the curl signs, the same rounding of every product and
+// the same summation order as scipy's CSR mat-vec over the assembled rows
+// (ascending column order, or descending for the H rows when exactly one
+// of the PEC/PMC masks was folded in).  All arithmetic uses explicit
+// round-to-nearest intrinsics so that no multiply-add is contracted.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wk {
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+
+template <typename T>
+struct FitParams {
+  int Nx, Ny, Nz;
+  long long N, NxNy;
+  T* E_in; T* H_in; T* E_out; T* H_out;
+  T* J;
+  int j_mode, use_cond;
+  const void* mat_id; int id_bytes;
+  const T* mat;
+  const T *Lx, *Ly, *Lz, *tLx, *tLy, *tLz;
+  const T *iAx, *iAy, *iAz, *itAx, *itAy, *itAz;
+  int pec_face[6], pmc_face[6];
+  int has_pec, has_pmc, h_desc;
+  T dt;
+  // beam
+  int beam_on, ixs, iys, dt_is_f32;
+  double dt64, b_qv, b_v, b_s0, b_c0, b_two_sig2, b_dx, b_dy;
+  float b_v32, dt32;
+  const double* zc;
+  int line_on;
+  long long line_step0, line_nsteps;
+  const T* line;
+  // capture
+  int cap_on, cap_i0, cap_j0, cap_ni, cap_nj;
+  long long cap_nt, cap_step0;
+  T* cap;
+  int* status;
+};
+
+__device__ __forceinline__ int load_id(const void* p, int bytes, long long n) {
+  if (bytes == 1) return ((const uint8_t*)p)[n];
+  if (bytes == 2) return ((const uint16_t*)p)[n];
+  return (int)((const uint32_t*)p)[n];
+}
+
+// Face masks: later faces overwrite earlier ones in the order x-lo, x-hi,
+// y-lo, y-hi, z-lo, z-hi (wakis/boundaries.py:92-101); component d is never
+// masked on the faces normal to it.
+__device__ __forceinline__ int face_val(const int* f, int d, int i, int j, int k,
+                                        int Nx, int Ny, int Nz) {
+  int v = 1;
+  if (d != 0) { if (i == 0) v = f[0]; if (i == Nx - 1) v = f[1]; }
+  if (d != 1) { if (j == 0) v = f[2]; if (j == Ny - 1) v = f[3]; }
+  if (d != 2) { if (k == 0) v = f[4]; if (k == Nz - 1) v = f[5]; }
+  return v;
+}
+
+// Cell coordinates of flat index n (0 <= n < N).
+struct Cell { int i, j, k; };
+__device__ __forceinline__ Cell cell_of(long long n, int Nx, int Ny) {
+  Cell c;
+  long long q = n / Nx;
+  c.i = (int)(n - q * Nx);
+  c.k = (int)(q / Ny);
+  c.j = (int)(q - (long long)c.k * Ny);
+  return c;
+}
+
+// Sum of four terms in ascending or descending order, starting from +0 as
+// scipy's csr_matvec does.
+template <typename T>
+__device__ __forceinline__ T sum4(T a, T b, T c, T d, bool desc) {
+  T z = T(0);
+  if (!desc) return add(add(add(add(z, a), b), c), d);
+  return add(add(add(add(z, d), c), b), a);
+}
+
+// Column factor of the H operator: primal length of the column component
+// at the column cell, 0 where the PEC mask removes that column.
+template <typename T>
+__device__ __forceinline__ T colL(const FitParams<T>& p, int d, int i, int j, int k) {
+  if (p.has_pec && !face_val(p.pec_face, d, i, j, k, p.Nx, p.Ny, p.Nz)) return T(0);
+  return d == 0 ? p.Lx[i] : (d == 1 ? p.Ly[j] : p.Lz[k]);
+}
+// Column factor of the E operator: dual length, 0 where the PMC mask
+// removes that H column.
+template <typename T>
+__device__ __forceinline__ T coltL(const FitParams<T>& p, int d, int i, int j, int k) {
+  if (p.has_pmc && !face_val(p.pmc_face, d, i, j, k, p.Nx, p.Ny, p.Nz)) return T(0);
+  return d == 0 ? p.tLx[i] : (d == 1 ? p.tLy[j] : p.tLz[k]);
+}
+
+// Neighbour cells in the flat-offset sense of upstream's difference
+// operators (P shifts by +1, +Nx, +Nx*Ny on the flat index and only stops at
+// the end of the block, wakis/solverFIT3D.py:207-209): stepping past i=Nx-1
+// lands on (0, j+1, k), past j=Ny-1 on (i, 0, k+1).
+__device__ __forceinline__ Cell plus_x(Cell c, int Nx, int Ny) {
+  Cell r = c; r.i++;
+  if (r.i == Nx) { r.i = 0; r.j++; if (r.j == Ny) { r.j = 0; r.k++; } }
+  return r;
+}
+__device__ __forceinline__ Cell plus_y(Cell c, int Ny) {
+  Cell r = c; r.j++;
+  if (r.j == Ny) { r.j = 0; r.k++; }
+  return r;
+}
+__device__ __forceinline__ Cell minus_x(Cell c, int Nx, int Ny) {
+  Cell r = c; r.i--;
+  if (r.i < 0) { r.i = Nx - 1; r.j--; if (r.j < 0) { r.j = Ny - 1; r.k--; } }
+  return r;
+}
+__device__ __forceinline__ Cell minus_y(Cell c, int Ny) {
+  Cell r = c; r.j--;
+  if (r.j < 0) { r.j = Ny - 1; r.k--; }
+  return r;
+}
+
+// H row update for component d at cell c (flat n), reading E from `Ein`
+// and H from `Hin`.  Returns the new H value.
+template <typename T>
+__device__ __forceinline__ T h_row(const FitParams<T>& p, const T* __restrict__ Ein,
+                                   T hold, int d, Cell c, long long n, int id) {
+  const long long N = p.N, NxNy = p.NxNy;
+  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
+  T iA = d == 0 ? p.iAx[c.j + (long long)c.k * Ny]
+                : (d == 1 ? p.iAy[c.i + (long long)c.k * Nx] : p.iAz[c.i + (long long)c.j * Nx]);
+  T R = mul(iA, p.mat[9 * id + 3 + d]);
+  if (p.has_pmc && !face_val(p.pmc_face, d, c.i, c.j, c.k, Nx, Ny, Nz)) R = T(0);
+  const T dt = p.dt;
+  // term(col comp e, column flat m, column cell cc, sign)
+  auto term = [&](int e, long long m, Cell cc, bool valid, T sgn) -> T {
+    if (!valid) return T(0);
+    T coef = mul(dt, mul(R, colL(p, e, cc.i, cc.j, cc.k)));
+    T v = mul(coef, Ein[(long long)e * N + m]);
+    return sgn > T(0) ? v : -v;
+  };
+  Cell kz = c; kz.k++;
+  bool vz = (n + NxNy) < N;
+  T t0, t1, t2, t3;
+  if (d == 0) {        // (C e)_x = +ey[n] - ey[n+NxNy] - ez[n] + ez[n+Nx]
+    Cell cy = plus_y(c, Ny);
+    t0 = term(1, n, c, true, T(1));
+    t1 = term(1, n + NxNy, kz, vz, T(-1));
+    t2 = term(2, n, c, true, T(-1));
+    t3 = term(2, n + Nx, cy, (n + Nx) < N, T(1));
+  } else if (d == 1) { // (C e)_y = -ex[n] + ex[n+NxNy] + ez[n] - ez[n+1]
+    Cell cx = plus_x(c, Nx, Ny);
+    t0 = term(0, n, c, true, T(-1));
+    t1 = term(0, n + NxNy, kz, vz, T(1));
+    t2 = term(2, n, c, true, T(1));
+    t3 = term(2, n + 1, cx, (n + 1) < N, T(-1));
+  } else {             // (C e)_z = +ex[n] - ex[n+Nx] - ey[n] + ey[n+1]
+    Cell cy = plus_y(c, Ny);
+    Cell cx = plus_x(c, Nx, Ny);
+    t0 = term(0, n, c, true, T(1));
+    t1 = term(0, n + Nx, cy, (n + Nx) < N, T(-1));
+    t2 = term(1, n, c, true, T(-1));
+    t3 = term(1, n + 1, cx, (n + 1) < N, T(1));
+  }
+  return sub(hold, sum4(t0, t1, t2, t3, p.h_desc != 0));
+}
+
+// Curl part of the E row for component d at cell c: sum_c B_rc * H_c, with
+// H values supplied by `hval(comp, flat)`.
+template <typename T, typename HV>
+__device__ __forceinline__ T e_curl(const FitParams<T>& p, int d, Cell c, long long n,
+                                    T ieps, HV hval) {
+  const long long NxNy = p.NxNy;
+  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
+  T itA = d == 0 ? p.itAx[c.j + (long long)c.k * Ny]
+                 : (d == 1 ? p.itAy[c.i + (long long)c.k * Nx] : p.itAz[c.i + (long long)c.j * Nx]);
+  T R = mul(ieps, itA);
+  if (p.has_pec && !face_val(p.pec_face, d, c.i, c.j, c.k, Nx, Ny, Nz)) R = T(0);
+  auto term = [&](int e, long long m, Cell cc, bool valid, T sgn) -> T {
+    if (!valid) return T(0);
+    T coef = mul(R, coltL(p, e, cc.i, cc.j, cc.k));
+    T v = mul(coef, hval(e, m));
+    return sgn > T(0) ? v : -v;
+  };
+  Cell km = c; km.k--;
+  bool vz = n >= NxNy;
+  T t0, t1, t2, t3;
+  if (d == 0) {        // +hy[n-NxNy] - hy[n] - hz[n-Nx] + hz[n]
+    Cell cy = minus_y(c, Ny);
+    t0 = term(1, n - NxNy, km, vz, T(1));
+    t1 = term(1, n, c, true, T(-1));
+    t2 = term(2, n - Nx, cy, n >= Nx, T(-1));
+    t3 = term(2, n, c, true, T(1));
+  } else if (d == 1) { // -hx[n-NxNy] + hx[n] + hz[n-1] - hz[n]
+    Cell cx = minus_x(c, Nx, Ny);
+    t0 = term(0, n - NxNy, km, vz, T(-1));
+    t1 = term(0, n, c, true, T(1));
+    t2 = term(2, n - 1, cx, n >= 1, T(1));
+    t3 = term(2, n, c, true, T(-1));
+  } else {             // +hx[n-Nx] - hx[n] - hy[n-1] + hy[n]
+    Cell cy = minus_y(c, Ny);
+    Cell cx = minus_x(c, Nx, Ny);
+    t0 = term(0, n - Nx, cy, n >= Nx, T(1));
+    t1 = term(0, n, c, true, T(-1));
+    t2 = term(1, n - 1, cx, n >= 1, T(-1));
+    t3 = term(1, n, c, true, T(1));
+  }
+  return sum4(t0, t1, t2, t3, false);
+}
+
+// Gaussian beam current on the line (ixs, iys) at step `step`
+// (wakis/sources.py:98-110).  With a float32 time step upstream evaluates
+// t = n*dt and v*t in float32 before the float64 profile; the value is
+// then stored into the dtype J array.
+template <typename T>
+__device__ __forceinline__ T beam_j(const FitParams<T>& p, long long step, int k) {
+  double vt;
+  if (p.dt_is_f32) {
+    float t32 = __fmul_rn((float)step, p.dt32);
+    vt = (double)__fmul_rn(p.b_v32, t32);
+  } else {
+    double t = __dmul_rn((double)step, p.dt64);
+    vt = __dmul_rn(p.b_v, t);
+  }
+  double s = __dsub_rn(p.zc[k], vt);
+  double u = __dsub_rn(s, p.b_s0);
+  double arg = __ddiv_rn(-__dmul_rn(u, u), p.b_two_sig2);
+  double prof = __dmul_rn(p.b_c0, exp(arg));
+  double jz = __ddiv_rn(__ddiv_rn(__dmul_rn(p.b_qv, prof), p.b_dx), p.b_dy);
+  return (T)jz;
+}
+
+}  // namespace wk

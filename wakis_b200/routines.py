@@ -1,0 +1,135 @@
+"""Time loops of the solver: ``wakesolve`` and ``emsolve`` (upstream
+wakis/routines.py:17-482).
+
+``wakesolve`` runs the whole loop on the device: the beam current and the
+capture of the Ez window around the test line (3x3 cells, or the line
+alone for compute_plane='longitudinal') are fused into the step kernel, the
+Ez history stays in device memory, and ``WakeSolver.solve`` integrates it
+there.  Only a user callback or field monitor makes the loop return to the
+host between steps, as upstream calls them every step.
+"""
+
+import time
+
+import numpy as np
+import torch
+
+from .sources import Beam
+
+
+class RoutinesMixin:
+    def wakesolve(self, wakelength, wake=None, callback=None, compute_plane="both",
+                  plot=False, save_J=False, add_space=None, use_field_monitor=False,
+                  field_monitor=None, **kwargs):
+        if wake is not None:
+            self.wake = wake
+        if self.wake is None:
+            raise AttributeError("Wake solver information not passed to the solver instantiation")
+        if add_space is not None:
+            self.wake.skip_cells = add_space
+        w = self.wake
+        self.xtest, self.ytest = w.xtest, w.ytest
+        self.ixt = int(np.abs(self.x - self.xtest).argmin())
+        self.iyt = int(np.abs(self.y - self.ytest).argmin())
+        longitudinal = compute_plane.lower() == "longitudinal"
+        if longitudinal:
+            xx, yy = self.ixt, self.iyt
+            i0, j0, ni, nj = self.ixt, self.iyt, 1, 1
+        else:
+            xx = slice(self.ixt - 1, self.ixt + 2)
+            yy = slice(self.iyt - 1, self.iyt + 2)
+            i0, j0, ni, nj = self.ixt - 1, self.iyt - 1, 3, 3
+            if i0 < 0 or j0 < 0 or i0 + 3 > self.Nx or j0 + 3 > self.Ny:
+                raise ValueError("the 3x3 Ez window around the test line leaves the grid")
+        w.wakelength = wakelength
+        self.ti, self.v = w.ti, w.v
+        z = self.z
+        tmax = (wakelength + self.ti * self.v + (z.max() - z.min())) / self.v
+        Nt = int(tmax / self.dt)
+        self.tmax, self.Nt = tmax, Nt
+
+        beam = Beam(q=w.q, sigmaz=w.sigmaz, beta=w.beta, xsource=w.xsource, ysource=w.ysource)
+        bp = beam.params(self)
+        hist = torch.zeros((ni * nj, self.Nz, max(Nt, 1)), dtype=self._E[0].dtype,
+                           device=self.device)
+        cap = (hist, i0, j0, ni, nj)
+
+        t0 = time.time()
+        if callback is None and not (use_field_monitor and field_monitor is not None):
+            self._advance(Nt, 0, beam=bp, capture=cap)
+        else:
+            for n in range(Nt):
+                self._advance(1, n, beam=bp, capture=cap)
+                if use_field_monitor and field_monitor is not None:
+                    field_monitor.update(self.E, self.dt)
+                if callback is not None:
+                    callback(self, n * self.dt)
+        torch.cuda.current_stream(self.device).synchronize()
+        self.beam = beam
+
+        w.xf, w.yf, w.zf = self.x[xx], self.y[yy], z[slice(0, self.Nz)]
+        w.dx, w.dy, w.dz = self.grid.dx, self.grid.dy, self.grid.dz
+        w.t = np.arange(0, Nt * self.dt, self.dt)
+        w.set_history(hist, n_steps=Nt, one_d=longitudinal)
+        w.solve(compute_plane=compute_plane)
+        self.logger.wakeSolver = w.logger.wakeSolver
+        self.logger.wakeSolver["wakelength"] = wakelength
+        self.logger.wakeSolver["simulationTime"] = time.time() - t0
+        if getattr(w, "save", False):
+            self.logger.save_logs(w.folder)
+
+    def emsolve(self, Nt, source=None, callback=None, **kwargs):
+        """Nt steps with an optional host source ``source.update(self, t)``
+        and callback (upstream routines.py:17-229, without HDF5 saving or
+        plotting).  ABC boundaries are updated after every step from the
+        n-2 snapshot as upstream does."""
+        self.Nt = Nt
+        if source is not None:
+            self.source = source
+        if self.activate_abc:
+            E2, H2 = self.get_abc()
+            E1, H1 = self.get_abc()
+        for n in range(Nt):
+            if source is not None:
+                source.update(self, n * self.dt)
+            self.one_step()
+            if self.activate_abc:
+                self.update_abc(E2, H2)
+                E2, H2 = E1, H1
+                E1, H1 = self.get_abc()
+            if callback is not None:
+                callback(self, n * self.dt)
+
+    # ABC snapshots (upstream boundaries.py:313-410).  Upstream's CPU path
+    # keeps views of the live arrays; these are copies, as on its GPU path.
+    def get_abc(self):
+        E_abc, H_abc = {}, {}
+        sl = {0: lambda p: (p, slice(None), slice(None)), 1: lambda p: (slice(None), p, slice(None)),
+              2: lambda p: (slice(None), slice(None), p)}
+        for a in range(3):
+            if self.bc_low[a].lower() == "abc":
+                E_abc[a], H_abc[a] = {}, {}
+                for d in "xyz":
+                    E_abc[a][d + "lo"] = self.E[(*sl[a](1), d)]
+                    H_abc[a][d + "lo"] = self.H[(*sl[a](1), d)]
+        for a in range(3):
+            if self.bc_high[a].lower() == "abc":
+                E_abc[a], H_abc[a] = {}, {}
+                for d in "xyz":
+                    E_abc[a][d + "hi"] = self.E[(*sl[a](-1), d)]
+                    H_abc[a][d + "hi"] = self.H[(*sl[a](-1), d)]
+        return E_abc, H_abc
+
+    def update_abc(self, E_abc, H_abc):
+        sl = {0: lambda p: (p, slice(None), slice(None)), 1: lambda p: (slice(None), p, slice(None)),
+              2: lambda p: (slice(None), slice(None), p)}
+        for a in range(3):
+            if self.bc_low[a].lower() == "abc":
+                for d in "xyz":
+                    self.E[(*sl[a](0), d)] = E_abc[a][d + "lo"]
+                    self.H[(*sl[a](0), d)] = H_abc[a][d + "lo"]
+        for a in range(3):
+            if self.bc_high[a].lower() == "abc":
+                for d in "xyz":
+                    self.E[(*sl[a](-1), d)] = E_abc[a][d + "hi"]
+                    self.H[(*sl[a](-1), d)] = H_abc[a][d + "hi"]

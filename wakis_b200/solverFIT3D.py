@@ -1,0 +1,344 @@
+"""``SolverFIT3D``: drop-in for upstream's FIT time-domain solver, stepping on
+a B200 through the ``libwakis_b200`` C ABI.
+
+Constructor and public attributes follow upstream (wakis/solverFIT3D.py:
+40-354).  ``one_step()`` replaces upstream ``_one_step`` (482-503) with one
+fused kernel launch per step; ``run(n)`` advances n steps in one call.
+State lives in ``torch`` CUDA tensors: ``E`` and ``H`` alternate between two
+buffers (the fused kernel reads one and writes the other); ``J`` is kept
+implicit while it equals sigma*E (after any step with conductivity) or zero,
+and is materialised in device memory when the caller reads or writes it.
+There is no CPU fallback: without a CUDA device or without the native
+library the constructor raises.
+"""
+
+import time
+
+import numpy as np
+import torch
+
+from . import _native
+from .coefficients import build as build_coefficients
+from .coefficients import dense_materials
+from .field import Field, StateField, torch_dtype
+from .logger import Logger
+from .routines import RoutinesMixin
+
+_J_ZERO, _J_SIGMA_E, _J_ARRAY = _native.WK_J_ZERO, _native.WK_J_SIGMA_E, _native.WK_J_ARRAY
+
+
+class _CurrentField(Field):
+    """J: materialised on first access, after which the solver reads it."""
+
+    def __init__(self, solver, buf, Nx, Ny, Nz, dtype):
+        self._solver = solver
+        super().__init__(Nx, Ny, Nz, dtype=dtype, device=buf.device, array=buf)
+
+    @property
+    def array(self):
+        self._solver._materialize_J()
+        return self._array
+
+    @array.setter
+    def array(self, value):
+        self.fromarray(value)
+
+
+class SolverFIT3D(RoutinesMixin):
+    def __init__(self, grid, wake=None, cfln=0.5, dt=None,
+                 bc_low=("Periodic", "Periodic", "Periodic"),
+                 bc_high=("Periodic", "Periodic", "Periodic"),
+                 use_stl=False, use_conductors=False, use_gpu=True, use_mpi=False,
+                 use_sibc=True, fmax=1e9, dtype=np.float64, n_pml=10, bg=(1.0, 1.0),
+                 verbose=1, device=None, backend="b200"):
+        if backend != "b200":
+            raise ValueError(f"backend {backend!r}: this package only provides 'b200'")
+        if use_mpi:
+            raise ValueError("use_mpi: see wakis_b200.slab for z-slab decomposition")
+        if not torch.cuda.is_available():
+            raise RuntimeError("wakis_b200.SolverFIT3D needs a CUDA device (no CPU fallback)")
+        self._lib = _native.lib()
+        t0 = time.time()
+        self.verbose = verbose
+        self.logger = Logger()
+        self.step_0 = True
+        self.nstep = 0
+        self.use_stl, self.use_gpu, self.use_mpi = use_stl, True, False
+        self.use_sibc = use_sibc
+        self.fmax = fmax
+        self.grid = grid
+        self.background = bg
+        self.Nx, self.Ny, self.Nz = grid.Nx, grid.Ny, grid.Nz
+        self.N = self.Nx * self.Ny * self.Nz
+        self.dx, self.dy, self.dz = grid.dx, grid.dy, grid.dz
+        self.x = grid.x[:-1] + self.dx / 2
+        self.y = grid.y[:-1] + self.dy / 2
+        self.z = grid.z[:-1] + self.dz / 2
+        self.wake = wake
+        if wake is not None and fmax == 1e9:
+            self.fmax = wake.fmax
+        self.dtype = np.dtype(dtype).type
+        self.bc_low, self.bc_high = list(bc_low), list(bc_high)
+        self.n_pml = n_pml
+        self.cfln = cfln
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+
+        c = build_coefficients(grid, self.bc_low, self.bc_high, dtype=self.dtype, bg=bg,
+                               use_stl=use_stl, use_sibc=use_sibc, fmax=self.fmax,
+                               n_pml=n_pml, cfln=cfln, dt=dt, verbose=verbose)
+        self._coef = c
+        self.use_conductivity = c.use_conductivity
+        self.activate_pml = c.activate_pml
+        self.activate_abc = c.activate_abc
+        self.dt = c.dt
+        if c.tau_min is not None:
+            self.tau_min = c.tau_min
+        self._upload()
+        self.solverInitializationTime = time.time() - t0
+        self.logger.solver.update(dict(dt=self.dt, bc_low=self.bc_low, bc_high=self.bc_high,
+                                       use_gpu=True, use_mpi=False, background=bg,
+                                       solverInitializationTime=self.solverInitializationTime))
+        self.logger.grid = grid.logger.grid
+
+    # ---------------------------------------------------------- device state
+    def _upload(self):
+        c, dev = self._coef, self.device
+        td = torch_dtype(self.dtype)
+        N3 = 3 * self.N
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+        self._E = [torch.zeros(N3, dtype=td, device=dev) for _ in range(2)]
+        self._H = [torch.zeros(N3, dtype=td, device=dev) for _ in range(2)]
+        self._J = torch.zeros(N3, dtype=td, device=dev)
+        self._par = 0
+        self._j_state = _J_ZERO
+        self._j_line = None          # (values tensor) of the last fused beam step
+        self._ids = t(c.ids)
+        self._table = t(c.table.ravel())
+        self._metrics = {k: t(getattr(c, k).ravel(order="F")) for k in
+                         ("Lx", "Ly", "Lz", "tLx", "tLy", "tLz", "iAx", "iAy", "iAz",
+                          "itAx", "itAy", "itAz")}
+        self._zc = torch.as_tensor(self.z, dtype=torch.float64, device=dev)
+        self._status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.E = StateField(self, self._E, self.Nx, self.Ny, self.Nz, self.dtype)
+        self.H = StateField(self, self._H, self.Nx, self.Ny, self.Nz, self.dtype)
+        self.J = _CurrentField(self, self._J, self.Nx, self.Ny, self.Nz, self.dtype)
+        self._dense = None
+
+        d = _native.FitDesc()
+        d.Nx, d.Ny, d.Nz = self.Nx, self.Ny, self.Nz
+        d.dtype = _native.WK_F64 if self.dtype == np.float64 else _native.WK_F32
+        d.E[0], d.E[1] = self._E[0].data_ptr(), self._E[1].data_ptr()
+        d.H[0], d.H[1] = self._H[0].data_ptr(), self._H[1].data_ptr()
+        d.J = self._J.data_ptr()
+        d.mat_id = self._ids.data_ptr()
+        d.id_bytes = c.id_bytes
+        d.mat_table = self._table.data_ptr()
+        d.n_mat = c.table.shape[0]
+        for k, v in self._metrics.items():
+            setattr(d, k, v.data_ptr())
+        for f in range(6):
+            d.pec_face[f] = c.pec_face[f]
+            d.pmc_face[f] = c.pmc_face[f]
+        d.has_pec, d.has_pmc, d.h_sum_desc = int(c.has_pec), int(c.has_pmc), int(c.h_sum_desc)
+        d.use_conductivity = int(self.use_conductivity)
+        d.zc = self._zc.data_ptr()
+        d.status = self._status.data_ptr()
+        self._desc = d
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _sync_desc(self):
+        d = self._desc
+        d.par = self._par
+        d.dt = float(self.dt)
+        d.dt_is_f32 = int(isinstance(self.dt, np.float32))
+        d.j_mode = self._j_state
+        d.use_conductivity = int(self.use_conductivity)
+        return d
+
+    # -------------------------------------------------------------- J state
+    def _field_written(self, fld):
+        """E is about to change between steps: upstream's stored J = sigma*E
+        must keep the old E, so materialise it first."""
+        if fld is self.E and self._j_state == _J_SIGMA_E:
+            self._materialize_J()
+
+    def _materialize_J(self):
+        if self._j_state == _J_ARRAY:
+            return
+        if self._j_state == _J_SIGMA_E:
+            _native.check(self._lib.wk_sigma_e(self._sync_desc(), self._J.data_ptr(),
+                                               self._stream()), "wk_sigma_e")
+        else:
+            self._J.zero_()
+            if self._j_line is not None:
+                jz = self._J[2 * self.N:3 * self.N].view(self.Nz, self.Ny, self.Nx)
+                ixs, iys, vals = self._j_line
+                jz[:, iys, ixs] = vals
+        self._j_line = None
+        self._j_state = _J_ARRAY
+
+    # ------------------------------------------------------------- stepping
+    def _first_step(self):
+        if self.step_0:
+            _native.check(self._lib.wk_zero_ghosts(self._sync_desc(), self._stream()),
+                          "wk_zero_ghosts")
+            self.step_0 = False
+
+    def _advance(self, n_steps, step0=0, beam=None, capture=None, split=False, line=None):
+        """Advance n_steps with optional fused beam (wakesolve Beam) and Ez
+        window capture.  ``step0`` is the global step index of the first
+        step (beam time t = step*dt, capture column)."""
+        if n_steps <= 0:
+            return
+        self._first_step()
+        d = self._sync_desc()
+        if beam is not None:
+            d.beam_on = 1
+            (d.ixs, d.iys, d.b_qv, d.b_v, d.b_s0, d.b_c0, d.b_two_sig2,
+             d.b_dx, d.b_dy) = beam
+        else:
+            d.beam_on = 0
+        if line is not None:
+            lbuf, lstep0, ixs, iys = line
+            d.line_on, d.line, d.line_step0 = 1, lbuf.data_ptr(), lstep0
+            d.line_nsteps, d.ixs, d.iys = lbuf.numel() // self.Nz, ixs, iys
+            if lbuf.numel() % self.Nz or not lbuf.is_contiguous():
+                raise ValueError("line buffer must hold whole Nz-long rows")
+        else:
+            d.line_on = 0
+        if capture is not None:
+            buf, i0, j0, ni, nj = capture[:5]
+            d.cap_on, d.cap, d.cap_i0, d.cap_j0 = 1, buf.data_ptr(), i0, j0
+            d.cap_ni, d.cap_nj, d.cap_nt = ni, nj, buf.shape[-1]
+            d.cap_step0 = capture[5] if len(capture) > 5 else 0
+            if buf.numel() != ni * nj * self.Nz * buf.shape[-1] or not buf.is_contiguous():
+                raise ValueError("capture buffer must be a contiguous (ni*nj, Nz, nt) tensor")
+        else:
+            d.cap_on = 0
+        if split:
+            rc = self._lib.wk_fit_step_split(d, n_steps, step0, self._stream())
+            _native.check(rc, "wk_fit_step_split")
+        else:
+            rc = self._lib.wk_fit_step(d, n_steps, step0, self._stream())
+            _native.check(rc, "wk_fit_step")
+            self._par ^= (n_steps & 1)
+        self.nstep += n_steps
+        if self.use_conductivity:
+            self._j_state = _J_SIGMA_E
+            self._j_line = None
+        elif beam is not None:
+            # non-conductive: J keeps the last beam line (upstream Field write)
+            self._materialize_line(beam, step0 + n_steps - 1)
+
+    def _materialize_line(self, beam, step):
+        from .sources import beam_line_values
+        ixs, iys = beam[0], beam[1]
+        vals = beam_line_values(self, beam, step)
+        if self._j_state == _J_ARRAY:
+            jz = self._J[2 * self.N:3 * self.N].view(self.Nz, self.Ny, self.Nx)
+            jz[:, iys, ixs] = vals
+        else:
+            self._j_line = (ixs, iys, vals)
+
+    def run_with_io(self, jz_lines, ez_out, step0=0, xtest=0.0, ytest=0.0, xsource=0.0,
+                    ysource=0.0):
+        """Advance len(jz_lines) steps exchanging data with host memory every
+        step, the data movement of upstream's GPU wakesolve loop
+        (wakis/routines.py:435-445): before step n the Jz line current of
+        the beam line (Nz values, ``jz_lines[n]``) is copied from host to
+        device, and the Ez values of the 3x3 test window captured before the
+        update (9 x Nz) are copied back into ``ez_out[n]``.  Both host tensors
+        should be pinned; all copies and steps are queued on the current
+        stream (call torch.cuda.synchronize() before reading ez_out)."""
+        n_steps, nz = jz_lines.shape
+        ixs = int(np.abs(self.x - xsource).argmin())
+        iys = int(np.abs(self.y - ysource).argmin())
+        ixt = int(np.abs(self.x - xtest).argmin())
+        iyt = int(np.abs(self.y - ytest).argmin())
+        if getattr(self, "_io_bufs", None) is None or self._io_bufs[0].shape[0] != nz:
+            td = self._E[0].dtype
+            self._io_bufs = (torch.empty(nz, dtype=td, device=self.device),
+                             torch.empty((9, nz, 1), dtype=td, device=self.device))
+        lbuf, cbuf = self._io_bufs
+        for n in range(n_steps):
+            lbuf.copy_(jz_lines[n], non_blocking=True)
+            self._advance(1, step0 + n, line=(lbuf, step0 + n, ixs, iys),
+                          capture=(cbuf, ixt - 1, iyt - 1, 3, 3, step0 + n))
+            ez_out[n].copy_(cbuf.view(9, nz), non_blocking=True)
+
+    def one_step(self):
+        """One leap-frog step (upstream _one_step, solverFIT3D.py:482-503)."""
+        self._advance(1)
+
+    def run(self, n_steps):
+        """n_steps leap-frog steps in one call."""
+        self._advance(int(n_steps))
+
+    # ---------------------------------------------------------- materials
+    def _dense_fields(self):
+        if self._dense is None:
+            ie, im, sg = dense_materials(self._coef)
+            mk = lambda a: Field(self.Nx, self.Ny, self.Nz, dtype=self.dtype, device=self.device,
+                                 array=torch.as_tensor(a, device=self.device))
+            self._dense = (mk(ie), mk(im), mk(sg))
+        return self._dense
+
+    @property
+    def ieps(self):
+        return self._dense_fields()[0]
+
+    @property
+    def imu(self):
+        return self._dense_fields()[1]
+
+    @property
+    def sigma(self):
+        return self._dense_fields()[2]
+
+    def update_tensors(self, tensor="all"):
+        """Re-derive the material ids/table from the (edited) ieps, imu,
+        sigma fields (upstream update_tensors, solverFIT3D.py:356-414)."""
+        ie, im, sg = (f.array for f in self._dense_fields())
+        N = self.N
+        rows = torch.stack([ie[0:N], ie[N:2 * N], ie[2 * N:], im[0:N], im[N:2 * N], im[2 * N:],
+                            sg[0:N], sg[N:2 * N], sg[2 * N:]], dim=1)
+        table, inv = torch.unique(rows, dim=0, return_inverse=True)
+        n_mat = table.shape[0]
+        id_t = torch.uint8 if n_mat <= 256 else (torch.int16 if n_mat <= 32768 else torch.int32)
+        self._ids = inv.to(id_t).contiguous()
+        self._table = table.contiguous().view(-1)
+        self._coef.table = table.cpu().numpy()
+        self._coef.ids = self._ids.cpu().numpy()
+        d = self._desc
+        d.mat_id, d.id_bytes = self._ids.data_ptr(), self._ids.element_size()
+        d.mat_table, d.n_mat = self._table.data_ptr(), n_mat
+        self.step_0 = False
+
+    # --------------------------------------------------------------- state
+    def reset_fields(self):
+        for b in self._E + self._H:
+            b.zero_()
+        self._J.zero_()
+        self._j_state = _J_ZERO
+        self._j_line = None
+
+    def save_state(self, filename="solver_state.npz", close=True):
+        """E, H, J to ``filename`` (npz; upstream writes HDF5,
+        solverFIT3D.py:886-935)."""
+        np.savez(filename, E=self.E.numpy(), H=self.H.numpy(), J=self.J.numpy())
+
+    def load_state(self, filename="solver_state.npz"):
+        st = np.load(filename)
+        self.E.fromarray(st["E"])
+        self.H.fromarray(st["H"])
+        self.J.fromarray(st["J"])
+
+    def read_state(self, filename="solver_state.npz"):
+        return np.load(filename)
+
+    def update_logger(self, attrs):
+        for a in attrs:
+            self.logger.solver[a] = getattr(self, a)

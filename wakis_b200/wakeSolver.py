@@ -1,0 +1,222 @@
+"""``WakeSolver``: wake potential and impedance from the Ez history, on the
+device (upstream wakis/wakeSolver.py:19-870).
+
+The constructor keeps upstream's parameters and defaults (22-208).  After
+``SolverFIT3D.wakesolve`` the Ez history is a device tensor laid out
+[window][k][step]; ``solve()`` runs
+
+* ``calc_long_WP_3d`` / ``calc_long_WP`` -> ``wk_wake_potential``,
+* ``calc_trans_WP``                     -> ``wk_trans_wake``,
+* ``calc_long_Z`` / ``calc_trans_Z``    -> ``wk_dft_bins`` (direct DFT of the
+  kept bins 0 <= f < fmax),
+
+with the s axis, the key order of the history and the frequency axis formed
+on the host by the same numpy expressions as upstream.
+"""
+
+import os
+
+import numpy as np
+import torch
+from scipy.constants import c as c_light
+
+from . import _native
+from .logger import Logger
+
+
+class WakeSolver:
+    def __init__(self, wakelength=None, q=1e-9, sigmaz=1e-3, beta=1.0, xsource=0.0,
+                 ysource=0.0, xtest=0.0, ytest=0.0, chargedist=None, ti=None, fmax=None,
+                 compute_plane="both", skip_cells=0, add_space=None, Ez_file=None, save=True,
+                 results_folder="results/", verbose=1, counter_moving=False):
+        self.verbose = verbose
+        self.q, self.sigmaz, self.beta = q, sigmaz, beta
+        self.v = self.beta * c_light
+        self.xsource, self.ysource = xsource, ysource
+        self.xtest, self.ytest = xtest, ytest
+        self.chargedist = chargedist
+        self.fmax = self.v / (3.0 * self.sigmaz) if fmax is None else fmax
+        self.skip_cells = skip_cells if add_space is None else add_space
+        self.compute_plane = compute_plane
+        self.counter_moving = counter_moving
+        if ti is not None:
+            self.ti = ti
+        else:
+            self.ti = 8.548921333333334 * self.sigmaz / (np.sqrt(self.beta) * self.v)
+        self.Ez_file = Ez_file
+        self.t = None
+        self.xf = self.yf = self.zf = None
+        self.wakelength = wakelength
+        self.s = self.lambdas = self.WP = self.WP_3d = None
+        self.n_transverse_cells = 1
+        self.WPx = self.WPy = self.f = self.Z = self.Zx = self.Zy = self.lambdaf = None
+        self.logger = Logger()
+        self.save = save
+        self.folder = results_folder if results_folder.endswith("/") else results_folder + "/"
+        if self.save:
+            os.makedirs(self.folder, exist_ok=True)
+        self._hist = None
+        self.logger.wakeSolver.update(dict(ti=self.ti, q=q, sigmaz=sigmaz, beta=beta,
+                                           xsource=xsource, ysource=ysource, xtest=xtest,
+                                           ytest=ytest, chargedist=chargedist,
+                                           skip_cells=self.skip_cells,
+                                           results_folder=self.folder))
+
+    # ------------------------------------------------------------ history
+    def set_history(self, hist, n_steps, one_d=False):
+        """Attach the device Ez history [window][k][step] of n_steps steps."""
+        self._hist = hist
+        self._hist_steps = int(n_steps)
+        self._hist_1d = bool(one_d)
+
+    def _key_order(self, n):
+        """Step index of each history column in upstream's read order: the
+        '#%05d' keys sorted as strings (wakeSolver.py:488-491)."""
+        keys = sorted("#" + str(i).zfill(5) for i in range(n))
+        return np.array([int(k[1:]) for k in keys], dtype=np.int64)
+
+    def _axis(self):
+        nt = len(self.t)
+        dt = self.t[2] - self.t[1]
+        zmax, zmin = np.max(self.zf), np.min(self.zf)
+        zz = slice(self.skip_cells, -self.skip_cells) if self.skip_cells != 0 else np.s_[:]
+        z = self.zf[zz]
+        if self.wakelength is not None:
+            wakelength = self.wakelength
+        else:
+            wakelength = nt * dt * self.v - (zmax - zmin) - self.ti * self.v
+            self.wakelength = wakelength
+        s = np.arange(-self.ti * self.v, wakelength, dt * self.v)
+        return nt, dt, zmin, zmax, z, s
+
+    def _wp(self, n_win, carry):
+        if self._hist is None:
+            raise RuntimeError("no Ez history: run SolverFIT3D.wakesolve first")
+        lib = _native.lib()
+        nt, dt, zmin, zmax, z, s = self._axis()
+        n_keys = self._hist_steps
+        nt = min(nt, n_keys)
+        dev = self._hist.device
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+        zt, dzt, st = f64(z), f64(self.dz), f64(s)
+        order = torch.as_tensor(self._key_order(n_keys), device=dev)
+        win = torch.arange(n_win, dtype=torch.int32, device=dev)
+        WP3d = torch.empty((n_win, len(s)), dtype=torch.float64, device=dev)
+        hdt = _native.WK_F64 if self._hist.dtype == torch.float64 else _native.WK_F32
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = lib.wk_wake_potential(
+            self._hist.data_ptr(), hdt, self._hist.shape[-1], self._hist.shape[1],
+            win.data_ptr(), n_win, int(carry), zt.data_ptr(), dzt.data_ptr(), len(z),
+            int(self.skip_cells), st.data_ptr(), len(s), order.data_ptr(), int(nt),
+            float(self.v), float(zmin), float(zmax), float(self.t[0]), float(self.ti),
+            float(dt), float(self.q * 1e12), int(self.counter_moving), WP3d.data_ptr(), stream)
+        _native.check(rc, "wk_wake_potential")
+        self.s = s
+        return WP3d
+
+    # -------------------------------------------------------------- solve
+    def solve(self, compute_plane=None, **kwargs):
+        cp = (compute_plane or self.compute_plane).lower()
+        for k, v in kwargs.items():
+            setattr(self, k, v)
+        if cp in ("both", "transverse"):
+            self.calc_long_WP_3d()
+            self.calc_trans_WP()
+            self.calc_long_Z()
+            self.calc_trans_Z()
+        elif cp == "longitudinal":
+            self.calc_long_WP()
+            self.calc_long_Z()
+
+    def calc_long_WP_3d(self, **kwargs):
+        if self._hist_1d:
+            raise ValueError("the Ez history holds the test line only (compute_plane="
+                             "'longitudinal'); the 3d wake needs the 3x3 window")
+        WP3d = self._wp(9, carry=True)
+        self._WP3d_dev = WP3d
+        self.WP_3d = WP3d.cpu().numpy().reshape(3, 3, -1)
+        self.WP = self.WP_3d[1, 1, :]
+        self._WP_dev = WP3d[4]
+
+    def calc_long_WP(self, **kwargs):
+        if not self._hist_1d:
+            raise ValueError("calc_long_WP needs the history of compute_plane='longitudinal'")
+        if self.skip_cells != 0:
+            # upstream assigns the full Nz line into nz rows (wakeSolver.py:390-392)
+            raise ValueError("could not broadcast input array: skip_cells with a 1-D history")
+        WP = self._wp(1, carry=False)
+        self._WP_dev = WP[0]
+        self.WP = WP[0].cpu().numpy()
+
+    def calc_trans_WP(self, **kwargs):
+        lib = _native.lib()
+        ds = self.s[2] - self.s[1]
+        dxf, dyf = np.diff(self.xf), np.diff(self.yf)
+        ns = len(self.s)
+        dev = self._WP3d_dev.device
+        WPx = torch.empty(ns, dtype=torch.float64, device=dev)
+        WPy = torch.empty(ns, dtype=torch.float64, device=dev)
+        rc = lib.wk_trans_wake(self._WP3d_dev.data_ptr(), ns, float(ds), float(dxf[0] + dxf[1]),
+                               float(dyf[0] + dyf[1]), WPx.data_ptr(), WPy.data_ptr(),
+                               torch.cuda.current_stream(dev).cuda_stream)
+        _native.check(rc, "wk_trans_wake")
+        self._WPx_dev, self._WPy_dev = WPx, WPy
+        self.WPx, self.WPy = WPx.cpu().numpy(), WPy.cpu().numpy()
+
+    def calc_lambdas_analytic(self, **kwargs):
+        self.lambdas = (1 / (self.sigmaz * np.sqrt(2 * np.pi))
+                        * np.exp(-(self.s ** 2) / (2 * self.sigmaz ** 2)))
+
+    def calc_lambdas(self, **kwargs):
+        chargedist = self.chargedist
+        if isinstance(chargedist, dict):
+            keys = list(chargedist.keys())
+            z, chargedist = chargedist[keys[0]], chargedist[keys[1]]
+        elif len(self.zf) == len(chargedist):
+            z = self.zf
+        else:
+            raise ValueError("Dimension error: check input dimensions")
+        self.lambdas = np.interp(self.s, z, np.asarray(chargedist) / self.q)
+
+    def _bins(self, signals, samples, fmax):
+        """DFT bins 0 <= f < fmax of np.fft.fft(x, n=N) for host/device signals."""
+        lib = _native.lib()
+        ds = np.mean(self.s[1:] - self.s[:-1])
+        fmax = self.fmax if fmax is None else fmax
+        N = int((self.v / ds) // fmax * samples)
+        ffft = np.fft.fftfreq(N, ds / self.v)
+        mask = np.logical_and(ffft >= 0, ffft < fmax)
+        nb = int(mask.sum())
+        if nb and not mask[:nb].all():
+            raise RuntimeError("kept DFT bins are not the leading bins")
+        ns = len(self.s)
+        dev = self._WP_dev.device
+        x = torch.stack([torch.as_tensor(sg, dtype=torch.float64, device=dev) for sg in signals])
+        x = x.contiguous()
+        out = torch.empty((len(signals), nb, 2), dtype=torch.float64, device=dev)
+        rc = lib.wk_dft_bins(x.data_ptr(), len(signals), ns, N, nb, out.data_ptr(),
+                             torch.cuda.current_stream(dev).cuda_stream)
+        _native.check(rc, "wk_dft_bins")
+        return ds, ffft[mask], torch.view_as_complex(out)
+
+    def calc_long_Z(self, samples=1001, fmax=None, **kwargs):
+        if self.lambdas is None and self.chargedist is not None:
+            self.calc_lambdas()
+        elif self.lambdas is None:
+            self.calc_lambdas_analytic()
+        lam = torch.as_tensor(self.lambdas * self.v, dtype=torch.float64, device=self._WP_dev.device)
+        ds, f, X = self._bins([lam, self._WP_dev * 1e12], samples, fmax)
+        lambdaf = X[0] * ds
+        WPf = X[1] * ds
+        self.f = f
+        self.Z = (-WPf / lambdaf).cpu().numpy()
+        self.lambdaf = lambdaf.cpu().numpy()
+        self._lambdaf_dev = lambdaf
+
+    def calc_trans_Z(self, samples=1001, fmax=None):
+        lam = torch.as_tensor(self.lambdas * self.v, dtype=torch.float64, device=self._WP_dev.device)
+        ds, f, X = self._bins([lam, self._WPx_dev * 1e12, self._WPy_dev * 1e12], samples, fmax)
+        lambdaf = X[0] * ds
+        self.Zx = (1j * (X[1] * ds) / lambdaf).cpu().numpy()
+        self.Zy = (1j * (X[2] * ds) / lambdaf).cpu().numpy()
+        self.fx = self.fy = f
