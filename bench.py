@@ -196,6 +196,8 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "march", "cell"])
+    ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
     args = ap.parse_args()
@@ -224,6 +226,8 @@ def main():
     shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else None
     g, w, s = workloads.build_b200(args.workload, dtype=dtype, shape=shape)
     N = s.N
+    s.kernel = args.kernel
+    s.tile = tuple(int(v) for v in args.tile.split("x"))
     bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
               ).params(s)
     ixt = int(np.abs(s.x - w.xtest).argmin())
@@ -293,7 +297,8 @@ def main():
             "config": {"workload": args.workload, "cells": N, "grid": [s.Nx, s.Ny, s.Nz],
                        "parallelism": f"replicas{ws}" if ws > 1 else "single",
                        "l2": "state 4x%.0f MB > L2, no flush" % (3 * N * np.dtype(dtype).itemsize / 1e6),
-                       "step": "fused beam + Ez 3x3 capture + H and E half-steps"},
+                       "step": "fused beam + Ez 3x3 capture + H and E half-steps",
+                       "kernel": args.kernel, "tile": args.tile},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": src,
                          "bytes_per_cell_step": bpc,

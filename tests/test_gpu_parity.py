@@ -45,12 +45,19 @@ def _valid(idx):
 VALID = [i for i in range(len(cases.STEP_CASES)) if _valid(i)]
 
 
-@pytest.mark.parametrize("split", [False, True])
+SCHEDULES = {"march": ("march", (0, 0)), "march_t1": ("march", (1, 1)),
+             "march_t2": ("march", (2, 3)), "cell": ("cell", (0, 0)), "split": None}
+
+
+@pytest.mark.parametrize("sched", list(SCHEDULES))
 @pytest.mark.parametrize("idx", VALID)
-def test_steps_without_beam_are_exact(idx, split):
+def test_steps_without_beam_are_exact(idx, sched):
     c = cases.STEP_CASES[idx]
     o = oracle_step_case(c)
     s = b200_step_case(c)
+    split = SCHEDULES[sched] is None
+    if not split:
+        s.kernel, s.tile = SCHEDULES[sched]
     assert s.dt == o.dt
     E0, H0 = cases.initial_fields(c, o.N)
     o.E[:], o.H[:] = E0, H0
@@ -64,11 +71,13 @@ def test_steps_without_beam_are_exact(idx, split):
     assert np.array_equal(s.J.numpy(), o.J)
 
 
+@pytest.mark.parametrize("sched", ["march", "cell"])
 @pytest.mark.parametrize("idx", VALID)
-def test_steps_with_fused_beam_match_upstream(idx, golden_dir):
+def test_steps_with_fused_beam_match_upstream(idx, sched, golden_dir):
     g = np.load(os.path.join(golden_dir, "step_cases.npz"))
     c = cases.STEP_CASES[idx]
     s = b200_step_case(c)
+    s.kernel, s.tile = SCHEDULES[sched]
     E0, H0 = cases.initial_fields(c, s.N)
     s.E.fromarray(E0)
     s.H.fromarray(H0)
@@ -184,3 +193,23 @@ def test_cavity_40_wakesolve_matches_oracle():
         assert rel_err(getattr(sb, f).numpy(), getattr(so, f)) <= FIELD_TOL, f
     for n in ("WP", "WP_3d", "WPx", "WPy", "Z", "Zx", "Zy"):
         assert rel_err(getattr(wb_, n), getattr(wo, n)) <= WAKE_TOL, n
+
+
+@pytest.mark.parametrize("tile", [(0, 0), (1, 4), (3, 5), (7, 1), (16, 24)])
+def test_march_equals_cell_kernel_with_beam_and_capture(tile):
+    """Plane-marching and per-cell kernels give identical fields and Ez
+    history (same arithmetic, different schedule), for several tiles."""
+    c = cases.WAKE_CASES[3]     # conductive background, PML, beta < 1
+    a, wa = b200_wake_case(c)
+    b, wb_ = b200_wake_case(c)
+    a.kernel, a.tile = "march", tile
+    b.kernel = "cell"
+    from wakis_b200.sources import Beam
+    bp = Beam(q=1e-9, sigmaz=0.004, beta=0.7).params(a)
+    ha = torch.zeros((9, a.Nz, 40), dtype=torch.float64, device="cuda")
+    hb = torch.zeros_like(ha)
+    a._advance(40, 0, beam=bp, capture=(ha, 5, 6, 3, 3))
+    b._advance(40, 0, beam=bp, capture=(hb, 5, 6, 3, 3))
+    assert np.array_equal(a.E.numpy(), b.E.numpy())
+    assert np.array_equal(a.H.numpy(), b.H.numpy())
+    assert torch.equal(ha, hb)

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libwakis_b200.so")
 
 WK_F64, WK_F32 = 0, 1
 WK_J_ZERO, WK_J_SIGMA_E, WK_J_ARRAY = 0, 1, 2
+WK_KERNEL_AUTO, WK_KERNEL_CELL, WK_KERNEL_MARCH = 0, 1, 2
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -38,6 +39,7 @@ class FitDesc(ctypes.Structure):
         ("line_on", _i), ("line_step0", _ll), ("line_nsteps", _ll), ("line", _vp),
         ("cap_on", _i), ("cap_i0", _i), ("cap_j0", _i), ("cap_ni", _i), ("cap_nj", _i),
         ("cap_nt", _ll), ("cap_step0", _ll), ("cap", _vp), ("status", _vp),
+        ("kernel", _i), ("tile_rows", _i), ("tile_planes", _i),
     ]
 
 

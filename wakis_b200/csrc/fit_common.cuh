@@ -129,11 +129,12 @@ __device__ __forceinline__ Cell minus_y(Cell c, int Ny) {
   return r;
 }
 
-// H row update for component d at cell c (flat n), reading E from `Ein`
-// and H from `Hin`.  Returns the new H value.
-template <typename T>
-__device__ __forceinline__ T h_row(const FitParams<T>& p, const T* __restrict__ Ein,
-                                   T hold, int d, Cell c, long long n, int id) {
+// H row update for component d at cell c (flat n).  `ev(e, kind)` returns
+// the old E component e at n (kind 0), n+1 (1), n+Nx (2) or n+Nx*Ny (3); it
+// is only called for terms whose flat index lies inside the grid.
+template <typename T, typename EV>
+__device__ __forceinline__ T h_row_acc(const FitParams<T>& p, T hold, int d, Cell c,
+                                       long long n, int id, EV ev) {
   const long long N = p.N, NxNy = p.NxNy;
   const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
   T iA = d == 0 ? p.iAx[c.j + (long long)c.k * Ny]
@@ -141,80 +142,99 @@ __device__ __forceinline__ T h_row(const FitParams<T>& p, const T* __restrict__ 
   T R = mul(iA, p.mat[9 * id + 3 + d]);
   if (p.has_pmc && !face_val(p.pmc_face, d, c.i, c.j, c.k, Nx, Ny, Nz)) R = T(0);
   const T dt = p.dt;
-  // term(col comp e, column flat m, column cell cc, sign)
-  auto term = [&](int e, long long m, Cell cc, bool valid, T sgn) -> T {
+  auto term = [&](int e, int kind, Cell cc, bool valid, bool pos) -> T {
     if (!valid) return T(0);
     T coef = mul(dt, mul(R, colL(p, e, cc.i, cc.j, cc.k)));
-    T v = mul(coef, Ein[(long long)e * N + m]);
-    return sgn > T(0) ? v : -v;
+    T v = mul(coef, ev(e, kind));
+    return pos ? v : -v;
   };
   Cell kz = c; kz.k++;
-  bool vz = (n + NxNy) < N;
+  const bool vz = (n + NxNy) < N, vy = (n + Nx) < N, vx = (n + 1) < N;
   T t0, t1, t2, t3;
   if (d == 0) {        // (C e)_x = +ey[n] - ey[n+NxNy] - ez[n] + ez[n+Nx]
     Cell cy = plus_y(c, Ny);
-    t0 = term(1, n, c, true, T(1));
-    t1 = term(1, n + NxNy, kz, vz, T(-1));
-    t2 = term(2, n, c, true, T(-1));
-    t3 = term(2, n + Nx, cy, (n + Nx) < N, T(1));
+    t0 = term(1, 0, c, true, true);
+    t1 = term(1, 3, kz, vz, false);
+    t2 = term(2, 0, c, true, false);
+    t3 = term(2, 2, cy, vy, true);
   } else if (d == 1) { // (C e)_y = -ex[n] + ex[n+NxNy] + ez[n] - ez[n+1]
     Cell cx = plus_x(c, Nx, Ny);
-    t0 = term(0, n, c, true, T(-1));
-    t1 = term(0, n + NxNy, kz, vz, T(1));
-    t2 = term(2, n, c, true, T(1));
-    t3 = term(2, n + 1, cx, (n + 1) < N, T(-1));
+    t0 = term(0, 0, c, true, false);
+    t1 = term(0, 3, kz, vz, true);
+    t2 = term(2, 0, c, true, true);
+    t3 = term(2, 1, cx, vx, false);
   } else {             // (C e)_z = +ex[n] - ex[n+Nx] - ey[n] + ey[n+1]
     Cell cy = plus_y(c, Ny);
     Cell cx = plus_x(c, Nx, Ny);
-    t0 = term(0, n, c, true, T(1));
-    t1 = term(0, n + Nx, cy, (n + Nx) < N, T(-1));
-    t2 = term(1, n, c, true, T(-1));
-    t3 = term(1, n + 1, cx, (n + 1) < N, T(1));
+    t0 = term(0, 0, c, true, true);
+    t1 = term(0, 2, cy, vy, false);
+    t2 = term(1, 0, c, true, false);
+    t3 = term(1, 1, cx, vx, true);
   }
   return sub(hold, sum4(t0, t1, t2, t3, p.h_desc != 0));
 }
 
+// H row reading E from a flat global array.
+template <typename T>
+__device__ __forceinline__ T h_row(const FitParams<T>& p, const T* __restrict__ Ein,
+                                   T hold, int d, Cell c, long long n, int id) {
+  const long long N = p.N;
+  const long long off[4] = {0, 1, (long long)p.Nx, p.NxNy};
+  auto ev = [&](int e, int kind) -> T { return Ein[(long long)e * N + n + off[kind]]; };
+  return h_row_acc(p, hold, d, c, n, id, ev);
+}
+
 // Curl part of the E row for component d at cell c: sum_c B_rc * H_c, with
-// H values supplied by `hval(comp, flat)`.
+// `hv(e, kind)` the new H component e at n (0), n-1 (1), n-Nx (2) or
+// n-Nx*Ny (3), only called for in-grid indices.
 template <typename T, typename HV>
-__device__ __forceinline__ T e_curl(const FitParams<T>& p, int d, Cell c, long long n,
-                                    T ieps, HV hval) {
+__device__ __forceinline__ T e_curl_acc(const FitParams<T>& p, int d, Cell c, long long n,
+                                        T ieps, HV hv) {
   const long long NxNy = p.NxNy;
   const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
   T itA = d == 0 ? p.itAx[c.j + (long long)c.k * Ny]
                  : (d == 1 ? p.itAy[c.i + (long long)c.k * Nx] : p.itAz[c.i + (long long)c.j * Nx]);
   T R = mul(ieps, itA);
   if (p.has_pec && !face_val(p.pec_face, d, c.i, c.j, c.k, Nx, Ny, Nz)) R = T(0);
-  auto term = [&](int e, long long m, Cell cc, bool valid, T sgn) -> T {
+  auto term = [&](int e, int kind, Cell cc, bool valid, bool pos) -> T {
     if (!valid) return T(0);
     T coef = mul(R, coltL(p, e, cc.i, cc.j, cc.k));
-    T v = mul(coef, hval(e, m));
-    return sgn > T(0) ? v : -v;
+    T v = mul(coef, hv(e, kind));
+    return pos ? v : -v;
   };
   Cell km = c; km.k--;
-  bool vz = n >= NxNy;
+  const bool vz = n >= NxNy, vy = n >= Nx, vx = n >= 1;
   T t0, t1, t2, t3;
   if (d == 0) {        // +hy[n-NxNy] - hy[n] - hz[n-Nx] + hz[n]
     Cell cy = minus_y(c, Ny);
-    t0 = term(1, n - NxNy, km, vz, T(1));
-    t1 = term(1, n, c, true, T(-1));
-    t2 = term(2, n - Nx, cy, n >= Nx, T(-1));
-    t3 = term(2, n, c, true, T(1));
+    t0 = term(1, 3, km, vz, true);
+    t1 = term(1, 0, c, true, false);
+    t2 = term(2, 2, cy, vy, false);
+    t3 = term(2, 0, c, true, true);
   } else if (d == 1) { // -hx[n-NxNy] + hx[n] + hz[n-1] - hz[n]
     Cell cx = minus_x(c, Nx, Ny);
-    t0 = term(0, n - NxNy, km, vz, T(-1));
-    t1 = term(0, n, c, true, T(1));
-    t2 = term(2, n - 1, cx, n >= 1, T(1));
-    t3 = term(2, n, c, true, T(-1));
+    t0 = term(0, 3, km, vz, false);
+    t1 = term(0, 0, c, true, true);
+    t2 = term(2, 1, cx, vx, true);
+    t3 = term(2, 0, c, true, false);
   } else {             // +hx[n-Nx] - hx[n] - hy[n-1] + hy[n]
     Cell cy = minus_y(c, Ny);
     Cell cx = minus_x(c, Nx, Ny);
-    t0 = term(0, n - Nx, cy, n >= Nx, T(1));
-    t1 = term(0, n, c, true, T(-1));
-    t2 = term(1, n - 1, cx, n >= 1, T(-1));
-    t3 = term(1, n, c, true, T(1));
+    t0 = term(0, 2, cy, vy, true);
+    t1 = term(0, 0, c, true, false);
+    t2 = term(1, 1, cx, vx, false);
+    t3 = term(1, 0, c, true, true);
   }
   return sum4(t0, t1, t2, t3, false);
+}
+
+// E-row curl with H values supplied by `hval(comp, flat)`.
+template <typename T, typename HV>
+__device__ __forceinline__ T e_curl(const FitParams<T>& p, int d, Cell c, long long n,
+                                    T ieps, HV hval) {
+  const long long off[4] = {0, 1, (long long)p.Nx, p.NxNy};
+  auto hv = [&](int e, int kind) -> T { return hval(e, n - off[kind]); };
+  return e_curl_acc(p, d, c, n, ieps, hv);
 }
 
 // Gaussian beam current on the line (ixs, iys) at step `step`

@@ -1,0 +1,75 @@
+// Helpers shared by the step kernels: Ez capture, J source of an E row,
+// descriptor -> kernel parameter conversion, and the plane-marching kernel
+// declaration.
+#pragma once
+#include "../../include/wakis_b200.h"
+#include "fit_common.cuh"
+
+namespace wk {
+
+constexpr int kMarchThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ void capture(const FitParams<T>& p, Cell c, long long n,
+                                        long long step, T ez) {
+  int a = c.i - p.cap_i0, b = c.j - p.cap_j0;
+  if (a >= 0 && a < p.cap_ni && b >= 0 && b < p.cap_nj) {
+    long long w = (long long)a * p.cap_nj + b;
+    p.cap[(w * p.Nz + c.k) * p.cap_nt + (step - p.cap_step0)] = ez;
+  }
+}
+
+// J value entering the E row of component d at cell n (before the update).
+template <typename T>
+__device__ __forceinline__ T j_in(const FitParams<T>& p, int d, Cell c, long long n,
+                                  long long step, T e_old, T sigma) {
+  if (d == 2 && c.i == p.ixs && c.j == p.iys) {
+    if (p.line_on) return p.line[(step - p.line_step0) * p.Nz + c.k];
+    if (p.beam_on) return beam_j(p, step, c.k);
+  }
+  if (p.j_mode == WK_J_SIGMA_E) return mul(sigma, e_old);
+  if (p.j_mode == WK_J_ARRAY) return p.J[(long long)d * p.N + n];
+  return T(0);
+}
+
+template <typename T>
+inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
+  FitParams<T> p;
+  p.Nx = d->Nx; p.Ny = d->Ny; p.Nz = d->Nz;
+  p.NxNy = (long long)d->Nx * d->Ny;
+  p.N = p.NxNy * d->Nz;
+  p.E_in = (T*)d->E[par]; p.H_in = (T*)d->H[par];
+  p.E_out = (T*)d->E[par ^ 1]; p.H_out = (T*)d->H[par ^ 1];
+  p.J = (T*)d->J;
+  p.j_mode = d->j_mode; p.use_cond = d->use_conductivity;
+  p.mat_id = d->mat_id; p.id_bytes = d->id_bytes;
+  p.mat = (const T*)d->mat_table;
+  p.Lx = (const T*)d->Lx; p.Ly = (const T*)d->Ly; p.Lz = (const T*)d->Lz;
+  p.tLx = (const T*)d->tLx; p.tLy = (const T*)d->tLy; p.tLz = (const T*)d->tLz;
+  p.iAx = (const T*)d->iAx; p.iAy = (const T*)d->iAy; p.iAz = (const T*)d->iAz;
+  p.itAx = (const T*)d->itAx; p.itAy = (const T*)d->itAy; p.itAz = (const T*)d->itAz;
+  for (int f = 0; f < 6; f++) { p.pec_face[f] = d->pec_face[f]; p.pmc_face[f] = d->pmc_face[f]; }
+  p.has_pec = d->has_pec; p.has_pmc = d->has_pmc; p.h_desc = d->h_sum_desc;
+  p.dt = (T)d->dt;
+  p.dt64 = d->dt; p.dt32 = (float)d->dt; p.dt_is_f32 = d->dt_is_f32;
+  p.beam_on = d->beam_on; p.ixs = d->ixs; p.iys = d->iys;
+  p.b_qv = d->b_qv; p.b_v = d->b_v; p.b_v32 = (float)d->b_v; p.b_s0 = d->b_s0;
+  p.b_c0 = d->b_c0; p.b_two_sig2 = d->b_two_sig2; p.b_dx = d->b_dx; p.b_dy = d->b_dy;
+  p.zc = d->zc;
+  p.line_on = d->line_on; p.line_step0 = d->line_step0; p.line_nsteps = d->line_nsteps;
+  p.line = (const T*)d->line;
+  p.cap_on = d->cap_on; p.cap_i0 = d->cap_i0; p.cap_j0 = d->cap_j0;
+  p.cap_ni = d->cap_ni; p.cap_nj = d->cap_nj; p.cap_nt = d->cap_nt; p.cap_step0 = d->cap_step0;
+  p.cap = (T*)d->cap;
+  p.status = d->status;
+  return p;
+}
+
+
+// Launch the plane-marching kernel (defined in fit_march.cu) with TY rows
+// and KC planes per block and `smem` bytes of dynamic shared memory.
+template <typename T>
+cudaError_t launch_march(const FitParams<T>& p, long long step, int TY, int KC, size_t smem,
+                         cudaStream_t st);
+
+}  // namespace wk

@@ -8,6 +8,7 @@
 #include "../../include/wakis_b200.h"
 #include "abi_internal.h"
 #include "fit_common.cuh"
+#include "fit_kernels.cuh"
 
 using namespace wk;
 
@@ -29,29 +30,6 @@ __global__ void k_zero_ghosts(FitParams<T> p) {
   if (c.i == p.Nx - 1) E[n] = T(0);
   if (c.j == p.Ny - 1) E[p.N + n] = T(0);
   if (c.k == p.Nz - 1) E[2 * p.N + n] = T(0);
-}
-
-template <typename T>
-__device__ __forceinline__ void capture(const FitParams<T>& p, Cell c, long long n,
-                                        long long step, T ez) {
-  int a = c.i - p.cap_i0, b = c.j - p.cap_j0;
-  if (a >= 0 && a < p.cap_ni && b >= 0 && b < p.cap_nj) {
-    long long w = (long long)a * p.cap_nj + b;
-    p.cap[(w * p.Nz + c.k) * p.cap_nt + (step - p.cap_step0)] = ez;
-  }
-}
-
-// J value entering the E row of component d at cell n (before the update).
-template <typename T>
-__device__ __forceinline__ T j_in(const FitParams<T>& p, int d, Cell c, long long n,
-                                  long long step, T e_old, T sigma) {
-  if (d == 2 && c.i == p.ixs && c.j == p.iys) {
-    if (p.line_on) return p.line[(step - p.line_step0) * p.Nz + c.k];
-    if (p.beam_on) return beam_j(p, step, c.k);
-  }
-  if (p.j_mode == WK_J_SIGMA_E) return mul(sigma, e_old);
-  if (p.j_mode == WK_J_ARRAY) return p.J[(long long)d * p.N + n];
-  return T(0);
 }
 
 // ---------------------------------------------------------------- split ---
@@ -158,48 +136,75 @@ __global__ void k_sigma_e(FitParams<T> p, T* J) {
   for (int d = 0; d < 3; d++) J[d * p.N + n] = mul(p.mat[9 * id + 6 + d], p.E_in[d * p.N + n]);
 }
 
+int blocks_for(long long N) { return (int)((N + kThreads - 1) / kThreads); }
+
+// Shared memory of the plane-marching kernel for TY rows per block.
 template <typename T>
-FitParams<T> make_params(const wk_fit_desc* d, int par) {
-  FitParams<T> p;
-  p.Nx = d->Nx; p.Ny = d->Ny; p.Nz = d->Nz;
-  p.NxNy = (long long)d->Nx * d->Ny;
-  p.N = p.NxNy * d->Nz;
-  p.E_in = (T*)d->E[par]; p.H_in = (T*)d->H[par];
-  p.E_out = (T*)d->E[par ^ 1]; p.H_out = (T*)d->H[par ^ 1];
-  p.J = (T*)d->J;
-  p.j_mode = d->j_mode; p.use_cond = d->use_conductivity;
-  p.mat_id = d->mat_id; p.id_bytes = d->id_bytes;
-  p.mat = (const T*)d->mat_table;
-  p.Lx = (const T*)d->Lx; p.Ly = (const T*)d->Ly; p.Lz = (const T*)d->Lz;
-  p.tLx = (const T*)d->tLx; p.tLy = (const T*)d->tLy; p.tLz = (const T*)d->tLz;
-  p.iAx = (const T*)d->iAx; p.iAy = (const T*)d->iAy; p.iAz = (const T*)d->iAz;
-  p.itAx = (const T*)d->itAx; p.itAy = (const T*)d->itAy; p.itAz = (const T*)d->itAz;
-  for (int f = 0; f < 6; f++) { p.pec_face[f] = d->pec_face[f]; p.pmc_face[f] = d->pmc_face[f]; }
-  p.has_pec = d->has_pec; p.has_pmc = d->has_pmc; p.h_desc = d->h_sum_desc;
-  p.dt = (T)d->dt;
-  p.dt64 = d->dt; p.dt32 = (float)d->dt; p.dt_is_f32 = d->dt_is_f32;
-  p.beam_on = d->beam_on; p.ixs = d->ixs; p.iys = d->iys;
-  p.b_qv = d->b_qv; p.b_v = d->b_v; p.b_v32 = (float)d->b_v; p.b_s0 = d->b_s0;
-  p.b_c0 = d->b_c0; p.b_two_sig2 = d->b_two_sig2; p.b_dx = d->b_dx; p.b_dy = d->b_dy;
-  p.zc = d->zc;
-  p.line_on = d->line_on; p.line_step0 = d->line_step0; p.line_nsteps = d->line_nsteps;
-  p.line = (const T*)d->line;
-  p.cap_on = d->cap_on; p.cap_i0 = d->cap_i0; p.cap_j0 = d->cap_j0;
-  p.cap_ni = d->cap_ni; p.cap_nj = d->cap_nj; p.cap_nt = d->cap_nt; p.cap_step0 = d->cap_step0;
-  p.cap = (T*)d->cap;
-  p.status = d->status;
-  return p;
+size_t march_smem(int Nx, int TY) {
+  return (size_t)(11LL * TY * Nx + 15LL * Nx) * sizeof(T);
 }
 
-int blocks_for(long long N) { return (int)((N + kThreads - 1) / kThreads); }
+struct MarchShape { int TY, KC; size_t smem; };
+
+// Rows per block: the largest count whose tile leaves room for two blocks
+// per SM (else one); planes per block: enough blocks for ~8 per SM.
+template <typename T>
+bool march_shape(const wk_fit_desc* d, MarchShape* ms) {
+  static int max_optin = -1, n_sm = 0;
+  if (max_optin < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const size_t two_per_sm = 110 * 1024;
+  int TY = d->tile_rows;
+  if (TY <= 0) {
+    TY = 0;
+    for (int t = 1; t <= d->Ny && (long long)t * d->Nx <= 2048; t++)
+      if (march_smem<T>(d->Nx, t) <= two_per_sm) TY = t;
+    if (TY == 0 && march_smem<T>(d->Nx, 1) <= (size_t)max_optin) TY = 1;
+    if (TY == 0) return false;
+  }
+  if (TY > d->Ny) TY = d->Ny;
+  size_t smem = march_smem<T>(d->Nx, TY);
+  if (smem > (size_t)max_optin) return false;
+  int nseg = (d->Ny + TY - 1) / TY;
+  int KC = d->tile_planes;
+  if (KC <= 0) {
+    long long want = 8LL * (n_sm > 0 ? n_sm : 148);
+    long long nch = (want + nseg - 1) / nseg;
+    KC = (int)((d->Nz + nch - 1) / nch);
+    if (KC < 4) KC = 4;
+  }
+  if (KC > d->Nz) KC = d->Nz;
+  ms->TY = TY; ms->KC = KC; ms->smem = smem;
+  return true;
+}
 
 template <typename T>
 int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t st) {
   int par = d->par;
-  for (int s = 0; s < n_steps; s++) {
-    FitParams<T> p = make_params<T>(d, par);
-    k_fused<T><<<blocks_for(p.N), kThreads, 0, st>>>(p, step0 + s);
-    par ^= 1;
+  MarchShape ms{0, 0, 0};
+  bool march = false;
+  if (d->kernel != WK_KERNEL_CELL) {
+    march = march_shape<T>(d, &ms);
+    if (!march && d->kernel == WK_KERNEL_MARCH)
+      return wk_fail(WK_E_SHAPE, "wk_fit_step: plane-marching tile does not fit (Nx=%d)", d->Nx);
+  }
+  if (march) {
+    for (int s = 0; s < n_steps; s++) {
+      FitParams<T> p = make_params<T>(d, par);
+      cudaError_t e = launch_march<T>(p, step0 + s, ms.TY, ms.KC, ms.smem, st);
+      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
+      par ^= 1;
+    }
+  } else {
+    for (int s = 0; s < n_steps; s++) {
+      FitParams<T> p = make_params<T>(d, par);
+      k_fused<T><<<blocks_for(p.N), kThreads, 0, st>>>(p, step0 + s);
+      par ^= 1;
+    }
   }
   return wk_check_launch("wk_fit_step");
 }

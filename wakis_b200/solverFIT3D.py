@@ -145,12 +145,19 @@ class SolverFIT3D(RoutinesMixin):
         d.zc = self._zc.data_ptr()
         d.status = self._status.data_ptr()
         self._desc = d
+        self.kernel = "auto"
+        self.tile = (0, 0)
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
 
+    _KERNELS = {"auto": _native.WK_KERNEL_AUTO, "cell": _native.WK_KERNEL_CELL,
+                "march": _native.WK_KERNEL_MARCH}
+
     def _sync_desc(self):
         d = self._desc
+        d.kernel = self._KERNELS[self.kernel]
+        d.tile_rows, d.tile_planes = int(self.tile[0]), int(self.tile[1])
         d.par = self._par
         d.dt = float(self.dt)
         d.dt_is_f32 = int(isinstance(self.dt, np.float32))
@@ -188,12 +195,20 @@ class SolverFIT3D(RoutinesMixin):
             self.step_0 = False
 
     def _advance(self, n_steps, step0=0, beam=None, capture=None, split=False, line=None):
-        """Advance n_steps with optional fused beam (wakesolve Beam) and Ez
-        window capture.  ``step0`` is the global step index of the first
-        step (beam time t = step*dt, capture column)."""
+        """Advance n_steps with optional fused beam (wakesolve Beam), host line
+        current and Ez window capture.  ``step0`` is the global step index of
+        the first step (beam time t = step*dt, capture column)."""
         if n_steps <= 0:
             return
         self._first_step()
+        if self.use_conductivity and self._j_state != _J_SIGMA_E and n_steps > 1:
+            # the J read by the first step is the stored one; every later step
+            # reads J = sigma*E of the step before (upstream 502-503)
+            self._launch(1, step0, beam, capture, split, line)
+            step0, n_steps = step0 + 1, n_steps - 1
+        self._launch(n_steps, step0, beam, capture, split, line)
+
+    def _launch(self, n_steps, step0, beam, capture, split, line):
         d = self._sync_desc()
         if beam is not None:
             d.beam_on = 1
@@ -229,14 +244,20 @@ class SolverFIT3D(RoutinesMixin):
         if self.use_conductivity:
             self._j_state = _J_SIGMA_E
             self._j_line = None
-        elif beam is not None:
-            # non-conductive: J keeps the last beam line (upstream Field write)
-            self._materialize_line(beam, step0 + n_steps - 1)
+        elif beam is not None or line is not None:
+            # non-conductive: J keeps the last line current (upstream Field write)
+            if line is not None:
+                lbuf, lstep0, ixs, iys = line
+                last = lbuf.view(-1, self.Nz)[step0 + n_steps - 1 - lstep0].clone()
+                self._store_line(ixs, iys, last)
+            else:
+                self._materialize_line(beam, step0 + n_steps - 1)
 
     def _materialize_line(self, beam, step):
         from .sources import beam_line_values
-        ixs, iys = beam[0], beam[1]
-        vals = beam_line_values(self, beam, step)
+        self._store_line(beam[0], beam[1], beam_line_values(self, beam, step))
+
+    def _store_line(self, ixs, iys, vals):
         if self._j_state == _J_ARRAY:
             jz = self._J[2 * self.N:3 * self.N].view(self.Nz, self.Ny, self.Nx)
             jz[:, iys, ixs] = vals
