@@ -196,7 +196,7 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "march", "cell"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "march", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
@@ -226,7 +226,8 @@ def main():
     shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else None
     g, w, s = workloads.build_b200(args.workload, dtype=dtype, shape=shape)
     N = s.N
-    s.kernel = args.kernel
+    split = args.kernel == "split"
+    s.kernel = "auto" if split else args.kernel
     s.tile = tuple(int(v) for v in args.tile.split("x"))
     bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
               ).params(s)
@@ -241,7 +242,7 @@ def main():
             dist.barrier()
 
     # warm-up (includes the first-step ghost zeroing)
-    s._advance(args.warmup, 0, beam=bp, capture=cap)
+    s._advance(args.warmup, 0, beam=bp, capture=cap, split=split)
     torch.cuda.synchronize()
     uuid = None
     try:
@@ -255,7 +256,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     e0.record(st)
-    s._advance(args.steps, args.warmup, beam=bp, capture=cap)
+    s._advance(args.steps, args.warmup, beam=bp, capture=cap, split=split)
     e1.record(st)
     torch.cuda.synchronize()
     barrier()
@@ -264,7 +265,7 @@ def main():
     if ws > 1:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
     ms = float(t_dev.item())
-    launches = args.steps  # one fused step kernel per step
+    launches = args.steps * (2 if split else 1)  # step kernels launched
 
     # end to end through the public API: per-step H2D line current, D2H window
     prof = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})

@@ -128,3 +128,56 @@ def e_update(coef, E, Hn, J, dt):
         curl = _sum4(terms, False)
         out[d * N:(d + 1) * N] = E[d * N:(d + 1) * N] + dt * (curl - ieps * J[d * N:(d + 1) * N])
     return out
+
+
+def lean_cells(shape, kind):
+    """Flat indices of the cells the kernels update with the lean formulas."""
+    n, i, j, k = _cells(shape)
+    Nx, Ny, Nz = shape
+    if kind == "h":
+        m = (i >= 1) & (i <= Nx - 3) & (j >= 1) & (j <= Ny - 3) & (k >= 1) & (k <= Nz - 3)
+    else:
+        m = (i >= 2) & (i <= Nx - 2) & (j >= 2) & (j <= Ny - 2) & (k >= 2) & (k <= Nz - 2)
+    return n[m]
+
+
+def h_lean(coef, E, H, dt, cells):
+    """The kernels' interior H update (h_lean in fit_common.cuh) on `cells`."""
+    Nx, Ny, Nz = coef.shape
+    N = Nx * Ny * Nz
+    n = cells
+    i, j, k = n % Nx, (n // Nx) % Ny, n // (Nx * Ny)
+    t = coef.table[coef.ids.astype(np.int64)[n]]
+    ex, ey, ez = (E[d * N:(d + 1) * N] for d in range(3))
+    R0, R1, R2 = coef.iAx[j, k] * t[:, 3], coef.iAy[i, k] * t[:, 4], coef.iAz[i, j] * t[:, 5]
+    Lx, Ly, Lz = coef.Lx[i], coef.Ly[j], coef.Lz[k]
+    desc = coef.h_sum_desc
+    out = []
+    a, b = dt * (R0 * Ly), dt * (R0 * Lz)
+    t0, t1, t2, t3 = a * ey[n], a * ey[n + Nx * Ny], b * ez[n], b * ez[n + Nx]
+    out.append(H[n] - ((((t3 - t2) - t1) + t0) if desc else (((t0 - t1) - t2) + t3)))
+    a, b = dt * (R1 * Lx), dt * (R1 * Lz)
+    t0, t1, t2, t3 = a * ex[n], a * ex[n + Nx * Ny], b * ez[n], b * ez[n + 1]
+    out.append(H[N + n] - ((((t2 - t3) + t1) - t0) if desc else (((t1 - t0) + t2) - t3)))
+    a, b = dt * (R2 * Lx), dt * (R2 * Ly)
+    t0, t1, t2, t3 = a * ex[n], a * ex[n + Nx], b * ey[n], b * ey[n + 1]
+    out.append(H[2 * N + n] - ((((t3 - t2) - t1) + t0) if desc else (((t0 - t1) - t2) + t3)))
+    return out
+
+
+def e_lean_curl(coef, Hn, cells):
+    Nx, Ny, Nz = coef.shape
+    N = Nx * Ny * Nz
+    n = cells
+    i, j, k = n % Nx, (n // Nx) % Ny, n // (Nx * Ny)
+    t = coef.table[coef.ids.astype(np.int64)[n]]
+    hx, hy, hz = (Hn[d * N:(d + 1) * N] for d in range(3))
+    R0, R1, R2 = t[:, 0] * coef.itAx[j, k], t[:, 1] * coef.itAy[i, k], t[:, 2] * coef.itAz[i, j]
+    tLx, tLy, tLz = coef.tLx[i], coef.tLy[j], coef.tLz[k]
+    c1, c2 = R0 * tLy, R0 * tLz
+    cx = (((c1 * hy[n - Nx * Ny]) - (c1 * hy[n])) - (c2 * hz[n - Nx])) + (c2 * hz[n])
+    c1, c2 = R1 * tLx, R1 * tLz
+    cy = (((c1 * hx[n]) - (c1 * hx[n - Nx * Ny])) + (c2 * hz[n - 1])) - (c2 * hz[n])
+    c1, c2 = R2 * tLx, R2 * tLy
+    cz = (((c1 * hx[n - Nx])) - (c1 * hx[n]) - (c2 * hy[n - 1])) + (c2 * hy[n])
+    return cx, cy, cz

@@ -118,3 +118,35 @@ def test_surface_mask_marks_both_sides_of_interface():
     m[2:4, 2:4, 2:4] = True
     s = geometry.surface_mask(m)
     assert s[2, 2, 2] and s[1, 2, 2] and not s[0, 0, 0]
+
+
+def test_lean_interior_formulas_equal_oracle():
+    """The kernels' interior-cell formulas (one coefficient per metric,
+    leading +0 dropped) give the oracle's values on interior cells."""
+    c = dict(cases.STEP_CASES[2])
+    c.update(shape=(9, 8, 10))
+    for bc, mats in ((["pec"] * 3, c["solids"]), (["periodic"] * 3, {})):
+        cc = dict(c, bc_low=bc, bc_high=bc, solids=mats)
+        for dtype in ("float64", "float32"):
+            cc["dtype"] = dtype
+            o = oracle_step_case(cc)
+            k = _coef(cc)
+            E0, H0 = cases.initial_fields(cc, o.N)
+            o.E[:], o.H[:] = E0, H0
+            o.zero_ghosts()
+            o.step_0 = False
+            E, H, J = o.E.copy(), o.H.copy(), o.J.copy()
+            o.one_step()
+            N = o.N
+            hc = emu.lean_cells(k.shape, "h")
+            hx, hy, hz = emu.h_lean(k, E, H, k.dt, hc)
+            assert hc.size > 0
+            for d, v in enumerate((hx, hy, hz)):
+                assert np.array_equal(v, o.H[d * N + hc])
+            ec = emu.lean_cells(k.shape, "e")
+            curl = emu.e_lean_curl(k, o.H, ec)
+            t = k.table[k.ids.astype(np.int64)[ec]]
+            for d in range(3):
+                ieps = t[:, d]
+                e_new = E[d * N + ec] + k.dt * (curl[d] - ieps * J[d * N + ec])
+                assert np.array_equal(e_new, o.E[d * N + ec])

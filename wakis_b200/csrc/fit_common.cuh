@@ -49,7 +49,22 @@ struct FitParams {
   long long cap_nt, cap_step0;
   T* cap;
   int* status;
+  unsigned nx_mul;   // fast division by Nx: q = umulhi(n, nx_mul) >> nx_shift
+  int nx_shift;
 };
+
+// Magic numbers for q = n / d (2 <= d, 0 <= n < 2^31): p = 31 + ceil(log2 d),
+// m = ceil(2^p / d), q = umulhi(n, m) >> (p - 32).
+inline void fast_div_magic(unsigned d, unsigned* m, int* shift) {
+  int l = 0;
+  while ((1ull << l) < d) l++;
+  const int p = 31 + l;
+  *m = (unsigned)(((1ull << p) + d - 1) / d);
+  *shift = p - 32;
+}
+__device__ __forceinline__ int fast_div(int n, unsigned m, int shift) {
+  return (int)(__umulhi((unsigned)n, m) >> shift);
+}
 
 __device__ __forceinline__ int load_id(const void* p, int bytes, long long n) {
   if (bytes == 1) return ((const uint8_t*)p)[n];
@@ -235,6 +250,64 @@ __device__ __forceinline__ T e_curl(const FitParams<T>& p, int d, Cell c, long l
   const long long off[4] = {0, 1, (long long)p.Nx, p.NxNy};
   auto hv = [&](int e, int kind) -> T { return hval(e, n - off[kind]); };
   return e_curl_acc(p, d, c, n, ieps, hv);
+}
+
+// Interior cells: no flat-offset wrap and no face mask touches the cell or
+// the neighbours its rows read, so every column length of a row is the
+// cell's own per-axis length and each coefficient appears twice.  Same
+// products, same order as h_row_acc / e_curl_acc; the leading "+0" of the
+// CSR sum is dropped (it can only change the sign of a zero).
+// H-row lean condition: 1 <= i <= Nx-3, 1 <= j <= Ny-3, 1 <= k <= Nz-3.
+// E-row lean condition: 2 <= i <= Nx-2, 2 <= j <= Ny-2, 2 <= k <= Nz-2.
+template <typename T>
+__device__ __forceinline__ bool lean_h(int i, int j, int k, int Nx, int Ny, int Nz) {
+  return i >= 1 && i <= Nx - 3 && j >= 1 && j <= Ny - 3 && k >= 1 && k <= Nz - 3;
+}
+template <typename T>
+__device__ __forceinline__ bool lean_e(int i, int j, int k, int Nx, int Ny, int Nz) {
+  return i >= 2 && i <= Nx - 2 && j >= 2 && j <= Ny - 2 && k >= 2 && k <= Nz - 2;
+}
+
+// E values: *0 at n, y1/z1 at n+1, x2/z2 at n+Nx, x3/y3 at n+Nx*Ny.
+template <typename T>
+__device__ __forceinline__ void h_lean(T dt, bool desc, T R0, T R1, T R2, T Lx, T Ly, T Lz,
+                                       T ex0, T ey0, T ez0, T ey1, T ez1, T ex2, T ez2,
+                                       T ex3, T ey3, T& hx, T& hy, T& hz) {
+  {  // x: +a*ey0 - a*ey3 - b*ez0 + b*ez2
+    const T a = mul(dt, mul(R0, Ly)), b = mul(dt, mul(R0, Lz));
+    const T t0 = mul(a, ey0), t1 = mul(a, ey3), t2 = mul(b, ez0), t3 = mul(b, ez2);
+    hx = sub(hx, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
+  }
+  {  // y: -a*ex0 + a*ex3 + b*ez0 - b*ez1
+    const T a = mul(dt, mul(R1, Lx)), b = mul(dt, mul(R1, Lz));
+    const T t0 = mul(a, ex0), t1 = mul(a, ex3), t2 = mul(b, ez0), t3 = mul(b, ez1);
+    hy = sub(hy, desc ? sub(add(sub(t2, t3), t1), t0) : sub(add(sub(t1, t0), t2), t3));
+  }
+  {  // z: +a*ex0 - a*ex2 - b*ey0 + b*ey1
+    const T a = mul(dt, mul(R2, Lx)), b = mul(dt, mul(R2, Ly));
+    const T t0 = mul(a, ex0), t1 = mul(a, ex2), t2 = mul(b, ey0), t3 = mul(b, ey1);
+    hz = sub(hz, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
+  }
+}
+
+// Curl parts of the three E rows.  H values: *0 at n, y1/z1 at n-1,
+// x2/z2 at n-Nx, x3/y3 at n-Nx*Ny; R* = ieps*itA of each row.
+template <typename T>
+__device__ __forceinline__ void e_lean(T R0, T R1, T R2, T tLx, T tLy, T tLz, T hx0, T hy0,
+                                       T hz0, T hy1, T hz1, T hx2, T hz2, T hx3, T hy3,
+                                       T& cx, T& cy, T& cz) {
+  {  // x: +c1*hy3 - c1*hy0 - c2*hz2 + c2*hz0
+    const T c1 = mul(R0, tLy), c2 = mul(R0, tLz);
+    cx = add(sub(sub(mul(c1, hy3), mul(c1, hy0)), mul(c2, hz2)), mul(c2, hz0));
+  }
+  {  // y: -c1*hx3 + c1*hx0 + c2*hz1 - c2*hz0
+    const T c1 = mul(R1, tLx), c2 = mul(R1, tLz);
+    cy = sub(add(sub(mul(c1, hx0), mul(c1, hx3)), mul(c2, hz1)), mul(c2, hz0));
+  }
+  {  // z: +c1*hx2 - c1*hx0 - c2*hy1 + c2*hy0
+    const T c1 = mul(R2, tLx), c2 = mul(R2, tLy);
+    cz = add(sub(sub(mul(c1, hx2), mul(c1, hx0)), mul(c2, hy1)), mul(c2, hy0));
+  }
 }
 
 // Gaussian beam current on the line (ixs, iys) at step `step`

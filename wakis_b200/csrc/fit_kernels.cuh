@@ -61,6 +61,7 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
   p.cap_on = d->cap_on; p.cap_i0 = d->cap_i0; p.cap_j0 = d->cap_j0;
   p.cap_ni = d->cap_ni; p.cap_nj = d->cap_nj; p.cap_nt = d->cap_nt; p.cap_step0 = d->cap_step0;
   p.cap = (T*)d->cap;
+  fast_div_magic((unsigned)d->Nx, &p.nx_mul, &p.nx_shift);
   p.status = d->status;
   return p;
 }

@@ -53,7 +53,9 @@ k_march(FitParams<T> p, long long step, int TY, int KC) {
     const long long base = (long long)kk * NxNy + (long long)j0 * Nx - Nx;
     for (int e = threadIdx.x; e < W; e += T_) {
       const long long q = base + e;
-      const bool ok = kk < Nz && q >= 0 && q < N;
+      // the range starts one row before plane kk, so for kk = Nz its first
+      // row is the last row of the grid: only the flat bounds decide
+      const bool ok = q >= 0 && q < N;
 #pragma unroll
       for (int d = 0; d < 3; d++) dst[d * Wst + e] = ok ? p.E_in[d * N + q] : T(0);
     }
@@ -77,22 +79,39 @@ k_march(FitParams<T> p, long long step, int TY, int KC) {
         for (int d = 0; d < 3; d++) Hs[d * LEst + e] = T(0);
         continue;
       }
-      const int r = e / Nx;
+      const int r = fast_div(e, p.nx_mul, p.nx_shift);
       Cell c;
       c.i = e - r * Nx;
       c.j = j0 - 1 + r;
       c.k = k;
       if (c.j < 0) { c.j += Ny; c.k -= 1; }
       const int id = load_id(p.mat_id, p.id_bytes, m);
-      auto ev = [&](int comp, int kind) -> T {
-        if (kind == 3) return Ek1[comp * Wst + e];
-        return Ek[comp * Wst + e + (kind == 1 ? 1 : (kind == 2 ? Nx : 0))];
-      };
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const T h = h_row_acc(p, p.H_in[d * N + m], d, c, m, id, ev);
-        Hs[d * LEst + e] = h;
-        if (!prologue && e >= Nx) p.H_out[d * N + m] = h;
+      T hx = p.H_in[m], hy = p.H_in[N + m], hz = p.H_in[2 * N + m];
+      const bool lean = lean_h<T>(c.i, c.j, c.k, Nx, Ny, Nz);
+      if (__all_sync(__activemask(), lean)) {
+        const T* mt = p.mat + 9 * id;
+        const T R0 = mul(p.iAx[c.j + (long long)c.k * Ny], mt[3]);
+        const T R1 = mul(p.iAy[c.i + (long long)c.k * Nx], mt[4]);
+        const T R2 = mul(p.iAz[c.i + (long long)c.j * Nx], mt[5]);
+        h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[c.i], p.Ly[c.j], p.Lz[c.k],
+               Ek[e], Ek[Wst + e], Ek[2 * Wst + e], Ek[Wst + e + 1], Ek[2 * Wst + e + 1],
+               Ek[e + Nx], Ek[2 * Wst + e + Nx], Ek1[e], Ek1[Wst + e], hx, hy, hz);
+      } else {
+        auto ev = [&](int comp, int kind) -> T {
+          if (kind == 3) return Ek1[comp * Wst + e];
+          return Ek[comp * Wst + e + (kind == 1 ? 1 : (kind == 2 ? Nx : 0))];
+        };
+        hx = h_row_acc(p, hx, 0, c, m, id, ev);
+        hy = h_row_acc(p, hy, 1, c, m, id, ev);
+        hz = h_row_acc(p, hz, 2, c, m, id, ev);
+      }
+      Hs[e] = hx;
+      Hs[LEst + e] = hy;
+      Hs[2 * LEst + e] = hz;
+      if (!prologue && e >= Nx) {
+        p.H_out[m] = hx;
+        p.H_out[N + m] = hy;
+        p.H_out[2 * N + m] = hz;
       }
     }
     __syncthreads();
@@ -102,27 +121,40 @@ k_march(FitParams<T> p, long long step, int TY, int KC) {
       for (int o = threadIdx.x; o < L; o += T_) {
         const long long n = s + o;
         const int e = o + Nx;
-        const int r = o / Nx;
+        const int r = fast_div(o, p.nx_mul, p.nx_shift);
         Cell c;
         c.i = o - r * Nx;
         c.j = j0 + r;
         c.k = k;
         const int id = load_id(p.mat_id, p.id_bytes, n);
-        auto hv = [&](int comp, int kind) -> T {
-          if (kind == 0) return Hs[comp * LEst + e];
-          if (kind == 1) return Hs[comp * LEst + e - 1];
-          if (kind == 2) return Hs[comp * LEst + e - Nx];
-          return Hp[comp * Lst + o];   // n - Nx*Ny (comp 0 or 1)
-        };
+        const T* mt = p.mat + 9 * id;
         if (p.cap_on) capture(p, c, n, step, Ek[2 * Wst + e]);
+        T curl[3];
+        const bool lean = lean_e<T>(c.i, c.j, c.k, Nx, Ny, Nz);
+        if (__all_sync(__activemask(), lean)) {
+          const T R0 = mul(mt[0], p.itAx[c.j + (long long)c.k * Ny]);
+          const T R1 = mul(mt[1], p.itAy[c.i + (long long)c.k * Nx]);
+          const T R2 = mul(mt[2], p.itAz[c.i + (long long)c.j * Nx]);
+          e_lean(R0, R1, R2, p.tLx[c.i], p.tLy[c.j], p.tLz[c.k], Hs[e], Hs[LEst + e],
+                 Hs[2 * LEst + e], Hs[LEst + e - 1], Hs[2 * LEst + e - 1], Hs[e - Nx],
+                 Hs[2 * LEst + e - Nx], Hp[o], Hp[Lst + o], curl[0], curl[1], curl[2]);
+        } else {
+          auto hv = [&](int comp, int kind) -> T {
+            if (kind == 0) return Hs[comp * LEst + e];
+            if (kind == 1) return Hs[comp * LEst + e - 1];
+            if (kind == 2) return Hs[comp * LEst + e - Nx];
+            return Hp[comp * Lst + o];   // n - Nx*Ny (comp 0 or 1)
+          };
+#pragma unroll
+          for (int d = 0; d < 3; d++) curl[d] = e_curl_acc(p, d, c, n, mt[d], hv);
+        }
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-          const T ieps = p.mat[9 * id + d];
-          const T sigma = p.mat[9 * id + 6 + d];
+          const T ieps = mt[d];
+          const T sigma = mt[6 + d];
           const T eold = Ek[d * Wst + e];
           const T jv = j_in(p, d, c, n, step, eold, sigma);
-          const T curl = e_curl_acc(p, d, c, n, ieps, hv);
-          const T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
+          const T enew = add(eold, mul(p.dt, sub(curl[d], mul(ieps, jv))));
           p.E_out[d * N + n] = enew;
           if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
         }
