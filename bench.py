@@ -196,7 +196,7 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "march", "cell", "split"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "fused", "march", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")

@@ -107,19 +107,23 @@ typedef struct wk_fit_desc {
   long long cap_nt, cap_step0;
   void* cap;               /* dtype elements                                 */
   int* status;             /* device status word (0 = ok), may be NULL       */
-  /* Kernel choice for wk_fit_step: WK_KERNEL_AUTO picks the plane-marching
-   * kernel when its shared-memory tile fits, else the per-cell kernel.
+  /* Kernel choice for wk_fit_step (WK_KERNEL_* below).
    * tile_rows / tile_planes (0 = automatic) set the rows per block and the
    * planes per block of the plane-marching kernel.                         */
   int kernel;
   int tile_rows, tile_planes;
 } wk_fit_desc;
 
-#define WK_KERNEL_AUTO 0
-#define WK_KERNEL_CELL 1   /* one thread per cell, H of backward neighbours
-                              recomputed (no shared memory)                 */
+#define WK_KERNEL_AUTO 0   /* WK_KERNEL_FUSED when Nx, Ny, Nz >= 5, else
+                              WK_KERNEL_CELL                                */
+#define WK_KERNEL_CELL 1   /* one thread per cell, general row code, H of
+                              the backward neighbours recomputed            */
 #define WK_KERNEL_MARCH 2  /* plane-marching, E planes staged in shared
                               memory (WK_E_SHAPE if the tile does not fit)  */
+#define WK_KERNEL_FUSED 3  /* one thread per cell in two launches: interior
+                              cells with single-coefficient rows, then the
+                              two-cell shell with the general row code
+                              (WK_E_SHAPE if a dimension is below 5)        */
 
 /* ABI version (WK_ABI_VERSION). */
 int wk_version(void);

@@ -45,8 +45,9 @@ def _valid(idx):
 VALID = [i for i in range(len(cases.STEP_CASES)) if _valid(i)]
 
 
-SCHEDULES = {"march": ("march", (0, 0)), "march_t1": ("march", (1, 1)),
-             "march_t2": ("march", (2, 3)), "cell": ("cell", (0, 0)), "split": None}
+SCHEDULES = {"fused": ("fused", (0, 0)), "march": ("march", (0, 0)),
+             "march_t1": ("march", (1, 1)), "march_t2": ("march", (2, 3)),
+             "cell": ("cell", (0, 0)), "split": None}
 
 
 @pytest.mark.parametrize("sched", list(SCHEDULES))
@@ -71,7 +72,7 @@ def test_steps_without_beam_are_exact(idx, sched):
     assert np.array_equal(s.J.numpy(), o.J)
 
 
-@pytest.mark.parametrize("sched", ["march", "cell"])
+@pytest.mark.parametrize("sched", ["fused", "march", "cell"])
 @pytest.mark.parametrize("idx", VALID)
 def test_steps_with_fused_beam_match_upstream(idx, sched, golden_dir):
     g = np.load(os.path.join(golden_dir, "step_cases.npz"))
@@ -195,14 +196,16 @@ def test_cavity_40_wakesolve_matches_oracle():
         assert rel_err(getattr(wb_, n), getattr(wo, n)) <= WAKE_TOL, n
 
 
-@pytest.mark.parametrize("tile", [(0, 0), (1, 4), (3, 5), (7, 1), (16, 24)])
-def test_march_equals_cell_kernel_with_beam_and_capture(tile):
-    """Plane-marching and per-cell kernels give identical fields and Ez
-    history (same arithmetic, different schedule), for several tiles."""
+@pytest.mark.parametrize("kernel,tile", [("march", (0, 0)), ("march", (1, 4)),
+                                         ("march", (3, 5)), ("march", (7, 1)),
+                                         ("march", (16, 24)), ("fused", (0, 0))])
+def test_schedules_equal_cell_kernel_with_beam_and_capture(kernel, tile):
+    """Plane-marching, interior/shell and per-cell kernels give identical
+    fields and Ez history (same arithmetic, different schedules)."""
     c = cases.WAKE_CASES[3]     # conductive background, PML, beta < 1
     a, wa = b200_wake_case(c)
     b, wb_ = b200_wake_case(c)
-    a.kernel, a.tile = "march", tile
+    a.kernel, a.tile = kernel, tile
     b.kernel = "cell"
     from wakis_b200.sources import Beam
     bp = Beam(q=1e-9, sigmaz=0.004, beta=0.7).params(a)

@@ -268,26 +268,42 @@ __device__ __forceinline__ bool lean_e(int i, int j, int k, int Nx, int Ny, int 
   return i >= 2 && i <= Nx - 2 && j >= 2 && j <= Ny - 2 && k >= 2 && k <= Nz - 2;
 }
 
-// E values: *0 at n, y1/z1 at n+1, x2/z2 at n+Nx, x3/y3 at n+Nx*Ny.
+// Single interior H rows.  For a row at cell c: x reads ey(c), ey(c+z),
+// ez(c), ez(c+y) with lengths Ly, Lz of c; y reads ex(c), ex(c+z), ez(c),
+// ez(c+x) with Lx, Lz; z reads ex(c), ex(c+y), ey(c), ey(c+x) with Lx, Ly.
+// R = iA*imu of the row.  Terms t0..t3 in column order, signs + - - +
+// (x, z) and - + + - (y).
+template <typename T>
+__device__ __forceinline__ T h_lean_x(T dt, bool desc, T R, T Ly, T Lz, T ey0, T ey3, T ez0,
+                                      T ez2, T hold) {
+  const T a = mul(dt, mul(R, Ly)), b = mul(dt, mul(R, Lz));
+  const T t0 = mul(a, ey0), t1 = mul(a, ey3), t2 = mul(b, ez0), t3 = mul(b, ez2);
+  return sub(hold, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
+}
+template <typename T>
+__device__ __forceinline__ T h_lean_y(T dt, bool desc, T R, T Lx, T Lz, T ex0, T ex3, T ez0,
+                                      T ez1, T hold) {
+  const T a = mul(dt, mul(R, Lx)), b = mul(dt, mul(R, Lz));
+  const T t0 = mul(a, ex0), t1 = mul(a, ex3), t2 = mul(b, ez0), t3 = mul(b, ez1);
+  return sub(hold, desc ? sub(add(sub(t2, t3), t1), t0) : sub(add(sub(t1, t0), t2), t3));
+}
+template <typename T>
+__device__ __forceinline__ T h_lean_z(T dt, bool desc, T R, T Lx, T Ly, T ex0, T ex2, T ey0,
+                                      T ey1, T hold) {
+  const T a = mul(dt, mul(R, Lx)), b = mul(dt, mul(R, Ly));
+  const T t0 = mul(a, ex0), t1 = mul(a, ex2), t2 = mul(b, ey0), t3 = mul(b, ey1);
+  return sub(hold, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
+}
+
+// All three rows of one interior cell.  E values: *0 at n, y1/z1 at n+1,
+// x2/z2 at n+Nx, x3/y3 at n+Nx*Ny.
 template <typename T>
 __device__ __forceinline__ void h_lean(T dt, bool desc, T R0, T R1, T R2, T Lx, T Ly, T Lz,
                                        T ex0, T ey0, T ez0, T ey1, T ez1, T ex2, T ez2,
                                        T ex3, T ey3, T& hx, T& hy, T& hz) {
-  {  // x: +a*ey0 - a*ey3 - b*ez0 + b*ez2
-    const T a = mul(dt, mul(R0, Ly)), b = mul(dt, mul(R0, Lz));
-    const T t0 = mul(a, ey0), t1 = mul(a, ey3), t2 = mul(b, ez0), t3 = mul(b, ez2);
-    hx = sub(hx, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
-  }
-  {  // y: -a*ex0 + a*ex3 + b*ez0 - b*ez1
-    const T a = mul(dt, mul(R1, Lx)), b = mul(dt, mul(R1, Lz));
-    const T t0 = mul(a, ex0), t1 = mul(a, ex3), t2 = mul(b, ez0), t3 = mul(b, ez1);
-    hy = sub(hy, desc ? sub(add(sub(t2, t3), t1), t0) : sub(add(sub(t1, t0), t2), t3));
-  }
-  {  // z: +a*ex0 - a*ex2 - b*ey0 + b*ey1
-    const T a = mul(dt, mul(R2, Lx)), b = mul(dt, mul(R2, Ly));
-    const T t0 = mul(a, ex0), t1 = mul(a, ex2), t2 = mul(b, ey0), t3 = mul(b, ey1);
-    hz = sub(hz, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
-  }
+  hx = h_lean_x(dt, desc, R0, Ly, Lz, ey0, ey3, ez0, ez2, hx);
+  hy = h_lean_y(dt, desc, R1, Lx, Lz, ex0, ex3, ez0, ez1, hy);
+  hz = h_lean_z(dt, desc, R2, Lx, Ly, ex0, ex2, ey0, ey1, hz);
 }
 
 // Curl parts of the three E rows.  H values: *0 at n, y1/z1 at n-1,

@@ -1,0 +1,172 @@
+// Fused FIT step without shared memory (sm_100a): interior + shell launches.
+//
+// One thread per cell reads the old state (E_in, H_in) and writes the new
+// state (E_out, H_out), so no block depends on another.  The E row of cell
+// n needs the new H at n, n-1, n-Nx and n-Nx*Ny; the thread recomputes those
+// H rows itself (3 full rows at n, 2 rows at each backward neighbour), with
+// the neighbour E values served by L1/L2 (each E value is read from DRAM
+// once per step: ~96 B of DRAM traffic per cell for FP64).
+//
+// The grid is split in two launches so that every warp runs one code path:
+// * k_interior: cells with 2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3,
+//   where no flat-offset wrap and no face mask can reach any row the cell
+//   needs; each metric coefficient is formed once (h_lean_* / e_lean).
+// * k_shell: the remaining cells (a shell two cells thick), enumerated
+//   compactly, with the general row code (masks, wraps, grid edges).
+#include "../../include/wakis_b200.h"
+#include "abi_internal.h"
+#include "fit_common.cuh"
+#include "fit_kernels.cuh"
+
+namespace wk {
+
+constexpr int kInteriorX = 128, kInteriorY = 2, kShellThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kInteriorX * kInteriorY)
+k_interior(FitParams<T> p, long long step) {
+  const int i = 2 + blockIdx.x * kInteriorX + threadIdx.x;
+  const int j = 2 + blockIdx.y * kInteriorY + threadIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const int Nx = p.Nx, Ny = p.Ny;
+  const long long N = p.N, sy = Nx, sz = p.NxNy;
+  const long long n = i + j * sy + k * sz;
+  const T* __restrict__ ex = p.E_in;
+  const T* __restrict__ ey = p.E_in + N;
+  const T* __restrict__ ez = p.E_in + 2 * N;
+  const T* __restrict__ hx = p.H_in;
+  const T* __restrict__ hy = p.H_in + N;
+  const T* __restrict__ hz = p.H_in + 2 * N;
+  const T dt = p.dt;
+  const bool desc = p.h_desc != 0;
+
+  const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+  const T* m1 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - 1);
+  const T* m2 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - sy);
+  const T* m3 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - sz);
+  const T Lxi = p.Lx[i], Lxm = p.Lx[i - 1];
+  const T Lyj = p.Ly[j], Lym = p.Ly[j - 1];
+  const T Lzk = p.Lz[k], Lzm = p.Lz[k - 1];
+
+  // E at n and around it
+  const T ex0 = ex[n], ey0 = ey[n], ez0 = ez[n];
+  // new H at n (three rows)
+  T hxn = hx[n], hyn = hy[n], hzn = hz[n];
+  {
+    const T R0 = mul(p.iAx[j + (long long)k * Ny], m0[3]);
+    const T R1 = mul(p.iAy[i + (long long)k * Nx], m0[4]);
+    const T R2 = mul(p.iAz[i + (long long)j * Nx], m0[5]);
+    h_lean(dt, desc, R0, R1, R2, Lxi, Lyj, Lzk, ex0, ey0, ez0, ey[n + 1], ez[n + 1],
+           ex[n + sy], ez[n + sy], ex[n + sz], ey[n + sz], hxn, hyn, hzn);
+  }
+  // new H at n-1: y and z rows of cell (i-1, j, k)
+  const long long a1 = n - 1;
+  const T ex_a1 = ex[a1];
+  const T hy1 = h_lean_y(dt, desc, mul(p.iAy[i - 1 + (long long)k * Nx], m1[4]), Lxm, Lzk,
+                         ex_a1, ex[a1 + sz], ez[a1], ez0, hy[a1]);
+  const T hz1 = h_lean_z(dt, desc, mul(p.iAz[i - 1 + (long long)j * Nx], m1[5]), Lxm, Lyj,
+                         ex_a1, ex[a1 + sy], ey[a1], ey0, hz[a1]);
+  // new H at n-Nx: x and z rows of cell (i, j-1, k)
+  const long long a2 = n - sy;
+  const T ey_a2 = ey[a2];
+  const T hx2 = h_lean_x(dt, desc, mul(p.iAx[j - 1 + (long long)k * Ny], m2[3]), Lym, Lzk,
+                         ey_a2, ey[a2 + sz], ez[a2], ez0, hx[a2]);
+  const T hz2 = h_lean_z(dt, desc, mul(p.iAz[i + (long long)(j - 1) * Nx], m2[5]), Lxi, Lym,
+                         ex[a2], ex0, ey_a2, ey[a2 + 1], hz[a2]);
+  // new H at n-Nx*Ny: x and y rows of cell (i, j, k-1)
+  const long long a3 = n - sz;
+  const T ez_a3 = ez[a3];
+  const T hx3 = h_lean_x(dt, desc, mul(p.iAx[j + (long long)(k - 1) * Ny], m3[3]), Lyj, Lzm,
+                         ey[a3], ey0, ez_a3, ez[a3 + sy], hx[a3]);
+  const T hy3 = h_lean_y(dt, desc, mul(p.iAy[i + (long long)(k - 1) * Nx], m3[4]), Lxi, Lzm,
+                         ex[a3], ex0, ez_a3, ez[a3 + 1], hy[a3]);
+
+  // E at n
+  T curl[3];
+  {
+    const T R0 = mul(m0[0], p.itAx[j + (long long)k * Ny]);
+    const T R1 = mul(m0[1], p.itAy[i + (long long)k * Nx]);
+    const T R2 = mul(m0[2], p.itAz[i + (long long)j * Nx]);
+    e_lean(R0, R1, R2, p.tLx[i], p.tLy[j], p.tLz[k], hxn, hyn, hzn, hy1, hz1, hx2, hz2, hx3,
+           hy3, curl[0], curl[1], curl[2]);
+  }
+  Cell c;
+  c.i = i; c.j = j; c.k = k;
+  const T eold[3] = {ex0, ey0, ez0};
+  if (p.cap_on) capture(p, c, n, step, ez0);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const T ieps = m0[d], sigma = m0[6 + d];
+    const T jv = j_in(p, d, c, n, step, eold[d], sigma);
+    const T enew = add(eold[d], mul(dt, sub(curl[d], mul(ieps, jv))));
+    p.E_out[d * N + n] = enew;
+    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+  }
+  p.H_out[n] = hxn;
+  p.H_out[N + n] = hyn;
+  p.H_out[2 * N + n] = hzn;
+}
+
+// Cell of the idx-th shell cell: planes k in {0,1,Nz-2,Nz-1}, then rows
+// j in {0,1,Ny-2,Ny-1} of the inner planes, then columns i in
+// {0,1,Nx-2,Nx-1} of the inner rows (needs Nx, Ny, Nz >= 5).
+__device__ __forceinline__ Cell shell_cell(long long idx, int Nx, int Ny, int Nz) {
+  Cell c;
+  const long long NxNy = (long long)Nx * Ny;
+  const long long A = 4 * NxNy;
+  if (idx < A) {
+    const int kk = (int)(idx / NxNy);
+    const long long rem = idx - kk * NxNy;
+    c.k = kk < 2 ? kk : Nz - 4 + kk;
+    c.j = (int)(rem / Nx);
+    c.i = (int)(rem - (long long)c.j * Nx);
+    return c;
+  }
+  idx -= A;
+  const long long B = 4LL * Nx * (Nz - 4);
+  if (idx < B) {
+    const long long t = idx / Nx;
+    c.i = (int)(idx - t * Nx);
+    const int jj = (int)(t % 4);
+    c.j = jj < 2 ? jj : Ny - 4 + jj;
+    c.k = 2 + (int)(t / 4);
+    return c;
+  }
+  idx -= B;
+  const int ii = (int)(idx % 4);
+  c.i = ii < 2 ? ii : Nx - 4 + ii;
+  const long long t = idx / 4;
+  c.j = 2 + (int)(t % (Ny - 4));
+  c.k = 2 + (int)(t / (Ny - 4));
+  return c;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kShellThreads) k_shell(FitParams<T> p, long long step,
+                                                          long long count) {
+  const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
+  if (idx >= count) return;
+  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
+  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
+  fused_cell_general(p, step, n, c);
+}
+
+template <typename T>
+cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st) {
+  dim3 blk(kInteriorX, kInteriorY);
+  dim3 grid((p.Nx - 4 + kInteriorX - 1) / kInteriorX, (p.Ny - 4 + kInteriorY - 1) / kInteriorY,
+            p.Nz - 4);
+  k_interior<T><<<grid, blk, 0, st>>>(p, step);
+  const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
+  k_shell<T><<<(unsigned)((count + kShellThreads - 1) / kShellThreads), kShellThreads, 0, st>>>(
+      p, step, count);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_interior_shell<double>(const FitParams<double>&, long long,
+                                                   cudaStream_t);
+template cudaError_t launch_interior_shell<float>(const FitParams<float>&, long long,
+                                                  cudaStream_t);
+
+}  // namespace wk

@@ -67,6 +67,66 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
 }
 
 
+// Fused step of one cell with the general row code: the new H of the cell
+// and of the three backward neighbours it needs is computed from the old
+// state, then the new E of the cell.
+template <typename T>
+__device__ __forceinline__ void fused_cell_general(const FitParams<T>& p, long long step,
+                                                   long long n, Cell c) {
+  const long long N = p.N;
+  int id = load_id(p.mat_id, p.id_bytes, n);
+  if (p.cap_on) capture(p, c, n, step, p.E_in[2 * N + n]);
+  T hn[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) hn[d] = h_row(p, p.E_in, p.H_in[d * N + n], d, c, n, id);
+  T hm1[3], hmy[3], hmz[3];
+  if (n >= 1) {
+    Cell cm = minus_x(c, p.Nx, p.Ny); long long m = n - 1;
+    int idm = load_id(p.mat_id, p.id_bytes, m);
+    hm1[1] = h_row(p, p.E_in, p.H_in[N + m], 1, cm, m, idm);
+    hm1[2] = h_row(p, p.E_in, p.H_in[2 * N + m], 2, cm, m, idm);
+  } else { hm1[1] = hm1[2] = T(0); }
+  hm1[0] = T(0);
+  if (n >= p.Nx) {
+    Cell cm = minus_y(c, p.Ny); long long m = n - p.Nx;
+    int idm = load_id(p.mat_id, p.id_bytes, m);
+    hmy[0] = h_row(p, p.E_in, p.H_in[m], 0, cm, m, idm);
+    hmy[2] = h_row(p, p.E_in, p.H_in[2 * N + m], 2, cm, m, idm);
+  } else { hmy[0] = hmy[2] = T(0); }
+  hmy[1] = T(0);
+  if (n >= p.NxNy) {
+    Cell cm = c; cm.k--; long long m = n - p.NxNy;
+    int idm = load_id(p.mat_id, p.id_bytes, m);
+    hmz[0] = h_row(p, p.E_in, p.H_in[m], 0, cm, m, idm);
+    hmz[1] = h_row(p, p.E_in, p.H_in[N + m], 1, cm, m, idm);
+  } else { hmz[0] = hmz[1] = T(0); }
+  hmz[2] = T(0);
+  auto hv = [&](int e, int kind) -> T {
+    if (kind == 0) return hn[e];
+    if (kind == 1) return hm1[e];
+    if (kind == 2) return hmy[e];
+    return hmz[e];
+  };
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    T ieps = p.mat[9 * id + d];
+    T sigma = p.mat[9 * id + 6 + d];
+    T eold = p.E_in[d * N + n];
+    T jv = j_in(p, d, c, n, step, eold, sigma);
+    T curl = e_curl_acc(p, d, c, n, ieps, hv);
+    T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
+    p.E_out[d * N + n] = enew;
+    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) p.H_out[d * N + n] = hn[d];
+}
+
+// Launch the interior (lean) and shell (general) fused kernels of one step
+// (fit_fused.cu); needs Nx, Ny, Nz >= 5.
+template <typename T>
+cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st);
+
 // Launch the plane-marching kernel (defined in fit_march.cu) with TY rows
 // and KC planes per block and `smem` bytes of dynamic shared memory.
 template <typename T>

@@ -69,62 +69,12 @@ __global__ void k_e_split(FitParams<T> p, long long step) {
 }
 
 // ---------------------------------------------------------------- fused ---
-// One thread per cell: the new H of the cell and of the three backward
-// neighbours it needs is computed from the old state, so the pass reads
-// only E_in/H_in and writes only E_out/H_out.
+// One thread per cell over the whole grid, general row code only.
 template <typename T>
 __global__ void k_fused(FitParams<T> p, long long step) {
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= p.N) return;
-  const long long N = p.N;
-  Cell c = cell_of(n, p.Nx, p.Ny);
-  int id = load_id(p.mat_id, p.id_bytes, n);
-  if (p.cap_on) capture(p, c, n, step, p.E_in[2 * N + n]);
-  T hn[3];
-#pragma unroll
-  for (int d = 0; d < 3; d++) hn[d] = h_row(p, p.E_in, p.H_in[d * N + n], d, c, n, id);
-  // backward neighbours (flat offsets 1, Nx, Nx*Ny)
-  T hm1[3], hmy[3], hmz[3];
-  if (n >= 1) {
-    Cell cm = minus_x(c, p.Nx, p.Ny); long long m = n - 1;
-    int idm = load_id(p.mat_id, p.id_bytes, m);
-    hm1[1] = h_row(p, p.E_in, p.H_in[N + m], 1, cm, m, idm);
-    hm1[2] = h_row(p, p.E_in, p.H_in[2 * N + m], 2, cm, m, idm);
-  } else { hm1[1] = hm1[2] = T(0); }
-  hm1[0] = T(0);
-  if (n >= p.Nx) {
-    Cell cm = minus_y(c, p.Ny); long long m = n - p.Nx;
-    int idm = load_id(p.mat_id, p.id_bytes, m);
-    hmy[0] = h_row(p, p.E_in, p.H_in[m], 0, cm, m, idm);
-    hmy[2] = h_row(p, p.E_in, p.H_in[2 * N + m], 2, cm, m, idm);
-  } else { hmy[0] = hmy[2] = T(0); }
-  hmy[1] = T(0);
-  if (n >= p.NxNy) {
-    Cell cm = c; cm.k--; long long m = n - p.NxNy;
-    int idm = load_id(p.mat_id, p.id_bytes, m);
-    hmz[0] = h_row(p, p.E_in, p.H_in[m], 0, cm, m, idm);
-    hmz[1] = h_row(p, p.E_in, p.H_in[N + m], 1, cm, m, idm);
-  } else { hmz[0] = hmz[1] = T(0); }
-  hmz[2] = T(0);
-  auto hval = [&](int e, long long m) -> T {
-    if (m == n) return hn[e];
-    if (m == n - 1) return hm1[e];
-    if (m == n - p.Nx) return hmy[e];
-    return hmz[e];
-  };
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    T ieps = p.mat[9 * id + d];
-    T sigma = p.mat[9 * id + 6 + d];
-    T eold = p.E_in[d * N + n];
-    T jv = j_in(p, d, c, n, step, eold, sigma);
-    T curl = e_curl(p, d, c, n, ieps, hval);
-    T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
-    p.E_out[d * N + n] = enew;
-    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
-  }
-#pragma unroll
-  for (int d = 0; d < 3; d++) p.H_out[d * N + n] = hn[d];
+  fused_cell_general(p, step, n, cell_of(n, p.Nx, p.Ny));
 }
 
 template <typename T>
@@ -187,9 +137,22 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   int par = d->par;
   MarchShape ms{0, 0, 0};
   bool march = false;
-  if (d->kernel != WK_KERNEL_CELL) {
+  const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
+                   (d->Ny - 4 + 1) / 2 <= 65535;
+  if (d->kernel == WK_KERNEL_FUSED && !big)
+    return wk_fail(WK_E_SHAPE, "wk_fit_step: interior/shell kernels need every dimension >= 5");
+  if (d->kernel == WK_KERNEL_FUSED || (d->kernel == WK_KERNEL_AUTO && big)) {
+    for (int s = 0; s < n_steps; s++) {
+      FitParams<T> p = make_params<T>(d, par);
+      cudaError_t e = launch_interior_shell<T>(p, step0 + s, st);
+      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
+      par ^= 1;
+    }
+    return wk_check_launch("wk_fit_step");
+  }
+  if (d->kernel == WK_KERNEL_MARCH) {
     march = march_shape<T>(d, &ms);
-    if (!march && d->kernel == WK_KERNEL_MARCH)
+    if (!march)
       return wk_fail(WK_E_SHAPE, "wk_fit_step: plane-marching tile does not fit (Nx=%d)", d->Nx);
   }
   if (march) {
