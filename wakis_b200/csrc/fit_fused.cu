@@ -21,6 +21,7 @@
 namespace wk {
 
 constexpr int kInteriorX = 128, kInteriorY = 2, kShellThreads = 256;
+constexpr int kColumnRows = 4;   // warps (rows j) per block of the column kernel
 
 template <typename T>
 __global__ void __launch_bounds__(kInteriorX * kInteriorY)
@@ -108,6 +109,118 @@ k_interior(FitParams<T> p, long long step) {
   p.H_out[2 * N + n] = hzn;
 }
 
+// Interior cells, one thread per (i, j) column marching kz planes.  Lane l
+// of a warp sits at i = i0 - 1 + l; lanes 1..31 own their cells, lane 0 only
+// supplies the new H of (i0-1, j) to lane 1 (shuffle).  Carried from plane
+// k-1 to k: E(n) x/y (loaded as E(n+Nx*Ny) one plane earlier), Ey(n-Nx), and
+// the new H(n-Nx*Ny) x/y.  The ±1 neighbours come from the adjacent lanes;
+// the H rows of (i, j-1) are recomputed.
+template <typename T>
+__global__ void __launch_bounds__(32 * kColumnRows)
+k_column(FitParams<T> p, long long step, int kz) {
+  const int lane = threadIdx.x;
+  const int i_raw = 2 + blockIdx.x * 31 - 1 + lane;
+  const int j = 2 + blockIdx.y * kColumnRows + threadIdx.y;
+  const int k0 = 2 + blockIdx.z * kz;
+  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
+  if (j > Ny - 3) return;                 // whole warp
+  const int k1 = min(k0 + kz, Nz - 2);
+  const bool owner = lane >= 1 && i_raw <= Nx - 3;
+  const int i = min(i_raw, Nx - 2);       // lanes past the last owner + 1 only feed shuffles
+  const long long N = p.N, sy = Nx, sz = p.NxNy;
+  const T* __restrict__ ex = p.E_in;
+  const T* __restrict__ ey = p.E_in + N;
+  const T* __restrict__ ez = p.E_in + 2 * N;
+  const T* __restrict__ hx = p.H_in;
+  const T* __restrict__ hy = p.H_in + N;
+  const T* __restrict__ hz = p.H_in + 2 * N;
+  const T dt = p.dt;
+  const bool desc = p.h_desc != 0;
+  const unsigned FULL = 0xffffffffu;
+
+  // per-column metrics
+  const T Lxi = p.Lx[i], Lyj = p.Ly[j], Lym = p.Ly[j - 1];
+  const T tLxi = p.tLx[i], tLyj = p.tLy[j];
+  const T iAz0 = p.iAz[i + (long long)j * Nx], iAzm = p.iAz[i + (long long)(j - 1) * Nx];
+  const T itAz0 = p.itAz[i + (long long)j * Nx];
+
+  // prologue: carried values for plane k0
+  long long n = i + j * sy + k0 * sz;
+  T exc = ex[n], eyc = ey[n], eymc = ey[n - sy];
+  T hxp, hyp;
+  {
+    const long long a = n - sz;
+    const T* m = p.mat + 9 * load_id(p.mat_id, p.id_bytes, a);
+    const T ez_a = ez[a];
+    hxp = h_lean_x(dt, desc, mul(p.iAx[j + (long long)(k0 - 1) * Ny], m[3]), Lyj,
+                   p.Lz[k0 - 1], ey[a], eyc, ez_a, ez[a + sy], hx[a]);
+    hyp = h_lean_y(dt, desc, mul(p.iAy[i + (long long)(k0 - 1) * Nx], m[4]), Lxi,
+                   p.Lz[k0 - 1], ex[a], exc, ez_a, ez[a + 1], hy[a]);
+  }
+
+  for (int k = k0; k < k1; k++, n += sz) {
+    const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+    const T* m2 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - sy);
+    const T Lzk = p.Lz[k];
+    const T ez0 = ez[n];
+    const T ex_pz = ex[n + sz], ey_pz = ey[n + sz];
+    const T ex_py = ex[n + sy], ez_py = ez[n + sy];
+    const T ex_my = ex[n - sy], ez_my = ez[n - sy];
+    const T ey_mypz = ey[n - sy + sz];
+    // +1 neighbours from lane + 1 (lane 31 loads its own)
+    T ey_p1 = __shfl_down_sync(FULL, eyc, 1);
+    T ez_p1 = __shfl_down_sync(FULL, ez0, 1);
+    T ey_myp1 = __shfl_down_sync(FULL, eymc, 1);
+    if (lane == 31) {
+      ey_p1 = ey[n + 1];
+      ez_p1 = ez[n + 1];
+      ey_myp1 = ey[n - sy + 1];
+    }
+    // new H at n
+    const T hxn = h_lean_x(dt, desc, mul(p.iAx[j + (long long)k * Ny], m0[3]), Lyj, Lzk, eyc,
+                           ey_pz, ez0, ez_py, hx[n]);
+    const T hyn = h_lean_y(dt, desc, mul(p.iAy[i + (long long)k * Nx], m0[4]), Lxi, Lzk, exc,
+                           ex_pz, ez0, ez_p1, hy[n]);
+    const T hzn = h_lean_z(dt, desc, mul(iAz0, m0[5]), Lxi, Lyj, exc, ex_py, eyc, ey_p1, hz[n]);
+    // new H at n - Nx (cell (i, j-1, k)): x and z rows
+    const T hx2 = h_lean_x(dt, desc, mul(p.iAx[j - 1 + (long long)k * Ny], m2[3]), Lym, Lzk,
+                           eymc, ey_mypz, ez_my, ez0, hx[n - sy]);
+    const T hz2 = h_lean_z(dt, desc, mul(iAzm, m2[5]), Lxi, Lym, ex_my, exc, eymc, ey_myp1,
+                           hz[n - sy]);
+    // new H at n - 1 from lane - 1
+    const T hy1 = __shfl_up_sync(FULL, hyn, 1);
+    const T hz1 = __shfl_up_sync(FULL, hzn, 1);
+    if (owner) {
+      T curl[3];
+      const T R0 = mul(m0[0], p.itAx[j + (long long)k * Ny]);
+      const T R1 = mul(m0[1], p.itAy[i + (long long)k * Nx]);
+      const T R2 = mul(m0[2], itAz0);
+      e_lean(R0, R1, R2, tLxi, tLyj, p.tLz[k], hxn, hyn, hzn, hy1, hz1, hx2, hz2, hxp, hyp,
+             curl[0], curl[1], curl[2]);
+      Cell c;
+      c.i = i; c.j = j; c.k = k;
+      const T eold[3] = {exc, eyc, ez0};
+      if (p.cap_on) capture(p, c, n, step, ez0);
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const T ieps = m0[d], sigma = m0[6 + d];
+        const T jv = j_in(p, d, c, n, step, eold[d], sigma);
+        const T enew = add(eold[d], mul(dt, sub(curl[d], mul(ieps, jv))));
+        p.E_out[d * N + n] = enew;
+        if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+      }
+      p.H_out[n] = hxn;
+      p.H_out[N + n] = hyn;
+      p.H_out[2 * N + n] = hzn;
+    }
+    exc = ex_pz;
+    eyc = ey_pz;
+    eymc = ey_mypz;
+    hxp = hxn;
+    hyp = hyn;
+  }
+}
+
 // Cell of the idx-th shell cell: planes k in {0,1,Nz-2,Nz-1}, then rows
 // j in {0,1,Ny-2,Ny-1} of the inner planes, then columns i in
 // {0,1,Nx-2,Nx-1} of the inner rows (needs Nx, Ny, Nz >= 5).
@@ -153,11 +266,19 @@ __global__ void __launch_bounds__(kShellThreads) k_shell(FitParams<T> p, long lo
 }
 
 template <typename T>
-cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st) {
-  dim3 blk(kInteriorX, kInteriorY);
-  dim3 grid((p.Nx - 4 + kInteriorX - 1) / kInteriorX, (p.Ny - 4 + kInteriorY - 1) / kInteriorY,
-            p.Nz - 4);
-  k_interior<T><<<grid, blk, 0, st>>>(p, step);
+cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,
+                                  int kz) {
+  if (kz <= 0) {
+    dim3 blk(kInteriorX, kInteriorY);
+    dim3 grid((p.Nx - 4 + kInteriorX - 1) / kInteriorX,
+              (p.Ny - 4 + kInteriorY - 1) / kInteriorY, p.Nz - 4);
+    k_interior<T><<<grid, blk, 0, st>>>(p, step);
+  } else {
+    dim3 blk(32, kColumnRows);
+    dim3 grid((p.Nx - 4 + 30) / 31, (p.Ny - 4 + kColumnRows - 1) / kColumnRows,
+              (p.Nz - 4 + kz - 1) / kz);
+    k_column<T><<<grid, blk, 0, st>>>(p, step, kz);
+  }
   const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
   k_shell<T><<<(unsigned)((count + kShellThreads - 1) / kShellThreads), kShellThreads, 0, st>>>(
       p, step, count);
@@ -165,8 +286,8 @@ cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStr
 }
 
 template cudaError_t launch_interior_shell<double>(const FitParams<double>&, long long,
-                                                   cudaStream_t);
+                                                   cudaStream_t, int);
 template cudaError_t launch_interior_shell<float>(const FitParams<float>&, long long,
-                                                  cudaStream_t);
+                                                  cudaStream_t, int);
 
 }  // namespace wk

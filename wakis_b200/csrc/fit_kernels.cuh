@@ -123,9 +123,11 @@ __device__ __forceinline__ void fused_cell_general(const FitParams<T>& p, long l
 }
 
 // Launch the interior (lean) and shell (general) fused kernels of one step
-// (fit_fused.cu); needs Nx, Ny, Nz >= 5.
+// (fit_fused.cu); needs Nx, Ny, Nz >= 5.  kz > 0 selects the column kernel
+// with kz planes per thread, kz = 0 the one-thread-per-cell interior kernel.
 template <typename T>
-cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st);
+cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,
+                                  int kz);
 
 // Launch the plane-marching kernel (defined in fit_march.cu) with TY rows
 // and KC planes per block and `smem` bytes of dynamic shared memory.

@@ -142,9 +142,21 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   if (d->kernel == WK_KERNEL_FUSED && !big)
     return wk_fail(WK_E_SHAPE, "wk_fit_step: interior/shell kernels need every dimension >= 5");
   if (d->kernel == WK_KERNEL_FUSED || (d->kernel == WK_KERNEL_AUTO && big)) {
+    // tile_planes: planes per thread of the column kernel (0 = automatic,
+    // -1 = one-thread-per-cell interior kernel)
+    int kz = d->tile_planes;
+    if (kz == 0) {
+      long long cols = (long long)((d->Nx - 4 + 30) / 31) * 32 * (d->Ny - 4);
+      long long want = 148LL * 2048 * 2;       // threads for ~2 waves
+      long long chunks = (want + cols - 1) / cols;
+      kz = (int)((d->Nz - 4 + chunks - 1) / chunks);
+      if (kz < 8) kz = 8;
+    }
+    if (kz < 0) kz = 0;
+    if (kz > 0 && (d->Nz - 4 + kz - 1) / kz > 65535) kz = (d->Nz - 4 + 65534) / 65535;
     for (int s = 0; s < n_steps; s++) {
       FitParams<T> p = make_params<T>(d, par);
-      cudaError_t e = launch_interior_shell<T>(p, step0 + s, st);
+      cudaError_t e = launch_interior_shell<T>(p, step0 + s, st, kz);
       if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
       par ^= 1;
     }
