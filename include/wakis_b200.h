@@ -124,6 +124,9 @@ typedef struct wk_fit_desc {
                               cells with single-coefficient rows, then the
                               two-cell shell with the general row code
                               (WK_E_SHAPE if a dimension is below 5)        */
+#define WK_KERNEL_TWOPASS 4 /* H pass then E pass, each an interior launch
+                              with single-coefficient rows plus a shell
+                              launch (WK_E_SHAPE if a dimension is below 5) */
 
 /* ABI version (WK_ABI_VERSION). */
 int wk_version(void);

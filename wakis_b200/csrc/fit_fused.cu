@@ -221,6 +221,69 @@ k_column(FitParams<T> p, long long step, int kz) {
   }
 }
 
+// ------------------------------------------------------------ two passes --
+// H pass then E pass over the interior (lean rows) and the shell (general
+// rows).  The H pass reads E_in, H_in and writes H_out; the E pass reads
+// E_in and the new H (H_out) and writes E_out; H_out may alias H_in and
+// E_out may alias E_in (each cell reads only its own old value of the field
+// it writes).
+constexpr int kPassX = 128, kPassY = 2;
+
+template <typename T>
+__global__ void __launch_bounds__(kPassX * kPassY) k_h_pass(FitParams<T> p) {
+  const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
+  const int j = 2 + blockIdx.y * kPassY + threadIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const long long N = p.N, sy = p.Nx, sz = p.NxNy;
+  const long long n = i + j * sy + k * sz;
+  const T* ex = p.E_in;
+  const T* ey = p.E_in + N;
+  const T* ez = p.E_in + 2 * N;
+  const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+  const T R0 = mul(p.iAx[j + (long long)k * p.Ny], m0[3]);
+  const T R1 = mul(p.iAy[i + (long long)k * p.Nx], m0[4]);
+  const T R2 = mul(p.iAz[i + (long long)j * p.Nx], m0[5]);
+  T hx = p.H_in[n], hy = p.H_in[N + n], hz = p.H_in[2 * N + n];
+  h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[i], p.Ly[j], p.Lz[k], ex[n], ey[n], ez[n],
+         ey[n + 1], ez[n + 1], ex[n + sy], ez[n + sy], ex[n + sz], ey[n + sz], hx, hy, hz);
+  p.H_out[n] = hx;
+  p.H_out[N + n] = hy;
+  p.H_out[2 * N + n] = hz;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPassX * kPassY) k_e_pass(FitParams<T> p, long long step) {
+  const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
+  const int j = 2 + blockIdx.y * kPassY + threadIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const long long N = p.N, sy = p.Nx, sz = p.NxNy;
+  const long long n = i + j * sy + k * sz;
+  const T* hx = p.H_out;
+  const T* hy = p.H_out + N;
+  const T* hz = p.H_out + 2 * N;
+  const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+  const T R0 = mul(m0[0], p.itAx[j + (long long)k * p.Ny]);
+  const T R1 = mul(m0[1], p.itAy[i + (long long)k * p.Nx]);
+  const T R2 = mul(m0[2], p.itAz[i + (long long)j * p.Nx]);
+  T curl[3];
+  e_lean(R0, R1, R2, p.tLx[i], p.tLy[j], p.tLz[k], hx[n], hy[n], hz[n], hy[n - 1], hz[n - 1],
+         hx[n - sy], hz[n - sy], hx[n - sz], hy[n - sz], curl[0], curl[1], curl[2]);
+  const T eold[3] = {p.E_in[n], p.E_in[N + n], p.E_in[2 * N + n]};
+  Cell c;
+  c.i = i; c.j = j; c.k = k;
+  if (p.cap_on) capture(p, c, n, step, eold[2]);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const T ieps = m0[d], sigma = m0[6 + d];
+    const T jv = j_in(p, d, c, n, step, eold[d], sigma);
+    const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
+    p.E_out[d * N + n] = enew;
+    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+  }
+}
+
 // Cell of the idx-th shell cell: planes k in {0,1,Nz-2,Nz-1}, then rows
 // j in {0,1,Ny-2,Ny-1} of the inner planes, then columns i in
 // {0,1,Nx-2,Nx-1} of the inner rows (needs Nx, Ny, Nz >= 5).
@@ -264,6 +327,60 @@ __global__ void __launch_bounds__(kShellThreads) k_shell(FitParams<T> p, long lo
   const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
   fused_cell_general(p, step, n, c);
 }
+
+template <typename T>
+__global__ void __launch_bounds__(kShellThreads) k_h_shell(FitParams<T> p, long long count) {
+  const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
+  if (idx >= count) return;
+  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
+  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
+  const int id = load_id(p.mat_id, p.id_bytes, n);
+  T h[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) h[d] = h_row(p, p.E_in, p.H_in[d * p.N + n], d, c, n, id);
+#pragma unroll
+  for (int d = 0; d < 3; d++) p.H_out[d * p.N + n] = h[d];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kShellThreads) k_e_shell(FitParams<T> p, long long step,
+                                                            long long count) {
+  const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
+  if (idx >= count) return;
+  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
+  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
+  const long long N = p.N;
+  const int id = load_id(p.mat_id, p.id_bytes, n);
+  const T* Hn = p.H_out;
+  auto hval = [&](int e, long long m) -> T { return Hn[e * N + m]; };
+  if (p.cap_on) capture(p, c, n, step, p.E_in[2 * N + n]);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const T ieps = p.mat[9 * id + d], sigma = p.mat[9 * id + 6 + d];
+    const T eold = p.E_in[d * N + n];
+    const T jv = j_in(p, d, c, n, step, eold, sigma);
+    const T curl = e_curl(p, d, c, n, ieps, hval);
+    const T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
+    p.E_out[d * N + n] = enew;
+    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+  }
+}
+
+template <typename T>
+cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st) {
+  dim3 blk(kPassX, kPassY);
+  dim3 grid((p.Nx - 4 + kPassX - 1) / kPassX, (p.Ny - 4 + kPassY - 1) / kPassY, p.Nz - 4);
+  const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
+  const unsigned sb = (unsigned)((count + kShellThreads - 1) / kShellThreads);
+  k_h_pass<T><<<grid, blk, 0, st>>>(p);
+  k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, count);
+  k_e_pass<T><<<grid, blk, 0, st>>>(p, step);
+  k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, count);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long, cudaStream_t);
+template cudaError_t launch_two_pass<float>(const FitParams<float>&, long long, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,

@@ -139,8 +139,17 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   bool march = false;
   const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
                    (d->Ny - 4 + 1) / 2 <= 65535;
-  if (d->kernel == WK_KERNEL_FUSED && !big)
+  if ((d->kernel == WK_KERNEL_FUSED || d->kernel == WK_KERNEL_TWOPASS) && !big)
     return wk_fail(WK_E_SHAPE, "wk_fit_step: interior/shell kernels need every dimension >= 5");
+  if (d->kernel == WK_KERNEL_TWOPASS) {
+    for (int s = 0; s < n_steps; s++) {
+      FitParams<T> p = make_params<T>(d, par);
+      cudaError_t e = launch_two_pass<T>(p, step0 + s, st);
+      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
+      par ^= 1;
+    }
+    return wk_check_launch("wk_fit_step");
+  }
   if (d->kernel == WK_KERNEL_FUSED || (d->kernel == WK_KERNEL_AUTO && big)) {
     // tile_planes: planes per thread of the column kernel (0 = automatic,
     // -1 = one-thread-per-cell interior kernel)
@@ -188,6 +197,16 @@ template <typename T>
 int run_split(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t st) {
   FitParams<T> p = make_params<T>(d, d->par);
   p.E_out = p.E_in; p.H_out = p.H_in;   // in place
+  const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
+                   (d->Ny - 4 + 1) / 2 <= 65535;
+  if (big && d->kernel != WK_KERNEL_CELL) {
+    for (int s = 0; s < n_steps; s++) {
+      cudaError_t e = launch_two_pass<T>(p, step0 + s, st);
+      if (e != cudaSuccess)
+        return wk_fail(-(int)e, "wk_fit_step_split: %s", cudaGetErrorString(e));
+    }
+    return wk_check_launch("wk_fit_step_split");
+  }
   for (int s = 0; s < n_steps; s++) {
     k_h_split<T><<<blocks_for(p.N), kThreads, 0, st>>>(p, step0 + s);
     k_e_split<T><<<blocks_for(p.N), kThreads, 0, st>>>(p, step0 + s);

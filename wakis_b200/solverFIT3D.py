@@ -152,7 +152,8 @@ class SolverFIT3D(RoutinesMixin):
         return torch.cuda.current_stream(self.device).cuda_stream
 
     _KERNELS = {"auto": _native.WK_KERNEL_AUTO, "cell": _native.WK_KERNEL_CELL,
-                "march": _native.WK_KERNEL_MARCH, "fused": _native.WK_KERNEL_FUSED}
+                "march": _native.WK_KERNEL_MARCH, "fused": _native.WK_KERNEL_FUSED,
+                "twopass": _native.WK_KERNEL_TWOPASS}
 
     def _sync_desc(self):
         d = self._desc
