@@ -47,7 +47,8 @@ VALID = [i for i in range(len(cases.STEP_CASES)) if _valid(i)]
 
 SCHEDULES = {"fused": ("fused", (0, 0)), "fused_cell": ("fused", (0, -1)),
              "fused_kz1": ("fused", (0, 1)), "fused_kz3": ("fused", (0, 3)),
-             "twopass": ("twopass", (0, 0)), "march": ("march", (0, 0)),
+             "twopass": ("twopass", (0, 0)), "twopass1": ("twopass", (0, 1)),
+             "twopass4": ("twopass", (0, 4)), "march": ("march", (0, 0)),
              "march_t1": ("march", (1, 1)), "march_t2": ("march", (2, 3)),
              "cell": ("cell", (0, 0)), "split": None}
 
@@ -202,7 +203,8 @@ def test_cavity_40_wakesolve_matches_oracle():
                                          ("march", (3, 5)), ("march", (7, 1)),
                                          ("march", (16, 24)), ("fused", (0, 0)),
                                          ("fused", (0, -1)), ("fused", (0, 2)),
-                                         ("fused", (0, 5)), ("twopass", (0, 0))])
+                                         ("fused", (0, 5)), ("twopass", (0, 0)),
+                                         ("twopass", (0, 1)), ("twopass", (0, 4))])
 def test_schedules_equal_cell_kernel_with_beam_and_capture(kernel, tile):
     """Plane-marching, interior/shell and per-cell kernels give identical
     fields and Ez history (same arithmetic, different schedules)."""

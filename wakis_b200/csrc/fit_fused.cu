@@ -229,58 +229,108 @@ k_column(FitParams<T> p, long long step, int kz) {
 // it writes).
 constexpr int kPassX = 128, kPassY = 2;
 
-template <typename T>
+// Each thread updates KB consecutive planes of its (i, j) column; all
+// loads of the KB cells are issued before any arithmetic, so a thread keeps
+// KB times more bytes in flight.
+template <typename T, int KB>
 __global__ void __launch_bounds__(kPassX * kPassY) k_h_pass(FitParams<T> p) {
   const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
   const int j = 2 + blockIdx.y * kPassY + threadIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * KB;
   if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const int nk = min(KB, p.Nz - 2 - k0);
   const long long N = p.N, sy = p.Nx, sz = p.NxNy;
-  const long long n = i + j * sy + k * sz;
+  const long long n0 = i + j * sy + k0 * sz;
   const T* ex = p.E_in;
   const T* ey = p.E_in + N;
   const T* ez = p.E_in + 2 * N;
-  const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
-  const T R0 = mul(p.iAx[j + (long long)k * p.Ny], m0[3]);
-  const T R1 = mul(p.iAy[i + (long long)k * p.Nx], m0[4]);
-  const T R2 = mul(p.iAz[i + (long long)j * p.Nx], m0[5]);
-  T hx = p.H_in[n], hy = p.H_in[N + n], hz = p.H_in[2 * N + n];
-  h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[i], p.Ly[j], p.Lz[k], ex[n], ey[n], ez[n],
-         ey[n + 1], ez[n + 1], ex[n + sy], ez[n + sy], ex[n + sz], ey[n + sz], hx, hy, hz);
-  p.H_out[n] = hx;
-  p.H_out[N + n] = hy;
-  p.H_out[2 * N + n] = hz;
+  T e0[KB][3], ep1[KB][2], epy[KB][2], epz[KB][2], h[KB][3];
+  int id[KB];
+#pragma unroll
+  for (int q = 0; q < KB; q++) {
+    if (q < nk) {
+      const long long n = n0 + q * sz;
+      id[q] = load_id(p.mat_id, p.id_bytes, n);
+      e0[q][0] = ex[n]; e0[q][1] = ey[n]; e0[q][2] = ez[n];
+      ep1[q][0] = ey[n + 1]; ep1[q][1] = ez[n + 1];
+      epy[q][0] = ex[n + sy]; epy[q][1] = ez[n + sy];
+      epz[q][0] = ex[n + sz]; epz[q][1] = ey[n + sz];
+      h[q][0] = p.H_in[n]; h[q][1] = p.H_in[N + n]; h[q][2] = p.H_in[2 * N + n];
+    }
+  }
+  const T iAz = p.iAz[i + (long long)j * p.Nx];
+  const T Lx = p.Lx[i], Ly = p.Ly[j];
+#pragma unroll
+  for (int q = 0; q < KB; q++) {
+    if (q < nk) {
+      const int k = k0 + q;
+      const long long n = n0 + q * sz;
+      const T* m0 = p.mat + 9 * id[q];
+      const T R0 = mul(p.iAx[j + (long long)k * p.Ny], m0[3]);
+      const T R1 = mul(p.iAy[i + (long long)k * p.Nx], m0[4]);
+      const T R2 = mul(iAz, m0[5]);
+      h_lean(p.dt, p.h_desc != 0, R0, R1, R2, Lx, Ly, p.Lz[k], e0[q][0], e0[q][1], e0[q][2],
+             ep1[q][0], ep1[q][1], epy[q][0], epy[q][1], epz[q][0], epz[q][1], h[q][0], h[q][1],
+             h[q][2]);
+      p.H_out[n] = h[q][0];
+      p.H_out[N + n] = h[q][1];
+      p.H_out[2 * N + n] = h[q][2];
+    }
+  }
 }
 
-template <typename T>
+template <typename T, int KB>
 __global__ void __launch_bounds__(kPassX * kPassY) k_e_pass(FitParams<T> p, long long step) {
   const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
   const int j = 2 + blockIdx.y * kPassY + threadIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * KB;
   if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const int nk = min(KB, p.Nz - 2 - k0);
   const long long N = p.N, sy = p.Nx, sz = p.NxNy;
-  const long long n = i + j * sy + k * sz;
+  const long long n0 = i + j * sy + k0 * sz;
   const T* hx = p.H_out;
   const T* hy = p.H_out + N;
   const T* hz = p.H_out + 2 * N;
-  const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
-  const T R0 = mul(m0[0], p.itAx[j + (long long)k * p.Ny]);
-  const T R1 = mul(m0[1], p.itAy[i + (long long)k * p.Nx]);
-  const T R2 = mul(m0[2], p.itAz[i + (long long)j * p.Nx]);
-  T curl[3];
-  e_lean(R0, R1, R2, p.tLx[i], p.tLy[j], p.tLz[k], hx[n], hy[n], hz[n], hy[n - 1], hz[n - 1],
-         hx[n - sy], hz[n - sy], hx[n - sz], hy[n - sz], curl[0], curl[1], curl[2]);
-  const T eold[3] = {p.E_in[n], p.E_in[N + n], p.E_in[2 * N + n]};
-  Cell c;
-  c.i = i; c.j = j; c.k = k;
-  if (p.cap_on) capture(p, c, n, step, eold[2]);
+  T h0[KB][3], hm1[KB][2], hmy[KB][2], hmz[KB][2], eold[KB][3];
+  int id[KB];
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const T ieps = m0[d], sigma = m0[6 + d];
-    const T jv = j_in(p, d, c, n, step, eold[d], sigma);
-    const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
-    p.E_out[d * N + n] = enew;
-    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+  for (int q = 0; q < KB; q++) {
+    if (q < nk) {
+      const long long n = n0 + q * sz;
+      id[q] = load_id(p.mat_id, p.id_bytes, n);
+      h0[q][0] = hx[n]; h0[q][1] = hy[n]; h0[q][2] = hz[n];
+      hm1[q][0] = hy[n - 1]; hm1[q][1] = hz[n - 1];
+      hmy[q][0] = hx[n - sy]; hmy[q][1] = hz[n - sy];
+      hmz[q][0] = hx[n - sz]; hmz[q][1] = hy[n - sz];
+      eold[q][0] = p.E_in[n]; eold[q][1] = p.E_in[N + n]; eold[q][2] = p.E_in[2 * N + n];
+    }
+  }
+  const T itAz = p.itAz[i + (long long)j * p.Nx];
+  const T tLx = p.tLx[i], tLy = p.tLy[j];
+#pragma unroll
+  for (int q = 0; q < KB; q++) {
+    if (q < nk) {
+      const int k = k0 + q;
+      const long long n = n0 + q * sz;
+      const T* m0 = p.mat + 9 * id[q];
+      const T R0 = mul(m0[0], p.itAx[j + (long long)k * p.Ny]);
+      const T R1 = mul(m0[1], p.itAy[i + (long long)k * p.Nx]);
+      const T R2 = mul(m0[2], itAz);
+      T curl[3];
+      e_lean(R0, R1, R2, tLx, tLy, p.tLz[k], h0[q][0], h0[q][1], h0[q][2], hm1[q][0],
+             hm1[q][1], hmy[q][0], hmy[q][1], hmz[q][0], hmz[q][1], curl[0], curl[1], curl[2]);
+      Cell c;
+      c.i = i; c.j = j; c.k = k;
+      if (p.cap_on) capture(p, c, n, step, eold[q][2]);
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const T ieps = m0[d], sigma = m0[6 + d];
+        const T jv = j_in(p, d, c, n, step, eold[q][d], sigma);
+        const T enew = add(eold[q][d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
+        p.E_out[d * N + n] = enew;
+        if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+      }
+    }
   }
 }
 
@@ -366,21 +416,35 @@ __global__ void __launch_bounds__(kShellThreads) k_e_shell(FitParams<T> p, long 
   }
 }
 
-template <typename T>
-cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st) {
+template <typename T, int KB>
+void two_pass_kb(const FitParams<T>& p, long long step, cudaStream_t st, unsigned sb,
+                 long long count) {
   dim3 blk(kPassX, kPassY);
-  dim3 grid((p.Nx - 4 + kPassX - 1) / kPassX, (p.Ny - 4 + kPassY - 1) / kPassY, p.Nz - 4);
+  dim3 grid((p.Nx - 4 + kPassX - 1) / kPassX, (p.Ny - 4 + kPassY - 1) / kPassY,
+            (p.Nz - 4 + KB - 1) / KB);
+  k_h_pass<T, KB><<<grid, blk, 0, st>>>(p);
+  k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, count);
+  k_e_pass<T, KB><<<grid, blk, 0, st>>>(p, step);
+  k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, count);
+}
+
+template <typename T>
+cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st, int kb) {
   const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
   const unsigned sb = (unsigned)((count + kShellThreads - 1) / kShellThreads);
-  k_h_pass<T><<<grid, blk, 0, st>>>(p);
-  k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, count);
-  k_e_pass<T><<<grid, blk, 0, st>>>(p, step);
-  k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, count);
+  if (kb >= 4)
+    two_pass_kb<T, 4>(p, step, st, sb, count);
+  else if (kb == 2)
+    two_pass_kb<T, 2>(p, step, st, sb, count);
+  else
+    two_pass_kb<T, 1>(p, step, st, sb, count);
   return cudaGetLastError();
 }
 
-template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long, cudaStream_t);
-template cudaError_t launch_two_pass<float>(const FitParams<float>&, long long, cudaStream_t);
+template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long, cudaStream_t,
+                                             int);
+template cudaError_t launch_two_pass<float>(const FitParams<float>&, long long, cudaStream_t,
+                                            int);
 
 template <typename T>
 cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,

@@ -131,8 +131,9 @@ cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStr
 
 // Launch the two-pass schedule (H pass, then E pass; interior lean kernels
 // and general shell kernels) of one step (fit_fused.cu); needs Nx, Ny, Nz >= 5.
+// kb = planes per thread (1, 2 or 4).
 template <typename T>
-cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st);
+cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st, int kb);
 
 // Launch the plane-marching kernel (defined in fit_march.cu) with TY rows
 // and KC planes per block and `smem` bytes of dynamic shared memory.

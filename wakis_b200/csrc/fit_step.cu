@@ -144,7 +144,7 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   if (d->kernel == WK_KERNEL_TWOPASS) {
     for (int s = 0; s < n_steps; s++) {
       FitParams<T> p = make_params<T>(d, par);
-      cudaError_t e = launch_two_pass<T>(p, step0 + s, st);
+      cudaError_t e = launch_two_pass<T>(p, step0 + s, st, d->tile_planes > 0 ? d->tile_planes : 2);
       if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
       par ^= 1;
     }
@@ -201,7 +201,7 @@ int run_split(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
                    (d->Ny - 4 + 1) / 2 <= 65535;
   if (big && d->kernel != WK_KERNEL_CELL) {
     for (int s = 0; s < n_steps; s++) {
-      cudaError_t e = launch_two_pass<T>(p, step0 + s, st);
+      cudaError_t e = launch_two_pass<T>(p, step0 + s, st, d->tile_planes > 0 ? d->tile_planes : 2);
       if (e != cudaSuccess)
         return wk_fail(-(int)e, "wk_fit_step_split: %s", cudaGetErrorString(e));
     }
