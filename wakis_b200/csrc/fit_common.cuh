@@ -31,6 +31,7 @@ struct FitParams {
   int j_mode, use_cond;
   const void* mat_id; int id_bytes;
   const T* mat;
+  int n_mat;
   const T *Lx, *Ly, *Lz, *tLx, *tLy, *tLz;
   const T *iAx, *iAy, *iAz, *itAx, *itAy, *itAz;
   int pec_face[6], pmc_face[6];

@@ -231,90 +231,121 @@ constexpr int kPassX = 128, kPassY = 2;
 
 // Each thread updates KB consecutive planes of its (i, j) column; all
 // loads of the KB cells are issued before any arithmetic, so a thread keeps
-// KB times more bytes in flight.
+// KB times more bytes in flight.  Neighbour offsets are 32-bit (Nx*Ny < 2^31)
+// from per-thread base pointers, and the material table is staged in shared
+// memory when it is small (mat_smem = its element count, else 0).
+// Resident blocks requested per SM (register cap) for KB planes per thread.
+constexpr int pass_min_blocks(size_t bytes, int kb) {
+  return kb == 1 ? (bytes == 8 ? 5 : 6) : (kb == 2 ? 3 : 2);
+}
+
+template <typename T>
+__device__ __forceinline__ const T* stage_table(const FitParams<T>& p, int mat_smem, T* sm) {
+  if (mat_smem == 0) return p.mat;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  for (int q = tid; q < mat_smem; q += blockDim.x * blockDim.y) sm[q] = p.mat[q];
+  __syncthreads();
+  return sm;
+}
+
 template <typename T, int KB>
-__global__ void __launch_bounds__(kPassX * kPassY) k_h_pass(FitParams<T> p) {
+__global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), KB))
+k_h_pass(FitParams<T> p, int mat_smem) {
+  extern __shared__ __align__(16) unsigned char pass_smem[];
+  const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
   const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
   const int j = 2 + blockIdx.y * kPassY + threadIdx.y;
   const int k0 = 2 + blockIdx.z * KB;
   if (i > p.Nx - 3 || j > p.Ny - 3) return;
   const int nk = min(KB, p.Nz - 2 - k0);
-  const long long N = p.N, sy = p.Nx, sz = p.NxNy;
-  const long long n0 = i + j * sy + k0 * sz;
-  const T* ex = p.E_in;
-  const T* ey = p.E_in + N;
-  const T* ez = p.E_in + 2 * N;
+  const long long N = p.N;
+  const int sy = p.Nx, sz = (int)p.NxNy;
+  const long long n0 = i + (long long)j * sy + (long long)k0 * sz;
+  const T* ex = p.E_in + n0;
+  const T* ey = p.E_in + N + n0;
+  const T* ez = p.E_in + 2 * N + n0;
+  const T* hx = p.H_in + n0;
+  const T* hy = p.H_in + N + n0;
+  const T* hz = p.H_in + 2 * N + n0;
   T e0[KB][3], ep1[KB][2], epy[KB][2], epz[KB][2], h[KB][3];
   int id[KB];
 #pragma unroll
   for (int q = 0; q < KB; q++) {
     if (q < nk) {
-      const long long n = n0 + q * sz;
-      id[q] = load_id(p.mat_id, p.id_bytes, n);
-      e0[q][0] = ex[n]; e0[q][1] = ey[n]; e0[q][2] = ez[n];
-      ep1[q][0] = ey[n + 1]; ep1[q][1] = ez[n + 1];
-      epy[q][0] = ex[n + sy]; epy[q][1] = ez[n + sy];
-      epz[q][0] = ex[n + sz]; epz[q][1] = ey[n + sz];
-      h[q][0] = p.H_in[n]; h[q][1] = p.H_in[N + n]; h[q][2] = p.H_in[2 * N + n];
+      const int o = q * sz;
+      id[q] = load_id(p.mat_id, p.id_bytes, n0 + o);
+      e0[q][0] = ex[o]; e0[q][1] = ey[o]; e0[q][2] = ez[o];
+      ep1[q][0] = ey[o + 1]; ep1[q][1] = ez[o + 1];
+      epy[q][0] = ex[o + sy]; epy[q][1] = ez[o + sy];
+      epz[q][0] = ex[o + sz]; epz[q][1] = ey[o + sz];
+      h[q][0] = hx[o]; h[q][1] = hy[o]; h[q][2] = hz[o];
     }
   }
-  const T iAz = p.iAz[i + (long long)j * p.Nx];
+  const T iAz = p.iAz[i + j * sy];
   const T Lx = p.Lx[i], Ly = p.Ly[j];
+  T* hxo = p.H_out + n0;
+  T* hyo = p.H_out + N + n0;
+  T* hzo = p.H_out + 2 * N + n0;
 #pragma unroll
   for (int q = 0; q < KB; q++) {
     if (q < nk) {
       const int k = k0 + q;
-      const long long n = n0 + q * sz;
-      const T* m0 = p.mat + 9 * id[q];
-      const T R0 = mul(p.iAx[j + (long long)k * p.Ny], m0[3]);
-      const T R1 = mul(p.iAy[i + (long long)k * p.Nx], m0[4]);
+      const int o = q * sz;
+      const T* m0 = mat + 9 * id[q];
+      const T R0 = mul(p.iAx[j + k * p.Ny], m0[3]);
+      const T R1 = mul(p.iAy[i + k * sy], m0[4]);
       const T R2 = mul(iAz, m0[5]);
       h_lean(p.dt, p.h_desc != 0, R0, R1, R2, Lx, Ly, p.Lz[k], e0[q][0], e0[q][1], e0[q][2],
              ep1[q][0], ep1[q][1], epy[q][0], epy[q][1], epz[q][0], epz[q][1], h[q][0], h[q][1],
              h[q][2]);
-      p.H_out[n] = h[q][0];
-      p.H_out[N + n] = h[q][1];
-      p.H_out[2 * N + n] = h[q][2];
+      hxo[o] = h[q][0];
+      hyo[o] = h[q][1];
+      hzo[o] = h[q][2];
     }
   }
 }
 
 template <typename T, int KB>
-__global__ void __launch_bounds__(kPassX * kPassY) k_e_pass(FitParams<T> p, long long step) {
+__global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), KB))
+k_e_pass(FitParams<T> p, long long step, int mat_smem) {
+  extern __shared__ __align__(16) unsigned char pass_smem[];
+  const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
   const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
   const int j = 2 + blockIdx.y * kPassY + threadIdx.y;
   const int k0 = 2 + blockIdx.z * KB;
   if (i > p.Nx - 3 || j > p.Ny - 3) return;
   const int nk = min(KB, p.Nz - 2 - k0);
-  const long long N = p.N, sy = p.Nx, sz = p.NxNy;
-  const long long n0 = i + j * sy + k0 * sz;
-  const T* hx = p.H_out;
-  const T* hy = p.H_out + N;
-  const T* hz = p.H_out + 2 * N;
+  const long long N = p.N;
+  const int sy = p.Nx, sz = (int)p.NxNy;
+  const long long n0 = i + (long long)j * sy + (long long)k0 * sz;
+  const T* hx = p.H_out + n0;
+  const T* hy = p.H_out + N + n0;
+  const T* hz = p.H_out + 2 * N + n0;
+  const T* exi = p.E_in + n0;
   T h0[KB][3], hm1[KB][2], hmy[KB][2], hmz[KB][2], eold[KB][3];
   int id[KB];
 #pragma unroll
   for (int q = 0; q < KB; q++) {
     if (q < nk) {
-      const long long n = n0 + q * sz;
-      id[q] = load_id(p.mat_id, p.id_bytes, n);
-      h0[q][0] = hx[n]; h0[q][1] = hy[n]; h0[q][2] = hz[n];
-      hm1[q][0] = hy[n - 1]; hm1[q][1] = hz[n - 1];
-      hmy[q][0] = hx[n - sy]; hmy[q][1] = hz[n - sy];
-      hmz[q][0] = hx[n - sz]; hmz[q][1] = hy[n - sz];
-      eold[q][0] = p.E_in[n]; eold[q][1] = p.E_in[N + n]; eold[q][2] = p.E_in[2 * N + n];
+      const int o = q * sz;
+      id[q] = load_id(p.mat_id, p.id_bytes, n0 + o);
+      h0[q][0] = hx[o]; h0[q][1] = hy[o]; h0[q][2] = hz[o];
+      hm1[q][0] = hy[o - 1]; hm1[q][1] = hz[o - 1];
+      hmy[q][0] = hx[o - sy]; hmy[q][1] = hz[o - sy];
+      hmz[q][0] = hx[o - sz]; hmz[q][1] = hy[o - sz];
+      eold[q][0] = exi[o]; eold[q][1] = exi[N + o]; eold[q][2] = exi[2 * N + o];
     }
   }
-  const T itAz = p.itAz[i + (long long)j * p.Nx];
+  const T itAz = p.itAz[i + j * sy];
   const T tLx = p.tLx[i], tLy = p.tLy[j];
 #pragma unroll
   for (int q = 0; q < KB; q++) {
     if (q < nk) {
       const int k = k0 + q;
-      const long long n = n0 + q * sz;
-      const T* m0 = p.mat + 9 * id[q];
-      const T R0 = mul(m0[0], p.itAx[j + (long long)k * p.Ny]);
-      const T R1 = mul(m0[1], p.itAy[i + (long long)k * p.Nx]);
+      const long long n = n0 + q * (long long)sz;
+      const T* m0 = mat + 9 * id[q];
+      const T R0 = mul(m0[0], p.itAx[j + k * p.Ny]);
+      const T R1 = mul(m0[1], p.itAy[i + k * sy]);
       const T R2 = mul(m0[2], itAz);
       T curl[3];
       e_lean(R0, R1, R2, tLx, tLy, p.tLz[k], h0[q][0], h0[q][1], h0[q][2], hm1[q][0],
@@ -422,9 +453,11 @@ void two_pass_kb(const FitParams<T>& p, long long step, cudaStream_t st, unsigne
   dim3 blk(kPassX, kPassY);
   dim3 grid((p.Nx - 4 + kPassX - 1) / kPassX, (p.Ny - 4 + kPassY - 1) / kPassY,
             (p.Nz - 4 + KB - 1) / KB);
-  k_h_pass<T, KB><<<grid, blk, 0, st>>>(p);
+  const int mat_smem = p.n_mat * 9 <= 1024 ? p.n_mat * 9 : 0;
+  const size_t smem = (size_t)mat_smem * sizeof(T);
+  k_h_pass<T, KB><<<grid, blk, smem, st>>>(p, mat_smem);
   k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, count);
-  k_e_pass<T, KB><<<grid, blk, 0, st>>>(p, step);
+  k_e_pass<T, KB><<<grid, blk, smem, st>>>(p, step, mat_smem);
   k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, count);
 }
 

@@ -44,6 +44,7 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
   p.j_mode = d->j_mode; p.use_cond = d->use_conductivity;
   p.mat_id = d->mat_id; p.id_bytes = d->id_bytes;
   p.mat = (const T*)d->mat_table;
+  p.n_mat = d->n_mat;
   p.Lx = (const T*)d->Lx; p.Ly = (const T*)d->Ly; p.Lz = (const T*)d->Lz;
   p.tLx = (const T*)d->tLx; p.tLy = (const T*)d->tLy; p.tLz = (const T*)d->tLz;
   p.iAx = (const T*)d->iAx; p.iAy = (const T*)d->iAy; p.iAz = (const T*)d->iAz;
