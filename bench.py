@@ -196,7 +196,7 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "fused", "twopass", "march", "cell", "split"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "slab", "fused", "twopass", "march", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
@@ -265,7 +265,11 @@ def main():
     if ws > 1:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
     ms = float(t_dev.item())
-    per_step = {"twopass": 4, "split": 4, "fused": 2, "auto": 2, "march": 1, "cell": 1}
+    planes = s.tile[1] if s.tile[1] > 0 else max(
+        2, (80 * 1024 * 1024) // (9 * np.dtype(dtype).itemsize * s.Nx * s.Ny))
+    nslab = -(-s.Nz // planes)
+    per_step = {"twopass": 4, "split": 4, "fused": 2, "auto": 2 * nslab, "slab": 2 * nslab,
+                "march": 1, "cell": 1}
     launches = args.steps * per_step[args.kernel]  # step kernels launched
 
     # end to end through the public API: per-step H2D line current, D2H window

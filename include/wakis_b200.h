@@ -127,6 +127,10 @@ typedef struct wk_fit_desc {
 #define WK_KERNEL_TWOPASS 4 /* H pass then E pass, each an interior launch
                               with single-coefficient rows plus a shell
                               launch (WK_E_SHAPE if a dimension is below 5) */
+#define WK_KERNEL_SLAB 5   /* the two passes slab by slab along z
+                              (tile_planes planes per slab, 0 = sized for
+                              L2) so the E pass re-reads the slab from L2
+                              (WK_E_SHAPE if a dimension is below 5)        */
 
 /* ABI version (WK_ABI_VERSION). */
 int wk_version(void);

@@ -479,6 +479,196 @@ template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long
 template cudaError_t launch_two_pass<float>(const FitParams<float>&, long long, cudaStream_t,
                                             int);
 
+// ------------------------------------------------------------- z slabs ----
+// The two passes run slab by slab along z: H pass of planes [ka, kb), then
+// E pass of the same planes, then the next slab.  H(k) needs E_old at k and
+// k+1 and E(k) needs H_new at k and k-1, so this order gives the same result
+// as two whole-grid passes, while the E pass re-reads the slab's E_in and
+// H_out from L2.  One launch per pass per slab: the first blocks are
+// interior tiles (single-coefficient rows), the remaining blocks cover the
+// slab's shell cells (general rows).
+struct SlabInfo {
+  int k_int0, n_int;         // interior planes [k_int0, k_int0 + n_int)
+  int gx, gy;                // interior tiles per plane (x, y)
+  long long nb_int;          // interior blocks
+  int F[4], nF;              // full shell planes in the slab
+  int lo, n_inner, S_in;     // inner shell planes [lo, lo + n_inner), cells per plane
+  long long shell_count;
+};
+
+__device__ __forceinline__ Cell slab_shell_cell(long long idx, int Nx, int Ny,
+                                                const SlabInfo& s) {
+  Cell c;
+  const long long NxNy = (long long)Nx * Ny;
+  if (idx < s.nF * NxNy) {
+    const int f = (int)(idx / NxNy);
+    const long long rem = idx - f * NxNy;
+    c.k = s.F[f];
+    c.j = (int)(rem / Nx);
+    c.i = (int)(rem - (long long)c.j * Nx);
+    return c;
+  }
+  idx -= s.nF * NxNy;
+  const long long pl = idx / s.S_in;
+  int r = (int)(idx - pl * s.S_in);
+  c.k = s.lo + (int)pl;
+  if (r < 4 * Nx) {
+    const int jj = r / Nx;
+    c.i = r - jj * Nx;
+    c.j = jj < 2 ? jj : Ny - 4 + jj;
+    return c;
+  }
+  r -= 4 * Nx;
+  const int ii = r % 4;
+  c.i = ii < 2 ? ii : Nx - 4 + ii;
+  c.j = 2 + r / 4;
+  return c;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), 1))
+k_h_slab(FitParams<T> p, SlabInfo s, int mat_smem) {
+  extern __shared__ __align__(16) unsigned char pass_smem[];
+  const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
+  const long long b = blockIdx.x;
+  const long long N = p.N;
+  if (b < s.nb_int) {
+    const int bx = (int)(b % s.gx);
+    const long long r = b / s.gx;
+    const int by = (int)(r % s.gy);
+    const int bz = (int)(r / s.gy);
+    const int i = 2 + bx * kPassX + threadIdx.x;
+    const int j = 2 + by * kPassY + threadIdx.y;
+    const int k = s.k_int0 + bz;
+    if (i > p.Nx - 3 || j > p.Ny - 3) return;
+    const int sy = p.Nx, sz = (int)p.NxNy;
+    const long long n = i + (long long)j * sy + (long long)k * sz;
+    const T* ex = p.E_in + n;
+    const T* ey = p.E_in + N + n;
+    const T* ez = p.E_in + 2 * N + n;
+    const T* m0 = mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+    T hx = p.H_in[n], hy = p.H_in[N + n], hz = p.H_in[2 * N + n];
+    const T R0 = mul(p.iAx[j + k * p.Ny], m0[3]);
+    const T R1 = mul(p.iAy[i + k * sy], m0[4]);
+    const T R2 = mul(p.iAz[i + j * sy], m0[5]);
+    h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[i], p.Ly[j], p.Lz[k], ex[0], ey[0], ez[0],
+           ey[1], ez[1], ex[sy], ez[sy], ex[sz], ey[sz], hx, hy, hz);
+    p.H_out[n] = hx;
+    p.H_out[N + n] = hy;
+    p.H_out[2 * N + n] = hz;
+  } else {
+    const long long idx = (b - s.nb_int) * (kPassX * kPassY) + threadIdx.x +
+                          threadIdx.y * kPassX;
+    if (idx >= s.shell_count) return;
+    const Cell c = slab_shell_cell(idx, p.Nx, p.Ny, s);
+    const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
+    const int id = load_id(p.mat_id, p.id_bytes, n);
+    T h[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) h[d] = h_row(p, p.E_in, p.H_in[d * N + n], d, c, n, id);
+#pragma unroll
+    for (int d = 0; d < 3; d++) p.H_out[d * N + n] = h[d];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), 1))
+k_e_slab(FitParams<T> p, long long step, SlabInfo s, int mat_smem) {
+  extern __shared__ __align__(16) unsigned char pass_smem[];
+  const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
+  const long long b = blockIdx.x;
+  const long long N = p.N;
+  if (b < s.nb_int) {
+    const int bx = (int)(b % s.gx);
+    const long long r = b / s.gx;
+    const int by = (int)(r % s.gy);
+    const int bz = (int)(r / s.gy);
+    const int i = 2 + bx * kPassX + threadIdx.x;
+    const int j = 2 + by * kPassY + threadIdx.y;
+    const int k = s.k_int0 + bz;
+    if (i > p.Nx - 3 || j > p.Ny - 3) return;
+    const int sy = p.Nx, sz = (int)p.NxNy;
+    const long long n = i + (long long)j * sy + (long long)k * sz;
+    const T* hx = p.H_out + n;
+    const T* hy = p.H_out + N + n;
+    const T* hz = p.H_out + 2 * N + n;
+    const T* m0 = mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+    const T eold[3] = {p.E_in[n], p.E_in[N + n], p.E_in[2 * N + n]};
+    const T R0 = mul(m0[0], p.itAx[j + k * p.Ny]);
+    const T R1 = mul(m0[1], p.itAy[i + k * sy]);
+    const T R2 = mul(m0[2], p.itAz[i + j * sy]);
+    T curl[3];
+    e_lean(R0, R1, R2, p.tLx[i], p.tLy[j], p.tLz[k], hx[0], hy[0], hz[0], hy[-1], hz[-1],
+           hx[-sy], hz[-sy], hx[-sz], hy[-sz], curl[0], curl[1], curl[2]);
+    Cell c;
+    c.i = i; c.j = j; c.k = k;
+    if (p.cap_on) capture(p, c, n, step, eold[2]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const T ieps = m0[d], sigma = m0[6 + d];
+      const T jv = j_in(p, d, c, n, step, eold[d], sigma);
+      const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
+      p.E_out[d * N + n] = enew;
+      if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+    }
+  } else {
+    const long long idx = (b - s.nb_int) * (kPassX * kPassY) + threadIdx.x +
+                          threadIdx.y * kPassX;
+    if (idx >= s.shell_count) return;
+    const Cell c = slab_shell_cell(idx, p.Nx, p.Ny, s);
+    const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
+    const int id = load_id(p.mat_id, p.id_bytes, n);
+    const T* Hn = p.H_out;
+    auto hval = [&](int e, long long m) -> T { return Hn[e * N + m]; };
+    if (p.cap_on) capture(p, c, n, step, p.E_in[2 * N + n]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const T ieps = p.mat[9 * id + d], sigma = p.mat[9 * id + 6 + d];
+      const T eold = p.E_in[d * N + n];
+      const T jv = j_in(p, d, c, n, step, eold, sigma);
+      const T curl = e_curl(p, d, c, n, ieps, hval);
+      const T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
+      p.E_out[d * N + n] = enew;
+      if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+    }
+  }
+}
+
+template <typename T>
+cudaError_t launch_slabs(const FitParams<T>& p, long long step, cudaStream_t st, int planes) {
+  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
+  const int mat_smem = p.n_mat * 9 <= 1024 ? p.n_mat * 9 : 0;
+  const size_t smem = (size_t)mat_smem * sizeof(T);
+  const int threads = kPassX * kPassY;
+  for (int ka = 0; ka < Nz; ka += planes) {
+    const int kb = min(ka + planes, Nz);
+    SlabInfo s;
+    s.k_int0 = max(ka, 2);
+    s.n_int = max(0, min(kb, Nz - 2) - s.k_int0);
+    s.gx = (Nx - 4 + kPassX - 1) / kPassX;
+    s.gy = (Ny - 4 + kPassY - 1) / kPassY;
+    s.nb_int = (long long)s.gx * s.gy * s.n_int;
+    s.nF = 0;
+    const int full[4] = {0, 1, Nz - 2, Nz - 1};
+    for (int f = 0; f < 4; f++)
+      if (full[f] >= ka && full[f] < kb) s.F[s.nF++] = full[f];
+    s.lo = max(ka, 2);
+    s.n_inner = max(0, min(kb, Nz - 2) - s.lo);
+    s.S_in = 4 * Nx + 4 * (Ny - 4);
+    s.shell_count = (long long)s.nF * Nx * Ny + (long long)s.n_inner * s.S_in;
+    const long long blocks = s.nb_int + (s.shell_count + threads - 1) / threads;
+    if (blocks == 0) continue;
+    dim3 blk(kPassX, kPassY);
+    k_h_slab<T><<<(unsigned)blocks, blk, smem, st>>>(p, s, mat_smem);
+    k_e_slab<T><<<(unsigned)blocks, blk, smem, st>>>(p, step, s, mat_smem);
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_slabs<double>(const FitParams<double>&, long long, cudaStream_t,
+                                          int);
+template cudaError_t launch_slabs<float>(const FitParams<float>&, long long, cudaStream_t, int);
+
 template <typename T>
 cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,
                                   int kz) {

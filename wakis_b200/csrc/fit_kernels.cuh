@@ -136,6 +136,11 @@ cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStr
 template <typename T>
 cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st, int kb);
 
+// Launch the z-slab two-pass schedule of one step (fit_fused.cu): for each
+// slab of `planes` planes, an H launch then an E launch; needs Nx, Ny, Nz >= 5.
+template <typename T>
+cudaError_t launch_slabs(const FitParams<T>& p, long long step, cudaStream_t st, int planes);
+
 // Launch the plane-marching kernel (defined in fit_march.cu) with TY rows
 // and KC planes per block and `smem` bytes of dynamic shared memory.
 template <typename T>

@@ -139,6 +139,23 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   bool march = false;
   const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
                    (d->Ny - 4 + 1) / 2 <= 65535;
+  if (d->kernel == WK_KERNEL_SLAB || (d->kernel == WK_KERNEL_AUTO && big)) {
+    if (!big) return wk_fail(WK_E_SHAPE, "wk_fit_step: slab kernels need every dimension >= 5");
+    int planes = d->tile_planes;
+    if (planes <= 0) {
+      // E_in, H_in and H_out of a slab (3 fields) within ~80 MB of L2
+      const long long per_plane = 9LL * sizeof(T) * d->Nx * d->Ny;
+      planes = (int)(80LL * 1024 * 1024 / per_plane);
+      if (planes < 2) planes = 2;
+    }
+    for (int s = 0; s < n_steps; s++) {
+      FitParams<T> p = make_params<T>(d, par);
+      cudaError_t e = launch_slabs<T>(p, step0 + s, st, planes);
+      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
+      par ^= 1;
+    }
+    return wk_check_launch("wk_fit_step");
+  }
   if ((d->kernel == WK_KERNEL_FUSED || d->kernel == WK_KERNEL_TWOPASS) && !big)
     return wk_fail(WK_E_SHAPE, "wk_fit_step: interior/shell kernels need every dimension >= 5");
   if (d->kernel == WK_KERNEL_TWOPASS) {
@@ -150,7 +167,7 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
     }
     return wk_check_launch("wk_fit_step");
   }
-  if (d->kernel == WK_KERNEL_FUSED || (d->kernel == WK_KERNEL_AUTO && big)) {
+  if (d->kernel == WK_KERNEL_FUSED) {
     // tile_planes: planes per thread of the column kernel (0 = automatic,
     // -1 = one-thread-per-cell interior kernel)
     int kz = d->tile_planes;
