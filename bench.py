@@ -268,7 +268,7 @@ def main():
     planes = s.tile[1] if s.tile[1] > 0 else max(
         2, (80 * 1024 * 1024) // (9 * np.dtype(dtype).itemsize * s.Nx * s.Ny))
     nslab = -(-s.Nz // planes)
-    per_step = {"twopass": 4, "split": 4, "fused": 2, "auto": 2 * nslab, "slab": 2 * nslab,
+    per_step = {"twopass": 4, "split": 4, "fused": 2, "auto": 4, "slab": 2 * nslab,
                 "march": 1, "cell": 1}
     launches = args.steps * per_step[args.kernel]  # step kernels launched
 

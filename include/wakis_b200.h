@@ -114,7 +114,7 @@ typedef struct wk_fit_desc {
   int tile_rows, tile_planes;
 } wk_fit_desc;
 
-#define WK_KERNEL_AUTO 0   /* WK_KERNEL_FUSED when Nx, Ny, Nz >= 5, else
+#define WK_KERNEL_AUTO 0   /* WK_KERNEL_TWOPASS when Nx, Ny, Nz >= 5, else
                               WK_KERNEL_CELL                                */
 #define WK_KERNEL_CELL 1   /* one thread per cell, general row code, H of
                               the backward neighbours recomputed            */
@@ -126,7 +126,9 @@ typedef struct wk_fit_desc {
                               (WK_E_SHAPE if a dimension is below 5)        */
 #define WK_KERNEL_TWOPASS 4 /* H pass then E pass, each an interior launch
                               with single-coefficient rows plus a shell
-                              launch (WK_E_SHAPE if a dimension is below 5) */
+                              launch; tile_planes = planes per thread (1, 2
+                              or 4; 0 = 1 for FP64, 2 for FP32)
+                              (WK_E_SHAPE if a dimension is below 5)        */
 #define WK_KERNEL_SLAB 5   /* the two passes slab by slab along z
                               (tile_planes planes per slab, 0 = sized for
                               L2) so the E pass re-reads the slab from L2
