@@ -37,7 +37,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_CELL = {"float64": 96, "float32": 48}
+BYTES_PER_CELL = {"float64": 96, "float32": 48, "fp32c": 48}
 METRIC = "Gcell-steps/s"
 
 
@@ -194,7 +194,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="lossy_256")
-    ap.add_argument("--dtype", default="float64", choices=["float64", "float32"])
+    ap.add_argument("--dtype", default="float64", choices=["float64", "float32", "fp32c"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "slab", "fused", "twopass", "march", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
@@ -222,9 +222,10 @@ def main():
     from wakis_b200 import workloads
     from wakis_b200.sources import Beam
     sp = workloads.spec(args.workload)
-    dtype = np.dtype(args.dtype).type
+    dtype = np.float64 if args.dtype == "fp32c" else np.dtype(args.dtype).type
     shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else None
-    g, w, s = workloads.build_b200(args.workload, dtype=dtype, shape=shape)
+    g, w, s = workloads.build_b200(args.workload, dtype=dtype, shape=shape,
+                                   precision="fp32c" if args.dtype == "fp32c" else None)
     N = s.N
     split = args.kernel == "split"
     s.kernel = "auto" if split else args.kernel
@@ -234,7 +235,7 @@ def main():
     ixt = int(np.abs(s.x - w.xtest).argmin())
     iyt = int(np.abs(s.y - w.ytest).argmin())
     total = args.warmup + args.steps
-    hist = torch.zeros((9, s.Nz, total), dtype=s._E[0].dtype, device=dev)
+    hist = torch.zeros((9, s.Nz, total), dtype=s._cap_dtype, device=dev)
     cap = (hist, ixt - 1, iyt - 1, 3, 3)
 
     def barrier():
@@ -275,9 +276,10 @@ def main():
     # end to end through the public API: per-step H2D line current, D2H window
     prof = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
     lines = np.stack([(prof.q * prof.v * prof.profile(s, n * s.dt) / s.dx[bp[0]] / s.dy[bp[1]])
-                      for n in range(total, total + args.steps)]).astype(dtype)
+                      for n in range(total, total + args.steps)])
+    lines = lines.astype(np.float64 if args.dtype == "fp32c" else dtype)
     jz = torch.from_numpy(lines).pin_memory()
-    ez = torch.empty((args.steps, 9, s.Nz), dtype=s._E[0].dtype).pin_memory()
+    ez = torch.empty((args.steps, 9, s.Nz), dtype=s._cap_dtype).pin_memory()
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -299,10 +301,12 @@ def main():
             "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.dtype == "float64" else "f32", "data": "synthetic",
+            "dtype": {"float64": "f64", "float32": "f32", "fp32c": "f32+i8 comp (f64 coef)"}[
+                args.dtype], "data": "synthetic",
             "config": {"workload": args.workload, "cells": N, "grid": [s.Nx, s.Ny, s.Nz],
                        "parallelism": f"replicas{ws}" if ws > 1 else "single",
-                       "l2": "state 4x%.0f MB > L2, no flush" % (3 * N * np.dtype(dtype).itemsize / 1e6),
+                       "l2": "state %.0f MB > L2, no flush" % (
+                           4 * 3 * N * s._E[0].element_size() / 1e6),
                        "step": "fused beam + Ez 3x3 capture + H and E half-steps",
                        "kernel": args.kernel, "tile": args.tile},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

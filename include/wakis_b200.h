@@ -34,6 +34,8 @@ extern "C" {
 
 #define WK_F64 0
 #define WK_F32 1
+#define WK_F32C 2   /* FP32 state with int8 compensation words (Ec, Hc);
+                       coefficient tables FP64; Ez capture FP64          */
 
 /* J source used by the E half-step (upstream computes E += dt*(B*H - ieps*J)
  * with J the stored current, solverFIT3D.py:492-503). */
@@ -45,7 +47,8 @@ extern "C" {
 
 /*
  * Geometry, coefficients and state of one FIT grid.  Field-type arrays
- * (E, H, J, metrics, material table) hold `dtype` elements.
+ * (E, H, J, metrics, material table) hold `dtype` elements; with WK_F32C
+ * the state (E, H, J) is float and the metrics and material table double.
  *
  * Metric tables (values as upstream's diagonal matrices hold them after the
  * boundary folding of wakis/boundaries.py:35-181, cast to dtype):
@@ -112,6 +115,11 @@ typedef struct wk_fit_desc {
    * planes per block of the plane-marching kernel.                         */
   int kernel;
   int tile_rows, tile_planes;
+  /* WK_F32C only: per-component compensation of E and H (int8, 3N each,
+   * ping-pong like E and H).  The compensation c of a float value v is
+   * q * 2^(e-30), e the binary exponent of v; v + c is the state.          */
+  void* Ec[2];
+  void* Hc[2];
 } wk_fit_desc;
 
 #define WK_KERNEL_AUTO 0   /* WK_KERNEL_TWOPASS when Nx, Ny, Nz >= 5, else

@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libwakis_b200.so")
 
-WK_F64, WK_F32 = 0, 1
+WK_F64, WK_F32, WK_F32C = 0, 1, 2
 WK_J_ZERO, WK_J_SIGMA_E, WK_J_ARRAY = 0, 1, 2
 WK_KERNEL_AUTO, WK_KERNEL_CELL, WK_KERNEL_MARCH, WK_KERNEL_FUSED, WK_KERNEL_TWOPASS = 0, 1, 2, 3, 4
 WK_KERNEL_SLAB = 5
@@ -41,6 +41,7 @@ class FitDesc(ctypes.Structure):
         ("cap_on", _i), ("cap_i0", _i), ("cap_j0", _i), ("cap_ni", _i), ("cap_nj", _i),
         ("cap_nt", _ll), ("cap_step0", _ll), ("cap", _vp), ("status", _vp),
         ("kernel", _i), ("tile_rows", _i), ("tile_planes", _i),
+        ("Ec", _vp * 2), ("Hc", _vp * 2),
     ]
 
 

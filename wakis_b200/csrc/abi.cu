@@ -36,11 +36,12 @@ int wk_validate_fit(const wk_fit_desc* d, const char* where) {
                    d->Nx, d->Ny, d->Nz);
   if ((long long)d->Nx * d->Ny * d->Nz > (1LL << 40))
     return wk_fail(WK_E_SHAPE, "%s: grid too large", where);
-  if (d->dtype != WK_F64 && d->dtype != WK_F32)
+  if (d->dtype != WK_F64 && d->dtype != WK_F32 && d->dtype != WK_F32C)
     return wk_fail(WK_E_DTYPE, "%s: dtype %d", where, d->dtype);
   if (d->id_bytes != 1 && d->id_bytes != 2 && d->id_bytes != 4)
     return wk_fail(WK_E_DTYPE, "%s: id_bytes %d", where, d->id_bytes);
-  int es = d->dtype == WK_F64 ? 8 : 4;
+  const int es = d->dtype == WK_F64 ? 8 : 4;          // state elements
+  const int ts = d->dtype == WK_F32 ? 4 : 8;          // table elements
   const void* req[] = {d->E[0], d->E[1], d->H[0], d->H[1], d->mat_id, d->mat_table,
                        d->Lx, d->Ly, d->Lz, d->tLx, d->tLy, d->tLz,
                        d->iAx, d->iAy, d->iAz, d->itAx, d->itAy, d->itAz};
@@ -49,7 +50,7 @@ int wk_validate_fit(const wk_fit_desc* d, const char* where) {
                          "iAx", "iAy", "iAz", "itAx", "itAy", "itAz"};
   for (int i = 0; i < 18; i++) {
     if (!req[i]) return wk_fail(WK_E_NULL, "%s: %s is NULL", where, names[i]);
-    int a = (i == 4) ? d->id_bytes : es;
+    int a = (i == 4) ? d->id_bytes : (i < 4 ? es : ts);
     if (!aligned(req[i], a)) return wk_fail(WK_E_ALIGN, "%s: %s misaligned", where, names[i]);
   }
   if (d->par != 0 && d->par != 1) return wk_fail(WK_E_MODE, "%s: par %d", where, d->par);
@@ -69,7 +70,7 @@ int wk_validate_fit(const wk_fit_desc* d, const char* where) {
       return wk_fail(WK_E_RANGE, "%s: line source (%d,%d) off grid", where, d->ixs, d->iys);
   }
   if (d->cap_on) {
-    if (!d->cap || !aligned(d->cap, es)) return wk_fail(WK_E_NULL, "%s: cap buffer", where);
+    if (!d->cap || !aligned(d->cap, ts)) return wk_fail(WK_E_NULL, "%s: cap buffer", where);
     if (d->cap_i0 < 0 || d->cap_j0 < 0 || d->cap_ni < 1 || d->cap_nj < 1 ||
         d->cap_i0 + d->cap_ni > d->Nx || d->cap_j0 + d->cap_nj > d->Ny || d->cap_nt < 1)
       return wk_fail(WK_E_RANGE, "%s: capture window off grid", where);

@@ -274,26 +274,37 @@ __device__ __forceinline__ bool lean_e(int i, int j, int k, int Nx, int Ny, int 
 // ez(c+x) with Lx, Lz; z reads ex(c), ex(c+y), ey(c), ey(c+x) with Lx, Ly.
 // R = iA*imu of the row.  Terms t0..t3 in column order, signs + - - +
 // (x, z) and - + + - (y).
+// Row sums S (H_new = H_old - S) from the two row coefficients a, b.
+template <typename T>
+__device__ __forceinline__ T hsum_x(bool desc, T a, T b, T ey0, T ey3, T ez0, T ez2) {
+  const T t0 = mul(a, ey0), t1 = mul(a, ey3), t2 = mul(b, ez0), t3 = mul(b, ez2);
+  return desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3);
+}
+template <typename T>
+__device__ __forceinline__ T hsum_y(bool desc, T a, T b, T ex0, T ex3, T ez0, T ez1) {
+  const T t0 = mul(a, ex0), t1 = mul(a, ex3), t2 = mul(b, ez0), t3 = mul(b, ez1);
+  return desc ? sub(add(sub(t2, t3), t1), t0) : sub(add(sub(t1, t0), t2), t3);
+}
+template <typename T>
+__device__ __forceinline__ T hsum_z(bool desc, T a, T b, T ex0, T ex2, T ey0, T ey1) {
+  const T t0 = mul(a, ex0), t1 = mul(a, ex2), t2 = mul(b, ey0), t3 = mul(b, ey1);
+  return desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3);
+}
+
 template <typename T>
 __device__ __forceinline__ T h_lean_x(T dt, bool desc, T R, T Ly, T Lz, T ey0, T ey3, T ez0,
                                       T ez2, T hold) {
-  const T a = mul(dt, mul(R, Ly)), b = mul(dt, mul(R, Lz));
-  const T t0 = mul(a, ey0), t1 = mul(a, ey3), t2 = mul(b, ez0), t3 = mul(b, ez2);
-  return sub(hold, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
+  return sub(hold, hsum_x(desc, mul(dt, mul(R, Ly)), mul(dt, mul(R, Lz)), ey0, ey3, ez0, ez2));
 }
 template <typename T>
 __device__ __forceinline__ T h_lean_y(T dt, bool desc, T R, T Lx, T Lz, T ex0, T ex3, T ez0,
                                       T ez1, T hold) {
-  const T a = mul(dt, mul(R, Lx)), b = mul(dt, mul(R, Lz));
-  const T t0 = mul(a, ex0), t1 = mul(a, ex3), t2 = mul(b, ez0), t3 = mul(b, ez1);
-  return sub(hold, desc ? sub(add(sub(t2, t3), t1), t0) : sub(add(sub(t1, t0), t2), t3));
+  return sub(hold, hsum_y(desc, mul(dt, mul(R, Lx)), mul(dt, mul(R, Lz)), ex0, ex3, ez0, ez1));
 }
 template <typename T>
 __device__ __forceinline__ T h_lean_z(T dt, bool desc, T R, T Lx, T Ly, T ex0, T ex2, T ey0,
                                       T ey1, T hold) {
-  const T a = mul(dt, mul(R, Lx)), b = mul(dt, mul(R, Ly));
-  const T t0 = mul(a, ex0), t1 = mul(a, ex2), t2 = mul(b, ey0), t3 = mul(b, ey1);
-  return sub(hold, desc ? add(sub(sub(t3, t2), t1), t0) : add(sub(sub(t0, t1), t2), t3));
+  return sub(hold, hsum_z(desc, mul(dt, mul(R, Lx)), mul(dt, mul(R, Ly)), ex0, ex2, ey0, ey1));
 }
 
 // All three rows of one interior cell.  E values: *0 at n, y1/z1 at n+1,
@@ -305,6 +316,21 @@ __device__ __forceinline__ void h_lean(T dt, bool desc, T R0, T R1, T R2, T Lx, 
   hx = h_lean_x(dt, desc, R0, Ly, Lz, ey0, ey3, ez0, ez2, hx);
   hy = h_lean_y(dt, desc, R1, Lx, Lz, ex0, ex3, ez0, ez1, hy);
   hz = h_lean_z(dt, desc, R2, Lx, Ly, ex0, ex2, ey0, ey1, hz);
+}
+
+// Curl of one E row from its two coefficients c1, c2 (signs per component
+// as in e_lean below).
+template <typename T>
+__device__ __forceinline__ T ecurl_x(T c1, T c2, T hy0, T hz2, T hy3, T hz0) {
+  return add(sub(sub(mul(c1, hy3), mul(c1, hy0)), mul(c2, hz2)), mul(c2, hz0));
+}
+template <typename T>
+__device__ __forceinline__ T ecurl_y(T c1, T c2, T hx0, T hz1, T hx3, T hz0) {
+  return sub(add(sub(mul(c1, hx0), mul(c1, hx3)), mul(c2, hz1)), mul(c2, hz0));
+}
+template <typename T>
+__device__ __forceinline__ T ecurl_z(T c1, T c2, T hx0, T hy1, T hx2, T hy0) {
+  return add(sub(sub(mul(c1, hx2), mul(c1, hx0)), mul(c2, hy1)), mul(c2, hy0));
 }
 
 // Curl parts of the three E rows.  H values: *0 at n, y1/z1 at n-1,

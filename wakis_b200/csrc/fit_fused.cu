@@ -365,40 +365,6 @@ k_e_pass(FitParams<T> p, long long step, int mat_smem) {
   }
 }
 
-// Cell of the idx-th shell cell: planes k in {0,1,Nz-2,Nz-1}, then rows
-// j in {0,1,Ny-2,Ny-1} of the inner planes, then columns i in
-// {0,1,Nx-2,Nx-1} of the inner rows (needs Nx, Ny, Nz >= 5).
-__device__ __forceinline__ Cell shell_cell(long long idx, int Nx, int Ny, int Nz) {
-  Cell c;
-  const long long NxNy = (long long)Nx * Ny;
-  const long long A = 4 * NxNy;
-  if (idx < A) {
-    const int kk = (int)(idx / NxNy);
-    const long long rem = idx - kk * NxNy;
-    c.k = kk < 2 ? kk : Nz - 4 + kk;
-    c.j = (int)(rem / Nx);
-    c.i = (int)(rem - (long long)c.j * Nx);
-    return c;
-  }
-  idx -= A;
-  const long long B = 4LL * Nx * (Nz - 4);
-  if (idx < B) {
-    const long long t = idx / Nx;
-    c.i = (int)(idx - t * Nx);
-    const int jj = (int)(t % 4);
-    c.j = jj < 2 ? jj : Ny - 4 + jj;
-    c.k = 2 + (int)(t / 4);
-    return c;
-  }
-  idx -= B;
-  const int ii = (int)(idx % 4);
-  c.i = ii < 2 ? ii : Nx - 4 + ii;
-  const long long t = idx / 4;
-  c.j = 2 + (int)(t % (Ny - 4));
-  c.k = 2 + (int)(t / (Ny - 4));
-  return c;
-}
-
 template <typename T>
 __global__ void __launch_bounds__(kShellThreads) k_shell(FitParams<T> p, long long step,
                                                           long long count) {

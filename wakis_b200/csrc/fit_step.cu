@@ -239,6 +239,7 @@ extern "C" int wk_zero_ghosts(const wk_fit_desc* d, void* stream) {
   int rc = wk_validate_fit(d, "wk_zero_ghosts");
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  if (d->dtype == WK_F32C) return wk_comp_zero_ghosts(d, st);
   long long N = (long long)d->Nx * d->Ny * d->Nz;
   if (d->dtype == WK_F64)
     k_zero_ghosts<double><<<blocks_for(N), kThreads, 0, st>>>(make_params<double>(d, d->par));
@@ -270,6 +271,7 @@ extern "C" int wk_fit_step(const wk_fit_desc* d, int n_steps, long long step0, v
   if (d->E[0] == d->E[1] || d->H[0] == d->H[1])
     return wk_fail(WK_E_MODE, "wk_fit_step: ping-pong buffers must be distinct");
   cudaStream_t st = (cudaStream_t)stream;
+  if (d->dtype == WK_F32C) return wk_comp_step(d, n_steps, step0, st);
   return d->dtype == WK_F64 ? run_fused<double>(d, n_steps, step0, st)
                             : run_fused<float>(d, n_steps, step0, st);
 }
@@ -281,6 +283,8 @@ extern "C" int wk_fit_step_split(const wk_fit_desc* d, int n_steps, long long st
   rc = check_steps(d, n_steps, step0, "wk_fit_step_split");
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  if (d->dtype == WK_F32C)
+    return wk_fail(WK_E_DTYPE, "wk_fit_step_split: WK_F32C runs through wk_fit_step");
   return d->dtype == WK_F64 ? run_split<double>(d, n_steps, step0, st)
                             : run_split<float>(d, n_steps, step0, st);
 }
@@ -290,6 +294,7 @@ extern "C" int wk_sigma_e(const wk_fit_desc* d, void* J, void* stream) {
   if (rc) return rc;
   if (!J) return wk_fail(WK_E_NULL, "wk_sigma_e: J is NULL");
   cudaStream_t st = (cudaStream_t)stream;
+  if (d->dtype == WK_F32C) return wk_comp_sigma_e(d, J, st);
   long long N = (long long)d->Nx * d->Ny * d->Nz;
   if (d->dtype == WK_F64)
     k_sigma_e<double><<<blocks_for(N), kThreads, 0, st>>>(make_params<double>(d, d->par), (double*)J);

@@ -50,7 +50,7 @@ class RoutinesMixin:
 
         beam = Beam(q=w.q, sigmaz=w.sigmaz, beta=w.beta, xsource=w.xsource, ysource=w.ysource)
         bp = beam.params(self)
-        hist = torch.zeros((ni * nj, self.Nz, max(Nt, 1)), dtype=self._E[0].dtype,
+        hist = torch.zeros((ni * nj, self.Nz, max(Nt, 1)), dtype=self._cap_dtype,
                            device=self.device)
         cap = (hist, i0, j0, ni, nj)
 

@@ -50,7 +50,11 @@ class SolverFIT3D(RoutinesMixin):
                  bc_high=("Periodic", "Periodic", "Periodic"),
                  use_stl=False, use_conductors=False, use_gpu=True, use_mpi=False,
                  use_sibc=True, fmax=1e9, dtype=np.float64, n_pml=10, bg=(1.0, 1.0),
-                 verbose=1, device=None, backend="b200"):
+                 verbose=1, device=None, backend="b200", precision=None):
+        """``precision="fp32c"`` keeps E and H as FP32 values plus int8
+        compensation words (Kahan-style updates) while the coefficients, the
+        time step, the Ez history and the wake integration stay FP64; it
+        requires dtype=np.float64 and every grid dimension >= 5."""
         if backend != "b200":
             raise ValueError(f"backend {backend!r}: this package only provides 'b200'")
         if use_mpi:
@@ -78,6 +82,15 @@ class SolverFIT3D(RoutinesMixin):
         if wake is not None and fmax == 1e9:
             self.fmax = wake.fmax
         self.dtype = np.dtype(dtype).type
+        if precision not in (None, "fp32c"):
+            raise ValueError(f"precision {precision!r}: None or 'fp32c'")
+        self.precision = precision
+        if precision == "fp32c":
+            if self.dtype != np.float64:
+                raise ValueError("precision='fp32c' needs dtype=np.float64 (FP64 coefficients)")
+            if min(grid.Nx, grid.Ny, grid.Nz) < 5:
+                raise ValueError("precision='fp32c' needs every grid dimension >= 5")
+        self.state_dtype = np.float32 if precision == "fp32c" else self.dtype
         self.bc_low, self.bc_high = list(bc_low), list(bc_high)
         self.n_pml = n_pml
         self.cfln = cfln
@@ -104,12 +117,17 @@ class SolverFIT3D(RoutinesMixin):
     # ---------------------------------------------------------- device state
     def _upload(self):
         c, dev = self._coef, self.device
-        td = torch_dtype(self.dtype)
+        td = torch_dtype(self.state_dtype)
         N3 = 3 * self.N
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
         self._E = [torch.zeros(N3, dtype=td, device=dev) for _ in range(2)]
         self._H = [torch.zeros(N3, dtype=td, device=dev) for _ in range(2)]
         self._J = torch.zeros(N3, dtype=td, device=dev)
+        comp = self.precision == "fp32c"
+        self._cap_dtype = torch.float64 if comp else td
+        if comp:
+            self._Ec = [torch.zeros(N3, dtype=torch.int8, device=dev) for _ in range(2)]
+            self._Hc = [torch.zeros(N3, dtype=torch.int8, device=dev) for _ in range(2)]
         self._par = 0
         self._j_state = _J_ZERO
         self._j_line = None          # (values tensor) of the last fused beam step
@@ -120,14 +138,19 @@ class SolverFIT3D(RoutinesMixin):
                           "itAx", "itAy", "itAz")}
         self._zc = torch.as_tensor(self.z, dtype=torch.float64, device=dev)
         self._status = torch.zeros(1, dtype=torch.int32, device=dev)
-        self.E = StateField(self, self._E, self.Nx, self.Ny, self.Nz, self.dtype)
-        self.H = StateField(self, self._H, self.Nx, self.Ny, self.Nz, self.dtype)
-        self.J = _CurrentField(self, self._J, self.Nx, self.Ny, self.Nz, self.dtype)
+        sd = self.state_dtype
+        self.E = StateField(self, self._E, self.Nx, self.Ny, self.Nz, sd)
+        self.H = StateField(self, self._H, self.Nx, self.Ny, self.Nz, sd)
+        self.J = _CurrentField(self, self._J, self.Nx, self.Ny, self.Nz, sd)
         self._dense = None
 
         d = _native.FitDesc()
         d.Nx, d.Ny, d.Nz = self.Nx, self.Ny, self.Nz
-        d.dtype = _native.WK_F64 if self.dtype == np.float64 else _native.WK_F32
+        d.dtype = (_native.WK_F32C if comp else
+                   (_native.WK_F64 if self.dtype == np.float64 else _native.WK_F32))
+        if comp:
+            d.Ec[0], d.Ec[1] = self._Ec[0].data_ptr(), self._Ec[1].data_ptr()
+            d.Hc[0], d.Hc[1] = self._Hc[0].data_ptr(), self._Hc[1].data_ptr()
         d.E[0], d.E[1] = self._E[0].data_ptr(), self._E[1].data_ptr()
         d.H[0], d.H[1] = self._H[0].data_ptr(), self._H[1].data_ptr()
         d.J = self._J.data_ptr()
@@ -169,9 +192,17 @@ class SolverFIT3D(RoutinesMixin):
     # -------------------------------------------------------------- J state
     def _field_written(self, fld):
         """E is about to change between steps: upstream's stored J = sigma*E
-        must keep the old E, so materialise it first."""
+        must keep the old E, so materialise it first.  With precision
+        'fp32c' the compensation words of a written field are reset."""
         if fld is self.E and self._j_state == _J_SIGMA_E:
+            if self.precision == "fp32c":
+                raise RuntimeError("precision='fp32c': E cannot be written between "
+                                   "conductive steps (J = sigma*E is kept implicit)")
             self._materialize_J()
+        if self.precision == "fp32c":
+            bufs = self._Ec if fld is self.E else (self._Hc if fld is self.H else None)
+            if bufs is not None:
+                bufs[self._par].zero_()
 
     def _materialize_J(self):
         if self._j_state == _J_ARRAY:
@@ -210,6 +241,9 @@ class SolverFIT3D(RoutinesMixin):
         self._launch(n_steps, step0, beam, capture, split, line)
 
     def _launch(self, n_steps, step0, beam, capture, split, line):
+        if self.precision == "fp32c" and self._j_state == _J_ARRAY:
+            raise RuntimeError("precision='fp32c' does not take a stored J array; "
+                               "use the fused beam / line source")
         d = self._sync_desc()
         if beam is not None:
             d.beam_on = 1
@@ -281,7 +315,7 @@ class SolverFIT3D(RoutinesMixin):
         ixt = int(np.abs(self.x - xtest).argmin())
         iyt = int(np.abs(self.y - ytest).argmin())
         if getattr(self, "_io_bufs", None) is None or self._io_bufs[0].shape[0] != nz:
-            td = self._E[0].dtype
+            td = self._cap_dtype
             self._io_bufs = (torch.empty(nz, dtype=td, device=self.device),
                              torch.empty((9, nz, 1), dtype=td, device=self.device))
         lbuf, cbuf = self._io_bufs

@@ -47,7 +47,7 @@ def cavity_mask(x, y, z):
     return geometry.cell_mask(cavity_shape(), x, y, z)
 
 
-def build_b200(name, dtype=np.float64, shape=None):
+def build_b200(name, dtype=np.float64, shape=None, precision=None):
     """(grid, wake, solver) of a workload on the device."""
     from .gridFIT3D import GridFIT3D
     from .solverFIT3D import SolverFIT3D
@@ -58,5 +58,5 @@ def build_b200(name, dtype=np.float64, shape=None):
     g.add_solid("cavity", cavity_mask(g.x, g.y, g.z), "vacuum")
     w = WakeSolver(save=False, verbose=0, **sp["wake"])
     s = SolverFIT3D(g, w, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
-                    dtype=dtype, n_pml=sp["n_pml"], verbose=0)
+                    dtype=dtype, n_pml=sp["n_pml"], verbose=0, precision=precision)
     return g, w, s
