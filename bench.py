@@ -196,7 +196,7 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32", "fp32c"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "slab", "fused", "twopass", "march", "cell", "split"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "slab", "fused", "twopass", "march", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
@@ -269,7 +269,7 @@ def main():
     planes = s.tile[1] if s.tile[1] > 0 else max(
         2, (80 * 1024 * 1024) // (9 * np.dtype(dtype).itemsize * s.Nx * s.Ny))
     nslab = -(-s.Nz // planes)
-    per_step = {"twopass": 4, "split": 4, "fused": 2, "auto": 4, "slab": 2 * nslab,
+    per_step = {"twopass": 4, "split": 4, "fused": 2, "auto": 4, "tma": 2, "slab": 2 * nslab,
                 "march": 1, "cell": 1}
     launches = args.steps * per_step[args.kernel]  # step kernels launched
 

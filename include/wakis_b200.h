@@ -137,6 +137,13 @@ typedef struct wk_fit_desc {
                               launch; tile_planes = planes per thread (1, 2
                               or 4; 0 = 1 for FP64, 2 for FP32)
                               (WK_E_SHAPE if a dimension is below 5)        */
+#define WK_KERNEL_TMA 6    /* fused step with TMA-loaded plane tiles in a
+                              shared-memory ring (interior) + shell launch;
+                              needs 16-byte row pitch (Nx*elem % 16 == 0),
+                              N*elem % 16 == 0 and every dimension >= 5;
+                              tile_planes = planes per block (0 = auto).
+                              A load that does not arrive within a bounded
+                              wait sets *status = 1 and the block returns. */
 #define WK_KERNEL_SLAB 5   /* the two passes slab by slab along z
                               (tile_planes planes per slab, 0 = sized for
                               L2) so the E pass re-reads the slab from L2

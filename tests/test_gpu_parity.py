@@ -259,3 +259,51 @@ def test_fp32c_wake_within_1e4_of_fp64(name):
     print(name, "fp32c vs fp64", err)
     assert err["WP"] <= 1e-4 and err["Z"] <= 1e-4
     assert rel_err(np.abs(runs["fp32c"][1].Z), np.abs(runs[None][1].Z)) <= 1e-4
+
+
+TMA_GRIDS = [((16, 12, 20), "float64"), ((24, 16, 30), "float64"), ((32, 20, 26), "float32"),
+             ((72, 18, 40), "float64")]
+
+
+@pytest.mark.parametrize("shape,dtype", TMA_GRIDS)
+@pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
+                                 (["periodic", "pec", "pml"], ["periodic", "pec", "pml"])])
+def test_tma_kernel_exact_against_oracle(shape, dtype, bcs):
+    """TMA-staged fused kernel (interior) + shell: value-for-value equal to
+    the oracle after several steps from random fields (no exponential)."""
+    c = dict(cases.STEP_CASES[2])     # conductive materials on the case boxes
+    c.update(shape=shape, dtype=dtype, bc_low=bcs[0], bc_high=bcs[1], steps=5, n_pml=3)
+    o = oracle_step_case(c)
+    s = b200_step_case(c)
+    s.kernel, s.tile = "tma", (0, 0)
+    E0, H0 = cases.initial_fields(c, o.N)
+    o.E[:], o.H[:] = E0, H0
+    s.E.fromarray(E0)
+    s.H.fromarray(H0)
+    for _ in range(c["steps"]):
+        o.one_step()
+    s._advance(c["steps"], 0)
+    assert int(s._status.item()) == 0
+    assert np.array_equal(s.E.numpy(), o.E)
+    assert np.array_equal(s.H.numpy(), o.H)
+
+
+@pytest.mark.parametrize("tile", [(0, 0), (0, 1), (0, 3), (0, 100)])
+def test_tma_equals_twopass_with_beam_and_capture(tile):
+    """40x40x80 PEC cavity workload, 60 steps with the fused beam and the Ez
+    window capture: TMA kernel (several planes-per-block) equals two-pass."""
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    _, wa, a = workloads.build_b200("cavity_40")
+    _, wb_, b = workloads.build_b200("cavity_40")
+    a.kernel, a.tile = "tma", tile
+    b.kernel = "twopass"
+    bp = Beam(q=1e-9, sigmaz=0.01, beta=1.0).params(a)
+    ha = torch.zeros((9, a.Nz, 60), dtype=torch.float64, device="cuda")
+    hb = torch.zeros_like(ha)
+    a._advance(60, 0, beam=bp, capture=(ha, 18, 18, 3, 3))
+    b._advance(60, 0, beam=bp, capture=(hb, 18, 18, 3, 3))
+    assert int(a._status.item()) == 0
+    assert np.array_equal(a.E.numpy(), b.E.numpy())
+    assert np.array_equal(a.H.numpy(), b.H.numpy())
+    assert torch.equal(ha, hb)

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libwakis_b200.so")
 WK_F64, WK_F32, WK_F32C = 0, 1, 2
 WK_J_ZERO, WK_J_SIGMA_E, WK_J_ARRAY = 0, 1, 2
 WK_KERNEL_AUTO, WK_KERNEL_CELL, WK_KERNEL_MARCH, WK_KERNEL_FUSED, WK_KERNEL_TWOPASS = 0, 1, 2, 3, 4
-WK_KERNEL_SLAB = 5
+WK_KERNEL_SLAB, WK_KERNEL_TMA = 5, 6
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int

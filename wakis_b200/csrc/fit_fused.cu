@@ -366,16 +366,6 @@ k_e_pass(FitParams<T> p, long long step, int mat_smem) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kShellThreads) k_shell(FitParams<T> p, long long step,
-                                                          long long count) {
-  const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
-  if (idx >= count) return;
-  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
-  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
-  fused_cell_general(p, step, n, c);
-}
-
-template <typename T>
 __global__ void __launch_bounds__(kShellThreads) k_h_shell(FitParams<T> p, long long count) {
   const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
   if (idx >= count) return;

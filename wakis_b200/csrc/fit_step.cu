@@ -139,6 +139,19 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   bool march = false;
   const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
                    (d->Ny - 4 + 1) / 2 <= 65535;
+  if (d->kernel == WK_KERNEL_TMA) {
+    FitParams<T> p0 = make_params<T>(d, par);
+    FitParams<T> p1 = make_params<T>(d, par ^ 1);
+    if (!tma_supported<T>(p0) || !tma_supported<T>(p1))
+      return wk_fail(WK_E_SHAPE, "wk_fit_step: TMA kernel needs a 16-byte row pitch, dims >= 5");
+    for (int s = 0; s < n_steps; s++) {
+      FitParams<T> p = make_params<T>(d, par);
+      cudaError_t e = launch_tma<T>(p, step0 + s, st, d->tile_planes);
+      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
+      par ^= 1;
+    }
+    return wk_check_launch("wk_fit_step");
+  }
   if (d->kernel == WK_KERNEL_SLAB) {
     if (!big) return wk_fail(WK_E_SHAPE, "wk_fit_step: slab kernels need every dimension >= 5");
     int planes = d->tile_planes;

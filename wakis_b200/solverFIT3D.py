@@ -176,7 +176,8 @@ class SolverFIT3D(RoutinesMixin):
 
     _KERNELS = {"auto": _native.WK_KERNEL_AUTO, "cell": _native.WK_KERNEL_CELL,
                 "march": _native.WK_KERNEL_MARCH, "fused": _native.WK_KERNEL_FUSED,
-                "twopass": _native.WK_KERNEL_TWOPASS, "slab": _native.WK_KERNEL_SLAB}
+                "twopass": _native.WK_KERNEL_TWOPASS, "slab": _native.WK_KERNEL_SLAB,
+                "tma": _native.WK_KERNEL_TMA}
 
     def _sync_desc(self):
         d = self._desc
