@@ -122,7 +122,8 @@ typedef struct wk_fit_desc {
   void* Hc[2];
 } wk_fit_desc;
 
-#define WK_KERNEL_AUTO 0   /* WK_KERNEL_TWOPASS when Nx, Ny, Nz >= 5, else
+#define WK_KERNEL_AUTO 0   /* WK_KERNEL_TMA when its conditions hold, else
+                              WK_KERNEL_TWOPASS when Nx, Ny, Nz >= 5, else
                               WK_KERNEL_CELL                                */
 #define WK_KERNEL_CELL 1   /* one thread per cell, general row code, H of
                               the backward neighbours recomputed            */
@@ -179,6 +180,18 @@ int wk_fit_step(const wk_fit_desc* d, int n_steps, long long step0, void* stream
  * to cross-check the fused kernel of wk_fit_step.
  */
 int wk_fit_step_split(const wk_fit_desc* d, int n_steps, long long step0, void* stream);
+
+/*
+ * wk_fit_step that also times the interior kernels of every step with CUDA
+ * events recorded on `stream` (the TMA kernel of WK_KERNEL_TMA, the H and E
+ * pass kernels of WK_KERNEL_TWOPASS, the two compensated pass kernels of
+ * WK_F32C; shell launches are not included), then waits for the stream.
+ * *ms_interior = summed interior-kernel time in ms, *n_launches = launches
+ * timed (0 for schedules without a separate interior kernel).  n_steps is
+ * limited to 4096.  No counterpart in the reference: a measurement hook.
+ */
+int wk_fit_step_timed(const wk_fit_desc* d, int n_steps, long long step0, void* stream,
+                      float* ms_interior, int* n_launches);
 
 /*
  * Materialise J = sigma*E_live (dtype) into `J` (3N).  Replaces the

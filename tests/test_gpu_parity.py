@@ -307,3 +307,18 @@ def test_tma_equals_twopass_with_beam_and_capture(tile):
     assert np.array_equal(a.E.numpy(), b.E.numpy())
     assert np.array_equal(a.H.numpy(), b.H.numpy())
     assert torch.equal(ha, hb)
+
+
+def test_timed_step_matches_untimed():
+    """wk_fit_step_timed: same state as wk_fit_step, one timed interior
+    launch per step for the TMA schedule, positive time."""
+    from wakis_b200 import workloads
+    _, _, a = workloads.build_b200("cavity_40")
+    _, _, b = workloads.build_b200("cavity_40")
+    timing = []
+    a._advance(12, 0, timing=timing)
+    b._advance(12, 0)
+    assert sum(t[1] for t in timing) == 12
+    assert sum(t[0] for t in timing) > 0
+    assert np.array_equal(a.E.numpy(), b.E.numpy())
+    assert np.array_equal(a.H.numpy(), b.H.numpy())

@@ -51,6 +51,8 @@ _SIGS = {
     "wk_zero_ghosts": (_i, [ctypes.POINTER(FitDesc), _vp]),
     "wk_fit_step": (_i, [ctypes.POINTER(FitDesc), _i, _ll, _vp]),
     "wk_fit_step_split": (_i, [ctypes.POINTER(FitDesc), _i, _ll, _vp]),
+    "wk_fit_step_timed": (_i, [ctypes.POINTER(FitDesc), _i, _ll, _vp,
+                               ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i)]),
     "wk_sigma_e": (_i, [ctypes.POINTER(FitDesc), _vp, _vp]),
     "wk_wake_potential": (_i, [_vp, _i, _ll, _i, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _i,
                                _vp, _ll, _d, _d, _d, _d, _d, _d, _d, _i, _vp, _vp]),

@@ -255,9 +255,13 @@ int wk_comp_step(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_
   for (int s = 0; s < n_steps; s++) {
     FitParams<double> p = make_params<double>(d, par);
     CompState cs = comp_state(d, par);
+    timer_begin(st);
     k_h_comp<<<grid, blk, 0, st>>>(p, cs);
+    timer_end(st);
     k_h_comp_shell<<<sb, 256, 0, st>>>(p, cs, count);
+    timer_begin(st);
     k_e_comp<<<grid, blk, 0, st>>>(p, cs, step0 + s);
+    timer_end(st);
     k_e_comp_shell<<<sb, 256, 0, st>>>(p, cs, step0 + s, count);
     par ^= 1;
   }

@@ -411,9 +411,13 @@ void two_pass_kb(const FitParams<T>& p, long long step, cudaStream_t st, unsigne
             (p.Nz - 4 + KB - 1) / KB);
   const int mat_smem = p.n_mat * 9 <= 1024 ? p.n_mat * 9 : 0;
   const size_t smem = (size_t)mat_smem * sizeof(T);
+  timer_begin(st);
   k_h_pass<T, KB><<<grid, blk, smem, st>>>(p, mat_smem);
+  timer_end(st);
   k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, count);
+  timer_begin(st);
   k_e_pass<T, KB><<<grid, blk, smem, st>>>(p, step, mat_smem);
+  timer_end(st);
   k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, count);
 }
 

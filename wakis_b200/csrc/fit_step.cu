@@ -5,6 +5,8 @@
 //                   always read the old state).
 // wk_fit_step_split two in-place passes (H, then E), the schedule of
 //                   upstream's _one_step (wakis/solverFIT3D.py:482-503).
+#include <vector>
+
 #include "../../include/wakis_b200.h"
 #include "abi_internal.h"
 #include "fit_common.cuh"
@@ -139,11 +141,16 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
   bool march = false;
   const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
                    (d->Ny - 4 + 1) / 2 <= 65535;
-  if (d->kernel == WK_KERNEL_TMA) {
+  bool use_tma = d->kernel == WK_KERNEL_TMA;
+  if (d->kernel == WK_KERNEL_TMA || (d->kernel == WK_KERNEL_AUTO && big)) {
     FitParams<T> p0 = make_params<T>(d, par);
     FitParams<T> p1 = make_params<T>(d, par ^ 1);
-    if (!tma_supported<T>(p0) || !tma_supported<T>(p1))
+    const bool ok = tma_supported<T>(p0) && tma_supported<T>(p1);
+    if (d->kernel == WK_KERNEL_TMA && !ok)
       return wk_fail(WK_E_SHAPE, "wk_fit_step: TMA kernel needs a 16-byte row pitch, dims >= 5");
+    use_tma = ok;
+  }
+  if (use_tma) {
     for (int s = 0; s < n_steps; s++) {
       FitParams<T> p = make_params<T>(d, par);
       cudaError_t e = launch_tma<T>(p, step0 + s, st, d->tile_planes);
@@ -287,6 +294,51 @@ extern "C" int wk_fit_step(const wk_fit_desc* d, int n_steps, long long step0, v
   if (d->dtype == WK_F32C) return wk_comp_step(d, n_steps, step0, st);
   return d->dtype == WK_F64 ? run_fused<double>(d, n_steps, step0, st)
                             : run_fused<float>(d, n_steps, step0, st);
+}
+
+thread_local KernelTimer* g_kernel_timer = nullptr;
+
+extern "C" int wk_fit_step_timed(const wk_fit_desc* d, int n_steps, long long step0,
+                                 void* stream, float* ms_interior, int* n_launches) {
+  if (!ms_interior || !n_launches)
+    return wk_fail(WK_E_NULL, "wk_fit_step_timed: NULL result pointer");
+  *ms_interior = 0.0f;
+  *n_launches = 0;
+  if (n_steps < 0 || n_steps > 4096)
+    return wk_fail(WK_E_RANGE, "wk_fit_step_timed: n_steps must be in [0, 4096]");
+  KernelTimer t;
+  std::vector<cudaEvent_t> ev(4 * (size_t)n_steps + 2);
+  int made = 0;
+  cudaError_t ce = cudaSuccess;
+  for (; made < (int)ev.size(); made++)
+    if ((ce = cudaEventCreate(&ev[made])) != cudaSuccess) break;
+  if (made < (int)ev.size()) {
+    for (int q = 0; q < made; q++) cudaEventDestroy(ev[q]);
+    return wk_fail(-(int)ce, "wk_fit_step_timed: %s", cudaGetErrorString(ce));
+  }
+  t.ev = ev.data();
+  t.cap = (int)ev.size() / 2;
+  g_kernel_timer = &t;
+  int rc = wk_fit_step(d, n_steps, step0, stream);
+  g_kernel_timer = nullptr;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (rc == WK_OK && e != cudaSuccess)
+    rc = wk_fail(-(int)e, "wk_fit_step_timed: %s", cudaGetErrorString(e));
+  if (rc == WK_OK && t.err != cudaSuccess)
+    rc = wk_fail(-(int)t.err, "wk_fit_step_timed: %s", cudaGetErrorString(t.err));
+  float total = 0.0f;
+  for (int q = 0; rc == WK_OK && q < t.n; q++) {
+    float ms = 0.0f;
+    e = cudaEventElapsedTime(&ms, ev[2 * q], ev[2 * q + 1]);
+    if (e != cudaSuccess) rc = wk_fail(-(int)e, "wk_fit_step_timed: %s", cudaGetErrorString(e));
+    total += ms;
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (rc == WK_OK) {
+    *ms_interior = total;
+    *n_launches = t.n;
+  }
+  return rc;
 }
 
 extern "C" int wk_fit_step_split(const wk_fit_desc* d, int n_steps, long long step0,

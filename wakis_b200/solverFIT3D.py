@@ -12,6 +12,7 @@ There is no CPU fallback: without a CUDA device or without the native
 library the constructor raises.
 """
 
+import ctypes
 import time
 
 import numpy as np
@@ -227,21 +228,25 @@ class SolverFIT3D(RoutinesMixin):
                           "wk_zero_ghosts")
             self.step_0 = False
 
-    def _advance(self, n_steps, step0=0, beam=None, capture=None, split=False, line=None):
+    def _advance(self, n_steps, step0=0, beam=None, capture=None, split=False, line=None,
+                 timing=None):
         """Advance n_steps with optional fused beam (wakesolve Beam), host line
         current and Ez window capture.  ``step0`` is the global step index of
-        the first step (beam time t = step*dt, capture column)."""
+        the first step (beam time t = step*dt, capture column).  With a list
+        ``timing``, the interior kernels are timed with CUDA events
+        (wk_fit_step_timed) and (ms, launches) is appended per launch call;
+        the call then waits for the stream."""
         if n_steps <= 0:
             return
         self._first_step()
         if self.use_conductivity and self._j_state != _J_SIGMA_E and n_steps > 1:
             # the J read by the first step is the stored one; every later step
             # reads J = sigma*E of the step before (upstream 502-503)
-            self._launch(1, step0, beam, capture, split, line)
+            self._launch(1, step0, beam, capture, split, line, timing)
             step0, n_steps = step0 + 1, n_steps - 1
-        self._launch(n_steps, step0, beam, capture, split, line)
+        self._launch(n_steps, step0, beam, capture, split, line, timing)
 
-    def _launch(self, n_steps, step0, beam, capture, split, line):
+    def _launch(self, n_steps, step0, beam, capture, split, line, timing=None):
         if self.precision == "fp32c" and self._j_state == _J_ARRAY:
             raise RuntimeError("precision='fp32c' does not take a stored J array; "
                                "use the fused beam / line source")
@@ -272,6 +277,13 @@ class SolverFIT3D(RoutinesMixin):
         if split:
             rc = self._lib.wk_fit_step_split(d, n_steps, step0, self._stream())
             _native.check(rc, "wk_fit_step_split")
+        elif timing is not None:
+            ms, nl = ctypes.c_float(0.0), ctypes.c_int(0)
+            rc = self._lib.wk_fit_step_timed(d, n_steps, step0, self._stream(),
+                                             ctypes.byref(ms), ctypes.byref(nl))
+            _native.check(rc, "wk_fit_step_timed")
+            self._par ^= (n_steps & 1)
+            timing.append((float(ms.value), int(nl.value)))
         else:
             rc = self._lib.wk_fit_step(d, n_steps, step0, self._stream())
             _native.check(rc, "wk_fit_step")
