@@ -117,6 +117,18 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(vals, ws, device=None):
+    """Element-wise max of a list of floats over all ranks, one all_reduce
+    (every rank calls it at the same point)."""
+    if ws <= 1:
+        return [float(v) for v in vals]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def run_reference(args):
     """CPU oracle on the host cores: Gcell-steps/s of upstream's scipy
     algorithm on a bounded sample (same geometry, 128x128x256)."""
@@ -264,28 +276,21 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
-    t_dev = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
-    ms = float(t_dev.item())
     # interior-kernel time of the same K steps, CUDA events around each
     # interior launch (wk_fit_step_timed), for the roofline of that kernel
     timing = []
     s._advance(args.steps, args.warmup + args.steps, beam=bp, capture=cap, timing=timing)
     ms_int = sum(t[0] for t in timing)
     n_int = sum(t[1] for t in timing)
-    t_int = torch.tensor([ms_int], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t_int, op=dist.ReduceOp.MAX)
-    ms_int = float(t_int.item())
-    # kernels launched per step: each interior launch has a shell launch
-    # beside it (TMA: 1 + 1, two-pass and FP32c: 2 + 2); the other
-    # schedules launch a fixed set
+    # kernels launched per step: TMA 1 interior + 2 shell launches,
+    # two-pass and FP32c 2 interior + 2 shell launches; the other schedules
+    # launch a fixed set
     planes = s.tile[1] if s.tile[1] > 0 else max(
         2, (80 * 1024 * 1024) // (9 * np.dtype(dtype).itemsize * s.Nx * s.Ny))
     nslab = -(-s.Nz // planes)
     fixed = {"split": 4, "fused": 2, "slab": 2 * nslab, "march": 1, "cell": 1}
-    per_step = fixed.get(args.kernel, 2 * n_int // max(args.steps, 1))
+    n_per = n_int // max(args.steps, 1)
+    per_step = fixed.get(args.kernel, {1: 3, 2: 4}.get(n_per, 2 * n_per))
     launches = args.steps * per_step  # step kernels launched in the timed region
     interior = (s.Nx - 4) * (s.Ny - 4) * (s.Nz - 4)
     schedule = {1: "tma", 2: "twopass"}.get(n_int // max(args.steps, 1), args.kernel)
@@ -304,10 +309,8 @@ def main():
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
     clocks = clk.stop()
-    t_e = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
-    t_e2e = float(t_e.item())
+    # device times and the end-to-end wall time: max over ranks
+    ms, ms_int, t_e2e = max_over_ranks([ms, ms_int, t_e2e], ws, dev)
 
     if rank == 0:
         value = N * args.steps * ws / (ms / 1e3) / 1e9

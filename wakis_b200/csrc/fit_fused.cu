@@ -365,47 +365,123 @@ k_e_pass(FitParams<T> p, long long step, int mat_smem) {
   }
 }
 
+// Shell launches of the two-pass and TMA schedules.  Blocks of 256 threads
+// are decoded once per block (32-bit): planes k in {0,1,Nz-2,Nz-1} row by
+// row (256 cells of a row per block), then rows j in {0,1,Ny-2,Ny-1} of the
+// inner planes, then the columns i in {0,1,Nx-2,Nx-1} of the inner rows (4
+// cells x 64 rows per block).  Cells that meet the single-coefficient
+// condition take the lean rows; the rest the general row code.
+struct ShellGrid {
+  int cx, cy;          // 256-cell chunks per row, 64-row chunks per column
+  int nbA, nbB, nbC;   // blocks of the three regions
+};
+
+inline ShellGrid shell_grid(int Nx, int Ny, int Nz) {
+  ShellGrid g;
+  g.cx = (Nx + kShellThreads - 1) / kShellThreads;
+  g.cy = (Ny - 4 + 63) / 64;
+  g.nbA = 4 * Ny * g.cx;
+  g.nbB = 4 * (Nz - 4) * g.cx;
+  g.nbC = g.cy * (Nz - 4);
+  return g;
+}
+
+__device__ __forceinline__ bool shell_cell_of(const ShellGrid& g, int b, int tid, int Nx, int Ny,
+                                              int Nz, Cell& c) {
+  if (b < g.nbA) {
+    const int r = b / g.cx, ck = b - r * g.cx;
+    const int kk = r / Ny;
+    c.j = r - kk * Ny;
+    c.k = kk < 2 ? kk : Nz - 4 + kk;
+    c.i = ck * kShellThreads + tid;
+    return c.i < Nx;
+  }
+  b -= g.nbA;
+  if (b < g.nbB) {
+    const int r = b / g.cx, ck = b - r * g.cx;
+    const int jj = r & 3;
+    c.k = 2 + (r >> 2);
+    c.j = jj < 2 ? jj : Ny - 4 + jj;
+    c.i = ck * kShellThreads + tid;
+    return c.i < Nx;
+  }
+  b -= g.nbB;
+  const int r = b / g.cy, cj = b - r * g.cy;
+  const int ii = tid & 3;
+  c.k = 2 + r;
+  c.i = ii < 2 ? ii : Nx - 4 + ii;
+  c.j = 2 + cj * 64 + (tid >> 2);
+  return c.j <= Ny - 3;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(kShellThreads) k_h_shell(FitParams<T> p, long long count) {
-  const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
-  if (idx >= count) return;
-  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
-  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
+__global__ void __launch_bounds__(kShellThreads) k_h_shell(FitParams<T> p, ShellGrid g) {
+  Cell c;
+  if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
+  const int Nx = p.Nx;
+  const long long N = p.N, NxNy = p.NxNy;
+  const long long n = c.i + (long long)c.j * Nx + (long long)c.k * NxNy;
   const int id = load_id(p.mat_id, p.id_bytes, n);
   T h[3];
+  if (lean_h<T>(c.i, c.j, c.k, Nx, p.Ny, p.Nz)) {
+    const T* E = p.E_in;
+    const T* m0 = p.mat + 9 * id;
+    const T R0 = mul(p.iAx[c.j + (long long)c.k * p.Ny], m0[3]);
+    const T R1 = mul(p.iAy[c.i + (long long)c.k * Nx], m0[4]);
+    const T R2 = mul(p.iAz[c.i + (long long)c.j * Nx], m0[5]);
+    h[0] = p.H_in[n];
+    h[1] = p.H_in[N + n];
+    h[2] = p.H_in[2 * N + n];
+    h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[c.i], p.Ly[c.j], p.Lz[c.k], E[n], E[N + n],
+           E[2 * N + n], E[N + n + 1], E[2 * N + n + 1], E[n + Nx], E[2 * N + n + Nx],
+           E[n + NxNy], E[N + n + NxNy], h[0], h[1], h[2]);
+  } else {
 #pragma unroll
-  for (int d = 0; d < 3; d++) h[d] = h_row(p, p.E_in, p.H_in[d * p.N + n], d, c, n, id);
+    for (int d = 0; d < 3; d++) h[d] = h_row(p, p.E_in, p.H_in[d * N + n], d, c, n, id);
+  }
 #pragma unroll
-  for (int d = 0; d < 3; d++) p.H_out[d * p.N + n] = h[d];
+  for (int d = 0; d < 3; d++) p.H_out[d * N + n] = h[d];
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kShellThreads) k_e_shell(FitParams<T> p, long long step,
-                                                            long long count) {
-  const long long idx = blockIdx.x * (long long)kShellThreads + threadIdx.x;
-  if (idx >= count) return;
-  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
-  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
-  const long long N = p.N;
+                                                            ShellGrid g) {
+  Cell c;
+  if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
+  const int Nx = p.Nx;
+  const long long N = p.N, NxNy = p.NxNy;
+  const long long n = c.i + (long long)c.j * Nx + (long long)c.k * NxNy;
   const int id = load_id(p.mat_id, p.id_bytes, n);
   const T* Hn = p.H_out;
-  auto hval = [&](int e, long long m) -> T { return Hn[e * N + m]; };
   if (p.cap_on) capture(p, c, n, step, p.E_in[2 * N + n]);
+  T curl[3];
+  const bool lean = lean_e<T>(c.i, c.j, c.k, Nx, p.Ny, p.Nz);
+  if (lean) {
+    const T* m0 = p.mat + 9 * id;
+    const T R0 = mul(m0[0], p.itAx[c.j + (long long)c.k * p.Ny]);
+    const T R1 = mul(m0[1], p.itAy[c.i + (long long)c.k * Nx]);
+    const T R2 = mul(m0[2], p.itAz[c.i + (long long)c.j * Nx]);
+    e_lean(R0, R1, R2, p.tLx[c.i], p.tLy[c.j], p.tLz[c.k], Hn[n], Hn[N + n], Hn[2 * N + n],
+           Hn[N + n - 1], Hn[2 * N + n - 1], Hn[n - Nx], Hn[2 * N + n - Nx], Hn[n - NxNy],
+           Hn[N + n - NxNy], curl[0], curl[1], curl[2]);
+  }
+  auto hval = [&](int e, long long m) -> T { return Hn[e * N + m]; };
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const T ieps = p.mat[9 * id + d], sigma = p.mat[9 * id + 6 + d];
     const T eold = p.E_in[d * N + n];
     const T jv = j_in(p, d, c, n, step, eold, sigma);
-    const T curl = e_curl(p, d, c, n, ieps, hval);
-    const T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
+    const T cu = lean ? curl[d] : e_curl(p, d, c, n, ieps, hval);
+    const T enew = add(eold, mul(p.dt, sub(cu, mul(ieps, jv))));
     p.E_out[d * N + n] = enew;
     if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
   }
 }
 
 template <typename T, int KB>
-void two_pass_kb(const FitParams<T>& p, long long step, cudaStream_t st, unsigned sb,
-                 long long count) {
+void two_pass_kb(const FitParams<T>& p, long long step, cudaStream_t st) {
+  const ShellGrid sg = shell_grid(p.Nx, p.Ny, p.Nz);
+  const unsigned sb = (unsigned)(sg.nbA + sg.nbB + sg.nbC);
   dim3 blk(kPassX, kPassY);
   dim3 grid((p.Nx - 4 + kPassX - 1) / kPassX, (p.Ny - 4 + kPassY - 1) / kPassY,
             (p.Nz - 4 + KB - 1) / KB);
@@ -414,25 +490,35 @@ void two_pass_kb(const FitParams<T>& p, long long step, cudaStream_t st, unsigne
   timer_begin(st);
   k_h_pass<T, KB><<<grid, blk, smem, st>>>(p, mat_smem);
   timer_end(st);
-  k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, count);
+  k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, sg);
   timer_begin(st);
   k_e_pass<T, KB><<<grid, blk, smem, st>>>(p, step, mat_smem);
   timer_end(st);
-  k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, count);
+  k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, sg);
 }
 
 template <typename T>
 cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st, int kb) {
-  const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
-  const unsigned sb = (unsigned)((count + kShellThreads - 1) / kShellThreads);
   if (kb >= 4)
-    two_pass_kb<T, 4>(p, step, st, sb, count);
+    two_pass_kb<T, 4>(p, step, st);
   else if (kb == 2)
-    two_pass_kb<T, 2>(p, step, st, sb, count);
+    two_pass_kb<T, 2>(p, step, st);
   else
-    two_pass_kb<T, 1>(p, step, st, sb, count);
+    two_pass_kb<T, 1>(p, step, st);
   return cudaGetLastError();
 }
+
+template <typename T>
+cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_t st) {
+  const ShellGrid sg = shell_grid(p.Nx, p.Ny, p.Nz);
+  const unsigned sb = (unsigned)(sg.nbA + sg.nbB + sg.nbC);
+  k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, sg);
+  k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, sg);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_shell_pair<double>(const FitParams<double>&, long long, cudaStream_t);
+template cudaError_t launch_shell_pair<float>(const FitParams<float>&, long long, cudaStream_t);
 
 template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long, cudaStream_t,
                                              int);

@@ -186,7 +186,13 @@ cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t 
 template <typename T>
 cudaError_t launch_slabs(const FitParams<T>& p, long long step, cudaStream_t st, int planes);
 
-// TMA-staged fused step (fit_tma.cu): interior tiles + shell launch.
+// Shell of a step whose interior was stepped by a fused kernel: H of the
+// shell cells from the old state, then E of the shell cells from the new H
+// (fit_fused.cu); needs Nx, Ny, Nz >= 5 and the interior H_out written.
+template <typename T>
+cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_t st);
+
+// TMA-staged fused step (fit_tma.cu): interior tiles + shell launches.
 template <typename T>
 bool tma_supported(const FitParams<T>& p);
 template <typename T>

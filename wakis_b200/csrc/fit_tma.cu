@@ -1,7 +1,8 @@
 // Fused FIT step with TMA-staged plane tiles (sm_100a).
 //
 // Interior cells only (2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3); the
-// shell runs in the k_shell launch.  Block (bx, by, bz) owns the tile
+// two-cell shell runs afterwards in an H launch and an E launch.  Block
+// (bx, by, bz) owns the tile
 // i in [i0, i0+64), j in [j0, j0+8) of planes [k0, k0+KC) and marches in z.
 // For plane k it needs E_old of planes k and k+1 on the box
 // x in [i0-2, i0+66), y in [j0-1, j0+9) and H_old of plane k on
@@ -452,9 +453,9 @@ cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, i
   timer_end(st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
-  k_shell<T><<<(unsigned)((count + 255) / 256), 256, 0, st>>>(p, step, count);
-  return cudaGetLastError();
+  // shell: H from the old state, then E from the new H (the interior H
+  // the shell E rows read is in H_out once k_tma is done)
+  return launch_shell_pair<T>(p, step, st);
 }
 
 template bool tma_supported<double>(const FitParams<double>&);
