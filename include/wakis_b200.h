@@ -115,9 +115,10 @@ typedef struct wk_fit_desc {
    * planes per block of the plane-marching kernel.                         */
   int kernel;
   int tile_rows, tile_planes;
-  /* WK_F32C only: per-component compensation of E and H (int8, 3N each,
-   * ping-pong like E and H).  The compensation c of a float value v is
-   * q * 2^(e-30), e the binary exponent of v; v + c is the state.          */
+  /* WK_F32C only: per-component compensation words of E and H (bf16 bit
+   * patterns, uint16, 3N each, ping-pong like E and H): the state is the
+   * float value v plus the bf16 value c (the rounding error of the last
+   * update).                                                               */
   void* Ec[2];
   void* Hc[2];
 } wk_fit_desc;

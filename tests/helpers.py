@@ -28,12 +28,13 @@ def b200_grid(c):
     return g
 
 
-def b200_step_case(c):
+def b200_step_case(c, precision=None):
     import wakis_b200 as wb
     g = b200_grid(c)
     return wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"],
                           dtype=np.dtype(c["dtype"]).type, bg=c["bg"], n_pml=c["n_pml"],
-                          use_stl=bool(c["solids"]), use_sibc=False, verbose=0)
+                          use_stl=bool(c["solids"]), use_sibc=False, verbose=0,
+                          precision=precision)
 
 
 def oracle_wake_case(c):

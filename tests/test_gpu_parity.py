@@ -322,3 +322,57 @@ def test_timed_step_matches_untimed():
     assert sum(t[0] for t in timing) > 0
     assert np.array_equal(a.E.numpy(), b.E.numpy())
     assert np.array_equal(a.H.numpy(), b.H.numpy())
+
+
+def _decoded(s, fld):
+    """FP32c state v + c of E or H as float64 numpy (flat 3N)."""
+    v = (s._E if fld == "E" else s._H)[s._par].double()
+    c = (s._Ec if fld == "E" else s._Hc)[s._par].double()
+    return (v + c).cpu().numpy()
+
+
+@pytest.mark.parametrize("tile", [(0, 0), (0, 3)])
+def test_fp32c_tma_close_to_twopass(tile):
+    """Compensated TMA kernel (float factors, packed f32x2 rows) against the
+    compensated two-pass kernels (FP64-formed coefficients per cell): 150
+    steps of the 40x40x80 cavity with beam and capture agree to ~1e-6
+    relative; the status word stays 0."""
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    _, _, a = workloads.build_b200("cavity_40", precision="fp32c")
+    _, _, b = workloads.build_b200("cavity_40", precision="fp32c")
+    a.kernel, a.tile = "tma", tile
+    b.kernel = "twopass"
+    bp = Beam(q=1e-9, sigmaz=0.01, beta=1.0).params(a)
+    ha = torch.zeros((9, a.Nz, 150), dtype=torch.float64, device="cuda")
+    hb = torch.zeros_like(ha)
+    a._advance(150, 0, beam=bp, capture=(ha, 18, 18, 3, 3))
+    b._advance(150, 0, beam=bp, capture=(hb, 18, 18, 3, 3))
+    assert int(a._status.item()) == 0
+    for f in "EH":
+        assert rel_err(_decoded(a, f), _decoded(b, f)) <= 2e-6
+    assert rel_err(ha.cpu().numpy(), hb.cpu().numpy()) <= 2e-6
+
+
+@pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
+                                 (["periodic", "pec", "pml"], ["periodic", "pec", "pml"])])
+def test_fp32c_tma_fields_close_to_oracle(bcs):
+    """Compensated TMA path from random fields on a 16x12x20 grid with
+    conductive materials: E and H after 8 steps within 1e-5 relative of the
+    FP64 oracle."""
+    c = dict(cases.STEP_CASES[2])
+    c.update(shape=(16, 12, 20), dtype="float64", bc_low=bcs[0], bc_high=bcs[1], steps=8,
+             n_pml=3)
+    o = oracle_step_case(c)
+    s = b200_step_case(c, precision="fp32c")
+    s.kernel = "tma"
+    E0, H0 = cases.initial_fields(c, o.N)
+    o.E[:], o.H[:] = E0, H0
+    s.E.fromarray(E0)
+    s.H.fromarray(H0)
+    for _ in range(c["steps"]):
+        o.one_step()
+    s._advance(c["steps"], 0)
+    assert int(s._status.item()) == 0
+    assert rel_err(_decoded(s, "E"), o.E) <= 1e-5
+    assert rel_err(_decoded(s, "H"), o.H) <= 1e-5

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwakis_b200.so")
-SOURCES = ["abi.cu", "fit_step.cu", "fit_march.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "wake.cu"]
+SOURCES = ["abi.cu", "fit_step.cu", "fit_march.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma_comp.cu",
+           "wake.cu"]
 HEADERS = ["abi_internal.h", "fit_common.cuh", "fit_kernels.cuh"]
 
 NVCC_FLAGS = [

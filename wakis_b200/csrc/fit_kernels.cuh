@@ -8,6 +8,57 @@
 namespace wk {
 
 constexpr int kMarchThreads = 256;
+constexpr int kShellBlock = 256;
+
+// Shell decomposition of the two-pass and TMA schedules.  Blocks of 256 threads
+// are decoded once per block (32-bit): planes k in {0,1,Nz-2,Nz-1} row by
+// row (256 cells of a row per block), then rows j in {0,1,Ny-2,Ny-1} of the
+// inner planes, then the columns i in {0,1,Nx-2,Nx-1} of the inner rows (4
+// cells x 64 rows per block).  Cells that meet the single-coefficient
+// condition take the lean rows; the rest the general row code.
+struct ShellGrid {
+  int cx, cy;          // 256-cell chunks per row, 64-row chunks per column
+  int nbA, nbB, nbC;   // blocks of the three regions
+};
+
+inline ShellGrid shell_grid(int Nx, int Ny, int Nz) {
+  ShellGrid g;
+  g.cx = (Nx + kShellBlock - 1) / kShellBlock;
+  g.cy = (Ny - 4 + 63) / 64;
+  g.nbA = 4 * Ny * g.cx;
+  g.nbB = 4 * (Nz - 4) * g.cx;
+  g.nbC = g.cy * (Nz - 4);
+  return g;
+}
+
+__device__ __forceinline__ bool shell_cell_of(const ShellGrid& g, int b, int tid, int Nx, int Ny,
+                                              int Nz, Cell& c) {
+  if (b < g.nbA) {
+    const int r = b / g.cx, ck = b - r * g.cx;
+    const int kk = r / Ny;
+    c.j = r - kk * Ny;
+    c.k = kk < 2 ? kk : Nz - 4 + kk;
+    c.i = ck * kShellBlock + tid;
+    return c.i < Nx;
+  }
+  b -= g.nbA;
+  if (b < g.nbB) {
+    const int r = b / g.cx, ck = b - r * g.cx;
+    const int jj = r & 3;
+    c.k = 2 + (r >> 2);
+    c.j = jj < 2 ? jj : Ny - 4 + jj;
+    c.i = ck * kShellBlock + tid;
+    return c.i < Nx;
+  }
+  b -= g.nbB;
+  const int r = b / g.cy, cj = b - r * g.cy;
+  const int ii = tid & 3;
+  c.k = 2 + r;
+  c.i = ii < 2 ? ii : Nx - 4 + ii;
+  c.j = 2 + cj * 64 + (tid >> 2);
+  return c.j <= Ny - 3;
+}
+
 
 template <typename T>
 __device__ __forceinline__ void capture(const FitParams<T>& p, Cell c, long long n,

@@ -33,6 +33,7 @@
 #include "abi_internal.h"
 #include "fit_common.cuh"
 #include "fit_kernels.cuh"
+#include "tma_util.cuh"
 
 namespace wk {
 
@@ -47,7 +48,6 @@ constexpr int kExt = kEW * (kTY + 1);                // 585
 constexpr int kHalo = kEW + kTY;                     // 73
 constexpr int kRow = 148;                            // per-plane metric values
 constexpr int kMatSmem = 32;                         // materials staged in smem
-constexpr long long kWaitLimit = 1LL << 24;
 
 // H box width: 66 doubles (528 B) or 68 floats (the inner box extent must
 // be a multiple of 16 bytes).
@@ -58,8 +58,6 @@ struct TmaMaps {
   CUtensorMap e[3];
   CUtensorMap h[3];
 };
-
-constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
 template <typename T>
 struct TmaLayout {
@@ -74,43 +72,6 @@ struct TmaLayout {
   static constexpr int bar_off = mat_off + round128(9 * kMatSmem * (int)sizeof(T));
   static constexpr int bytes = bar_off + (kES + kHS) * 8 + 128;   // + base alignment
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// Bounded wait; false when the limit is reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long it = 0; it < kWaitLimit; it++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
-                                            int z, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
 
 // Ext-tile index (row width 65, origin at (i0-1, j0-1)) of tile cell o.
 __device__ __forceinline__ int ext_of_tile(int o) { return (o / kTX + 1) * kEW + o % kTX + 1; }
@@ -351,20 +312,6 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 }
 
 // ----------------------------------------------------------------- host --
-static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-
-static bool get_encode() {
-  if (g_encode) return true;
-  cudaDriverEntryPointQueryResult q;
-  void* fn = nullptr;
-  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
-          cudaSuccess ||
-      q != cudaDriverEntryPointSuccess || !fn)
-    return false;
-  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-  return true;
-}
-
 template <typename T>
 static bool encode_comp(CUtensorMap* map, const T* base, int Nx, int Ny, int Nz, int bx,
                         int by) {
@@ -374,7 +321,7 @@ static bool encode_comp(CUtensorMap* map, const T* base, int Nx, int Ny, int Nz,
   cuuint64_t gstr[2] = {(cuuint64_t)Nx * sizeof(T), (cuuint64_t)Nx * Ny * sizeof(T)};
   cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   cuuint32_t est[3] = {1, 1, 1};
-  CUresult r = g_encode(map, dt, 3, (void*)base, gdim, gstr, box, est,
+  CUresult r = tma_encode_fn()(map, dt, 3, (void*)base, gdim, gstr, box, est,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
@@ -389,7 +336,7 @@ bool tma_supported(const FitParams<T>& p) {
   if (p.N >= (1LL << 31)) return false;
   if ((p.Nx * sizeof(T)) % 16 != 0 || (p.N * sizeof(T)) % 16 != 0) return false;
   if (((uintptr_t)p.E_in % 16) || ((uintptr_t)p.H_in % 16)) return false;
-  return get_encode();
+  return tma_encode_fn() != nullptr;
 }
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
@@ -416,22 +363,6 @@ static cudaError_t tma_occupancy(TmaOcc** out) {
   }
   *out = &o;
   return cudaSuccess;
-}
-
-// Planes per block when none is given: the chunk length KC in [4, 64]
-// minimising (waves of blocks) x (KC + 2), the 2 standing for the prologue
-// plane and the pipeline fill of each block.
-static int tma_auto_kc(long long tiles, int planes, long long slots) {
-  int best = 8;
-  long long best_cost = -1;
-  for (int kc = 4; kc <= 64; kc++) {
-    const long long gz = (planes + kc - 1) / kc;
-    const long long waves = (tiles * gz + slots - 1) / slots;
-    const long long cost = waves * (kc + 2);
-    if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = kc; }
-    if (kc >= planes) break;
-  }
-  return best;
 }
 
 template <typename T>

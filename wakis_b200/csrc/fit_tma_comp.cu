@@ -1,0 +1,510 @@
+// FP32-compensated fused FIT step with TMA-staged float plane tiles (sm_100a).
+//
+// State: float E, H plus bf16 compensation words (fit_comp.cuh); every update
+// is a Kahan step y = delta + c followed by TwoSum(v, y), so v + c keeps ~32
+// significant bits over many steps.  The update factors are formed in FP64
+// from the FP64 metric and material tables and rounded once to float
+// (dt folded in); the rows then run in float.
+//
+// Interior cells only (2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3); the
+// shell runs afterwards in the compensated shell launches.  Block
+// (bx, by, bz) owns the tile i in [i0, i0+64), j in [j0, j0+8) of planes
+// [k0, k0+KC) and marches in z.  Thread 0 issues cp.async.bulk.tensor loads
+// (no multicast) of E (68x10 floats from (i0-2, j0-1), three planes in a
+// ring) and H (68x9 floats, two planes) into shared memory, each slot
+// completing on its own mbarrier; the loads of E(k+2) and H(k+1) go out at
+// the start of plane k.
+//
+// Threads work on pairs of cells (i, i+1) with packed f32x2 arithmetic:
+// warps 0-7 own the 256 pairs of the tile (row = warp, pair = lane) in both
+// half-steps, warp 8 the 32 pairs of the halo row j0-1, and 9 lanes of warp
+// 9 the halo column i0-1 (single cells).  The halo H is recomputed with the
+// same compensated update as its owner's, so it is the value the owner
+// stores.  The new Hx, Hy of a tile pair stay in registers as H(k-1) of the
+// next plane.  Material ids, compensation words and the per-plane factor
+// rows of plane k+1 are loaded while plane k is computed.  Every mbarrier
+// wait is bounded: on timeout the block sets the status word, waits
+// (bounded) for its loads in flight and returns.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/wakis_b200.h"
+#include "abi_internal.h"
+#include "fit_comp.cuh"
+#include "fit_common.cuh"
+#include "fit_kernels.cuh"
+#include "tma_util.cuh"
+
+namespace wk {
+
+namespace {
+
+constexpr int cTX = 64, cTY = 8;
+constexpr int cBX = 68, cBY = 10;         // E box (floats): x from i0-2, y from j0-1
+constexpr int cHBY = 9;                   // H box rows (68 wide)
+constexpr int cES = 3, cHS = 2;
+constexpr int cThreads = 320;
+constexpr int cEW = 66;                   // Hs row: index eb*66 + ea + 1
+constexpr int cExt = cEW * (cTY + 1);     // 594
+constexpr int cMat = 64;                  // materials (16 floats each) in smem
+constexpr int cMatW = 16;
+// per-plane factor rows (floats): H x-row (per ext row j), H y-row (per ext
+// column i, stored at ea+1 so that pairs are 8-byte aligned), E x-row (per
+// tile row), E y-row (per tile column); dt folded in
+constexpr int R_HXA = 0, R_HXB = 10, R_HYA = 20, R_HYB = 86, R_EXA = 152, R_EXB = 160,
+              R_EYA = 168, R_EYB = 232, cRow = 296;
+
+struct CompMaps {
+  CUtensorMap e[3];
+  CUtensorMap h[3];
+};
+
+struct CLayout {
+  static constexpr int eslot = round128(cBX * cBY * 4);
+  static constexpr int hslot = round128(cBX * cHBY * 4);
+  static constexpr int e_off = 0;
+  static constexpr int h_off = e_off + cES * 3 * eslot;
+  static constexpr int hs_off = h_off + cHS * 3 * hslot;
+  static constexpr int row_off = hs_off + round128(3 * cExt * 4);
+  static constexpr int mat_off = row_off + round128(2 * cRow * 4);
+  static constexpr int bar_off = mat_off + round128(cMat * cMatW * 4);
+  static constexpr int bytes = bar_off + (cES + cHS) * 8 + 128;
+};
+
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b, one rounding: fma(b, -1, a)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 ld2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+__device__ __forceinline__ void st2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+__device__ __forceinline__ float2 bcast(float v) { return make_float2(v, v); }
+
+// two bf16 words (cell i in the low half) <-> float2
+__device__ __forceinline__ float2 cdec2(uint32_t w) {
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+__device__ __forceinline__ uint32_t cenc2(float2 e) {
+  uint32_t w;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(e.y), "f"(e.x));
+  return w;
+}
+// v + c + delta -> (t, c'): Kahan step, then TwoSum
+__device__ __forceinline__ float2 cadd2(float2 v, uint32_t& w, float2 delta) {
+  const float2 y = add2(delta, cdec2(w));
+  const float2 t = add2(v, y);
+  const float2 bp = sub2(t, v);
+  const float2 ap = sub2(t, bp);
+  const float2 e = add2(sub2(v, ap), sub2(y, bp));
+  w = cenc2(e);
+  return t;
+}
+
+// Factor-row entry r of plane q = dt * f[q] * g[q], f an inverse area and g
+// a length (FP64, rounded once to float).  RowSrc holds, per thread, where f
+// and g of its entry live (element q*fs of f, q*gs of g); the loads of the
+// next plane are issued while this plane is computed.
+struct RowSrc {
+  const double* f;
+  const double* g;
+  int fs, gs;
+};
+
+__device__ __forceinline__ RowSrc row_src(const FitParams<double>& p, int r, int i0, int j0) {
+  const int Nx = p.Nx, Ny = p.Ny;
+  RowSrc s{nullptr, nullptr, 0, 0};
+  if (r < R_HXB) {
+    const int j = j0 - 1 + (r - R_HXA);
+    if (r - R_HXA < 9 && j < Ny) s = RowSrc{p.iAx + j, p.Ly + j, Ny, 0};
+  } else if (r < R_HYA) {
+    const int j = j0 - 1 + (r - R_HXB);
+    if (r - R_HXB < 9 && j < Ny) s = RowSrc{p.iAx + j, p.Lz, Ny, 1};
+  } else if (r < R_HYB) {
+    const int i = i0 - 2 + (r - R_HYA);
+    if (r > R_HYA && i < Nx) s = RowSrc{p.iAy + i, p.Lx + i, Nx, 0};
+  } else if (r < R_EXA) {
+    const int i = i0 - 2 + (r - R_HYB);
+    if (r > R_HYB && i < Nx) s = RowSrc{p.iAy + i, p.Lz, Nx, 1};
+  } else if (r < R_EXB) {
+    const int j = j0 + (r - R_EXA);
+    if (j < Ny) s = RowSrc{p.itAx + j, p.tLy + j, Ny, 0};
+  } else if (r < R_EYA) {
+    const int j = j0 + (r - R_EXB);
+    if (j < Ny) s = RowSrc{p.itAx + j, p.tLz, Ny, 1};
+  } else if (r < R_EYB) {
+    const int i = i0 + (r - R_EYA);
+    if (i < Nx) s = RowSrc{p.itAy + i, p.tLx + i, Nx, 0};
+  } else if (r < cRow) {
+    const int i = i0 + (r - R_EYB);
+    if (i < Nx) s = RowSrc{p.itAy + i, p.tLz, Nx, 1};
+  }
+  return s;
+}
+__device__ __forceinline__ void row_load(const RowSrc& s, int q, double& f, double& g) {
+  if (s.f) {
+    f = s.f[(long long)q * s.fs];
+    g = s.g[(long long)q * s.gs];
+  } else {
+    f = 0.0;
+    g = 0.0;
+  }
+}
+__device__ __forceinline__ float row_value(double dt, double f, double g) {
+  return (float)((dt * f) * g);
+}
+
+template <typename IdT>
+__global__ void __launch_bounds__(cThreads, 2)
+k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
+           long long step, int KC) {
+  using Lay = CLayout;
+  constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4;
+  extern __shared__ __align__(128) unsigned char sm_raw[];
+  unsigned char* sm = sm_raw + ((128 - (smem_u32(sm_raw) & 127)) & 127);
+  float* Eb = reinterpret_cast<float*>(sm + Lay::e_off);
+  float* Hb = reinterpret_cast<float*>(sm + Lay::h_off);
+  float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][cExt]
+  float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][cRow]
+  float* mt = reinterpret_cast<float*>(sm + Lay::mat_off);    // [n_mat][16]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Lay::bar_off);
+
+  const int Nx = p.Nx, Ny = p.Ny;
+  const long long N = p.N, NxNy = p.NxNy;
+  const int i0 = 2 + blockIdx.x * cTX, j0 = 2 + blockIdx.y * cTY;
+  const int k0 = 2 + blockIdx.z * KC, k1 = min(k0 + KC, p.Nz - 2);
+  const int xs = i0 - 2, ys = j0 - 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int pstart = k0 - 1;
+  const uint32_t e_bytes = 3u * cBX * cBY * 4u, h_bytes = 3u * cBX * cHBY * 4u;
+
+  if (tid == 0) {
+    for (int s = 0; s < cES + cHS; s++) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  auto issue_e = [&](int q) {
+    const int slot = (q - pstart) % cES;
+    mbar_expect_tx(&bar[slot], e_bytes);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      tma_load_3d(Eb + (slot * 3 + d) * SE, &maps.e[d], xs, ys, q, &bar[slot]);
+  };
+  auto issue_h = [&](int q) {
+    const int slot = (q - pstart) % cHS;
+    mbar_expect_tx(&bar[cES + slot], h_bytes);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      tma_load_3d(Hb + (slot * 3 + d) * SH, &maps.h[d], xs, ys, q, &bar[cES + slot]);
+  };
+  auto wait_e = [&](int q) {
+    return mbar_wait(&bar[(q - pstart) % cES], (uint32_t)(((q - pstart) / cES) & 1));
+  };
+  auto wait_h = [&](int q) {
+    return mbar_wait(&bar[cES + (q - pstart) % cHS], (uint32_t)(((q - pstart) / cHS) & 1));
+  };
+  int e_hi = pstart - 1, h_hi = pstart - 1;
+  if (tid == 0) {
+    for (int q = pstart; q <= min(pstart + cES - 1, k1); q++) { issue_e(q); e_hi = q; }
+    for (int q = pstart; q <= min(pstart + cHS - 1, k1 - 1); q++) { issue_h(q); h_hi = q; }
+  }
+
+  // role: 0 tile pair, 1 halo-row pair, 2 halo-column cell, 3 idle
+  const int role = warp < 8 ? 0 : (warp == 8 ? 1 : (lane < cTY + 1 ? 2 : 3));
+  int ea, eb;
+  if (role == 0) { ea = 2 * lane + 1; eb = warp + 1; }
+  else if (role == 1) { ea = 2 * lane + 1; eb = 0; }
+  else { ea = 0; eb = lane; }
+  const int ci = i0 - 1 + ea, cj = j0 - 1 + eb;          // first cell of the item
+  const bool pair = role < 2;
+  const bool hval = role < 3 && ci <= Nx - 3 && cj <= Ny - 3;
+  const bool eval = role == 0 && hval;
+  const int bi = eb * cBX + ea + 1;                       // E / H box index
+  const int hi = eb * cEW + ea + 1;                       // Hs index
+  const long long nb = ci + (long long)cj * Nx;           // flat index at k = 0
+
+  // plane-invariant z-row factors
+  float2 hza = bcast(0.f), hzb = bcast(0.f), eza = bcast(0.f), ezb = bcast(0.f);
+  if (hval) {
+    const double dt = p.dt;
+    float a[2], b[2], c[2], d[2];
+    for (int u = 0; u < (pair ? 2 : 1); u++) {
+      const int i = ci + u;
+      const double iaz = p.iAz[i + (long long)cj * Nx], itaz = p.itAz[i + (long long)cj * Nx];
+      a[u] = (float)((dt * iaz) * p.Lx[i]);
+      b[u] = (float)((dt * iaz) * p.Ly[cj]);
+      c[u] = (float)((dt * itaz) * p.tLx[i]);
+      d[u] = (float)((dt * itaz) * p.tLy[cj]);
+    }
+    hza = make_float2(a[0], pair ? a[1] : 0.f);
+    hzb = make_float2(b[0], pair ? b[1] : 0.f);
+    eza = make_float2(c[0], pair ? c[1] : 0.f);
+    ezb = make_float2(d[0], pair ? d[1] : 0.f);
+  }
+  // float material table: imu, ieps, dt*ieps, dt*ieps*sigma
+  for (int q = tid; q < p.n_mat * 3; q += cThreads) {
+    const int m = q / 3, d = q - m * 3;
+    const double* m0 = p.mat + 9 * m;
+    mt[m * cMatW + d] = (float)m0[3 + d];
+    mt[m * cMatW + 4 + d] = (float)m0[d];
+    mt[m * cMatW + 8 + d] = (float)(p.dt * m0[d]);
+    mt[m * cMatW + 12 + d] = (float)((p.dt * m0[d]) * m0[6 + d]);
+  }
+  // ids, compensation words and factor row of the first plane
+  auto load_ids = [&](int q, int& a0, int& a1) {
+    const long long n = nb + (long long)q * NxNy;
+    const IdT* ids = static_cast<const IdT*>(p.mat_id);
+    a0 = (int)ids[n];
+    a1 = pair ? (int)ids[n + 1] : a0;
+  };
+  auto load_comp = [&](const comp_t* base, int q, uint32_t* w) {
+    const long long n = nb + (long long)q * NxNy;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      w[d] = pair ? *reinterpret_cast<const uint32_t*>(base + d * N + n)
+                  : (uint32_t)base[d * N + n];
+  };
+  int id0 = 0, id1 = 0;
+  uint32_t hc[3] = {0, 0, 0}, ec[3] = {0, 0, 0};
+  if (hval) {
+    load_ids(pstart, id0, id1);
+    load_comp(cs.Hc_in, pstart, hc);
+  }
+  const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
+  if (tid < cRow) {
+    double f, g;
+    row_load(rsrc, pstart, f, g);
+    Rw[(pstart & 1) * cRow + tid] = row_value(p.dt, f, g);
+  }
+  float2 hxp = bcast(0.f), hyp = bcast(0.f);
+  const float2 zero2 = bcast(0.f);
+
+  bool ok = true;
+  int pl = pstart;
+  for (; pl < k1; pl++) {
+    bool got = true;
+    if (tid == 0) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
+    ok = __syncthreads_and(got);
+    if (!ok) break;
+    const bool prologue = pl == pstart;
+    if (tid == 0 && !prologue) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      if (pl + cES - 1 <= k1) { issue_e(pl + cES - 1); e_hi = pl + cES - 1; }
+      if (pl + cHS - 1 <= k1 - 1) { issue_h(pl + cHS - 1); h_hi = pl + cHS - 1; }
+    }
+    // prefetch plane pl+1: ids, compensation words, factor-row inputs
+    const bool more = pl + 1 < k1;
+    int nid0 = 0, nid1 = 0;
+    uint32_t nhc[3] = {0, 0, 0}, nec[3] = {0, 0, 0};
+    double rf = 0.0, rg = 0.0;
+    if (more) {
+      if (hval) {
+        load_ids(pl + 1, nid0, nid1);
+        load_comp(cs.Hc_in, pl + 1, nhc);
+      }
+      if (eval) load_comp(cs.Ec_in, pl + 1, nec);
+      if (tid < cRow) row_load(rsrc, pl + 1, rf, rg);
+    }
+    const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
+    const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
+    const float* Hk = Hb + ((pl - pstart) % cHS) * 3 * SH;
+    const float* R = Rw + (pl & 1) * cRow;
+    const long long n = nb + (long long)pl * NxNy;
+
+    // ---- new H of the owned item (tile pairs only in the prologue)
+    float2 hxn = zero2, hyn = zero2;
+    if (hval && (!prologue || role == 0)) {
+      const float* m0 = mt + id0 * cMatW;
+      const float* m1 = mt + id1 * cMatW;
+      float2 ex0, ey0, ez0, ey1, ez1, ex2, ez2, ex3, ey3, hx, hy, hz, ya, yb;
+      if (pair) {
+        ex0 = ld2(Ek + bi); ey0 = ld2(Ek + SE + bi); ez0 = ld2(Ek + 2 * SE + bi);
+        ey1 = make_float2(ey0.y, Ek[SE + bi + 2]);
+        ez1 = make_float2(ez0.y, Ek[2 * SE + bi + 2]);
+        ex2 = ld2(Ek + bi + cBX); ez2 = ld2(Ek + 2 * SE + bi + cBX);
+        ex3 = ld2(Ek1 + bi); ey3 = ld2(Ek1 + SE + bi);
+        hx = ld2(Hk + bi); hy = ld2(Hk + SH + bi); hz = ld2(Hk + 2 * SH + bi);
+        ya = ld2(R + R_HYA + ea + 1); yb = ld2(R + R_HYB + ea + 1);
+      } else {
+        ex0 = bcast(Ek[bi]); ey0 = bcast(Ek[SE + bi]); ez0 = bcast(Ek[2 * SE + bi]);
+        ey1 = bcast(Ek[SE + bi + 1]); ez1 = bcast(Ek[2 * SE + bi + 1]);
+        ex2 = bcast(Ek[bi + cBX]); ez2 = bcast(Ek[2 * SE + bi + cBX]);
+        ex3 = bcast(Ek1[bi]); ey3 = bcast(Ek1[SE + bi]);
+        hx = bcast(Hk[bi]); hy = bcast(Hk[SH + bi]); hz = bcast(Hk[2 * SH + bi]);
+        ya = bcast(R[R_HYA + ea + 1]); yb = bcast(R[R_HYB + ea + 1]);
+      }
+      const float4 u0 = *reinterpret_cast<const float4*>(m0);
+      const float4 u1 = *reinterpret_cast<const float4*>(m1);
+      const float2 mux = make_float2(u0.x, u1.x), muy = make_float2(u0.y, u1.y),
+                   muz = make_float2(u0.z, u1.z);
+      // S_x = a (ey0 - ey3) + b (ez2 - ez0)   (a = dt iAx Ly imu_x, b = dt iAx Lz imu_x)
+      const float2 sx = fma2(mul2(mux, bcast(R[R_HXA + eb])), sub2(ey0, ey3),
+                             mul2(mul2(mux, bcast(R[R_HXB + eb])), sub2(ez2, ez0)));
+      // S_y = a (ex3 - ex0) + b (ez0 - ez1)   (a = dt iAy Lx imu_y, b = dt iAy Lz imu_y)
+      const float2 sy = fma2(mul2(muy, ya), sub2(ex3, ex0), mul2(mul2(muy, yb), sub2(ez0, ez1)));
+      // S_z = a (ex0 - ex2) + b (ey1 - ey0)   (a = dt iAz Lx imu_z, b = dt iAz Ly imu_z)
+      const float2 sz = fma2(mul2(muz, hza), sub2(ex0, ex2), mul2(mul2(muz, hzb), sub2(ey1, ey0)));
+      const float2 m1v = bcast(-1.0f);
+      hx = cadd2(hx, hc[0], mul2(sx, m1v));
+      hy = cadd2(hy, hc[1], mul2(sy, m1v));
+      hz = cadd2(hz, hc[2], mul2(sz, m1v));
+      if (pair) {
+        st2(Hs + hi, hx); st2(Hs + cExt + hi, hy); st2(Hs + 2 * cExt + hi, hz);
+      } else {
+        Hs[hi] = hx.x; Hs[cExt + hi] = hy.x; Hs[2 * cExt + hi] = hz.x;
+      }
+      hxn = hx;
+      hyn = hy;
+      if (role == 0 && !prologue) {
+        st2(cs.H_out + n, hx); st2(cs.H_out + N + n, hy); st2(cs.H_out + 2 * N + n, hz);
+        *reinterpret_cast<uint32_t*>(cs.Hc_out + n) = hc[0];
+        *reinterpret_cast<uint32_t*>(cs.Hc_out + N + n) = hc[1];
+        *reinterpret_cast<uint32_t*>(cs.Hc_out + 2 * N + n) = hc[2];
+      }
+    }
+    __syncthreads();
+
+    // ---- new E of the tile pair
+    if (eval && !prologue) {
+      const float* m0 = mt + id0 * cMatW;
+      const float* m1 = mt + id1 * cMatW;
+      const int b = eb - 1, a = ea - 1;
+      const float2 hx0 = ld2(Hs + hi), hy0 = ld2(Hs + cExt + hi), hz0 = ld2(Hs + 2 * cExt + hi);
+      const float2 hy1 = make_float2(Hs[cExt + hi - 1], hy0.x);
+      const float2 hz1 = make_float2(Hs[2 * cExt + hi - 1], hz0.x);
+      const float2 hx2 = ld2(Hs + hi - cEW), hz2 = ld2(Hs + 2 * cExt + hi - cEW);
+      const float4 w0 = *reinterpret_cast<const float4*>(m0 + 4);
+      const float4 w1 = *reinterpret_cast<const float4*>(m1 + 4);
+      const float2 iex = make_float2(w0.x, w1.x), iey = make_float2(w0.y, w1.y),
+                   iez = make_float2(w0.z, w1.z);
+      const float4 s0 = *reinterpret_cast<const float4*>(m0 + 12);
+      const float4 s1 = *reinterpret_cast<const float4*>(m1 + 12);
+      const float2 sg[3] = {make_float2(s0.x, s1.x), make_float2(s0.y, s1.y),
+                            make_float2(s0.z, s1.z)};
+      // curl_x = c1 (hy3 - hy0) + c2 (hz0 - hz2)   (c1 = dt ieps_x itAx tLy, c2 = .. tLz)
+      float2 cu[3];
+      cu[0] = fma2(mul2(iex, bcast(R[R_EXA + b])), sub2(hyp, hy0),
+                   mul2(mul2(iex, bcast(R[R_EXB + b])), sub2(hz0, hz2)));
+      // curl_y = c1 (hx0 - hx3) + c2 (hz1 - hz0)   (c1 = dt ieps_y itAy tLx, c2 = .. tLz)
+      cu[1] = fma2(mul2(iey, ld2(R + R_EYA + a)), sub2(hx0, hxp),
+                   mul2(mul2(iey, ld2(R + R_EYB + a)), sub2(hz1, hz0)));
+      // curl_z = c1 (hx2 - hx0) + c2 (hy0 - hy1)   (c1 = dt ieps_z itAz tLx, c2 = .. tLy)
+      cu[2] = fma2(mul2(iez, eza), sub2(hx2, hx0), mul2(mul2(iez, ezb), sub2(hy0, hy1)));
+      float2 ev[3] = {ld2(Ek + bi), ld2(Ek + SE + bi), ld2(Ek + 2 * SE + bi)};
+      if (p.cap_on) {
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          Cell c;
+          c.i = ci + u; c.j = cj; c.k = pl;
+          const float v = u ? ev[2].y : ev[2].x;
+          const comp_t q = (comp_t)(u ? (ec[2] >> 16) : (ec[2] & 0xffffu));
+          capture(p, c, n + u, step, comp_value(v, q));
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        float2 jt = zero2;   // dt*ieps*J of the row
+        if (p.j_mode == WK_J_SIGMA_E)
+          jt = mul2(sg[d], ev[d]);
+        if (d == 2 && cj == p.iys && (p.ixs == ci || p.ixs == ci + 1) &&
+            (p.line_on || p.beam_on)) {
+          const double jb = p.line_on ? p.line[(step - p.line_step0) * p.Nz + pl]
+                                      : beam_j(p, step, pl);
+          if (p.ixs == ci) jt.x = (float)((double)m0[10] * jb);
+          else jt.y = (float)((double)m1[10] * jb);
+        }
+        ev[d] = cadd2(ev[d], ec[d], sub2(cu[d], jt));
+      }
+      st2(cs.E_out + n, ev[0]); st2(cs.E_out + N + n, ev[1]); st2(cs.E_out + 2 * N + n, ev[2]);
+      *reinterpret_cast<uint32_t*>(cs.Ec_out + n) = ec[0];
+      *reinterpret_cast<uint32_t*>(cs.Ec_out + N + n) = ec[1];
+      *reinterpret_cast<uint32_t*>(cs.Ec_out + 2 * N + n) = ec[2];
+    }
+    hxp = hxn;
+    hyp = hyn;
+    id0 = nid0; id1 = nid1;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      hc[d] = nhc[d];
+      ec[d] = nec[d];
+    }
+    if (more && tid < cRow) Rw[((pl + 1) & 1) * cRow + tid] = row_value(p.dt, rf, rg);
+  }
+  if (!ok) {
+    if (tid == 0) {
+      if (p.status) atomicExch(p.status, 1);
+      for (int q = pl; q <= e_hi; q++) wait_e(q);
+      for (int q = pl; q <= h_hi; q++) wait_h(q);
+    }
+    __syncthreads();
+  }
+}
+
+bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int by) {
+  cuuint64_t gdim[3] = {(cuuint64_t)Nx, (cuuint64_t)Ny, (cuuint64_t)Nz};
+  cuuint64_t gstr[2] = {(cuuint64_t)Nx * 4, (cuuint64_t)Nx * Ny * 4};
+  cuuint32_t box[3] = {(cuuint32_t)cBX, (cuuint32_t)by, 1};
+  cuuint32_t est[3] = {1, 1, 1};
+  CUresult r = tma_encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, gdim,
+                               gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+int g_comp_sms[3][64], g_comp_per_sm[3][64];
+bool g_comp_attr[3][64];
+
+}  // namespace
+
+bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
+  if (p.Nx < 5 || p.Ny < 5 || p.Nz < 5) return false;
+  if (p.N >= (1LL << 30)) return false;
+  if (p.Nx % 4 != 0 || p.n_mat > cMat) return false;
+  for (int q = 0; q < 2; q++)
+    if (((uintptr_t)d->E[q] % 16) || ((uintptr_t)d->H[q] % 16) || ((uintptr_t)d->Ec[q] % 4) ||
+        ((uintptr_t)d->Hc[q] % 4))
+      return false;
+  return tma_encode_fn() != nullptr;
+}
+
+cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, int par,
+                            long long step, cudaStream_t st, int KC) {
+  CompState cs = comp_state(d, par);
+  CompMaps maps;
+  for (int c = 0; c < 3; c++) {
+    if (!encode_f32(&maps.e[c], cs.E_in + c * p.N, p.Nx, p.Ny, p.Nz, cBY) ||
+        !encode_f32(&maps.h[c], cs.H_in + c * p.N, p.Nx, p.Ny, p.Nz, cHBY))
+      return cudaErrorInvalidValue;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  const int ib = p.id_bytes == 1 ? 0 : (p.id_bytes == 2 ? 1 : 2);
+  auto kern = ib == 0 ? k_tma_comp<uint8_t> : (ib == 1 ? k_tma_comp<uint16_t> : k_tma_comp<uint32_t>);
+  if (!g_comp_attr[ib][dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CLayout::bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&g_comp_sms[ib][dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_comp_per_sm[ib][dev], kern, cThreads,
+                                                      CLayout::bytes);
+    if (e != cudaSuccess) return e;
+    if (g_comp_per_sm[ib][dev] < 1) g_comp_per_sm[ib][dev] = 1;
+    g_comp_attr[ib][dev] = true;
+  }
+  const int gx = (p.Nx - 4 + cTX - 1) / cTX, gy = (p.Ny - 4 + cTY - 1) / cTY;
+  if (KC <= 0)
+    KC = tma_auto_kc((long long)gx * gy, p.Nz - 4,
+                     (long long)g_comp_sms[ib][dev] * g_comp_per_sm[ib][dev]);
+  const int gz = (p.Nz - 4 + KC - 1) / KC;
+  timer_begin(st);
+  kern<<<dim3(gx, gy, gz), cThreads, CLayout::bytes, st>>>(p, cs, maps, step, KC);
+  timer_end(st);
+  return cudaGetLastError();
+}
+
+}  // namespace wk

@@ -1,0 +1,84 @@
+// TMA and mbarrier helpers shared by the TMA-staged step kernels (sm_100a):
+// shared-memory addresses, mbarrier init / expect-tx / bounded wait, a 3-D
+// tiled bulk tensor load (no multicast) and the tensor-map encoder.
+#pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wk {
+
+constexpr long long kWaitLimit = 1LL << 24;   // mbarrier polls before giving up
+
+constexpr int round128(int b) { return (b + 127) / 128 * 128; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait; false when the limit is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < kWaitLimit; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// cuTensorMapEncodeTiled from the driver, fetched once through the runtime
+// (the library links only the CUDA runtime); nullptr when unavailable.
+inline PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+  if (g_encode) return g_encode;
+  cudaDriverEntryPointQueryResult q;
+  void* fn = nullptr;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+          cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return nullptr;
+  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  return g_encode;
+}
+
+// Planes per block when none is given: the chunk length KC in [4, 64]
+// minimising (waves of blocks) x (KC + 2), the 2 standing for the prologue
+// plane and the pipeline fill of each block.
+inline int tma_auto_kc(long long tiles, int planes, long long slots) {
+  int best = 8;
+  long long best_cost = -1;
+  for (int kc = 4; kc <= 64; kc++) {
+    const long long gz = (planes + kc - 1) / kc;
+    const long long waves = (tiles * gz + slots - 1) / slots;
+    const long long cost = waves * (kc + 2);
+    if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = kc; }
+    if (kc >= planes) break;
+  }
+  return best;
+}
+
+}  // namespace wk

@@ -52,7 +52,7 @@ class SolverFIT3D(RoutinesMixin):
                  use_stl=False, use_conductors=False, use_gpu=True, use_mpi=False,
                  use_sibc=True, fmax=1e9, dtype=np.float64, n_pml=10, bg=(1.0, 1.0),
                  verbose=1, device=None, backend="b200", precision=None):
-        """``precision="fp32c"`` keeps E and H as FP32 values plus int8
+        """``precision="fp32c"`` keeps E and H as FP32 values plus bf16
         compensation words (Kahan-style updates) while the coefficients, the
         time step, the Ez history and the wake integration stay FP64; it
         requires dtype=np.float64 and every grid dimension >= 5."""
@@ -127,8 +127,8 @@ class SolverFIT3D(RoutinesMixin):
         comp = self.precision == "fp32c"
         self._cap_dtype = torch.float64 if comp else td
         if comp:
-            self._Ec = [torch.zeros(N3, dtype=torch.int8, device=dev) for _ in range(2)]
-            self._Hc = [torch.zeros(N3, dtype=torch.int8, device=dev) for _ in range(2)]
+            self._Ec = [torch.zeros(N3, dtype=torch.bfloat16, device=dev) for _ in range(2)]
+            self._Hc = [torch.zeros(N3, dtype=torch.bfloat16, device=dev) for _ in range(2)]
         self._par = 0
         self._j_state = _J_ZERO
         self._j_line = None          # (values tensor) of the last fused beam step
