@@ -174,6 +174,153 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_accuracy(args):
+    """FP32-compensated against FP64 on one grid (rank 0 only): one JSON
+    line with the relative errors of WP, WPx, WPy, |Z|, Re Z, Im Z, |Zx| and
+    the Gcell-steps/s of both whole wakesolve runs (CUDA events)."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from wakis_b200 import workloads
+    name = args.workload if args.workload != "lossy_256" else "precision_448"
+    shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else None
+    r = workloads.precision_compare(name, shape=shape, wakelength=args.wakelength)
+    line = {"metric": "FP32c vs FP64 relative error (max|a-b|/max|b|)", "workload": name,
+            "grid": list(shape or workloads.spec(name)["shape"]), "wakelength": r["wakelength"],
+            "errors": r["errors"], "fp64": r["fp64"], "fp32c": r["fp32c"],
+            "speed_ratio": r["fp32c"]["gcell_steps_per_s"] / r["fp64"]["gcell_steps_per_s"],
+            "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    """Batched form (rank 0 only): `--batch` pillbox cavities stepped in one
+    captured CUDA graph (wakis_b200.batch), FP32c unless --dtype says
+    otherwise; aggregate Gcell-steps/s over all instances."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from wakis_b200 import batch
+    params = batch.pillbox_params(args.batch, seed=0)
+    prec = None if args.dtype in ("float64", "float32") else "fp32c"
+    dt = np.float32 if args.dtype == "float32" else np.float64
+
+    def run(precision, dtype):
+        t0 = time.perf_counter()
+        built = [batch.build_pillbox(**q, precision=precision, dtype=dtype) for q in params]
+        t_build = time.perf_counter() - t0
+        b = batch.BatchedWakeSolve([x[2] for x in built], args.batch_steps)
+        t1 = time.perf_counter()
+        tm = b.run()
+        t_run = time.perf_counter() - t1
+        res = [(np.array(x[1].WP), np.array(x[1].Z)) for x in built]
+        shapes = [(x[2].Nx, x[2].Ny, x[2].Nz) for x in built]
+        del built, b
+        torch.cuda.empty_cache()
+        return tm, res, shapes, t_build, t_run
+
+    tm, res, shapes, t_build, t_run = run(prec, dt)
+    cells = tm["cells"]
+    line = {"metric": METRIC, "value": tm["gcell_steps_per_s"], "unit": "Gcell-steps/s",
+            "n_gpus": 1, "steps": args.batch_steps, "warmup": 0,
+            "ms_per_step": tm["ms"] / args.batch_steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"float64": "f64", "float32": "f32"}.get(args.dtype, "f32+bf16 comp"),
+            "data": "synthetic",
+            "config": {"workload": f"batch_{args.batch}_pillboxes_seed0", "instances": args.batch,
+                       "cells_total": cells, "grids_min": min(shapes), "grids_max": max(shapes),
+                       "graph": "2 steps of every instance per replay, 8 streams"},
+            "e2e": {"value": cells * args.batch_steps / t_run / 1e9, "unit": "Gcell-steps/s",
+                    "note": "wall clock of the batched run incl. the wake integration",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "build_s": t_build}
+    if args.batch_compare and prec == "fp32c":
+        tm64, res64, _, _, _ = run(None, np.float64)
+
+        def rel(a, b):
+            den = np.max(np.abs(b))
+            return float(np.max(np.abs(a - b)) / den) if den else 0.0
+
+        ewp = [rel(a[0], b[0]) for a, b in zip(res, res64)]
+        ez = [rel(np.abs(a[1]), np.abs(b[1])) for a, b in zip(res, res64)]
+        line["per_instance_error_vs_fp64"] = {"WP_max": max(ewp), "absZ_max": max(ez),
+                                              "WP": ewp, "absZ": ez}
+        line["fp64_value"] = tm64["gcell_steps_per_s"]
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args):
+    """Differentiation form (rank 0 only).  The cavity_40 geometry on
+    128x128x256 cells (PEC walls) with a central 64^3 design region of
+    per-cell eps_r ~ U[1, 10] and sigma ~ U[0, 10] S/m (seed 1); loss =
+    int_{0.5}^{3 GHz} |Z_par|^2 df; FP32 forward and adjoint with
+    sqrt(N)-step checkpoints; 16 random directions checked against central
+    differences of FP64 forward runs."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from wakis_b200 import workloads
+    from wakis_b200.adjoint import ImpedanceDesign
+    shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else (128, 128, 256)
+    nsteps = args.adjoint_steps
+    rng = np.random.default_rng(1)
+
+    def problem(dtype):
+        _, _, s = workloads.build_b200("cavity_40", dtype=dtype, shape=shape)
+        m = np.zeros(shape, bool)
+        c = [n // 2 for n in shape]
+        h = [min(32, n // 4) for n in shape]
+        m[c[0] - h[0]:c[0] + h[0], c[1] - h[1]:c[1] + h[1], c[2] - h[2]:c[2] + h[2]] = True
+        return ImpedanceDesign(s, m, n_steps=nsteps), int(m.sum())
+
+    t0 = time.perf_counter()
+    p32, nd = problem(np.float32)
+    t_setup = time.perf_counter() - t0
+    er = rng.uniform(1.0, 10.0, nd)
+    sg = rng.uniform(0.0, 10.0, nd)
+    p32.set_params(er, sg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L = p32.forward()
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ge, gs = p32.backward()
+    torch.cuda.synchronize()
+    t_bwd = time.perf_counter() - t0
+    N = p32.s.N
+    del p32
+    torch.cuda.empty_cache()
+    p64, _ = problem(np.float64)
+    errs = []
+    for _ in range(16):
+        ve = rng.standard_normal(nd)
+        vs = rng.standard_normal(nd)
+        he = hs = 1e-3
+        p64.set_params(er + he * ve, sg + hs * vs)
+        lp = p64.forward(keep=False)
+        p64.set_params(er - he * ve, sg - hs * vs)
+        lm = p64.forward(keep=False)
+        fd = (lp - lm) / 2.0
+        ad = he * float(ge @ ve) + hs * float(gs @ vs)
+        errs.append(abs(ad - fd) / abs(fd) if fd else abs(ad))
+    line = {"metric": "adjoint gradient vs central differences (relative)", "grid": list(shape),
+            "design_cells": nd, "steps": nsteps, "loss": L,
+            "grad_rel_err_max": max(errs), "grad_rel_err": errs,
+            "forward_s": t_fwd, "backward_s": t_bwd, "setup_s": t_setup,
+            "forward_gcell_steps_per_s": N * nsteps / t_fwd / 1e9,
+            "backward_gcell_steps_per_s": N * nsteps / t_bwd / 1e9,
+            "dtype": "f32 forward/adjoint, f64 finite differences",
+            "sigma_range": [0.0, 10.0], "eps_r_range": [1.0, 10.0], "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def cpu_baseline(args, budget_s=20.0):
     """Single-thread oracle on a bounded sample (rank 0, N=1 only)."""
     from oracle import fit as ofit
@@ -214,12 +361,36 @@ def main():
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="FP32c vs FP64 wakesolve on the same grid (default workload "
+                         "precision_448): relative WP / Z errors and both rates")
+    ap.add_argument("--wakelength", type=float, default=None)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="batched form: this many random pillbox cavities (seed 0) in "
+                         "one captured CUDA graph, FP32c, --batch-steps steps each")
+    ap.add_argument("--batch-steps", type=int, default=4000)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="differentiation form: 128x128x256 cavity with a 64^3 design region, "
+                         "FP32 forward + adjoint (4000 steps), gradient checked on 16 random "
+                         "directions against central differences of FP64 forward runs")
+    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--batch-compare", action="store_true",
+                    help="also run the batch in FP64 and report per-instance WP/|Z| errors")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.accuracy:
+        run_accuracy(args)
+        return
+    if args.batch:
+        run_batch(args)
+        return
+    if args.adjoint:
+        run_adjoint(args)
         return
 
     import torch

@@ -121,6 +121,13 @@ typedef struct wk_fit_desc {
    * update).                                                               */
   void* Ec[2];
   void* Hc[2];
+  /* Optional device step counter (may be NULL).  When set, the step index
+   * of the s-th step of a call is *step_dev + s (step0 is ignored), so one
+   * captured CUDA graph can be replayed for consecutive steps; the host
+   * cannot check the capture/line ranges then, and the kernels skip capture
+   * columns and line rows outside their buffers.  Only the TMA and two-pass
+   * schedules (and WK_F32C) take it; every dimension must be >= 5.          */
+  const long long* step_dev;
 } wk_fit_desc;
 
 #define WK_KERNEL_AUTO 0   /* WK_KERNEL_TMA when its conditions hold, else
@@ -150,6 +157,40 @@ typedef struct wk_fit_desc {
                               (tile_planes planes per slab, 0 = sized for
                               L2) so the E pass re-reads the slab from L2
                               (WK_E_SHAPE if a dimension is below 5)        */
+
+/*
+ * Add `inc` to the device counter *ctr (one thread, on `stream`): advances
+ * wk_fit_desc.step_dev between replays of a captured step graph.  No
+ * counterpart in the reference.
+ */
+int wk_counter_add(long long* ctr, long long inc, void* stream);
+
+/*
+ * Adjoint (reverse-mode) FIT step, used for gradients of a wake/impedance
+ * loss with respect to per-cell eps_r and sigma.  No counterpart in the
+ * reference: these are the transposes of the operators of
+ * SolverFIT3D._one_step (wakis/solverFIT3D.py:482-503).  A^T (rows: E
+ * entries, columns: H entries) and B0^T (rows: H, columns: E; B = diag(ieps)
+ * B0) are CSR matrices (int64 row pointers, int32 columns, dtype values) in
+ * the flat 3N ordering of the fields.  All vectors have 3N dtype entries.
+ *   wk_adj_h:    lH_out = lH_in + dt * B0^T (ieps .* lE)
+ *   wk_adj_e:    lE_out = decay .* lE_in - A^T lH      (decay = 1 - dt ieps sigma m)
+ *   wk_adj_grad: for each listed cell c (flat index < N),
+ *                gI[q] += sum_comp lE1 (E1 - E0) / ieps,
+ *                gS[q] += -dt sum_comp ieps lE1 E0 smask   (when use_sigma)
+ *                (double accumulators, one entry per listed cell).
+ * lH_in may equal lH_out and lE_in may equal lE_out.
+ */
+int wk_adj_h(int dtype, const long long* rowptr, const int* col, const void* val,
+             long long nrows, const void* lamE, const void* ieps, double dt,
+             const void* lamH_in, void* lamH_out, void* stream);
+int wk_adj_e(int dtype, const long long* rowptr, const int* col, const void* val,
+             long long nrows, const void* lamH, const void* lamE_in, const void* decay,
+             void* lamE_out, void* stream);
+int wk_adj_grad(int dtype, const long long* cells, long long ncell, long long N,
+                const void* lamE1, const void* E0, const void* E1, const void* ieps,
+                const void* smask, int use_sigma, double dt, double* gI, double* gS,
+                void* stream);
 
 /* ABI version (WK_ABI_VERSION). */
 int wk_version(void);

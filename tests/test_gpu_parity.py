@@ -376,3 +376,103 @@ def test_fp32c_tma_fields_close_to_oracle(bcs):
     assert int(s._status.item()) == 0
     assert rel_err(_decoded(s, "E"), o.E) <= 1e-5
     assert rel_err(_decoded(s, "H"), o.H) <= 1e-5
+
+
+def _small_pillboxes(precision=None):
+    from wakis_b200 import batch
+    ps = [dict(R=0.020, L=0.030, beta=0.9, sigma=1e4), dict(R=0.026, L=0.036, beta=0.6, sigma=3e5),
+          dict(R=0.022, L=0.040, beta=1.0, sigma=2e3)]
+    return [batch.build_pillbox(**q, cell=2e-3, precision=precision) for q in ps]
+
+
+def test_batched_graph_equals_individual_wakesolve():
+    """Three uneven pillboxes stepped in one replayed CUDA graph (device step
+    counter, 4 streams) give the same WP and Z, value for value, as separate
+    wakesolve runs of the same instances."""
+    from wakis_b200 import batch
+    inst = _small_pillboxes()
+    b = batch.BatchedWakeSolve([x[2] for x in inst], 121, streams=4)
+    b.run()
+    solo = _small_pillboxes()
+    for (g, w, s), (g2, w2, s2) in zip(inst, solo):
+        wl = batch.BatchedWakeSolve.wakelength_for(s2, 121)
+        s2.wakesolve(wakelength=wl)
+        assert s2.Nt == 121
+        assert int(s._status.item()) == 0
+        assert np.array_equal(np.asarray(w.WP), np.asarray(w2.WP))
+        assert np.array_equal(np.asarray(w.Z), np.asarray(w2.Z))
+        assert np.array_equal(s.E.numpy(), s2.E.numpy())
+
+
+def test_batched_fp32c_close_to_fp64():
+    """The same batch in FP32c: WP and |Z| of every instance within 1e-4 of
+    the FP64 batch."""
+    from wakis_b200 import batch
+    a = _small_pillboxes("fp32c")
+    b = _small_pillboxes()
+    batch.BatchedWakeSolve([x[2] for x in a], 200, streams=2).run()
+    batch.BatchedWakeSolve([x[2] for x in b], 200, streams=2).run()
+    for (_, wa, _), (_, wb_, _) in zip(a, b):
+        assert rel_err(np.asarray(wa.WP), np.asarray(wb_.WP)) <= 1e-4
+        assert rel_err(np.abs(np.asarray(wa.Z)), np.abs(np.asarray(wb_.Z))) <= 1e-4
+
+
+def _design_problem(dtype, n_steps=800):
+    """cavity_40 geometry with an 8x8x8-cell design region at the centre,
+    PEC walls (dt not clamped), FP32 or FP64."""
+    from wakis_b200 import workloads
+    from wakis_b200.adjoint import ImpedanceDesign
+    _, _, s = workloads.build_b200("cavity_40", dtype=dtype)
+    m = np.zeros((s.Nx, s.Ny, s.Nz), bool)
+    m[16:24, 16:24, 36:44] = True
+    return ImpedanceDesign(s, m, f_band=(0.5e9, 3e9), n_steps=n_steps, segment=30)
+
+
+def test_adjoint_operators_match_step_kernels():
+    """A and B0 assembled on the host reproduce the step kernels: from
+    random (E, H) one FP64 step equals H - A E, E + dt ieps (B0 H')."""
+    from wakis_b200 import workloads
+    from wakis_b200.adjoint import assemble_operators
+    _, _, s = workloads.build_b200("cavity_40")
+    A, B0 = assemble_operators(s)
+    rng = np.random.default_rng(3)
+    E0 = rng.standard_normal(3 * s.N)
+    H0 = rng.standard_normal(3 * s.N)
+    s._first_step()
+    s.E.fromarray(E0)
+    s.H.fromarray(H0)
+    E0, H0 = s.E.numpy().copy(), s.H.numpy().copy()     # ghosts as the kernel sees them
+    s._advance(1, 0)
+    H1 = H0 - A @ E0
+    ie = s.ieps.numpy()
+    E1 = E0 + float(s.dt) * ie * (B0 @ H1)
+    assert rel_err(s.H.numpy(), H1) <= 1e-13
+    assert rel_err(s.E.numpy(), E1) <= 1e-13
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-5), (np.float32, 2e-3)])
+def test_adjoint_gradient_matches_central_differences(dtype, tol):
+    """dL/d(eps_r, sigma) of L = int_{0.5}^{3 GHz} |Z|^2 df from the adjoint
+    against central finite differences of FP64 forward runs along 4 random
+    directions of the 1024 parameters."""
+    rng = np.random.default_rng(1)
+    nd = 512
+    er = rng.uniform(1.0, 10.0, nd)
+    sg = rng.uniform(0.0, 10.0, nd)
+    p = _design_problem(dtype)
+    p.set_params(er, sg)
+    L = p.forward()
+    ge, gs = p.backward()
+    assert L > 0 and np.all(np.isfinite(ge)) and np.all(np.isfinite(gs))
+    q = _design_problem(np.float64)
+    for t in range(4):
+        ve = rng.standard_normal(nd)
+        vs = rng.standard_normal(nd)
+        he, hs = 1e-3, 1e-3
+        q.set_params(er + he * ve, sg + hs * vs)
+        lp = q.forward(keep=False)
+        q.set_params(er - he * ve, sg - hs * vs)
+        lm = q.forward(keep=False)
+        fd = (lp - lm) / 2.0
+        ad = he * ge @ ve + hs * gs @ vs
+        assert abs(ad - fd) <= tol * abs(fd), (t, ad, fd)

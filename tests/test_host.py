@@ -150,3 +150,28 @@ def test_lean_interior_formulas_equal_oracle():
                 ieps = t[:, d]
                 e_new = E[d * N + ec] + k.dt * (curl[d] - ieps * J[d * N + ec])
                 assert np.array_equal(e_new, o.E[d * N + ec])
+
+
+@pytest.mark.parametrize("idx", VALID)
+def test_adjoint_operators_equal_oracle_matrices(idx):
+    """The host assembly behind the adjoint kernels reproduces upstream's
+    operators: A = dt * iDa iDmu C Ds and diag(ieps) B0 = iDeps itDa C^T tDs
+    (the oracle's scipy matrices) on every valid step case."""
+    from types import SimpleNamespace
+    from wakis_b200.adjoint import assemble_operators
+    c = cases.STEP_CASES[idx]
+    o = oracle_step_case(c)
+    k = _coef(c)
+    nx, ny, nz = c["shape"]
+    fake = SimpleNamespace(_coef=k, Nx=nx, Ny=ny, Nz=nz, dt=k.dt)
+    A, B0 = assemble_operators(fake)
+    dtA = (float(k.dt) * o.A.astype(np.float64)).toarray()
+    Bo = o.B.astype(np.float64).toarray()
+    ie = o.ieps.astype(np.float64)
+    scale = np.max(np.abs(dtA)) or 1.0
+    assert np.max(np.abs(A.toarray() - dtA)) <= 1e-6 * scale if c["dtype"] == "float32" \
+        else np.max(np.abs(A.toarray() - dtA)) <= 1e-14 * scale
+    B = ie[:, None] * B0.toarray()
+    scale = np.max(np.abs(Bo)) or 1.0
+    tol = 1e-6 if c["dtype"] == "float32" else 1e-14
+    assert np.max(np.abs(B - Bo)) <= tol * scale

@@ -42,6 +42,7 @@ class FitDesc(ctypes.Structure):
         ("cap_nt", _ll), ("cap_step0", _ll), ("cap", _vp), ("status", _vp),
         ("kernel", _i), ("tile_rows", _i), ("tile_planes", _i),
         ("Ec", _vp * 2), ("Hc", _vp * 2),
+        ("step_dev", _vp),
     ]
 
 
@@ -54,6 +55,11 @@ _SIGS = {
     "wk_fit_step_timed": (_i, [ctypes.POINTER(FitDesc), _i, _ll, _vp,
                                ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i)]),
     "wk_sigma_e": (_i, [ctypes.POINTER(FitDesc), _vp, _vp]),
+    "wk_counter_add": (_i, [_vp, _ll, _vp]),
+    "wk_adj_h": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, ctypes.c_double, _vp, _vp, _vp]),
+    "wk_adj_e": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp]),
+    "wk_adj_grad": (_i, [_i, _vp, _ll, _ll, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_double,
+                         _vp, _vp, _vp]),
     "wk_wake_potential": (_i, [_vp, _i, _ll, _i, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _i,
                                _vp, _ll, _d, _d, _d, _d, _d, _d, _d, _i, _vp, _vp]),
     "wk_trans_wake": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp]),

@@ -1,0 +1,343 @@
+"""Gradients of an impedance-band loss with respect to per-cell eps_r and
+sigma: reverse-mode (adjoint) FIT stepping with checkpointed forward states.
+
+Upstream has no differentiation; this follows the forward path of
+``wakesolve`` (wakis/routines.py:231-482) with the longitudinal wake
+(wakis/wakeSolver.py:310-420) and impedance (631-700), and differentiates
+
+    L = integral over [f0, f1] of |Z_par(f)|^2 df        (trapezoid on the bins)
+
+with respect to eps_r and sigma of the cells of a design region, at a fixed
+time step (the relaxation-time clamp of the constructor is not re-evaluated).
+
+* Forward: the solver steps n_steps with the fused beam and the capture of Ez
+  on the test line; (E, H) are copied every ``segment`` steps (sqrt(n_steps)
+  by default).
+* Loss: WP(s) and the kept DFT bins of Z are rebuilt from the captured
+  history with torch operations (same s axis, int() time index and negative
+  index wrap as the wake kernel), so torch autograd gives dL/dEz(k, n).
+* Backward: segment by segment from the end, the forward states of the
+  segment are recomputed from its checkpoint, then the adjoint steps
+  (``wk_adj_h``, ``wk_adj_e``: CSR products with A^T and B0^T assembled on
+  the host from the same coefficient tables the step kernels read) run
+  backwards with dL/dEz injected at the test line, and ``wk_adj_grad``
+  accumulates the parameter adjoints of every step.
+
+``ImpedanceLoss`` wraps this in a torch.autograd.Function.
+"""
+
+import ctypes
+
+import numpy as np
+import torch
+from scipy import sparse
+from scipy.constants import epsilon_0 as EPS_0
+
+from . import _native
+
+_TERMS_H = {0: [(1, "0", 1), (1, "z", -1), (2, "0", -1), (2, "y", 1)],
+            1: [(0, "0", -1), (0, "z", 1), (2, "0", 1), (2, "x", -1)],
+            2: [(0, "0", 1), (0, "y", -1), (1, "0", -1), (1, "x", 1)]}
+_TERMS_E = {0: [(1, "z", 1), (1, "0", -1), (2, "y", -1), (2, "0", 1)],
+            1: [(0, "z", -1), (0, "0", 1), (2, "x", 1), (2, "0", -1)],
+            2: [(0, "y", 1), (0, "0", -1), (1, "x", -1), (1, "0", 1)]}
+
+
+def _face_val(f, d, i, j, k, Nx, Ny, Nz):
+    """Face mask of component d (later faces win: x-lo, x-hi, y-lo, y-hi,
+    z-lo, z-hi; wakis/boundaries.py:92-101), vectorised over cells."""
+    v = np.ones(i.shape, np.float64)
+    if d != 0:
+        v[i == 0] = f[0]
+        v[i == Nx - 1] = f[1]
+    if d != 1:
+        v[j == 0] = f[2]
+        v[j == Ny - 1] = f[3]
+    if d != 2:
+        v[k == 0] = f[4]
+        v[k == Nz - 1] = f[5]
+    return v
+
+
+def assemble_operators(solver):
+    """(A, B0) as scipy CSR (float64, 3N x 3N): H' = H - A E and
+    E' = E + dt diag(ieps) (B0 H' - J), built from the solver's compact
+    coefficient set with the kernels' conventions (flat-offset neighbours,
+    PEC column / PMC row masks for A, PEC row / PMC column masks for B0)."""
+    c = solver._coef
+    Nx, Ny, Nz = solver.Nx, solver.Ny, solver.Nz
+    N = Nx * Ny * Nz
+    NxNy = Nx * Ny
+    n = np.arange(N, dtype=np.int64)
+    i, j, k = n % Nx, (n // Nx) % Ny, n // NxNy
+    dt = float(solver.dt)
+    imu = np.asarray(c.table, np.float64)[np.asarray(c.ids, np.int64)][:, 3:6]
+    L = [np.asarray(c.Lx, np.float64), np.asarray(c.Ly, np.float64), np.asarray(c.Lz, np.float64)]
+    tL = [np.asarray(c.tLx, np.float64), np.asarray(c.tLy, np.float64),
+          np.asarray(c.tLz, np.float64)]
+    iA = [np.asarray(c.iAx, np.float64)[j, k], np.asarray(c.iAy, np.float64)[i, k],
+          np.asarray(c.iAz, np.float64)[i, j]]
+    itA = [np.asarray(c.itAx, np.float64)[j, k], np.asarray(c.itAy, np.float64)[i, k],
+           np.asarray(c.itAz, np.float64)[i, j]]
+    off = {"0": 0, "x": 1, "y": Nx, "z": NxNy}
+    rows_a, cols_a, vals_a, rows_b, cols_b, vals_b = [], [], [], [], [], []
+    coord = lambda m: (m % Nx, (m // Nx) % Ny, m // NxNy)
+    for d in range(3):
+        R = iA[d] * imu[:, d]
+        if c.has_pmc:
+            R = R * _face_val(c.pmc_face, d, i, j, k, Nx, Ny, Nz)
+        for e, o, sg in _TERMS_H[d]:
+            m = n + off[o]
+            ok = m < N
+            nn, mm = n[ok], m[ok]
+            im_, jm, km = coord(mm)
+            col = L[e][(im_, jm, km)[e]]
+            if c.has_pec:
+                col = col * _face_val(c.pec_face, e, im_, jm, km, Nx, Ny, Nz)
+            rows_a.append(d * N + nn)
+            cols_a.append(e * N + mm)
+            vals_a.append(sg * dt * R[ok] * col)
+        R = itA[d].copy()
+        if c.has_pec:
+            R = R * _face_val(c.pec_face, d, i, j, k, Nx, Ny, Nz)
+        for e, o, sg in _TERMS_E[d]:
+            m = n - off[o]
+            ok = m >= 0
+            nn, mm = n[ok], m[ok]
+            im_, jm, km = coord(mm)
+            col = tL[e][(im_, jm, km)[e]]
+            if c.has_pmc:
+                col = col * _face_val(c.pmc_face, e, im_, jm, km, Nx, Ny, Nz)
+            rows_b.append(d * N + nn)
+            cols_b.append(e * N + mm)
+            vals_b.append(sg * R[ok] * col)
+    cat = np.concatenate
+    A = sparse.csr_matrix((cat(vals_a), (cat(rows_a), cat(cols_a))), shape=(3 * N, 3 * N))
+    B0 = sparse.csr_matrix((cat(vals_b), (cat(rows_b), cat(cols_b))), shape=(3 * N, 3 * N))
+    return A, B0
+
+
+class _DevCSR:
+    """CSR matrix on the device: int64 row pointers, int32 columns."""
+
+    def __init__(self, m, dtype, device):
+        m = m.tocsr()
+        m.sort_indices()
+        self.n = m.shape[0]
+        self.rowptr = torch.as_tensor(m.indptr.astype(np.int64), device=device)
+        self.col = torch.as_tensor(m.indices.astype(np.int32), device=device)
+        self.val = torch.as_tensor(m.data, dtype=dtype, device=device)
+
+
+class ImpedanceDesign:
+    """Loss and gradient of L = int_{f0}^{f1} |Z_par|^2 df over the per-cell
+    eps_r and sigma of `design` (boolean (Nx, Ny, Nz) mask) for one solver
+    (dtype float32 or float64, built with its WakeSolver).  n_steps fixes
+    Nt (the wakelength is set so that upstream's Nt formula gives it)."""
+
+    def __init__(self, solver, design, f_band=(0.5e9, 3e9), n_steps=4000, segment=None,
+                 samples=1001):
+        s = self.s = solver
+        if s.precision is not None:
+            raise ValueError("ImpedanceDesign needs a plain float32 / float64 solver")
+        self.dev = s.device
+        self.tdtype = torch.float64 if s.dtype == np.float64 else torch.float32
+        self.wk = _native.WK_F64 if s.dtype == np.float64 else _native.WK_F32
+        mask = np.asarray(design, bool)
+        self.cells_np = np.flatnonzero(mask.ravel(order="F")).astype(np.int64)
+        self.cells = torch.as_tensor(self.cells_np, device=self.dev)
+        self.n_steps = int(n_steps)
+        self.segment = int(segment) if segment else max(1, int(round(np.sqrt(self.n_steps))))
+        self.f_band = f_band
+        self.samples = samples
+        A, B0 = assemble_operators(s)
+        self.AT = _DevCSR(A.T, self.tdtype, self.dev)
+        self.B0T = _DevCSR(B0.T, self.tdtype, self.dev)
+        N = s.N
+        ie, _, sg = s._dense_fields()
+        self.ieps0 = ie.array.clone()
+        self.sigma0 = sg.array.clone()
+        self.eps_r = None
+        self.sigma = None
+        self.lib = _native.lib()
+        # the beam line's z entries take the beam current, not sigma*E
+        w = s.wake
+        self.ixs = int(np.abs(s.x - w.xsource).argmin())
+        self.iys = int(np.abs(s.y - w.ysource).argmin())
+        sm = torch.ones(3 * N, dtype=self.tdtype, device=self.dev)
+        beam_cells = self.ixs + self.iys * s.Nx + torch.arange(s.Nz, device=self.dev) * s.Nx * s.Ny
+        sm[2 * N + beam_cells] = 0
+        self.smask = sm
+        self._ws = None
+        self._prepare_loss()
+
+    # ---------------------------------------------------------- parameters
+    def set_params(self, eps_r, sigma):
+        """Per-design-cell eps_r and sigma (length n_cells each)."""
+        s, N = self.s, self.s.N
+        er = torch.as_tensor(np.asarray(eps_r, np.float64), device=self.dev)
+        sg = torch.as_tensor(np.asarray(sigma, np.float64), device=self.dev)
+        ie = self.ieps0.clone().double()
+        sgm = self.sigma0.clone().double()
+        for d in range(3):
+            ie[d * N + self.cells] = 1.0 / (er * EPS_0)
+            sgm[d * N + self.cells] = sg
+        f_ie, _, f_sg = s._dense_fields()
+        f_ie.array.copy_(ie.to(f_ie.array.dtype))
+        f_sg.array.copy_(sgm.to(f_sg.array.dtype))
+        s.update_tensors()
+        s.use_conductivity = bool((sgm != 0).any().item()) or s.use_conductivity
+        self.ieps = f_ie.array.to(self.tdtype).contiguous()
+        self.sig = f_sg.array.to(self.tdtype).contiguous()
+        self.eps_r, self.sigma = er, sg
+
+    # ---------------------------------------------------------------- loss
+    def _prepare_loss(self):
+        s, w = self.s, self.s.wake
+        z = s.z
+        self.wakelength = ((self.n_steps + 0.5) * float(s.dt) * w.v - w.ti * w.v
+                           - (z.max() - z.min()))
+        nt, dt = self.n_steps, float(s.dt)
+        zmin = float(np.min(z))
+        s_axis = np.arange(-w.ti * w.v, self.wakelength, dt * w.v)
+        it = np.empty((len(s_axis), s.Nz), np.int64)
+        for k in range(s.Nz):
+            ts = (z[k] + s_axis) / w.v - zmin / w.v - 0.0 + w.ti
+            it[:, k] = (ts / dt).astype(np.int64)
+        ok = (it < nt) & (it >= -nt)
+        it = np.where(it < 0, it + nt, it)
+        it[~ok] = 0
+        self.s_axis = s_axis
+        self.it = torch.as_tensor(it, device=self.dev)
+        self.itok = torch.as_tensor(ok, device=self.dev, dtype=torch.float64)
+        self.dz = torch.as_tensor(np.asarray(s.grid.dz, np.float64)[:s.Nz], device=self.dev)
+        ds = float(np.mean(s_axis[1:] - s_axis[:-1]))
+        N = int((w.v / ds) // w.fmax * self.samples)
+        f = np.fft.fftfreq(N, ds / w.v)
+        keep = np.flatnonzero((f >= 0) & (f < w.fmax))
+        band = keep[(f[keep] >= self.f_band[0]) & (f[keep] <= self.f_band[1])]
+        self.f = torch.as_tensor(f[band], device=self.dev)
+        idx = np.arange(len(s_axis))
+        F = np.exp(-2j * np.pi * np.outer(band, idx) / N)
+        self.F = torch.as_tensor(F, device=self.dev)
+        lam = (1 / (w.sigmaz * np.sqrt(2 * np.pi))) * np.exp(-(s_axis ** 2) / (2 * w.sigmaz ** 2))
+        self.lamf = self.F @ torch.as_tensor(lam * w.v, device=self.dev).to(torch.complex128)
+        self.qscale = w.q * 1e12
+
+    def loss_from_history(self, ez):
+        """L from the test-line history ez (Nz, Nt) float64 (torch, may
+        require grad): WP(s) = sum_k Ez(k, it(s, k)) dz_k / (q 1e12),
+        Z = -DFT(WP 1e12) / DFT(lambda v) on the kept bins in the band."""
+        nz = ez.shape[0]
+        vals = ez[torch.arange(nz, device=self.dev)[None, :], self.it]
+        WP = (vals * self.itok * self.dz[None, :]).sum(dim=1) / self.qscale
+        Z = -(self.F @ (WP * 1e12).to(torch.complex128)) / self.lamf
+        p = Z.real ** 2 + Z.imag ** 2
+        return torch.trapezoid(p, self.f)
+
+    # ------------------------------------------------------------- forward
+    def _live(self):
+        s = self.s
+        return s._E[s._par], s._H[s._par]
+
+    def forward(self, keep=True):
+        """Step n_steps from zero fields with beam and test-line capture;
+        returns L (float).  With keep, (E, H) are copied every `segment`
+        steps for the backward pass."""
+        s = self.s
+        s.reset_fields()
+        s.step_0 = True
+        s.nstep = 0
+        ws = s._wake_setup(self.wakelength, compute_plane="longitudinal")
+        if ws["Nt"] != self.n_steps:
+            raise RuntimeError(f"step count {ws['Nt']} != {self.n_steps}")
+        self._ws = ws
+        self.ckpt = {}
+        K = self.segment
+        n = 0
+        while n < self.n_steps:
+            if keep:
+                E, H = self._live()
+                self.ckpt[n] = (E.clone(), H.clone())
+            m = min(K, self.n_steps - n)
+            s._advance(m, n, beam=ws["beam_params"], capture=ws["capture"])
+            n += m
+        self.hist = ws["hist"][0].double()
+        return float(self.loss_from_history(self.hist).item())
+
+    # ------------------------------------------------------------ backward
+    def _restore(self, n):
+        s = self.s
+        E, H = self._live()
+        E.copy_(self.ckpt[n][0])
+        H.copy_(self.ckpt[n][1])
+        s.step_0 = False
+        s.nstep = n
+        s._j_state = 1 if (n >= 1 and s.use_conductivity) else 0   # WK_J_SIGMA_E / ZERO
+
+    def backward(self):
+        """(dL/d eps_r, dL/d sigma) of the design cells (numpy float64)."""
+        s, N, lib = self.s, self.s.N, self.lib
+        ez = self.hist.clone().requires_grad_(True)
+        L = self.loss_from_history(ez)
+        (g_hist,) = torch.autograd.grad(L, ez)
+        g_hist = g_hist.to(self.tdtype)
+        ixt = int(np.abs(s.x - s.wake.xtest).argmin())
+        iyt = int(np.abs(s.y - s.wake.ytest).argmin())
+        zidx = 2 * N + ixt + iyt * s.Nx + torch.arange(s.Nz, device=self.dev) * s.Nx * s.Ny
+        lE = torch.zeros(3 * N, dtype=self.tdtype, device=self.dev)
+        lH = torch.zeros(3 * N, dtype=self.tdtype, device=self.dev)
+        gI = torch.zeros(len(self.cells_np), dtype=torch.float64, device=self.dev)
+        gS = torch.zeros_like(gI)
+        dt = float(s.dt)
+        cond = bool(s.use_conductivity)
+        decay = (1.0 - dt * self.ieps.double() * self.sig.double() * self.smask.double()
+                 ).to(self.tdtype) if cond else torch.ones_like(lE)
+        ones = torch.ones_like(lE)
+        st = torch.cuda.current_stream(self.dev).cuda_stream
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+        bp = self._ws["beam_params"]
+        starts = sorted(self.ckpt)
+        for a in reversed(starts):
+            b = min(a + self.segment, self.n_steps)
+            self._restore(a)
+            Es = [self._live()[0].clone()]
+            for n in range(a, b):
+                s._advance(1, n, beam=bp)
+                Es.append(self._live()[0].clone())
+            for n in range(b - 1, a - 1, -1):
+                use_sig = int(cond and n >= 1)
+                _native.check(lib.wk_adj_grad(
+                    self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(Es[n - a]),
+                    ptr(Es[n + 1 - a]), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
+                    ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
+                _native.check(lib.wk_adj_h(
+                    self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
+                    self.B0T.n, ptr(lE), ptr(self.ieps), dt, ptr(lH), ptr(lH),
+                    ctypes.c_void_p(st)), "wk_adj_h")
+                _native.check(lib.wk_adj_e(
+                    self.wk, ptr(self.AT.rowptr), ptr(self.AT.col), ptr(self.AT.val), self.AT.n,
+                    ptr(lH), ptr(lE), ptr(decay if use_sig else ones), ptr(lE),
+                    ctypes.c_void_p(st)), "wk_adj_e")
+                lE[zidx] += g_hist[:, n]
+        er = self.eps_r
+        g_eps = gI * (-1.0 / (EPS_0 * er * er))
+        return g_eps.cpu().numpy(), gS.cpu().numpy()
+
+
+class ImpedanceLoss(torch.autograd.Function):
+    """L(eps_r, sigma) of an ImpedanceDesign as a differentiable torch op:
+    forward runs the checkpointed forward pass, backward the adjoint."""
+
+    @staticmethod
+    def forward(ctx, eps_r, sigma, problem):
+        problem.set_params(eps_r.detach().cpu().numpy(), sigma.detach().cpu().numpy())
+        L = problem.forward(keep=True)
+        ctx.problem = problem
+        return torch.tensor(L, dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, gout):
+        ge, gs = ctx.problem.backward()
+        g = float(gout)
+        return (torch.as_tensor(ge * g), torch.as_tensor(gs * g), None)

@@ -50,6 +50,7 @@ struct FitParams {
   long long cap_nt, cap_step0;
   T* cap;
   int* status;
+  const long long* step_dev;   // optional device step counter
   unsigned nx_mul;   // fast division by Nx: q = umulhi(n, nx_mul) >> nx_shift
   int nx_shift;
 };
@@ -351,6 +352,13 @@ __device__ __forceinline__ void e_lean(T R0, T R1, T R2, T tLx, T tLy, T tLz, T 
     const T c1 = mul(R2, tLx), c2 = mul(R2, tLy);
     cz = add(sub(sub(mul(c1, hx2), mul(c1, hx0)), mul(c2, hy1)), mul(c2, hy0));
   }
+}
+
+// Step index of a kernel launched for step `step`: offset by the device
+// counter when one is attached (replayed step graphs).
+template <typename T>
+__device__ __forceinline__ long long step_index(const FitParams<T>& p, long long step) {
+  return p.step_dev ? step + *p.step_dev : step;
 }
 
 // Gaussian beam current on the line (ixs, iys) at step `step`

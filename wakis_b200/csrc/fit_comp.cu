@@ -62,6 +62,7 @@ k_h_comp(FitParams<double> p, CompState st) {
 
 __global__ void __launch_bounds__(kCompX * kCompY)
 k_e_comp(FitParams<double> p, CompState st, long long step) {
+  step = step_index(p, step);
   const int i = 2 + blockIdx.x * kCompX + threadIdx.x;
   const int j = 2 + blockIdx.y * kCompY + threadIdx.y;
   const int k = 2 + blockIdx.z;
@@ -147,6 +148,7 @@ __global__ void __launch_bounds__(kShellBlock) k_h_comp_shell(FitParams<double> 
 
 __global__ void __launch_bounds__(kShellBlock) k_e_comp_shell(FitParams<double> p, CompState st,
                                                                long long step, ShellGrid g) {
+  step = step_index(p, step);
   Cell c;
   if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
   const int Nx = p.Nx;

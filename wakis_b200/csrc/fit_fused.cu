@@ -308,6 +308,7 @@ k_h_pass(FitParams<T> p, int mat_smem) {
 template <typename T, int KB>
 __global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), KB))
 k_e_pass(FitParams<T> p, long long step, int mat_smem) {
+  step = step_index(p, step);
   extern __shared__ __align__(16) unsigned char pass_smem[];
   const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
   const int i = 2 + blockIdx.x * kPassX + threadIdx.x;
@@ -399,6 +400,7 @@ __global__ void __launch_bounds__(kShellThreads) k_h_shell(FitParams<T> p, Shell
 template <typename T>
 __global__ void __launch_bounds__(kShellThreads) k_e_shell(FitParams<T> p, long long step,
                                                             ShellGrid g) {
+  step = step_index(p, step);
   Cell c;
   if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
   const int Nx = p.Nx;

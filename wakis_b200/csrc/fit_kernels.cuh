@@ -64,9 +64,10 @@ template <typename T>
 __device__ __forceinline__ void capture(const FitParams<T>& p, Cell c, long long n,
                                         long long step, T ez) {
   int a = c.i - p.cap_i0, b = c.j - p.cap_j0;
-  if (a >= 0 && a < p.cap_ni && b >= 0 && b < p.cap_nj) {
+  const long long t = step - p.cap_step0;
+  if (a >= 0 && a < p.cap_ni && b >= 0 && b < p.cap_nj && t >= 0 && t < p.cap_nt) {
     long long w = (long long)a * p.cap_nj + b;
-    p.cap[(w * p.Nz + c.k) * p.cap_nt + (step - p.cap_step0)] = ez;
+    p.cap[(w * p.Nz + c.k) * p.cap_nt + t] = ez;
   }
 }
 
@@ -75,7 +76,10 @@ template <typename T>
 __device__ __forceinline__ T j_in(const FitParams<T>& p, int d, Cell c, long long n,
                                   long long step, T e_old, T sigma) {
   if (d == 2 && c.i == p.ixs && c.j == p.iys) {
-    if (p.line_on) return p.line[(step - p.line_step0) * p.Nz + c.k];
+    if (p.line_on) {
+      const long long t = step - p.line_step0;
+      return (t >= 0 && t < p.line_nsteps) ? p.line[t * p.Nz + c.k] : T(0);
+    }
     if (p.beam_on) return beam_j(p, step, c.k);
   }
   if (p.j_mode == WK_J_SIGMA_E) return mul(sigma, e_old);
@@ -115,6 +119,7 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
   p.cap = (T*)d->cap;
   fast_div_magic((unsigned)d->Nx, &p.nx_mul, &p.nx_shift);
   p.status = d->status;
+  p.step_dev = d->step_dev;
   return p;
 }
 
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(256) k_shell(FitParams<T> p, long long step,
   if (idx >= count) return;
   const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
   const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
-  fused_cell_general(p, step, n, c);
+  fused_cell_general(p, step_index(p, step), n, c);
 }
 
 // Launch the interior (lean) and shell (general) fused kernels of one step

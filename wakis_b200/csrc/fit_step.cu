@@ -286,8 +286,20 @@ static int check_steps(const wk_fit_desc* d, int n_steps, long long step0, const
 extern "C" int wk_fit_step(const wk_fit_desc* d, int n_steps, long long step0, void* stream) {
   int rc = wk_validate_fit(d, "wk_fit_step");
   if (rc) return rc;
-  rc = check_steps(d, n_steps, step0, "wk_fit_step");
-  if (rc) return rc;
+  if (d->step_dev) {
+    // device step counter: the capture / line ranges are checked by the
+    // kernels; only the schedules that read the counter take it
+    const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5;
+    const bool sched = d->dtype == WK_F32C || d->kernel == WK_KERNEL_AUTO ||
+                       d->kernel == WK_KERNEL_TMA || d->kernel == WK_KERNEL_TWOPASS;
+    if (!big || !sched)
+      return wk_fail(WK_E_MODE, "wk_fit_step: step_dev needs the TMA or two-pass schedule "
+                                "and every dimension >= 5");
+    step0 = 0;
+  } else {
+    rc = check_steps(d, n_steps, step0, "wk_fit_step");
+    if (rc) return rc;
+  }
   if (d->E[0] == d->E[1] || d->H[0] == d->H[1])
     return wk_fail(WK_E_MODE, "wk_fit_step: ping-pong buffers must be distinct");
   cudaStream_t st = (cudaStream_t)stream;
@@ -297,6 +309,18 @@ extern "C" int wk_fit_step(const wk_fit_desc* d, int n_steps, long long step0, v
 }
 
 thread_local KernelTimer* g_kernel_timer = nullptr;
+
+namespace {
+__global__ void k_counter_add(long long* ctr, long long inc) { *ctr += inc; }
+}  // namespace
+
+extern "C" int wk_counter_add(long long* ctr, long long inc, void* stream) {
+  if (!ctr) return wk_fail(WK_E_NULL, "wk_counter_add: NULL counter");
+  if ((uintptr_t)ctr % sizeof(long long))
+    return wk_fail(WK_E_ALIGN, "wk_counter_add: counter not 8-byte aligned");
+  k_counter_add<<<1, 1, 0, (cudaStream_t)stream>>>(ctr, inc);
+  return wk_check_launch("wk_counter_add");
+}
 
 extern "C" int wk_fit_step_timed(const wk_fit_desc* d, int n_steps, long long step0,
                                  void* stream, float* ms_interior, int* n_launches) {

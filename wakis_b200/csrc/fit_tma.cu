@@ -96,6 +96,7 @@ __device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int 
 template <typename T>
 __global__ void __launch_bounds__(kTmaThreads, 2)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
+  step = step_index(p, step);
   using Lay = TmaLayout<T>;
   constexpr int HBX = h_box_x<T>();
   constexpr int SE = Lay::eslot / (int)sizeof(T);    // elements per E slot

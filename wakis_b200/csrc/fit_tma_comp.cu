@@ -161,6 +161,7 @@ template <typename IdT>
 __global__ void __launch_bounds__(cThreads, 2)
 k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
            long long step, int KC) {
+  step = step_index(p, step);
   using Lay = CLayout;
   constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4;
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -410,7 +411,9 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
           jt = mul2(sg[d], ev[d]);
         if (d == 2 && cj == p.iys && (p.ixs == ci || p.ixs == ci + 1) &&
             (p.line_on || p.beam_on)) {
-          const double jb = p.line_on ? p.line[(step - p.line_step0) * p.Nz + pl]
+          const long long lt = step - p.line_step0;
+          const double jb = p.line_on ? ((lt >= 0 && lt < p.line_nsteps)
+                                             ? p.line[lt * p.Nz + pl] : 0.0)
                                       : beam_j(p, step, pl);
           if (p.ixs == ci) jt.x = (float)((double)m0[10] * jb);
           else jt.y = (float)((double)m1[10] * jb);

@@ -169,16 +169,22 @@ class STLSolid(Shape):
 
 
 # ------------------------------------------------------------ cell masks ---
-def cell_mask(shape, x, y, z):
-    """(Nx, Ny, Nz) mask: a cell is inside when any of its 8 corners is."""
-    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
-    inside = np.asarray(shape.contains(X, Y, Z), bool)
+def cell_mask(shape, x, y, z, chunk=64):
+    """(Nx, Ny, Nz) mask: a cell is inside when any of its 8 corners is.
+    Corner tests run in slabs of `chunk` cell planes along z, so large grids
+    need no full-size coordinate arrays."""
+    x, y, z = (np.asarray(v, float) for v in (x, y, z))
     nx, ny, nz = len(x) - 1, len(y) - 1, len(z) - 1
     m = np.zeros((nx, ny, nz), bool)
-    for a in (0, 1):
-        for b in (0, 1):
-            for c in (0, 1):
-                m |= inside[a:a + nx, b:b + ny, c:c + nz]
+    for k0 in range(0, nz, chunk):
+        k1 = min(nz, k0 + chunk)
+        X, Y, Z = np.meshgrid(x, y, z[k0:k1 + 1], indexing="ij")
+        inside = np.asarray(shape.contains(X, Y, Z), bool)
+        n = k1 - k0
+        for a in (0, 1):
+            for b in (0, 1):
+                for c in (0, 1):
+                    m[:, :, k0:k1] |= inside[a:a + nx, b:b + ny, c:c + n]
     return m
 
 

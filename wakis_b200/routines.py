@@ -21,6 +21,25 @@ class RoutinesMixin:
     def wakesolve(self, wakelength, wake=None, callback=None, compute_plane="both",
                   plot=False, save_J=False, add_space=None, use_field_monitor=False,
                   field_monitor=None, **kwargs):
+        ws = self._wake_setup(wakelength, wake, compute_plane, add_space)
+        bp, cap, Nt = ws["beam_params"], ws["capture"], ws["Nt"]
+        t0 = time.time()
+        if callback is None and not (use_field_monitor and field_monitor is not None):
+            self._advance(Nt, 0, beam=bp, capture=cap)
+        else:
+            for n in range(Nt):
+                self._advance(1, n, beam=bp, capture=cap)
+                if use_field_monitor and field_monitor is not None:
+                    field_monitor.update(self.E, self.dt)
+                if callback is not None:
+                    callback(self, n * self.dt)
+        torch.cuda.current_stream(self.device).synchronize()
+        self._wake_finish(ws, time.time() - t0)
+
+    def _wake_setup(self, wakelength, wake=None, compute_plane="both", add_space=None):
+        """Everything wakesolve prepares before stepping (upstream
+        routines.py:322-375): test indices, Nt from the wakelength, the beam
+        parameters and the device Ez history with its capture window."""
         if wake is not None:
             self.wake = wake
         if self.wake is None:
@@ -47,34 +66,25 @@ class RoutinesMixin:
         tmax = (wakelength + self.ti * self.v + (z.max() - z.min())) / self.v
         Nt = int(tmax / self.dt)
         self.tmax, self.Nt = tmax, Nt
-
         beam = Beam(q=w.q, sigmaz=w.sigmaz, beta=w.beta, xsource=w.xsource, ysource=w.ysource)
-        bp = beam.params(self)
         hist = torch.zeros((ni * nj, self.Nz, max(Nt, 1)), dtype=self._cap_dtype,
                            device=self.device)
-        cap = (hist, i0, j0, ni, nj)
+        return {"beam": beam, "beam_params": beam.params(self), "hist": hist,
+                "capture": (hist, i0, j0, ni, nj), "Nt": Nt, "longitudinal": longitudinal,
+                "xx": xx, "yy": yy, "compute_plane": compute_plane}
 
-        t0 = time.time()
-        if callback is None and not (use_field_monitor and field_monitor is not None):
-            self._advance(Nt, 0, beam=bp, capture=cap)
-        else:
-            for n in range(Nt):
-                self._advance(1, n, beam=bp, capture=cap)
-                if use_field_monitor and field_monitor is not None:
-                    field_monitor.update(self.E, self.dt)
-                if callback is not None:
-                    callback(self, n * self.dt)
-        torch.cuda.current_stream(self.device).synchronize()
-        self.beam = beam
-
-        w.xf, w.yf, w.zf = self.x[xx], self.y[yy], z[slice(0, self.Nz)]
+    def _wake_finish(self, ws, elapsed=0.0):
+        """Integrate the captured Ez history (upstream routines.py:462-482)."""
+        w, z = self.wake, self.z
+        self.beam = ws["beam"]
+        w.xf, w.yf, w.zf = self.x[ws["xx"]], self.y[ws["yy"]], z[slice(0, self.Nz)]
         w.dx, w.dy, w.dz = self.grid.dx, self.grid.dy, self.grid.dz
-        w.t = np.arange(0, Nt * self.dt, self.dt)
-        w.set_history(hist, n_steps=Nt, one_d=longitudinal)
-        w.solve(compute_plane=compute_plane)
+        w.t = np.arange(0, ws["Nt"] * self.dt, self.dt)
+        w.set_history(ws["hist"], n_steps=ws["Nt"], one_d=ws["longitudinal"])
+        w.solve(compute_plane=ws["compute_plane"])
         self.logger.wakeSolver = w.logger.wakeSolver
-        self.logger.wakeSolver["wakelength"] = wakelength
-        self.logger.wakeSolver["simulationTime"] = time.time() - t0
+        self.logger.wakeSolver["wakelength"] = w.wakelength
+        self.logger.wakeSolver["simulationTime"] = elapsed
         if getattr(w, "save", False):
             self.logger.save_logs(w.folder)
 

@@ -246,11 +246,15 @@ class SolverFIT3D(RoutinesMixin):
             step0, n_steps = step0 + 1, n_steps - 1
         self._launch(n_steps, step0, beam, capture, split, line, timing)
 
-    def _launch(self, n_steps, step0, beam, capture, split, line, timing=None):
+    def _step_desc(self, beam=None, capture=None, line=None):
+        """The step descriptor with the fused beam (Beam.params tuple), the
+        host line current (buffer, step0, ixs, iys) and the Ez window capture
+        (buffer, i0, j0, ni, nj[, step0]) filled in."""
         if self.precision == "fp32c" and self._j_state == _J_ARRAY:
             raise RuntimeError("precision='fp32c' does not take a stored J array; "
                                "use the fused beam / line source")
         d = self._sync_desc()
+        d.step_dev = None
         if beam is not None:
             d.beam_on = 1
             (d.ixs, d.iys, d.b_qv, d.b_v, d.b_s0, d.b_c0, d.b_two_sig2,
@@ -274,6 +278,10 @@ class SolverFIT3D(RoutinesMixin):
                 raise ValueError("capture buffer must be a contiguous (ni*nj, Nz, nt) tensor")
         else:
             d.cap_on = 0
+        return d
+
+    def _launch(self, n_steps, step0, beam, capture, split, line, timing=None):
+        d = self._step_desc(beam, capture, line)
         if split:
             rc = self._lib.wk_fit_step_split(d, n_steps, step0, self._stream())
             _native.check(rc, "wk_fit_step_split")
@@ -390,6 +398,9 @@ class SolverFIT3D(RoutinesMixin):
     def reset_fields(self):
         for b in self._E + self._H:
             b.zero_()
+        if self.precision == "fp32c":
+            for b in self._Ec + self._Hc:
+                b.zero_()
         self._J.zero_()
         self._j_state = _J_ZERO
         self._j_line = None

@@ -13,6 +13,10 @@ of their corners is inside the cavity or the pipe.
   ends; bunch sigma_z = 5 mm, beta = 1, wakelength 5 m.  The conductive
   background clamps dt to the relaxation time eps_0/sigma = 8.85e-16 s, as
   upstream does (wakis/solverFIT3D.py:301-310).
+* ``precision_448`` 448x448x896 cells (180 M), the cavity_40 geometry and
+  boundaries plus a dielectric cube insert (eps_r = 4, sigma = 10 S/m, 20 mm
+  side, centred at x = +5 mm); sigma_z = 10 mm, beta = 1, wakelength 3 m.
+  The FP32-compensated state is compared with FP64 on this grid.
 """
 
 import numpy as np
@@ -40,6 +44,12 @@ def spec(name):
                     wake=dict(q=1e-9, sigmaz=5e-3, beta=1.0, xsource=0.0, ysource=0.0,
                               xtest=0.0, ytest=0.0),
                     wakelength=5.0)
+    if name == "precision_448":
+        sp = spec("cavity_40")
+        sp.update(shape=(448, 448, 896), wakelength=3.0,
+                  insert=dict(box=(-0.005, 0.015, -0.010, 0.010, -0.010, 0.010),
+                              material=[4.0, 1.0, 10.0]))
+        return sp
     raise KeyError(name)
 
 
@@ -56,7 +66,56 @@ def build_b200(name, dtype=np.float64, shape=None, precision=None):
     shp = shape or sp["shape"]
     g = GridFIT3D(*BOUNDS, *shp, verbose=0)
     g.add_solid("cavity", cavity_mask(g.x, g.y, g.z), "vacuum")
+    if "insert" in sp:
+        ins = sp["insert"]
+        g.add_solid("insert", geometry.cell_mask(geometry.Box(*ins["box"], tol=1e-12),
+                                                 g.x, g.y, g.z), ins["material"])
     w = WakeSolver(save=False, verbose=0, **sp["wake"])
     s = SolverFIT3D(g, w, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
                     dtype=dtype, n_pml=sp["n_pml"], verbose=0, precision=precision)
     return g, w, s
+
+
+def precision_compare(name="precision_448", shape=None, wakelength=None, max_steps=None):
+    """Run wakesolve twice on the same grid, FP64 and FP32-compensated, and
+    return the relative errors (max|a-b| / max|b|) of the FP32c results
+    against FP64 together with both stepping rates.  The FP64 solver is
+    released before the FP32c one is built."""
+    import time
+
+    import torch
+
+    sp = spec(name)
+    wl = wakelength if wakelength is not None else sp["wakelength"]
+
+    def rel(a, b):
+        a, b = np.asarray(a), np.asarray(b)
+        den = np.max(np.abs(b)) if b.size else 0.0
+        return float(np.max(np.abs(a - b)) / den) if den else 0.0
+
+    out, res = {}, {}
+    for prec in (None, "fp32c"):
+        t0 = time.perf_counter()
+        g, w, s = build_b200(name, dtype=np.float64, shape=shape, precision=prec)
+        t_build = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        s.wakesolve(wakelength=wl)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        key = "fp32c" if prec else "fp64"
+        res[key] = {n: np.array(getattr(w, n)) for n in ("s", "WP", "WPx", "WPy", "f", "Z",
+                                                        "Zx", "Zy")}
+        out[key] = {"steps": int(s.Nt), "cells": int(s.N), "wakesolve_ms": ms,
+                    "gcell_steps_per_s": s.N * s.Nt / (ms / 1e3) / 1e9, "build_s": t_build}
+        del g, w, s
+        torch.cuda.empty_cache()
+    a, b = res["fp32c"], res["fp64"]
+    out["errors"] = {"WP": rel(a["WP"], b["WP"]), "WPx": rel(a["WPx"], b["WPx"]),
+                     "WPy": rel(a["WPy"], b["WPy"]), "absZ": rel(np.abs(a["Z"]), np.abs(b["Z"])),
+                     "ReZ": rel(a["Z"].real, b["Z"].real), "ImZ": rel(a["Z"].imag, b["Z"].imag),
+                     "absZx": rel(np.abs(a["Zx"]), np.abs(b["Zx"]))}
+    out["wakelength"] = wl
+    return out
