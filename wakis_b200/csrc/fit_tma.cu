@@ -93,8 +93,10 @@ __device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int 
   return a[idx];
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kTmaThreads, 2)
+// SM: the material table fits in shared memory (n_mat <= kMatSmem); the
+// table reads are then shared-memory loads.
+template <typename T, bool SM>
+__global__ void __launch_bounds__(kTmaThreads, sizeof(T) == 8 ? 2 : 3)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
   step = step_index(p, step);
   using Lay = TmaLayout<T>;
@@ -185,11 +187,9 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   else if (tid < kEW + kTY + 1) { const int j = j0 - 1 + tid - kEW; sLy[tid - kEW] = j < Ny ? p.Ly[j] : T(0); }
   else if (tid < kEW + kTY + 1 + kTX) { const int i = i0 + tid - kEW - kTY - 1; stLx[tid - kEW - kTY - 1] = i < Nx ? p.tLx[i] : T(0); }
   else if (tid < kEW + kTY + 1 + kTX + kTY) { const int j = j0 + tid - kEW - kTY - 1 - kTX; stLy[tid - kEW - kTY - 1 - kTX] = j < Ny ? p.tLy[j] : T(0); }
-  const T* mat = p.mat;
-  if (p.n_mat <= kMatSmem) {
+  if (SM)
     for (int q = tid; q < 9 * p.n_mat; q += kTmaThreads) smat[q] = p.mat[q];
-    mat = smat;
-  }
+  const T* mat = SM ? smat : p.mat;
   // ids and metric row of the first plane
   int id[2];
 #pragma unroll
@@ -342,22 +342,22 @@ bool tma_supported(const FitParams<T>& p) {
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
 struct TmaOcc { int sms = 0, per_sm = 0; bool attr = false; };
-static TmaOcc g_occ[2][64];
+static TmaOcc g_occ[2][2][64];
 
-template <typename T>
+template <typename T, bool SM>
 static cudaError_t tma_occupancy(TmaOcc** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][dev];
+  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][dev];
   if (!o.attr) {
     const int smem = TmaLayout<T>::bytes;
-    e = cudaFuncSetAttribute(k_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = cudaFuncSetAttribute(k_tma<T, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T>, kTmaThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM>, kTmaThreads, smem);
     if (e != cudaSuccess) return e;
     if (o.per_sm < 1) o.per_sm = 1;
     o.attr = true;
@@ -374,14 +374,18 @@ cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, i
         !encode_comp<T>(&maps.h[d], p.H_in + d * p.N, p.Nx, p.Ny, p.Nz, h_box_x<T>(), kHBY))
       return cudaErrorInvalidValue;
   }
+  const bool sm_table = p.n_mat <= kMatSmem;
   TmaOcc* occ = nullptr;
-  cudaError_t e = tma_occupancy<T>(&occ);
+  cudaError_t e = sm_table ? tma_occupancy<T, true>(&occ) : tma_occupancy<T, false>(&occ);
   if (e != cudaSuccess) return e;
   const int gx = (p.Nx - 4 + kTX - 1) / kTX, gy = (p.Ny - 4 + kTY - 1) / kTY;
   if (KC <= 0) KC = tma_auto_kc((long long)gx * gy, p.Nz - 4, (long long)occ->sms * occ->per_sm);
   const int gz = (p.Nz - 4 + KC - 1) / KC;
   timer_begin(st);
-  k_tma<T><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
+  if (sm_table)
+    k_tma<T, true><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
+  else
+    k_tma<T, false><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
   timer_end(st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
