@@ -175,8 +175,9 @@ int wk_counter_add(long long* ctr, long long inc, void* stream);
  * the flat 3N ordering of the fields.  All vectors have 3N dtype entries.
  *   wk_adj_h:    lH_out = lH_in + dt * B0^T (ieps .* lE)
  *   wk_adj_e:    lE_out = decay .* lE_in - A^T lH      (decay = 1 - dt ieps sigma m)
- *   wk_adj_grad: for each listed cell c (flat index < N),
- *                gI[q] += sum_comp lE1 (E1 - E0) / ieps,
+ *   wk_adj_grad: for each listed cell c = cells[q] (flat index < N),
+ *                gI[q] += sum_comp lE1 inc[comp*ncell + q]     (inc: FP64,
+ *                         dt (B0 H' - J) of the listed entries),
  *                gS[q] += -dt sum_comp ieps lE1 E0 smask   (when use_sigma)
  *                (double accumulators, one entry per listed cell).
  * lH_in may equal lH_out and lE_in may equal lE_out.
@@ -188,7 +189,7 @@ int wk_adj_e(int dtype, const long long* rowptr, const int* col, const void* val
              long long nrows, const void* lamH, const void* lamE_in, const void* decay,
              void* lamE_out, void* stream);
 int wk_adj_grad(int dtype, const long long* cells, long long ncell, long long N,
-                const void* lamE1, const void* E0, const void* E1, const void* ieps,
+                const void* lamE1, const double* inc, const void* E0, const void* ieps,
                 const void* smask, int use_sigma, double dt, double* gI, double* gS,
                 void* stream);
 

@@ -21,7 +21,9 @@ time step (the relaxation-time clamp of the constructor is not re-evaluated).
   (``wk_adj_h``, ``wk_adj_e``: CSR products with A^T and B0^T assembled on
   the host from the same coefficient tables the step kernels read) run
   backwards with dL/dEz injected at the test line, and ``wk_adj_grad``
-  accumulates the parameter adjoints of every step.
+  accumulates the parameter adjoints of every step (the eps increment
+  dt (B0 H' - J) of the design entries is re-formed in FP64 from the
+  recomputed H', so a float state loses nothing to E' - E cancellation).
 
 ``ImpedanceLoss`` wraps this in a torch.autograd.Function.
 """
@@ -154,6 +156,13 @@ class ImpedanceDesign:
         self.AT = _DevCSR(A.T, self.tdtype, self.dev)
         self.B0T = _DevCSR(B0.T, self.tdtype, self.dev)
         N = s.N
+        nc = len(self.cells_np)
+        # rows of B0 at the design entries (FP64): the E increment there is
+        # formed as dt (B0 H' - J) instead of E' - E
+        rows = np.concatenate([d * N + self.cells_np for d in range(3)])
+        self.rows = torch.as_tensor(rows, device=self.dev)
+        self.Bd = _DevCSR(B0[rows, :], torch.float64, self.dev)
+        self.zd = torch.zeros(3 * nc, dtype=torch.float64, device=self.dev)
         ie, _, sg = s._dense_fields()
         self.ieps0 = ie.array.clone()
         self.sigma0 = sg.array.clone()
@@ -168,6 +177,11 @@ class ImpedanceDesign:
         beam_cells = self.ixs + self.iys * s.Nx + torch.arange(s.Nz, device=self.dev) * s.Nx * s.Ny
         sm[2 * N + beam_cells] = 0
         self.smask = sm
+        ci = self.cells_np % s.Nx
+        cj = (self.cells_np // s.Nx) % s.Ny
+        on = np.flatnonzero((ci == self.ixs) & (cj == self.iys))
+        self.beam_rows = torch.as_tensor(2 * nc + on, device=self.dev)
+        self.beam_k = torch.as_tensor(self.cells_np[on] // (s.Nx * s.Ny), device=self.dev)
         self._ws = None
         self._prepare_loss()
 
@@ -189,6 +203,7 @@ class ImpedanceDesign:
         s.use_conductivity = bool((sgm != 0).any().item()) or s.use_conductivity
         self.ieps = f_ie.array.to(self.tdtype).contiguous()
         self.sig = f_sg.array.to(self.tdtype).contiguous()
+        self.sig_d = self.sig.double()[self.rows]
         self.eps_r, self.sigma = er, sg
 
     # ---------------------------------------------------------------- loss
@@ -298,18 +313,34 @@ class ImpedanceDesign:
         ptr = lambda t: ctypes.c_void_p(t.data_ptr())
         bp = self._ws["beam_params"]
         starts = sorted(self.ckpt)
+        from .sources import beam_line_values
         for a in reversed(starts):
             b = min(a + self.segment, self.n_steps)
             self._restore(a)
             Es = [self._live()[0].clone()]
+            incs = []
             for n in range(a, b):
                 s._advance(1, n, beam=bp)
-                Es.append(self._live()[0].clone())
+                E1, H1 = self._live()
+                Es.append(E1.clone())
+                # dt (B0 H' - J) at the design entries, FP64
+                bh = torch.empty_like(self.zd)
+                Hd = H1.double().contiguous()
+                _native.check(lib.wk_adj_e(
+                    _native.WK_F64, ptr(self.Bd.rowptr), ptr(self.Bd.col), ptr(self.Bd.val),
+                    self.Bd.n, ptr(Hd), ptr(self.zd), ptr(self.zd), ptr(bh),
+                    ctypes.c_void_p(st)), "wk_adj_e")
+                J = (self.sig_d * Es[n - a].double()[self.rows] if (cond and n >= 1)
+                     else torch.zeros_like(self.zd))
+                if len(self.beam_rows):
+                    jb = beam_line_values(s, bp, n).double()
+                    J[self.beam_rows] = jb[self.beam_k]
+                incs.append((dt * (-bh - J)).contiguous())
             for n in range(b - 1, a - 1, -1):
                 use_sig = int(cond and n >= 1)
                 _native.check(lib.wk_adj_grad(
-                    self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(Es[n - a]),
-                    ptr(Es[n + 1 - a]), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
+                    self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(incs[n - a]),
+                    ptr(Es[n - a]), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
                     ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
                 _native.check(lib.wk_adj_h(
                     self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),

@@ -96,6 +96,9 @@ class BatchedWakeSolve:
             ws = s._wake_setup(wl, compute_plane=self.compute_plane)
             if ws["Nt"] != self.n_steps:
                 raise RuntimeError(f"step count {ws['Nt']} != {self.n_steps}")
+            if wl <= -s.wake.ti * s.wake.v:
+                raise ValueError(f"{self.n_steps} steps do not reach past the domain "
+                                 f"(wakelength {wl:.4g} m): no wake samples")
             states.append(ws)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()

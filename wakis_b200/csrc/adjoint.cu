@@ -10,8 +10,10 @@
 //   lH = lH' + dt B0^T (ieps lE')                        (wk_adj_h)
 //   lE = (1 - dt ieps sigma m) lE' - A^T lH  (+ source)  (wk_adj_e)
 // (m = 1 where J = sigma E holds), and the parameter adjoints of step n are
-//   d/d ieps_c  += sum_comp lE' (E' - E) / ieps          (wk_adj_grad)
-//   d/d sigma_c += -dt sum_comp ieps lE' E m.
+//   d/d ieps_c  += sum_comp lE' dt (B0 H' - J)             (wk_adj_grad)
+//   d/d sigma_c += -dt sum_comp ieps lE' E m,
+// the increment dt (B0 H' - J) of the design entries being formed in FP64
+// by the caller (no cancellation of E' - E in a float state).
 // A^T and B0^T are CSR matrices assembled on the host from the same
 // coefficient tables the step kernels read (one thread per row; ~4 entries
 // per row), in the state dtype.
@@ -54,9 +56,9 @@ k_adj_e(const long long* __restrict__ rowptr, const int* __restrict__ col,
 template <typename T>
 __global__ void __launch_bounds__(kAdjThreads)
 k_adj_grad(const long long* __restrict__ cells, long long ncell, long long N,
-           const T* __restrict__ lamE1, const T* __restrict__ E0, const T* __restrict__ E1,
-           const T* __restrict__ ieps, const T* __restrict__ smask, int use_sigma, double dt,
-           double* gI, double* gS) {
+           const T* __restrict__ lamE1, const double* __restrict__ inc,
+           const T* __restrict__ E0, const T* __restrict__ ieps, const T* __restrict__ smask,
+           int use_sigma, double dt, double* gI, double* gS) {
   const long long q = blockIdx.x * (long long)kAdjThreads + threadIdx.x;
   if (q >= ncell) return;
   const long long n = cells[q];
@@ -64,9 +66,9 @@ k_adj_grad(const long long* __restrict__ cells, long long ncell, long long N,
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const long long x = d * N + n;
-    const double l = (double)lamE1[x], ie = (double)ieps[x];
-    if (ie != 0.0) gi += l * ((double)E1[x] - (double)E0[x]) / ie;
-    if (use_sigma) gs -= dt * ie * l * (double)E0[x] * (double)smask[x];
+    const double l = (double)lamE1[x];
+    gi += l * inc[d * ncell + q];
+    if (use_sigma) gs -= dt * (double)ieps[x] * l * (double)E0[x] * (double)smask[x];
   }
   gI[q] += gi;
   gS[q] += gs;
@@ -124,22 +126,22 @@ extern "C" int wk_adj_e(int dtype, const long long* rowptr, const int* col, cons
 }
 
 extern "C" int wk_adj_grad(int dtype, const long long* cells, long long ncell, long long N,
-                           const void* lamE1, const void* E0, const void* E1, const void* ieps,
-                           const void* smask, int use_sigma, double dt, double* gI, double* gS,
-                           void* stream) {
+                           const void* lamE1, const double* inc, const void* E0,
+                           const void* ieps, const void* smask, int use_sigma, double dt,
+                           double* gI, double* gS, void* stream) {
   int rc = check_common(dtype, cells, lamE1, ncell, "wk_adj_grad");
   if (rc) return rc;
-  if (!E0 || !E1 || !ieps || !smask || !gI || !gS)
+  if (!inc || !E0 || !ieps || !smask || !gI || !gS)
     return wk_fail(WK_E_NULL, "wk_adj_grad: NULL pointer");
   if (ncell == 0) return WK_OK;
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == WK_F64)
     k_adj_grad<double><<<blocks(ncell), kAdjThreads, 0, st>>>(
-        cells, ncell, N, (const double*)lamE1, (const double*)E0, (const double*)E1,
-        (const double*)ieps, (const double*)smask, use_sigma, dt, gI, gS);
+        cells, ncell, N, (const double*)lamE1, inc, (const double*)E0, (const double*)ieps,
+        (const double*)smask, use_sigma, dt, gI, gS);
   else
     k_adj_grad<float><<<blocks(ncell), kAdjThreads, 0, st>>>(
-        cells, ncell, N, (const float*)lamE1, (const float*)E0, (const float*)E1,
-        (const float*)ieps, (const float*)smask, use_sigma, dt, gI, gS);
+        cells, ncell, N, (const float*)lamE1, inc, (const float*)E0, (const float*)ieps,
+        (const float*)smask, use_sigma, dt, gI, gS);
   return wk_check_launch("wk_adj_grad");
 }
