@@ -193,6 +193,16 @@ int wk_adj_grad(int dtype, const long long* cells, long long ncell, long long N,
                 const void* smask, int use_sigma, double dt, double* gI, double* gS,
                 void* stream);
 
+/*
+ * Frequency-domain monitor update: for f < nf and d < 3,
+ * acc[f][d][n] += E_d[n] * phases[f] (complex double, interleaved re/im,
+ * acc laid out [nf][3][N] in the flat field order).  Replaces the loop of
+ * FieldMonitor.update (wakis/field_monitors.py:60-107); the caller forms
+ * phases[f] = exp(-2j pi f_f t).  nf <= 64, acc 16-byte aligned.
+ */
+int wk_field_monitor(const void* E, int dtype, long long N, const double* phases, int nf,
+                     double* acc, void* stream);
+
 /* ABI version (WK_ABI_VERSION). */
 int wk_version(void);
 

@@ -97,3 +97,27 @@ def wake_mask(case, x, y, z):
             for c in (0, 1):
                 m |= inside[a:a + m.shape[0], b:b + m.shape[1], c:c + m.shape[2]]
     return m
+
+
+# emsolve with each hard source of upstream sources.py on a small vacuum box
+# (square transverse grid: WavePacket builds its profile on meshgrid(x, y))
+SOURCE_BOUNDS = (-0.01, 0.01, -0.01, 0.01, -0.015, 0.015)
+SOURCE_CASES = [
+    dict(kind="PlaneWave", kw=dict(zs=0, f=8e9, nodes=1), shape=(16, 16, 24),
+         bc_low=["periodic", "periodic", "pec"], bc_high=["periodic", "periodic", "pml"], Nt=40),
+    dict(kind="WavePacket", kw=dict(zs=0, sigmaz=0.004, sigmaxy=0.004, wavelength=0.01),
+         shape=(16, 16, 24), bc_low=["pec", "pec", "pec"], bc_high=["pec", "pec", "pml"],
+         Nt=40),
+    dict(kind="Dipole", kw=dict(field="Ez", nodes=5), shape=(16, 16, 24),
+         bc_low=["pec"] * 3, bc_high=["pec"] * 3, Nt=30),
+    dict(kind="Dipole", kw=dict(field="H", component="y", f=6e9, xs=4, ys=5, zs=7,
+                                amplitude=2.0, phase=0.3),
+         shape=(16, 16, 24), bc_low=["pec"] * 3, bc_high=["pmc", "pec", "pml"], Nt=30),
+    dict(kind="Pulse", kw=dict(field="Ez", shape="Harris", L=0.006), shape=(16, 16, 24),
+         bc_low=["pec"] * 3, bc_high=["pec"] * 3, Nt=60),
+    dict(kind="Pulse", kw=dict(field="Jz", shape="Gaussian", L=0.004, amplitude=1e3),
+         shape=(16, 16, 24), bc_low=["pec", "pec", "pml"], bc_high=["pec", "pec", "pml"], Nt=60),
+    dict(kind="Pulse", kw=dict(field="E", component="x", shape="Rectangular", L=0.002,
+                               xs=slice(4, 9), ys=7, zs=10),
+         shape=(16, 16, 24), bc_low=["pec"] * 3, bc_high=["pec"] * 3, Nt=40),
+]

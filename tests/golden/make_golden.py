@@ -17,6 +17,8 @@ Outputs (all small, committed):
   beam driving Jz.
 * ``wake_cases.npz``  WP, WP_3d, WPx, WPy, Z, Zx, Zy, f, s of upstream
   ``wakesolve`` + ``WakeSolver.solve`` on small cavities.
+* ``source_cases.npz``  E, H, J after upstream ``emsolve`` driven by each
+  hard source (PlaneWave, WavePacket, Dipole, Pulse) on a small vacuum box.
 
 The case definitions live in ``tests/cases.py`` so that the tests rebuild the
 same inputs without the upstream package.
@@ -128,8 +130,29 @@ def wake_cases(wakis):
     print("wake_cases.npz:", len(cases.WAKE_CASES), "cases")
 
 
+def source_cases(wakis):
+    out = {}
+    for idx, c in enumerate(cases.SOURCE_CASES):
+        g = wakis.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)
+        s = wakis.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                              bg="vacuum", use_stl=False, use_sibc=False)
+        src = getattr(wakis.sources, c["kind"])(**c["kw"])
+        s.emsolve(c["Nt"], source=src)
+        for f in "EHJ":
+            out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+        out[f"c{idx}_dt"] = np.array(s.dt)
+    np.savez_compressed(os.path.join(HERE, "source_cases.npz"), **out)
+    print("source_cases.npz:", len(cases.SOURCE_CASES), "cases")
+
+
 if __name__ == "__main__":
     wakis = refshim.install()
-    upstream_test001()
-    step_cases(wakis)
-    wake_cases(wakis)
+    only = sys.argv[1:]
+    if not only or "test001" in only:
+        upstream_test001()
+    if not only or "step" in only:
+        step_cases(wakis)
+    if not only or "wake" in only:
+        wake_cases(wakis)
+    if not only or "source" in only:
+        source_cases(wakis)

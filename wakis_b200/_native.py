@@ -56,6 +56,7 @@ _SIGS = {
                                ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i)]),
     "wk_sigma_e": (_i, [ctypes.POINTER(FitDesc), _vp, _vp]),
     "wk_counter_add": (_i, [_vp, _ll, _vp]),
+    "wk_field_monitor": (_i, [_vp, _i, _ll, _vp, _i, _vp, _vp]),
     "wk_adj_h": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, ctypes.c_double, _vp, _vp, _vp]),
     "wk_adj_e": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp]),
     "wk_adj_grad": (_i, [_i, _vp, _ll, _ll, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_double,

@@ -31,6 +31,8 @@ def default_device(use_gpu=True):
 class Field:
     """3-vector field on an (Nx, Ny, Nz) grid backed by a flat torch tensor."""
 
+    xp = torch   # array module of the storage (upstream: numpy or cupy)
+
     def __init__(self, Nx, Ny, Nz, dtype=float, use_ones=False, use_gpu=True, device=None,
                  array=None):
         self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)

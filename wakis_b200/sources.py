@@ -1,14 +1,20 @@
 """Time-dependent sources (upstream wakis/sources.py).
 
-``Beam`` keeps upstream's ``update(solver, t)`` contract (sources.py:76-110):
-called by a user loop it writes the Gaussian line current into ``solver.J``.
-Inside ``wakesolve`` the same current is computed by the step kernel
-itself (``beam_params``), so no per-step host work or transfer is needed.
+Every source keeps upstream's duck-typed ``update(solver, t)`` contract
+(sources.py:11-14): ``emsolve`` calls it before each step and it writes its
+values into ``solver.E``, ``solver.H`` or ``solver.J`` (device fields).
+``Beam`` (sources.py:76-110) is also computed by the step kernel itself
+inside ``wakesolve`` (``beam_params``), so no per-step host work or transfer
+is needed there.  ``PlaneWave``, ``WavePacket``, ``Dipole`` and ``Pulse``
+(sources.py:142-762) are hard sources on a slice or a point; their values
+are formed on the host with the same expressions as upstream and written
+with one device copy per field and step.
 """
 
 import numpy as np
 import torch
 from scipy.constants import c as c_light
+from scipy.constants import mu_0
 
 
 class Beam:
@@ -71,3 +77,171 @@ def beam_line_values(solver, beam_params, step):
     prof = c0 * np.exp(-((s - s0) ** 2) / two_sig2)
     vals = (qv * prof / bdx / bdy).astype(solver.dtype)
     return torch.as_tensor(vals, device=solver.device)
+
+
+class PlaneWave:
+    """Plane wave moving in +z, imposed on the plane zs over (xs, ys): Hy and
+    Ex follow cos(w t + phase) until tmax = nodes / f, then 0
+    (upstream sources.py:142-283)."""
+
+    def __init__(self, xs=None, ys=None, zs=0, nodes=None, f=None, amplitude=1.0, beta=1.0,
+                 phase=0):
+        self.nodes, self.beta = nodes, beta
+        self.xs, self.ys, self.zs = xs, ys, zs
+        self.f, self.amplitude, self.phase = f, amplitude, phase
+        self.is_first_update = True
+        self.vp = self.beta * c_light
+        self.w = 2 * np.pi * self.f
+        self.kz = self.w / c_light
+        self.tmax = np.inf if self.nodes is None else self.nodes / self.f
+
+    def update(self, solver, t):
+        if self.is_first_update:
+            self.xs = slice(0, solver.Nx) if self.xs is None else self.xs
+            self.ys = slice(0, solver.Ny) if self.ys is None else self.ys
+            self.is_first_update = False
+        if t <= self.tmax:
+            wave = np.cos(self.w * t + self.phase)
+            solver.H[self.xs, self.ys, self.zs, "y"] = -self.amplitude * wave
+            solver.E[self.xs, self.ys, self.zs, "x"] = (self.amplitude * wave
+                                                        / (self.kz / (mu_0 * self.vp)))
+        else:
+            solver.H[self.xs, self.ys, self.zs, "y"] = 0.0
+            solver.E[self.xs, self.ys, self.zs, "x"] = 0.0
+
+
+class WavePacket:
+    """Gaussian wave packet (transverse sigmaxy, longitudinal sigmaz, delay
+    tinj) imposed on the plane zs: Hy and Ex (upstream sources.py:285-456).
+    The transverse profile is built on meshgrid(x, y) in upstream's default
+    'xy' orientation."""
+
+    def __init__(self, xs=None, ys=None, zs=0, sigmaz=None, sigmaxy=None, tinj=None,
+                 wavelength=None, f=None, amplitude=1.0, beta=1.0, phase=0):
+        self.beta = beta
+        self.xs, self.ys, self.zs = xs, ys, zs
+        self.f, self.wavelength = f, wavelength
+        self.sigmaxy, self.sigmaz, self.tinj = sigmaxy, sigmaz, tinj
+        self.amplitude, self.phase = amplitude, phase
+        if self.f is None:
+            self.f = c_light / self.wavelength
+        self.w = 2 * np.pi * self.f
+        if self.tinj is None and self.sigmaz is not None:
+            self.tinj = 6 * self.sigmaz
+        self.is_first_update = True
+
+    def update(self, solver, t):
+        if self.is_first_update:
+            self.xs = slice(0, solver.Nx) if self.xs is None else self.xs
+            self.ys = slice(0, solver.Ny) if self.ys is None else self.ys
+            if self.sigmaz is None:
+                self.sigmaz = 10 * np.mean(solver.dz)
+            if self.sigmaxy is None:
+                self.sigmaxy = 5 * np.mean([np.mean(solver.dx), np.mean(solver.dy)])
+            if self.tinj is None:
+                self.tinj = 6 * self.sigmaz
+            self.is_first_update = False
+        s0 = solver.z.min() - self.tinj
+        s = solver.z.min() - self.beta * c_light * t
+        X, Y = np.meshgrid(solver.x[self.xs], solver.y[self.ys])
+        gxy = np.exp(-(X ** 2 + Y ** 2) / (2 * self.sigmaxy ** 2))
+        gt = np.exp(-((s - s0) ** 2) / (2 * self.sigmaz ** 2))
+        wave = np.cos(self.w * t + self.phase)
+        solver.H[self.xs, self.ys, self.zs, "y"] = -self.amplitude * wave * gxy * gt
+        solver.E[self.xs, self.ys, self.zs, "x"] = (self.amplitude * mu_0 * c_light * wave
+                                                    * gxy * gt)
+
+
+def _field_of(solver, name):
+    if name == "E":
+        return solver.E
+    if name == "H":
+        return solver.H
+    if name == "J":
+        return solver.J
+    return None
+
+
+class Dipole:
+    """Sinusoidal point (or slice) source amplitude*sin(w t + phase) on one
+    component of E, H or J; f defaults to nodes periods over the z transit
+    time of light (upstream sources.py:458-567)."""
+
+    def __init__(self, field="E", component="z", xs=None, ys=None, zs=None, nodes=10, f=None,
+                 amplitude=1.0, phase=0):
+        self.nodes = nodes
+        self.xs, self.ys, self.zs = xs, ys, zs
+        self.f, self.field, self.component = f, field, component
+        self.amplitude, self.phase = amplitude, phase
+        if len(field) == 2:
+            self.field, self.component = field[0], field[1]
+        self.is_first_update = True
+
+    def update(self, solver, t):
+        if self.is_first_update:
+            self.xs = int(solver.Nx / 2) if self.xs is None else self.xs
+            self.ys = int(solver.Ny / 2) if self.ys is None else self.ys
+            self.zs = int(solver.Nz / 2) if self.zs is None else self.zs
+            if self.f is None:
+                self.f = self.nodes / ((solver.z.max() - solver.z.min()) / c_light)
+            self.w = 2 * np.pi * self.f
+            self.is_first_update = False
+        fld = _field_of(solver, self.field)
+        if fld is None:
+            print(f'Field "{self.field}" not valid, should be "E", "H" or "J"]')
+            return
+        fld[self.xs, self.ys, self.zs, self.component] = (self.amplitude
+                                                          * np.sin(self.w * t + self.phase))
+
+
+class Pulse:
+    """Pulse with a 'Harris', 'Gaussian' or 'Rectangular' time profile of
+    width L (c*t units, default 50 dt) and delay on one component of E, H or
+    J (upstream sources.py:569-762)."""
+
+    def __init__(self, field="E", component="z", xs=None, ys=None, zs=None, shape="Harris",
+                 L=None, amplitude=1.0, delay=0.0):
+        self.xs, self.ys, self.zs = xs, ys, zs
+        self.field, self.component = field, component
+        self.shape, self.L, self.amplitude, self.delay = shape, L, amplitude, delay
+        if len(field) == 2:
+            self.field, self.component = field[0], field[1]
+        shapes = {"harris": self.harris_pulse, "gaussian": self.gaussian_pulse,
+                  "rectangular": self.rectangular_pulse}
+        if shape.lower() in shapes:
+            self.tprofile = shapes[shape.lower()]
+        else:   # upstream prints and leaves the profile unset
+            print('** shape does not, match available types: "Harris", "Gaussian", '
+                  '"Rectangular"')
+        self.is_first_update = True
+
+    def harris_pulse(self, t):
+        t = t * c_light - self.delay
+        harris = lambda u: (10 - 15 * np.cos(2 * np.pi / self.L * u)
+                            + 6 * np.cos(4 * np.pi / self.L * u)
+                            - np.cos(6 * np.pi / self.L * u)) / 32
+        if np.ndim(t) == 0:
+            return harris(t) if t < self.L else 0.0
+        return harris(t)
+
+    def gaussian_pulse(self, t):
+        t = t * c_light - self.delay
+        return np.exp(-((t - 5 * (self.L / 10)) ** 2) / (2 * (self.L / 10) ** 2))
+
+    def rectangular_pulse(self, t):
+        t = t * c_light - self.delay
+        return 1.0 if (t < self.L and t > 0.0) else 0.0
+
+    def update(self, solver, t):
+        if self.is_first_update:
+            self.xs = int(solver.Nx / 2) if self.xs is None else self.xs
+            self.ys = int(solver.Ny / 2) if self.ys is None else self.ys
+            self.zs = int(solver.Nz / 2) if self.zs is None else self.zs
+            if self.L is None:
+                self.L = 50 * solver.dt
+            self.is_first_update = False
+        fld = _field_of(solver, self.field)
+        if fld is None:
+            print(f'Field "{self.field}" not valid, should be "E", "H" or "J"]')
+            return
+        fld[self.xs, self.ys, self.zs, self.component] = self.amplitude * self.tprofile(t)
