@@ -517,7 +517,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"float64": "f64", "float32": "f32", "fp32c": "f32+i8 comp (f64 coef)"}[
+            "dtype": {"float64": "f64", "float32": "f32", "fp32c": "f32+bf16 comp (f64-formed coef)"}[
                 args.dtype], "data": "synthetic",
             "config": {"workload": args.workload, "cells": N, "grid": [s.Nx, s.Ny, s.Nz],
                        "parallelism": f"replicas{ws}" if ws > 1 else "single",
