@@ -94,8 +94,9 @@ __device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int 
 }
 
 // SM: the material table fits in shared memory (n_mat <= kMatSmem); the
-// table reads are then shared-memory loads.
-template <typename T, bool SM>
+// table reads are then shared-memory loads.  JM: the J mode of the launch
+// (WK_J_ZERO, WK_J_SIGMA_E or WK_J_ARRAY), fixed at compile time.
+template <typename T, bool SM, int JM>
 __global__ void __launch_bounds__(kTmaThreads, sizeof(T) == 8 ? 2 : 3)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
   step = step_index(p, step);
@@ -282,13 +283,18 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         Cell cc;
         cc.i = ci[r]; cc.j = cj[r]; cc.k = pl;
         if (p.cap_on) capture(p, cc, n, step, eold[2]);
+        const bool src = (p.line_on || p.beam_on) && cc.i == p.ixs && cc.j == p.iys;
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const T ieps = m0[d], sigma = m0[6 + d];
-          const T jv = j_in(p, d, cc, n, step, eold[d], sigma);
+          // J entering the row (the j_in rules with the mode fixed)
+          T jv = T(0);
+          if (JM == WK_J_SIGMA_E) jv = mul(sigma, eold[d]);
+          if (JM == WK_J_ARRAY) jv = p.J[d * N + n];
+          if (d == 2 && src) jv = j_in(p, d, cc, n, step, eold[d], sigma);
           const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
           p.E_out[d * N + n] = enew;
-          if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
+          if (JM == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
         }
       }
     }
@@ -342,22 +348,24 @@ bool tma_supported(const FitParams<T>& p) {
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
 struct TmaOcc { int sms = 0, per_sm = 0; bool attr = false; };
-static TmaOcc g_occ[2][2][64];
+static TmaOcc g_occ[2][2][3][64];
 
-template <typename T, bool SM>
+template <typename T, bool SM, int JM>
 static cudaError_t tma_occupancy(TmaOcc** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][dev];
+  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][dev];
   if (!o.attr) {
     const int smem = TmaLayout<T>::bytes;
-    e = cudaFuncSetAttribute(k_tma<T, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = cudaFuncSetAttribute(k_tma<T, SM, JM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM>, kTmaThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM>, kTmaThreads,
+                                                      smem);
     if (e != cudaSuccess) return e;
     if (o.per_sm < 1) o.per_sm = 1;
     o.attr = true;
@@ -375,18 +383,27 @@ cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, i
       return cudaErrorInvalidValue;
   }
   const bool sm_table = p.n_mat <= kMatSmem;
-  TmaOcc* occ = nullptr;
-  cudaError_t e = sm_table ? tma_occupancy<T, true>(&occ) : tma_occupancy<T, false>(&occ);
-  if (e != cudaSuccess) return e;
+  const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
   const int gx = (p.Nx - 4 + kTX - 1) / kTX, gy = (p.Ny - 4 + kTY - 1) / kTY;
-  if (KC <= 0) KC = tma_auto_kc((long long)gx * gy, p.Nz - 4, (long long)occ->sms * occ->per_sm);
-  const int gz = (p.Nz - 4 + KC - 1) / KC;
-  timer_begin(st);
-  if (sm_table)
-    k_tma<T, true><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
-  else
-    k_tma<T, false><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
-  timer_end(st);
+  auto go = [&](auto kern, TmaOcc* occ) {
+    if (KC <= 0)
+      KC = tma_auto_kc((long long)gx * gy, p.Nz - 4, (long long)occ->sms * occ->per_sm);
+    const int gz = (p.Nz - 4 + KC - 1) / KC;
+    timer_begin(st);
+    kern<<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
+    timer_end(st);
+  };
+  TmaOcc* occ = nullptr;
+  cudaError_t e;
+#define WK_TMA_CASE(SMV, JMV)                                          \
+  if (sm_table == SMV && jm == JMV) {                                  \
+    e = tma_occupancy<T, SMV, JMV>(&occ);                              \
+    if (e != cudaSuccess) return e;                                    \
+    go(k_tma<T, SMV, JMV>, occ);                                       \
+  }
+  WK_TMA_CASE(true, 0) WK_TMA_CASE(true, 1) WK_TMA_CASE(true, 2)
+  WK_TMA_CASE(false, 0) WK_TMA_CASE(false, 1) WK_TMA_CASE(false, 2)
+#undef WK_TMA_CASE
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // shell: H from the old state, then E from the new H (the interior H
