@@ -157,7 +157,9 @@ __device__ __forceinline__ float row_value(double dt, double f, double g) {
   return (float)((dt * f) * g);
 }
 
-template <typename IdT>
+// IdT: material id type; SIG: the J entering a row is sigma * E (the
+// conductive J mode) rather than zero.
+template <typename IdT, bool SIG>
 __global__ void __launch_bounds__(cThreads, 2)
 k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
            long long step, int KC) {
@@ -407,7 +409,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         float2 jt = zero2;   // dt*ieps*J of the row
-        if (p.j_mode == WK_J_SIGMA_E)
+        if (SIG)
           jt = mul2(sg[d], ev[d]);
         if (d == 2 && cj == p.iys && (p.ixs == ci || p.ixs == ci + 1) &&
             (p.line_on || p.beam_on)) {
@@ -457,8 +459,8 @@ bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int
   return r == CUDA_SUCCESS;
 }
 
-int g_comp_sms[3][64], g_comp_per_sm[3][64];
-bool g_comp_attr[3][64];
+int g_comp_sms[6][64], g_comp_per_sm[6][64];
+bool g_comp_attr[6][64];
 
 }  // namespace
 
@@ -487,22 +489,28 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   const int ib = p.id_bytes == 1 ? 0 : (p.id_bytes == 2 ? 1 : 2);
-  auto kern = ib == 0 ? k_tma_comp<uint8_t> : (ib == 1 ? k_tma_comp<uint16_t> : k_tma_comp<uint32_t>);
-  if (!g_comp_attr[ib][dev]) {
+  const bool sig = p.j_mode == WK_J_SIGMA_E;
+  const int slot = ib * 2 + (sig ? 1 : 0);
+  using K = void (*)(FitParams<double>, CompState, const CompMaps, long long, int);
+  const K kerns[6] = {k_tma_comp<uint8_t, false>,  k_tma_comp<uint8_t, true>,
+                      k_tma_comp<uint16_t, false>, k_tma_comp<uint16_t, true>,
+                      k_tma_comp<uint32_t, false>, k_tma_comp<uint32_t, true>};
+  const K kern = kerns[slot];
+  if (!g_comp_attr[slot][dev]) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CLayout::bytes);
     if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&g_comp_sms[ib][dev], cudaDevAttrMultiProcessorCount, dev);
+    e = cudaDeviceGetAttribute(&g_comp_sms[slot][dev], cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_comp_per_sm[ib][dev], kern, cThreads,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_comp_per_sm[slot][dev], kern, cThreads,
                                                       CLayout::bytes);
     if (e != cudaSuccess) return e;
-    if (g_comp_per_sm[ib][dev] < 1) g_comp_per_sm[ib][dev] = 1;
-    g_comp_attr[ib][dev] = true;
+    if (g_comp_per_sm[slot][dev] < 1) g_comp_per_sm[slot][dev] = 1;
+    g_comp_attr[slot][dev] = true;
   }
   const int gx = (p.Nx - 4 + cTX - 1) / cTX, gy = (p.Ny - 4 + cTY - 1) / cTY;
   if (KC <= 0)
     KC = tma_auto_kc((long long)gx * gy, p.Nz - 4,
-                     (long long)g_comp_sms[ib][dev] * g_comp_per_sm[ib][dev]);
+                     (long long)g_comp_sms[slot][dev] * g_comp_per_sm[slot][dev]);
   const int gz = (p.Nz - 4 + KC - 1) / KC;
   timer_begin(st);
   kern<<<dim3(gx, gy, gz), cThreads, CLayout::bytes, st>>>(p, cs, maps, step, KC);
