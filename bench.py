@@ -468,17 +468,23 @@ def main():
     s._advance(args.steps, args.warmup + args.steps, beam=bp, capture=cap, timing=timing)
     ms_int = sum(t[0] for t in timing)
     n_int = sum(t[1] for t in timing)
-    # kernels launched per step: TMA 1 interior + 2 shell launches,
-    # two-pass and FP32c 2 interior + 2 shell launches; the other schedules
-    # launch a fixed set
+    # kernels launched per step: TMA 1 (every face PEC-masked) or 1 interior
+    # + 2 shell launches, two-pass 2 interior + 2 shell launches; the other
+    # schedules launch a fixed set
     planes = s.tile[1] if s.tile[1] > 0 else max(
         2, (80 * 1024 * 1024) // (9 * np.dtype(dtype).itemsize * s.Nx * s.Ny))
     nslab = -(-s.Nz // planes)
     fixed = {"split": 4, "fused": 2, "slab": 2 * nslab, "march": 1, "cell": 1}
     n_per = n_int // max(args.steps, 1)
-    per_step = fixed.get(args.kernel, {1: 3, 2: 4}.get(n_per, 2 * n_per))
+    # the TMA schedule needs no shell launch when every face is PEC-masked
+    pec_faces = all(b.lower() in ("pec", "electric", "pml") for b in s.bc_low + s.bc_high)
+    tma_per_step = 1 if (pec_faces and args.dtype != "fp32c") else 3
+    per_step = fixed.get(args.kernel, {1: tma_per_step, 2: 4}.get(n_per, 2 * n_per))
     launches = args.steps * per_step  # step kernels launched in the timed region
-    interior = (s.Nx - 4) * (s.Ny - 4) * (s.Nz - 4)
+    # cells the interior kernel updates: the whole grid for the full-domain
+    # TMA kernel, else the interior without the two-cell shell
+    interior = (N if (per_step == 1 and n_per == 1)
+                else (s.Nx - 4) * (s.Ny - 4) * (s.Nz - 4))
     schedule = {1: "tma", 2: "twopass"}.get(n_int // max(args.steps, 1), args.kernel)
 
     # end to end through the public API: per-step H2D line current, D2H window
@@ -509,7 +515,7 @@ def main():
             achieved = bpc * interior * args.steps / (ms_int / 1e3) / 1e9
             kernel_note = (f"interior kernel(s) of the {schedule} schedule: {n_int} launches, "
                            f"{ms_int / args.steps:.4f} ms per step, {bpc} B x {interior} "
-                           f"interior cells per step")
+                           f"cells per step")
         else:
             achieved = step_gbs
             kernel_note = "whole step (no separate interior kernel)"

@@ -59,10 +59,23 @@ struct TmaMaps {
   CUtensorMap h[3];
 };
 
-template <typename T>
+// Box geometry.  The interior variant loads E on x in [i0-2, i0+66) and H
+// on [i0-2, i0+64) (i0 = 2 + 64 bx); the full-domain variant (FULL, tiles
+// from i0 = 64 bx) starts both boxes at i0-4 so that the x offset stays
+// 16-byte aligned for float and double: E 72 wide, H 68 wide.
+template <typename T, bool FULL>
+struct TmaGeom {
+  static constexpr int ebx = FULL ? kTX + 8 : kBX;            // E box width
+  static constexpr int hbx = FULL ? kTX + 4 : h_box_x<T>();   // H box width
+  static constexpr int xo = FULL ? 3 : 1;                     // box x of ext column 0
+  static constexpr int xs_off = FULL ? 4 : 2;                 // box start = i0 - xs_off
+};
+
+template <typename T, bool FULL>
 struct TmaLayout {
-  static constexpr int eslot = round128(kBX * kBY * (int)sizeof(T));          // per comp
-  static constexpr int hslot = round128(h_box_x<T>() * kHBY * (int)sizeof(T));
+  using G = TmaGeom<T, FULL>;
+  static constexpr int eslot = round128(G::ebx * kBY * (int)sizeof(T));        // per comp
+  static constexpr int hslot = round128(G::hbx * kHBY * (int)sizeof(T));
   static constexpr int e_off = 0;
   static constexpr int h_off = e_off + kES * 3 * eslot;
   static constexpr int hs_off = h_off + kHS * 3 * hslot;
@@ -80,14 +93,17 @@ __device__ __forceinline__ int ext_of_halo(int h) { return h < kEW ? h : (h - kE
 
 // Per-plane metric row of plane q: [0,9) iAx(j0-1..j0+7), [9,74) iAy(i0-1..i0+63),
 // [74,82) itAx(j0..j0+7), [82,146) itAy(i0..i0+63), 146 Lz, 147 tLz.
+// Entries outside the grid (index < 0 or beyond the last cell, plane q
+// outside [0, Nz)) read as 0.
 template <typename T>
 __device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int i0, int j0) {
+  if (q < 0 || q >= p.Nz) return T(0);
   int idx;
   const T* a;
-  if (r < 9) { idx = j0 - 1 + r; a = p.iAx; if (idx >= p.Ny) return T(0); idx += q * p.Ny; }
-  else if (r < 74) { idx = i0 - 10 + r; a = p.iAy; if (idx >= p.Nx) return T(0); idx += q * p.Nx; }
-  else if (r < 82) { idx = j0 - 74 + r; a = p.itAx; if (idx >= p.Ny) return T(0); idx += q * p.Ny; }
-  else if (r < 146) { idx = i0 - 82 + r; a = p.itAy; if (idx >= p.Nx) return T(0); idx += q * p.Nx; }
+  if (r < 9) { idx = j0 - 1 + r; a = p.iAx; if (idx < 0 || idx >= p.Ny) return T(0); idx += q * p.Ny; }
+  else if (r < 74) { idx = i0 - 10 + r; a = p.iAy; if (idx < 0 || idx >= p.Nx) return T(0); idx += q * p.Nx; }
+  else if (r < 82) { idx = j0 - 74 + r; a = p.itAx; if (idx < 0 || idx >= p.Ny) return T(0); idx += q * p.Ny; }
+  else if (r < 146) { idx = i0 - 82 + r; a = p.itAy; if (idx < 0 || idx >= p.Nx) return T(0); idx += q * p.Nx; }
   else if (r == 146) return p.Lz[q];
   else return p.tLz[q];
   return a[idx];
@@ -96,12 +112,24 @@ __device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int 
 // SM: the material table fits in shared memory (n_mat <= kMatSmem); the
 // table reads are then shared-memory loads.  JM: the J mode of the launch
 // (WK_J_ZERO, WK_J_SIGMA_E or WK_J_ARRAY), fixed at compile time.
-template <typename T, bool SM, int JM>
+// FULL: every face of the grid carries the PEC column mask (pec, electric or
+// pml on all six faces, no PMC).  The tiles then cover the whole grid and the
+// cells next to a face use the same single-coefficient rows with the masked
+// terms set to zero: an E entry tangential to a face it lies on enters no H
+// row, and an E row tangential to its face gets no curl.  The neighbours that
+// the flat-offset operators reach by wrapping (i+1 past Nx-1, j+1 past Ny-1)
+// are tangential to the opposite face, so every wrapped term is masked and
+// the grid needs no shell launch.  Warps with no cell on or next to a face
+// take the unmasked rows.
+template <typename T, bool SM, int JM, bool FULL>
 __global__ void __launch_bounds__(kTmaThreads, sizeof(T) == 8 ? 2 : 3)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
   step = step_index(p, step);
-  using Lay = TmaLayout<T>;
-  constexpr int HBX = h_box_x<T>();
+  using Lay = TmaLayout<T, FULL>;
+  using G = TmaGeom<T, FULL>;
+  constexpr int HBX = G::hbx;
+  constexpr int EBX = G::ebx;
+  constexpr int XO = G::xo;
   constexpr int SE = Lay::eslot / (int)sizeof(T);    // elements per E slot
   constexpr int SH = Lay::hslot / (int)sizeof(T);    // elements per H slot
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -119,12 +147,13 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 
   const int Nx = p.Nx, Ny = p.Ny;
   const long long N = p.N, NxNy = p.NxNy;
-  const int i0 = 2 + blockIdx.x * kTX, j0 = 2 + blockIdx.y * kTY;
-  const int k0 = 2 + blockIdx.z * KC, k1 = min(k0 + KC, p.Nz - 2);
-  const int xs = i0 - 2, ys = j0 - 1;
+  const int Nz = p.Nz;
+  const int i0 = (FULL ? 0 : 2) + blockIdx.x * kTX, j0 = (FULL ? 0 : 2) + blockIdx.y * kTY;
+  const int k0 = (FULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, FULL ? Nz : Nz - 2);
+  const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x;
   const int pstart = k0 - 1;
-  const uint32_t e_bytes = (uint32_t)(3 * kBX * kBY * sizeof(T));
+  const uint32_t e_bytes = (uint32_t)(3 * EBX * kBY * sizeof(T));
   const uint32_t h_bytes = (uint32_t)(3 * HBX * kHBY * sizeof(T));
 
   if (tid == 0) {
@@ -172,9 +201,23 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     ci[r] = i0 - 1 + ext[r] % kEW;
     cj[r] = j0 - 1 + ext[r] / kEW;
     const bool own = r == 0 || two || halo;
-    hval[r] = own && ci[r] <= Nx - 3 && cj[r] <= Ny - 3;
+    hval[r] = FULL ? (own && ci[r] >= 0 && ci[r] <= Nx - 1 && cj[r] >= 0 && cj[r] <= Ny - 1)
+                   : (own && ci[r] <= Nx - 3 && cj[r] <= Ny - 3);
     eval[r] = (r == 0 || two) && hval[r];
   }
+  // face flags of the owned cells (FULL): at the cell, and of the +x / +y
+  // neighbour (a wrapped neighbour counts as on the face)
+  bool xf0[2], xf1[2], yf0[2], yf1[2];
+  bool nearface = false;
+#pragma unroll
+  for (int r = 0; r < 2; r++) {
+    xf0[r] = ci[r] == 0 || ci[r] == Nx - 1;
+    xf1[r] = ci[r] + 1 >= Nx - 1;
+    yf0[r] = cj[r] == 0 || cj[r] == Ny - 1;
+    yf1[r] = cj[r] + 1 >= Ny - 1;
+    if (hval[r]) nearface |= xf0[r] || xf1[r] || yf0[r] || yf1[r];
+  }
+  const bool warp_face = FULL && __any_sync(0xffffffffu, nearface);
   const bool desc = p.h_desc != 0;
   // plane-invariant metrics
   T iAz[2], itAz[2];
@@ -184,8 +227,8 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     iAz[r] = hval[r] ? p.iAz[m] : T(0);
     itAz[r] = eval[r] ? p.itAz[m] : T(0);
   }
-  if (tid < kEW) sLx[tid] = i0 - 1 + tid < Nx ? p.Lx[i0 - 1 + tid] : T(0);
-  else if (tid < kEW + kTY + 1) { const int j = j0 - 1 + tid - kEW; sLy[tid - kEW] = j < Ny ? p.Ly[j] : T(0); }
+  if (tid < kEW) sLx[tid] = (i0 - 1 + tid >= 0 && i0 - 1 + tid < Nx) ? p.Lx[i0 - 1 + tid] : T(0);
+  else if (tid < kEW + kTY + 1) { const int j = j0 - 1 + tid - kEW; sLy[tid - kEW] = (j >= 0 && j < Ny) ? p.Ly[j] : T(0); }
   else if (tid < kEW + kTY + 1 + kTX) { const int i = i0 + tid - kEW - kTY - 1; stLx[tid - kEW - kTY - 1] = i < Nx ? p.tLx[i] : T(0); }
   else if (tid < kEW + kTY + 1 + kTX + kTY) { const int j = j0 + tid - kEW - kTY - 1 - kTX; stLy[tid - kEW - kTY - 1 - kTX] = j < Ny ? p.tLy[j] : T(0); }
   if (SM)
@@ -195,7 +238,9 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   int id[2];
 #pragma unroll
   for (int r = 0; r < 2; r++)
-    id[r] = hval[r] ? load_id(p.mat_id, p.id_bytes, ci[r] + (long long)cj[r] * Nx + (long long)pstart * NxNy) : 0;
+    id[r] = (hval[r] && pstart >= 0)
+                ? load_id(p.mat_id, p.id_bytes, ci[r] + (long long)cj[r] * Nx + (long long)pstart * NxNy)
+                : 0;
   if (tid < kRow) Rw[(pstart & 1) * kRow + tid] = row_value(p, tid, pstart, i0, j0);
   T hxp[2] = {T(0), T(0)}, hyp[2] = {T(0), T(0)};
 
@@ -229,25 +274,52 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     const T* R = Rw + (pl & 1) * kRow;
     const long long off = (long long)pl * NxNy;
 
-    // new H of the owned cells (tile cells only in the prologue)
+    // plane face flags (FULL): at the plane and of the +z neighbour
+    const bool zf0 = pl == 0 || pl == Nz - 1, zf1 = pl + 1 >= Nz - 1;
+    const bool masked = FULL && (warp_face || zf0 || zf1);
+
+    // new H of the owned cells (tile cells only in the prologue; FULL: no H
+    // below plane 0, the ext cells outside the grid hold 0)
     T hxn[2], hyn[2];
 #pragma unroll
     for (int r = 0; r < 2; r++) {
       hxn[r] = hyn[r] = T(0);
       const bool tile_cell = r == 0 || two;
-      if (!hval[r] || (prologue && !tile_cell)) continue;
+      if (FULL && (r == 0 || two || halo) && !hval[r]) {
+        const int e = ext[r];
+        Hs[e] = T(0);
+        Hs[kExt + e] = T(0);
+        Hs[2 * kExt + e] = T(0);
+      }
+      if (!hval[r] || (prologue && !tile_cell) || (FULL && pl < 0)) continue;
       const int e = ext[r];
       const int ea = e % kEW, eb = e / kEW;
-      const int bi = eb * kBX + ea + 1;
-      const int hb = eb * HBX + ea + 1;
+      const int bi = eb * EBX + ea + XO;
+      const int hb = eb * HBX + ea + XO;
       const T* m0 = mat + 9 * id[r];
       const T R0 = mul(R[eb], m0[3]);
       const T R1 = mul(R[9 + ea], m0[4]);
       const T R2 = mul(iAz[r], m0[5]);
       T hx = Hk[hb], hy = Hk[SH + hb], hz = Hk[2 * SH + hb];
-      h_lean(p.dt, desc, R0, R1, R2, sLx[ea], sLy[eb], R[146], Ek[bi], Ek[SE + bi],
-             Ek[2 * SE + bi], Ek[SE + bi + 1], Ek[2 * SE + bi + 1], Ek[bi + kBX],
-             Ek[2 * SE + bi + kBX], Ek1[bi], Ek1[SE + bi], hx, hy, hz);
+      T ex0 = Ek[bi], ey0 = Ek[SE + bi], ez0 = Ek[2 * SE + bi];
+      T ey1 = Ek[SE + bi + 1], ez1 = Ek[2 * SE + bi + 1];
+      T ex2 = Ek[bi + EBX], ez2 = Ek[2 * SE + bi + EBX];
+      T ex3 = Ek1[bi], ey3 = Ek1[SE + bi];
+      if (masked) {
+        // E column entries tangential to a face they lie on are masked
+        const T z = T(0);
+        ex0 = (yf0[r] || zf0) ? z : ex0;
+        ey0 = (xf0[r] || zf0) ? z : ey0;
+        ez0 = (xf0[r] || yf0[r]) ? z : ez0;
+        ey1 = (xf1[r] || zf0) ? z : ey1;
+        ez1 = (xf1[r] || yf0[r]) ? z : ez1;
+        ex2 = (yf1[r] || zf0) ? z : ex2;
+        ez2 = (xf0[r] || yf1[r]) ? z : ez2;
+        ex3 = (yf0[r] || zf1) ? z : ex3;
+        ey3 = (xf0[r] || zf1) ? z : ey3;
+      }
+      h_lean(p.dt, desc, R0, R1, R2, sLx[ea], sLy[eb], R[146], ex0, ey0, ez0, ey1, ez1, ex2,
+             ez2, ex3, ey3, hx, hy, hz);
       Hs[e] = hx;
       Hs[kExt + e] = hy;
       Hs[2 * kExt + e] = hz;
@@ -269,7 +341,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         if (!eval[r]) continue;
         const int e = ext[r];
         const int a = e % kEW - 1, b = e / kEW - 1;
-        const int bi = (b + 1) * kBX + a + 2;
+        const int bi = (b + 1) * EBX + a + 1 + XO;
         const long long n = ci[r] + (long long)cj[r] * Nx + off;
         const T* m0 = mat + 9 * id[r];
         const T R0 = mul(m0[0], R[74 + b]);
@@ -279,6 +351,12 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         e_lean(R0, R1, R2, stLx[a], stLy[b], tLz, Hs[e], Hs[kExt + e], Hs[2 * kExt + e],
                Hs[kExt + e - 1], Hs[2 * kExt + e - 1], Hs[e - kEW], Hs[2 * kExt + e - kEW],
                hxp[r], hyp[r], curl[0], curl[1], curl[2]);
+        if (masked) {
+          // E rows tangential to the face the cell lies on get no curl
+          if (yf0[r] || zf0) curl[0] = T(0);
+          if (xf0[r] || zf0) curl[1] = T(0);
+          if (xf0[r] || yf0[r]) curl[2] = T(0);
+        }
         const T eold[3] = {Ek[bi], Ek[SE + bi], Ek[2 * SE + bi]};
         Cell cc;
         cc.i = ci[r]; cc.j = cj[r]; cc.k = pl;
@@ -348,24 +426,24 @@ bool tma_supported(const FitParams<T>& p) {
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
 struct TmaOcc { int sms = 0, per_sm = 0; bool attr = false; };
-static TmaOcc g_occ[2][2][3][64];
+static TmaOcc g_occ[2][2][3][2][64];
 
-template <typename T, bool SM, int JM>
+template <typename T, bool SM, int JM, bool FULL>
 static cudaError_t tma_occupancy(TmaOcc** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][dev];
+  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][FULL ? 1 : 0][dev];
   if (!o.attr) {
-    const int smem = TmaLayout<T>::bytes;
-    e = cudaFuncSetAttribute(k_tma<T, SM, JM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const int smem = TmaLayout<T, FULL>::bytes;
+    e = cudaFuncSetAttribute(k_tma<T, SM, JM, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM>, kTmaThreads,
-                                                      smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, FULL>,
+                                                      kTmaThreads, smem);
     if (e != cudaSuccess) return e;
     if (o.per_sm < 1) o.per_sm = 1;
     o.attr = true;
@@ -374,43 +452,73 @@ static cudaError_t tma_occupancy(TmaOcc** out) {
   return cudaSuccess;
 }
 
+// Every face carries the PEC column mask and no face the PMC row mask.
 template <typename T>
-cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC) {
+static bool all_faces_pec(const FitParams<T>& p) {
+  if (!p.has_pec || p.has_pmc) return false;
+  for (int f = 0; f < 6; f++)
+    if (p.pec_face[f] != 0) return false;
+  return true;
+}
+
+template <typename T, bool SM, int JM, bool FULL>
+static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cudaStream_t st,
+                                      int KC) {
+  using G = TmaGeom<T, FULL>;
   TmaMaps maps;
   for (int d = 0; d < 3; d++) {
-    if (!encode_comp<T>(&maps.e[d], p.E_in + d * p.N, p.Nx, p.Ny, p.Nz, kBX, kBY) ||
-        !encode_comp<T>(&maps.h[d], p.H_in + d * p.N, p.Nx, p.Ny, p.Nz, h_box_x<T>(), kHBY))
+    if (!encode_comp<T>(&maps.e[d], p.E_in + d * p.N, p.Nx, p.Ny, p.Nz, G::ebx, kBY) ||
+        !encode_comp<T>(&maps.h[d], p.H_in + d * p.N, p.Nx, p.Ny, p.Nz, G::hbx, kHBY))
       return cudaErrorInvalidValue;
   }
-  const bool sm_table = p.n_mat <= kMatSmem;
-  const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
-  const int gx = (p.Nx - 4 + kTX - 1) / kTX, gy = (p.Ny - 4 + kTY - 1) / kTY;
-  auto go = [&](auto kern, TmaOcc* occ) {
-    if (KC <= 0)
-      KC = tma_auto_kc((long long)gx * gy, p.Nz - 4, (long long)occ->sms * occ->per_sm);
-    const int gz = (p.Nz - 4 + KC - 1) / KC;
-    timer_begin(st);
-    kern<<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T>::bytes, st>>>(p, maps, step, KC);
-    timer_end(st);
-  };
   TmaOcc* occ = nullptr;
-  cudaError_t e;
-#define WK_TMA_CASE(SMV, JMV)                                          \
-  if (sm_table == SMV && jm == JMV) {                                  \
-    e = tma_occupancy<T, SMV, JMV>(&occ);                              \
-    if (e != cudaSuccess) return e;                                    \
-    go(k_tma<T, SMV, JMV>, occ);                                       \
-  }
-  WK_TMA_CASE(true, 0) WK_TMA_CASE(true, 1) WK_TMA_CASE(true, 2)
-  WK_TMA_CASE(false, 0) WK_TMA_CASE(false, 1) WK_TMA_CASE(false, 2)
-#undef WK_TMA_CASE
+  cudaError_t e = tma_occupancy<T, SM, JM, FULL>(&occ);
+  if (e != cudaSuccess) return e;
+  const int span_x = FULL ? p.Nx : p.Nx - 4, span_y = FULL ? p.Ny : p.Ny - 4;
+  const int planes = FULL ? p.Nz : p.Nz - 4;
+  const int gx = (span_x + kTX - 1) / kTX, gy = (span_y + kTY - 1) / kTY;
+  if (KC <= 0)
+    KC = tma_auto_kc((long long)gx * gy, planes, (long long)occ->sms * occ->per_sm);
+  const int gz = (planes + KC - 1) / KC;
+  timer_begin(st);
+  k_tma<T, SM, JM, FULL><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T, FULL>::bytes, st>>>(
+      p, maps, step, KC);
+  timer_end(st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (FULL) return cudaSuccess;
   // shell: H from the old state, then E from the new H (the interior H
   // the shell E rows read is in H_out once k_tma is done)
   return launch_shell_pair<T>(p, step, st);
 }
 
+// One step with the TMA kernel: the full-domain variant when every face is
+// PEC-masked (no shell launch), else the interior variant plus the shell.
+template <typename T>
+cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC) {
+  const bool sm_table = p.n_mat <= kMatSmem;
+  const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
+  const bool full = all_faces_pec(p);
+#define WK_TMA_CASE(SMV, JMV, FV)                                       \
+  if (sm_table == SMV && jm == JMV && full == FV)                       \
+    return launch_tma_variant<T, SMV, JMV, FV>(p, step, st, KC);
+  WK_TMA_CASE(true, 0, true) WK_TMA_CASE(true, 1, true) WK_TMA_CASE(true, 2, true)
+  WK_TMA_CASE(false, 0, true) WK_TMA_CASE(false, 1, true) WK_TMA_CASE(false, 2, true)
+  WK_TMA_CASE(true, 0, false) WK_TMA_CASE(true, 1, false) WK_TMA_CASE(true, 2, false)
+  WK_TMA_CASE(false, 0, false) WK_TMA_CASE(false, 1, false) WK_TMA_CASE(false, 2, false)
+#undef WK_TMA_CASE
+  return cudaErrorInvalidValue;
+}
+
+// Launches per step of the TMA schedule for these parameters: 1 (full-domain
+// kernel) or 3 (interior kernel + two shell launches).
+template <typename T>
+int tma_launches_per_step(const FitParams<T>& p) {
+  return all_faces_pec(p) ? 1 : 3;
+}
+
+template int tma_launches_per_step<double>(const FitParams<double>&);
+template int tma_launches_per_step<float>(const FitParams<float>&);
 template bool tma_supported<double>(const FitParams<double>&);
 template bool tma_supported<float>(const FitParams<float>&);
 template cudaError_t launch_tma<double>(const FitParams<double>&, long long, cudaStream_t, int);
