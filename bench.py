@@ -478,7 +478,7 @@ def main():
     n_per = n_int // max(args.steps, 1)
     # the TMA schedule needs no shell launch when every face is PEC-masked
     pec_faces = all(b.lower() in ("pec", "electric", "pml") for b in s.bc_low + s.bc_high)
-    tma_per_step = 1 if (pec_faces and args.dtype != "fp32c") else 3
+    tma_per_step = 1 if pec_faces else 3
     per_step = fixed.get(args.kernel, {1: tma_per_step, 2: 4}.get(n_per, 2 * n_per))
     launches = args.steps * per_step  # step kernels launched in the timed region
     # cells the interior kernel updates: the whole grid for the full-domain

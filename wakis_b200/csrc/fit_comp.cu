@@ -242,11 +242,14 @@ int wk_comp_step(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_
     FitParams<double> p = make_params<double>(d, par);
     CompState cs = comp_state(d, par);
     if (tma) {
-      // fused interior, then the shell: H from the old state, E from the new H
+      // fused step (whole grid when every face is PEC-masked, else the
+      // interior, then the shell: H from the old state, E from the new H)
       cudaError_t e = launch_tma_comp(d, p, par, step0 + s, st, d->tile_planes);
       if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
-      k_h_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, sg);
-      k_e_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, step0 + s, sg);
+      if (!tma_comp_full(p)) {
+        k_h_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, sg);
+        k_e_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, step0 + s, sg);
+      }
     } else {
       timer_begin(st);
       k_h_comp<<<grid, blk, 0, st>>>(p, cs);

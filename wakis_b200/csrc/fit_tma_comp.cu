@@ -59,9 +59,20 @@ struct CompMaps {
   CUtensorMap h[3];
 };
 
+// FULL (every face PEC-masked): tiles from i0 = 64 bx cover the whole grid
+// and both boxes start at i0-4 (16-byte aligned): E 72 wide, H 68 wide.
+template <bool FULL>
+struct CGeom {
+  static constexpr int ebx = FULL ? cTX + 8 : cBX;   // E box width
+  static constexpr int hbx = cBX;                    // H box width (68)
+  static constexpr int xo = FULL ? 3 : 1;            // box x of ext column 0
+  static constexpr int xs_off = FULL ? 4 : 2;        // box start = i0 - xs_off
+};
+
+template <bool FULL>
 struct CLayout {
-  static constexpr int eslot = round128(cBX * cBY * 4);
-  static constexpr int hslot = round128(cBX * cHBY * 4);
+  static constexpr int eslot = round128(CGeom<FULL>::ebx * cBY * 4);
+  static constexpr int hslot = round128(CGeom<FULL>::hbx * cHBY * 4);
   static constexpr int e_off = 0;
   static constexpr int h_off = e_off + cES * 3 * eslot;
   static constexpr int hs_off = h_off + cHS * 3 * hslot;
@@ -119,16 +130,16 @@ __device__ __forceinline__ RowSrc row_src(const FitParams<double>& p, int r, int
   RowSrc s{nullptr, nullptr, 0, 0};
   if (r < R_HXB) {
     const int j = j0 - 1 + (r - R_HXA);
-    if (r - R_HXA < 9 && j < Ny) s = RowSrc{p.iAx + j, p.Ly + j, Ny, 0};
+    if (r - R_HXA < 9 && j >= 0 && j < Ny) s = RowSrc{p.iAx + j, p.Ly + j, Ny, 0};
   } else if (r < R_HYA) {
     const int j = j0 - 1 + (r - R_HXB);
-    if (r - R_HXB < 9 && j < Ny) s = RowSrc{p.iAx + j, p.Lz, Ny, 1};
+    if (r - R_HXB < 9 && j >= 0 && j < Ny) s = RowSrc{p.iAx + j, p.Lz, Ny, 1};
   } else if (r < R_HYB) {
     const int i = i0 - 2 + (r - R_HYA);
-    if (r > R_HYA && i < Nx) s = RowSrc{p.iAy + i, p.Lx + i, Nx, 0};
+    if (r > R_HYA && i >= 0 && i < Nx) s = RowSrc{p.iAy + i, p.Lx + i, Nx, 0};
   } else if (r < R_EXA) {
     const int i = i0 - 2 + (r - R_HYB);
-    if (r > R_HYB && i < Nx) s = RowSrc{p.iAy + i, p.Lz, Nx, 1};
+    if (r > R_HYB && i >= 0 && i < Nx) s = RowSrc{p.iAy + i, p.Lz, Nx, 1};
   } else if (r < R_EXB) {
     const int j = j0 + (r - R_EXA);
     if (j < Ny) s = RowSrc{p.itAx + j, p.tLy + j, Ny, 0};
@@ -144,8 +155,8 @@ __device__ __forceinline__ RowSrc row_src(const FitParams<double>& p, int r, int
   }
   return s;
 }
-__device__ __forceinline__ void row_load(const RowSrc& s, int q, double& f, double& g) {
-  if (s.f) {
+__device__ __forceinline__ void row_load(const RowSrc& s, int q, int Nz, double& f, double& g) {
+  if (s.f && q >= 0 && q < Nz) {
     f = s.f[(long long)q * s.fs];
     g = s.g[(long long)q * s.gs];
   } else {
@@ -158,14 +169,21 @@ __device__ __forceinline__ float row_value(double dt, double f, double g) {
 }
 
 // IdT: material id type; SIG: the J entering a row is sigma * E (the
-// conductive J mode) rather than zero.
-template <typename IdT, bool SIG>
+// conductive J mode) rather than zero.  FULL: every face carries the PEC
+// column mask (no PMC); the tiles cover the whole grid and the cells on or
+// next to a face use the same rows with the masked entries set to zero (E
+// entries tangential to a face they lie on enter no H row; E rows tangential
+// to their face get no curl; wrapped flat-offset neighbours are always
+// masked), so no shell launch follows.
+template <typename IdT, bool SIG, bool FULL>
 __global__ void __launch_bounds__(cThreads, 2)
 k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
            long long step, int KC) {
   step = step_index(p, step);
-  using Lay = CLayout;
+  using Lay = CLayout<FULL>;
+  using G = CGeom<FULL>;
   constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4;
+  constexpr int EBX = G::ebx, XO = G::xo;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   unsigned char* sm = sm_raw + ((128 - (smem_u32(sm_raw) & 127)) & 127);
   float* Eb = reinterpret_cast<float*>(sm + Lay::e_off);
@@ -177,12 +195,13 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
 
   const int Nx = p.Nx, Ny = p.Ny;
   const long long N = p.N, NxNy = p.NxNy;
-  const int i0 = 2 + blockIdx.x * cTX, j0 = 2 + blockIdx.y * cTY;
-  const int k0 = 2 + blockIdx.z * KC, k1 = min(k0 + KC, p.Nz - 2);
-  const int xs = i0 - 2, ys = j0 - 1;
+  const int Nz = p.Nz;
+  const int i0 = (FULL ? 0 : 2) + blockIdx.x * cTX, j0 = (FULL ? 0 : 2) + blockIdx.y * cTY;
+  const int k0 = (FULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, FULL ? Nz : Nz - 2);
+  const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int pstart = k0 - 1;
-  const uint32_t e_bytes = 3u * cBX * cBY * 4u, h_bytes = 3u * cBX * cHBY * 4u;
+  const uint32_t e_bytes = 3u * EBX * cBY * 4u, h_bytes = 3u * G::hbx * cHBY * 4u;
 
   if (tid == 0) {
     for (int s = 0; s < cES + cHS; s++) mbar_init(&bar[s], 1);
@@ -222,9 +241,18 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   else { ea = 0; eb = lane; }
   const int ci = i0 - 1 + ea, cj = j0 - 1 + eb;          // first cell of the item
   const bool pair = role < 2;
-  const bool hval = role < 3 && ci <= Nx - 3 && cj <= Ny - 3;
+  const bool hval = FULL ? (role < 3 && ci >= 0 && ci <= Nx - 1 && cj >= 0 && cj <= Ny - 1)
+                         : (role < 3 && ci <= Nx - 3 && cj <= Ny - 3);
   const bool eval = role == 0 && hval;
-  const int bi = eb * cBX + ea + 1;                       // E / H box index
+  const int bi = eb * EBX + ea + XO;                      // E box index
+  const int hbi = eb * G::hbx + ea + XO;                  // H box index
+  // face flags (FULL) of the item's cells (x per lane) and of the +x / +y
+  // neighbours (a wrapped neighbour counts as on the face)
+  const bool xf0a = ci == 0 || ci == Nx - 1, xf0b = ci + 1 == Nx - 1;
+  const bool xf1a = ci + 1 >= Nx - 1, xf1b = ci + 2 >= Nx - 1;
+  const bool yf0 = cj == 0 || cj == Ny - 1, yf1 = cj + 1 >= Ny - 1;
+  const bool nearface = hval && (xf0a || xf1a || (pair && (xf0b || xf1b)) || yf0 || yf1);
+  const bool warp_face = FULL && __any_sync(0xffffffffu, nearface);
   const int hi = eb * cEW + ea + 1;                       // Hs index
   const long long nb = ci + (long long)cj * Nx;           // flat index at k = 0
 
@@ -271,14 +299,14 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   };
   int id0 = 0, id1 = 0;
   uint32_t hc[3] = {0, 0, 0}, ec[3] = {0, 0, 0};
-  if (hval) {
+  if (hval && pstart >= 0) {
     load_ids(pstart, id0, id1);
     load_comp(cs.Hc_in, pstart, hc);
   }
   const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
   if (tid < cRow) {
     double f, g;
-    row_load(rsrc, pstart, f, g);
+    row_load(rsrc, pstart, Nz, f, g);
     Rw[(pstart & 1) * cRow + tid] = row_value(p.dt, f, g);
   }
   float2 hxp = bcast(0.f), hyp = bcast(0.f);
@@ -308,7 +336,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         load_comp(cs.Hc_in, pl + 1, nhc);
       }
       if (eval) load_comp(cs.Ec_in, pl + 1, nec);
-      if (tid < cRow) row_load(rsrc, pl + 1, rf, rg);
+      if (tid < cRow) row_load(rsrc, pl + 1, Nz, rf, rg);
     }
     const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
     const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
@@ -316,9 +344,21 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     const float* R = Rw + (pl & 1) * cRow;
     const long long n = nb + (long long)pl * NxNy;
 
-    // ---- new H of the owned item (tile pairs only in the prologue)
+    // plane face flags (FULL): at the plane and of the +z neighbour
+    const bool zf0 = pl == 0 || pl == Nz - 1, zf1 = pl + 1 >= Nz - 1;
+    const bool masked = FULL && (warp_face || zf0 || zf1);
+
+    // ---- new H of the owned item (tile pairs only in the prologue; FULL:
+    // no H below plane 0, items outside the grid hold 0)
     float2 hxn = zero2, hyn = zero2;
-    if (hval && (!prologue || role == 0)) {
+    if (FULL && role < 3 && !hval) {
+      if (pair) {
+        st2(Hs + hi, zero2); st2(Hs + cExt + hi, zero2); st2(Hs + 2 * cExt + hi, zero2);
+      } else {
+        Hs[hi] = 0.f; Hs[cExt + hi] = 0.f; Hs[2 * cExt + hi] = 0.f;
+      }
+    }
+    if (hval && (!prologue || role == 0) && !(FULL && pl < 0)) {
       const float* m0 = mt + id0 * cMatW;
       const float* m1 = mt + id1 * cMatW;
       float2 ex0, ey0, ez0, ey1, ez1, ex2, ez2, ex3, ey3, hx, hy, hz, ya, yb;
@@ -326,17 +366,32 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         ex0 = ld2(Ek + bi); ey0 = ld2(Ek + SE + bi); ez0 = ld2(Ek + 2 * SE + bi);
         ey1 = make_float2(ey0.y, Ek[SE + bi + 2]);
         ez1 = make_float2(ez0.y, Ek[2 * SE + bi + 2]);
-        ex2 = ld2(Ek + bi + cBX); ez2 = ld2(Ek + 2 * SE + bi + cBX);
+        ex2 = ld2(Ek + bi + EBX); ez2 = ld2(Ek + 2 * SE + bi + EBX);
         ex3 = ld2(Ek1 + bi); ey3 = ld2(Ek1 + SE + bi);
-        hx = ld2(Hk + bi); hy = ld2(Hk + SH + bi); hz = ld2(Hk + 2 * SH + bi);
+        hx = ld2(Hk + hbi); hy = ld2(Hk + SH + hbi); hz = ld2(Hk + 2 * SH + hbi);
         ya = ld2(R + R_HYA + ea + 1); yb = ld2(R + R_HYB + ea + 1);
       } else {
         ex0 = bcast(Ek[bi]); ey0 = bcast(Ek[SE + bi]); ez0 = bcast(Ek[2 * SE + bi]);
         ey1 = bcast(Ek[SE + bi + 1]); ez1 = bcast(Ek[2 * SE + bi + 1]);
-        ex2 = bcast(Ek[bi + cBX]); ez2 = bcast(Ek[2 * SE + bi + cBX]);
+        ex2 = bcast(Ek[bi + EBX]); ez2 = bcast(Ek[2 * SE + bi + EBX]);
         ex3 = bcast(Ek1[bi]); ey3 = bcast(Ek1[SE + bi]);
-        hx = bcast(Hk[bi]); hy = bcast(Hk[SH + bi]); hz = bcast(Hk[2 * SH + bi]);
+        hx = bcast(Hk[hbi]); hy = bcast(Hk[SH + hbi]); hz = bcast(Hk[2 * SH + hbi]);
         ya = bcast(R[R_HYA + ea + 1]); yb = bcast(R[R_HYB + ea + 1]);
+      }
+      if (masked) {
+        // E column entries tangential to a face they lie on are masked
+        auto m2 = [](float2 v, bool ma, bool mb) {
+          return make_float2(ma ? 0.f : v.x, mb ? 0.f : v.y);
+        };
+        ex0 = m2(ex0, yf0 || zf0, yf0 || zf0);
+        ey0 = m2(ey0, xf0a || zf0, xf0b || zf0);
+        ez0 = m2(ez0, xf0a || yf0, xf0b || yf0);
+        ey1 = m2(ey1, xf1a || zf0, xf1b || zf0);
+        ez1 = m2(ez1, xf1a || yf0, xf1b || yf0);
+        ex2 = m2(ex2, yf1 || zf0, yf1 || zf0);
+        ez2 = m2(ez2, xf0a || yf1, xf0b || yf1);
+        ex3 = m2(ex3, yf0 || zf1, yf0 || zf1);
+        ey3 = m2(ey3, xf0a || zf1, xf0b || zf1);
       }
       const float4 u0 = *reinterpret_cast<const float4*>(m0);
       const float4 u1 = *reinterpret_cast<const float4*>(m1);
@@ -395,6 +450,12 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
                    mul2(mul2(iey, ld2(R + R_EYB + a)), sub2(hz1, hz0)));
       // curl_z = c1 (hx2 - hx0) + c2 (hy0 - hy1)   (c1 = dt ieps_z itAz tLx, c2 = .. tLy)
       cu[2] = fma2(mul2(iez, eza), sub2(hx2, hx0), mul2(mul2(iez, ezb), sub2(hy0, hy1)));
+      if (masked) {
+        // E rows tangential to the face the cell lies on get no curl
+        if (yf0 || zf0) cu[0] = zero2;
+        cu[1] = make_float2((xf0a || zf0) ? 0.f : cu[1].x, (xf0b || zf0) ? 0.f : cu[1].y);
+        cu[2] = make_float2((xf0a || yf0) ? 0.f : cu[2].x, (xf0b || yf0) ? 0.f : cu[2].y);
+      }
       float2 ev[3] = {ld2(Ek + bi), ld2(Ek + SE + bi), ld2(Ek + 2 * SE + bi)};
       if (p.cap_on) {
 #pragma unroll
@@ -447,10 +508,10 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   }
 }
 
-bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int by) {
+bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int bx, int by) {
   cuuint64_t gdim[3] = {(cuuint64_t)Nx, (cuuint64_t)Ny, (cuuint64_t)Nz};
   cuuint64_t gstr[2] = {(cuuint64_t)Nx * 4, (cuuint64_t)Nx * Ny * 4};
-  cuuint32_t box[3] = {(cuuint32_t)cBX, (cuuint32_t)by, 1};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   cuuint32_t est[3] = {1, 1, 1};
   CUresult r = tma_encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, gdim,
                                gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -459,10 +520,17 @@ bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int
   return r == CUDA_SUCCESS;
 }
 
-int g_comp_sms[6][64], g_comp_per_sm[6][64];
-bool g_comp_attr[6][64];
+int g_comp_sms[12][64], g_comp_per_sm[12][64];
+bool g_comp_attr[12][64];
 
 }  // namespace
+
+bool tma_comp_full(const FitParams<double>& p) {
+  if (!p.has_pec || p.has_pmc) return false;
+  for (int f = 0; f < 6; f++)
+    if (p.pec_face[f] != 0) return false;
+  return true;
+}
 
 bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
   if (p.Nx < 5 || p.Ny < 5 || p.Nz < 5) return false;
@@ -477,11 +545,13 @@ bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
 
 cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, int par,
                             long long step, cudaStream_t st, int KC) {
+  const bool full = tma_comp_full(p);
   CompState cs = comp_state(d, par);
   CompMaps maps;
+  const int ebx = full ? CGeom<true>::ebx : CGeom<false>::ebx;
   for (int c = 0; c < 3; c++) {
-    if (!encode_f32(&maps.e[c], cs.E_in + c * p.N, p.Nx, p.Ny, p.Nz, cBY) ||
-        !encode_f32(&maps.h[c], cs.H_in + c * p.N, p.Nx, p.Ny, p.Nz, cHBY))
+    if (!encode_f32(&maps.e[c], cs.E_in + c * p.N, p.Nx, p.Ny, p.Nz, ebx, cBY) ||
+        !encode_f32(&maps.h[c], cs.H_in + c * p.N, p.Nx, p.Ny, p.Nz, cBX, cHBY))
       return cudaErrorInvalidValue;
   }
   int dev = 0;
@@ -490,30 +560,37 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   const int ib = p.id_bytes == 1 ? 0 : (p.id_bytes == 2 ? 1 : 2);
   const bool sig = p.j_mode == WK_J_SIGMA_E;
-  const int slot = ib * 2 + (sig ? 1 : 0);
+  const int slot = (full ? 6 : 0) + ib * 2 + (sig ? 1 : 0);
   using K = void (*)(FitParams<double>, CompState, const CompMaps, long long, int);
-  const K kerns[6] = {k_tma_comp<uint8_t, false>,  k_tma_comp<uint8_t, true>,
-                      k_tma_comp<uint16_t, false>, k_tma_comp<uint16_t, true>,
-                      k_tma_comp<uint32_t, false>, k_tma_comp<uint32_t, true>};
+  const K kerns[12] = {
+      k_tma_comp<uint8_t, false, false>,  k_tma_comp<uint8_t, true, false>,
+      k_tma_comp<uint16_t, false, false>, k_tma_comp<uint16_t, true, false>,
+      k_tma_comp<uint32_t, false, false>, k_tma_comp<uint32_t, true, false>,
+      k_tma_comp<uint8_t, false, true>,   k_tma_comp<uint8_t, true, true>,
+      k_tma_comp<uint16_t, false, true>,  k_tma_comp<uint16_t, true, true>,
+      k_tma_comp<uint32_t, false, true>,  k_tma_comp<uint32_t, true, true>};
   const K kern = kerns[slot];
+  const int smem = full ? CLayout<true>::bytes : CLayout<false>::bytes;
   if (!g_comp_attr[slot][dev]) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CLayout::bytes);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&g_comp_sms[slot][dev], cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_comp_per_sm[slot][dev], kern, cThreads,
-                                                      CLayout::bytes);
+                                                      smem);
     if (e != cudaSuccess) return e;
     if (g_comp_per_sm[slot][dev] < 1) g_comp_per_sm[slot][dev] = 1;
     g_comp_attr[slot][dev] = true;
   }
-  const int gx = (p.Nx - 4 + cTX - 1) / cTX, gy = (p.Ny - 4 + cTY - 1) / cTY;
+  const int span_x = full ? p.Nx : p.Nx - 4, span_y = full ? p.Ny : p.Ny - 4;
+  const int planes = full ? p.Nz : p.Nz - 4;
+  const int gx = (span_x + cTX - 1) / cTX, gy = (span_y + cTY - 1) / cTY;
   if (KC <= 0)
-    KC = tma_auto_kc((long long)gx * gy, p.Nz - 4,
+    KC = tma_auto_kc((long long)gx * gy, planes,
                      (long long)g_comp_sms[slot][dev] * g_comp_per_sm[slot][dev]);
-  const int gz = (p.Nz - 4 + KC - 1) / KC;
+  const int gz = (planes + KC - 1) / KC;
   timer_begin(st);
-  kern<<<dim3(gx, gy, gz), cThreads, CLayout::bytes, st>>>(p, cs, maps, step, KC);
+  kern<<<dim3(gx, gy, gz), cThreads, smem, st>>>(p, cs, maps, step, KC);
   timer_end(st);
   return cudaGetLastError();
 }
