@@ -481,10 +481,17 @@ def main():
     tma_per_step = 1 if pec_faces else 3
     per_step = fixed.get(args.kernel, {1: tma_per_step, 2: 4}.get(n_per, 2 * n_per))
     launches = args.steps * per_step  # step kernels launched in the timed region
-    # cells the interior kernel updates: the whole grid for the full-domain
-    # TMA kernel, else the interior without the two-cell shell
-    interior = (N if (per_step == 1 and n_per == 1)
-                else (s.Nx - 4) * (s.Ny - 4) * (s.Nz - 4))
+    # cells the TMA / interior kernel updates: the whole grid when every face
+    # is PEC-masked, all of x and y when the x/y faces are, else the interior
+    # without the two-cell shell
+    xy_pec = all(b.lower() in ("pec", "electric", "pml")
+                 for b in s.bc_low[:2] + s.bc_high[:2])
+    if n_per == 1 and per_step == 1:
+        interior = N
+    elif n_per == 1 and xy_pec:
+        interior = s.Nx * s.Ny * (s.Nz - 4)
+    else:
+        interior = (s.Nx - 4) * (s.Ny - 4) * (s.Nz - 4)
     schedule = {1: "tma", 2: "twopass"}.get(n_int // max(args.steps, 1), args.kernel)
 
     # end to end through the public API: per-step H2D line current, D2H window

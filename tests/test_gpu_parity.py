@@ -267,7 +267,10 @@ TMA_GRIDS = [((16, 12, 20), "float64"), ((24, 16, 30), "float64"), ((32, 20, 26)
 
 @pytest.mark.parametrize("shape,dtype", TMA_GRIDS)
 @pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
-                                 (["periodic", "pec", "pml"], ["periodic", "pec", "pml"])])
+                                 (["periodic", "pec", "pml"], ["periodic", "pec", "pml"]),
+                                 (["pec", "pec", "abc"], ["pec", "pec", "abc"]),
+                                 (["pec", "electric", "periodic"], ["pml", "pec", "periodic"]),
+                                 (["pec", "pec", "pec"], ["pec", "pec", "abc"])])
 def test_tma_kernel_exact_against_oracle(shape, dtype, bcs):
     """TMA-staged fused kernel (interior) + shell: value-for-value equal to
     the oracle after several steps from random fields (no exponential)."""

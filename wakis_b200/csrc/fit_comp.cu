@@ -246,9 +246,12 @@ int wk_comp_step(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_
       // interior, then the shell: H from the old state, E from the new H)
       cudaError_t e = launch_tma_comp(d, p, par, step0 + s, st, d->tile_planes);
       if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
-      if (!tma_comp_full(p)) {
-        k_h_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, sg);
-        k_e_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, step0 + s, sg);
+      const int mode = tma_comp_mode(p);
+      if (mode != 1) {
+        const ShellGrid g2 = shell_grid(d->Nx, d->Ny, d->Nz, mode == 2);
+        const unsigned sb2 = (unsigned)(g2.nbA + g2.nbB + g2.nbC);
+        k_h_comp_shell<<<sb2, kShellBlock, 0, st>>>(p, cs, g2);
+        k_e_comp_shell<<<sb2, kShellBlock, 0, st>>>(p, cs, step0 + s, g2);
       }
     } else {
       timer_begin(st);

@@ -58,8 +58,10 @@ inline CompState comp_state(const wk_fit_desc* d, int par) {
 bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p);
 cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, int par,
                             long long step, cudaStream_t st, int KC);
-// True when every face carries the PEC column mask (no PMC): the compensated
-// TMA kernel then covers the whole grid and no shell launch follows.
-bool tma_comp_full(const FitParams<double>& p);
+// Mode of the compensated TMA kernel for these faces: 1 when every face
+// carries the PEC column mask (whole grid, no shell launch), 2 when the four
+// x/y faces do (shell launches over the four z-boundary planes only), else 0
+// (interior + full shell); never with PMC faces.
+int tma_comp_mode(const FitParams<double>& p);
 
 }  // namespace wk

@@ -464,16 +464,19 @@ cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t 
 }
 
 template <typename T>
-cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_t st) {
-  const ShellGrid sg = shell_grid(p.Nx, p.Ny, p.Nz);
+cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_t st,
+                              bool planes_only) {
+  const ShellGrid sg = shell_grid(p.Nx, p.Ny, p.Nz, planes_only);
   const unsigned sb = (unsigned)(sg.nbA + sg.nbB + sg.nbC);
   k_h_shell<T><<<sb, kShellThreads, 0, st>>>(p, sg);
   k_e_shell<T><<<sb, kShellThreads, 0, st>>>(p, step, sg);
   return cudaGetLastError();
 }
 
-template cudaError_t launch_shell_pair<double>(const FitParams<double>&, long long, cudaStream_t);
-template cudaError_t launch_shell_pair<float>(const FitParams<float>&, long long, cudaStream_t);
+template cudaError_t launch_shell_pair<double>(const FitParams<double>&, long long, cudaStream_t,
+                                               bool);
+template cudaError_t launch_shell_pair<float>(const FitParams<float>&, long long, cudaStream_t,
+                                              bool);
 
 template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long, cudaStream_t,
                                              int);

@@ -21,13 +21,13 @@ struct ShellGrid {
   int nbA, nbB, nbC;   // blocks of the three regions
 };
 
-inline ShellGrid shell_grid(int Nx, int Ny, int Nz) {
+inline ShellGrid shell_grid(int Nx, int Ny, int Nz, bool planes_only = false) {
   ShellGrid g;
   g.cx = (Nx + kShellBlock - 1) / kShellBlock;
   g.cy = (Ny - 4 + 63) / 64;
   g.nbA = 4 * Ny * g.cx;
-  g.nbB = 4 * (Nz - 4) * g.cx;
-  g.nbC = g.cy * (Nz - 4);
+  g.nbB = planes_only ? 0 : 4 * (Nz - 4) * g.cx;
+  g.nbC = planes_only ? 0 : g.cy * (Nz - 4);
   return g;
 }
 
@@ -246,7 +246,8 @@ cudaError_t launch_slabs(const FitParams<T>& p, long long step, cudaStream_t st,
 // shell cells from the old state, then E of the shell cells from the new H
 // (fit_fused.cu); needs Nx, Ny, Nz >= 5 and the interior H_out written.
 template <typename T>
-cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_t st);
+cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_t st,
+                              bool planes_only = false);
 
 // TMA-staged fused step (fit_tma.cu): interior tiles + shell launches.
 template <typename T>

@@ -112,21 +112,28 @@ __device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int 
 // SM: the material table fits in shared memory (n_mat <= kMatSmem); the
 // table reads are then shared-memory loads.  JM: the J mode of the launch
 // (WK_J_ZERO, WK_J_SIGMA_E or WK_J_ARRAY), fixed at compile time.
-// FULL: every face of the grid carries the PEC column mask (pec, electric or
-// pml on all six faces, no PMC).  The tiles then cover the whole grid and the
-// cells next to a face use the same single-coefficient rows with the masked
-// terms set to zero: an E entry tangential to a face it lies on enters no H
-// row, and an E row tangential to its face gets no curl.  The neighbours that
-// the flat-offset operators reach by wrapping (i+1 past Nx-1, j+1 past Ny-1)
-// are tangential to the opposite face, so every wrapped term is masked and
-// the grid needs no shell launch.  Warps with no cell on or next to a face
-// take the unmasked rows.
-template <typename T, bool SM, int JM, bool FULL>
+// MODE 0: interior cells only (2 <= i, j, k <= N-3), the two-cell shell runs
+// in separate launches.  MODE 1: every face of the grid carries the PEC
+// column mask (pec, electric or pml on all six faces, no PMC); the tiles
+// cover the whole grid and the cells next to a face use the same
+// single-coefficient rows with the masked terms set to zero: an E entry
+// tangential to a face it lies on enters no H row, and an E row tangential
+// to its face gets no curl.  The neighbours that the flat-offset operators
+// reach by wrapping (i+1 past Nx-1, j+1 past Ny-1) are tangential to the
+// opposite face, so every wrapped term is masked and no shell launch
+// follows.  MODE 2: the four x/y faces are PEC-masked and the z faces are
+// not (ABC, periodic): the tiles cover all of x and y for the planes
+// 2 <= k <= Nz-3 (no z face is involved there), and the shell launches
+// cover only the planes k in {0, 1, Nz-2, Nz-1}.  Warps with no cell on or
+// next to a face take the unmasked rows.
+template <typename T, bool SM, int JM, int MODE>
 __global__ void __launch_bounds__(kTmaThreads, sizeof(T) == 8 ? 2 : 3)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
+  constexpr bool FULL = MODE != 0;     // tiles cover x and y entirely
+  constexpr bool ZFULL = MODE == 1;    // ... and every plane
   step = step_index(p, step);
-  using Lay = TmaLayout<T, FULL>;
-  using G = TmaGeom<T, FULL>;
+  using Lay = TmaLayout<T, (MODE != 0)>;
+  using G = TmaGeom<T, (MODE != 0)>;
   constexpr int HBX = G::hbx;
   constexpr int EBX = G::ebx;
   constexpr int XO = G::xo;
@@ -149,7 +156,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   const long long N = p.N, NxNy = p.NxNy;
   const int Nz = p.Nz;
   const int i0 = (FULL ? 0 : 2) + blockIdx.x * kTX, j0 = (FULL ? 0 : 2) + blockIdx.y * kTY;
-  const int k0 = (FULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, FULL ? Nz : Nz - 2);
+  const int k0 = (ZFULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, ZFULL ? Nz : Nz - 2);
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x;
   const int pstart = k0 - 1;
@@ -274,8 +281,8 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     const T* R = Rw + (pl & 1) * kRow;
     const long long off = (long long)pl * NxNy;
 
-    // plane face flags (FULL): at the plane and of the +z neighbour
-    const bool zf0 = pl == 0 || pl == Nz - 1, zf1 = pl + 1 >= Nz - 1;
+    // plane face flags (MODE 1): at the plane and of the +z neighbour
+    const bool zf0 = ZFULL && (pl == 0 || pl == Nz - 1), zf1 = ZFULL && pl + 1 >= Nz - 1;
     const bool masked = FULL && (warp_face || zf0 || zf1);
 
     // new H of the owned cells (tile cells only in the prologue; FULL: no H
@@ -291,7 +298,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         Hs[kExt + e] = T(0);
         Hs[2 * kExt + e] = T(0);
       }
-      if (!hval[r] || (prologue && !tile_cell) || (FULL && pl < 0)) continue;
+      if (!hval[r] || (prologue && !tile_cell) || (ZFULL && pl < 0)) continue;
       const int e = ext[r];
       const int ea = e % kEW, eb = e / kEW;
       const int bi = eb * EBX + ea + XO;
@@ -426,23 +433,23 @@ bool tma_supported(const FitParams<T>& p) {
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
 struct TmaOcc { int sms = 0, per_sm = 0; bool attr = false; };
-static TmaOcc g_occ[2][2][3][2][64];
+static TmaOcc g_occ[2][2][3][3][64];
 
-template <typename T, bool SM, int JM, bool FULL>
+template <typename T, bool SM, int JM, int MODE>
 static cudaError_t tma_occupancy(TmaOcc** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][FULL ? 1 : 0][dev];
+  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][MODE][dev];
   if (!o.attr) {
-    const int smem = TmaLayout<T, FULL>::bytes;
-    e = cudaFuncSetAttribute(k_tma<T, SM, JM, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const int smem = TmaLayout<T, (MODE != 0)>::bytes;
+    e = cudaFuncSetAttribute(k_tma<T, SM, JM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, FULL>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, MODE>,
                                                       kTmaThreads, smem);
     if (e != cudaSuccess) return e;
     if (o.per_sm < 1) o.per_sm = 1;
@@ -452,19 +459,20 @@ static cudaError_t tma_occupancy(TmaOcc** out) {
   return cudaSuccess;
 }
 
-// Every face carries the PEC column mask and no face the PMC row mask.
+// TMA mode of a grid: 1 when every face carries the PEC column mask, 2
+// when the four x/y faces do (z faces free), else 0; never with PMC faces.
 template <typename T>
-static bool all_faces_pec(const FitParams<T>& p) {
-  if (!p.has_pec || p.has_pmc) return false;
-  for (int f = 0; f < 6; f++)
-    if (p.pec_face[f] != 0) return false;
-  return true;
+static int tma_mode(const FitParams<T>& p) {
+  if (!p.has_pec || p.has_pmc) return 0;
+  for (int f = 0; f < 4; f++)
+    if (p.pec_face[f] != 0) return 0;
+  return (p.pec_face[4] == 0 && p.pec_face[5] == 0) ? 1 : 2;
 }
 
-template <typename T, bool SM, int JM, bool FULL>
+template <typename T, bool SM, int JM, int MODE>
 static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cudaStream_t st,
                                       int KC) {
-  using G = TmaGeom<T, FULL>;
+  using G = TmaGeom<T, (MODE != 0)>;
   TmaMaps maps;
   for (int d = 0; d < 3; d++) {
     if (!encode_comp<T>(&maps.e[d], p.E_in + d * p.N, p.Nx, p.Ny, p.Nz, G::ebx, kBY) ||
@@ -472,49 +480,50 @@ static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cud
       return cudaErrorInvalidValue;
   }
   TmaOcc* occ = nullptr;
-  cudaError_t e = tma_occupancy<T, SM, JM, FULL>(&occ);
+  cudaError_t e = tma_occupancy<T, SM, JM, MODE>(&occ);
   if (e != cudaSuccess) return e;
-  const int span_x = FULL ? p.Nx : p.Nx - 4, span_y = FULL ? p.Ny : p.Ny - 4;
-  const int planes = FULL ? p.Nz : p.Nz - 4;
+  const int span_x = MODE ? p.Nx : p.Nx - 4, span_y = MODE ? p.Ny : p.Ny - 4;
+  const int planes = MODE == 1 ? p.Nz : p.Nz - 4;
   const int gx = (span_x + kTX - 1) / kTX, gy = (span_y + kTY - 1) / kTY;
   if (KC <= 0)
     KC = tma_auto_kc((long long)gx * gy, planes, (long long)occ->sms * occ->per_sm);
   const int gz = (planes + KC - 1) / KC;
   timer_begin(st);
-  k_tma<T, SM, JM, FULL><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T, FULL>::bytes, st>>>(
-      p, maps, step, KC);
+  k_tma<T, SM, JM, MODE><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T, (MODE != 0)>::bytes,
+                           st>>>(p, maps, step, KC);
   timer_end(st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (FULL) return cudaSuccess;
-  // shell: H from the old state, then E from the new H (the interior H
-  // the shell E rows read is in H_out once k_tma is done)
-  return launch_shell_pair<T>(p, step, st);
+  if (MODE == 1) return cudaSuccess;
+  // shell (MODE 2: the four boundary planes only): H from the old state, then
+  // E from the new H (the H the shell E rows read is in H_out once k_tma is
+  // done)
+  return launch_shell_pair<T>(p, step, st, MODE == 2);
 }
 
-// One step with the TMA kernel: the full-domain variant when every face is
-// PEC-masked (no shell launch), else the interior variant plus the shell.
+// One step with the TMA kernel in the mode the faces allow (see k_tma).
 template <typename T>
 cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC) {
   const bool sm_table = p.n_mat <= kMatSmem;
   const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
-  const bool full = all_faces_pec(p);
-#define WK_TMA_CASE(SMV, JMV, FV)                                       \
-  if (sm_table == SMV && jm == JMV && full == FV)                       \
-    return launch_tma_variant<T, SMV, JMV, FV>(p, step, st, KC);
-  WK_TMA_CASE(true, 0, true) WK_TMA_CASE(true, 1, true) WK_TMA_CASE(true, 2, true)
-  WK_TMA_CASE(false, 0, true) WK_TMA_CASE(false, 1, true) WK_TMA_CASE(false, 2, true)
-  WK_TMA_CASE(true, 0, false) WK_TMA_CASE(true, 1, false) WK_TMA_CASE(true, 2, false)
-  WK_TMA_CASE(false, 0, false) WK_TMA_CASE(false, 1, false) WK_TMA_CASE(false, 2, false)
+  const int mode = tma_mode(p);
+#define WK_TMA_CASE(SMV, JMV)                                                         \
+  if (sm_table == SMV && jm == JMV) {                                                 \
+    if (mode == 1) return launch_tma_variant<T, SMV, JMV, 1>(p, step, st, KC);        \
+    if (mode == 2) return launch_tma_variant<T, SMV, JMV, 2>(p, step, st, KC);        \
+    return launch_tma_variant<T, SMV, JMV, 0>(p, step, st, KC);                       \
+  }
+  WK_TMA_CASE(true, 0) WK_TMA_CASE(true, 1) WK_TMA_CASE(true, 2)
+  WK_TMA_CASE(false, 0) WK_TMA_CASE(false, 1) WK_TMA_CASE(false, 2)
 #undef WK_TMA_CASE
   return cudaErrorInvalidValue;
 }
 
-// Launches per step of the TMA schedule for these parameters: 1 (full-domain
-// kernel) or 3 (interior kernel + two shell launches).
+// Launches per step of the TMA schedule for these parameters: 1 (every face
+// PEC-masked) or 3 (TMA kernel + two shell launches).
 template <typename T>
 int tma_launches_per_step(const FitParams<T>& p) {
-  return all_faces_pec(p) ? 1 : 3;
+  return tma_mode(p) == 1 ? 1 : 3;
 }
 
 template int tma_launches_per_step<double>(const FitParams<double>&);

@@ -169,19 +169,24 @@ __device__ __forceinline__ float row_value(double dt, double f, double g) {
 }
 
 // IdT: material id type; SIG: the J entering a row is sigma * E (the
-// conductive J mode) rather than zero.  FULL: every face carries the PEC
-// column mask (no PMC); the tiles cover the whole grid and the cells on or
-// next to a face use the same rows with the masked entries set to zero (E
-// entries tangential to a face they lie on enter no H row; E rows tangential
-// to their face get no curl; wrapped flat-offset neighbours are always
-// masked), so no shell launch follows.
-template <typename IdT, bool SIG, bool FULL>
+// conductive J mode) rather than zero.  MODE 0: interior cells, the shell
+// follows in separate launches.  MODE 1: every face carries the PEC column
+// mask (no PMC); the tiles cover the whole grid and the cells on or next to
+// a face use the same rows with the masked entries set to zero (E entries
+// tangential to a face they lie on enter no H row; E rows tangential to
+// their face get no curl; wrapped flat-offset neighbours are always
+// masked), so no shell launch follows.  MODE 2: the x/y faces are PEC-masked
+// and the z faces are not; the tiles cover all of x and y for the planes
+// 2 <= k <= Nz-3 and the shell launches cover only the four boundary planes.
+template <typename IdT, bool SIG, int MODE>
 __global__ void __launch_bounds__(cThreads, 2)
 k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
            long long step, int KC) {
+  constexpr bool FULL = MODE != 0;     // tiles cover x and y entirely
+  constexpr bool ZFULL = MODE == 1;    // ... and every plane
   step = step_index(p, step);
-  using Lay = CLayout<FULL>;
-  using G = CGeom<FULL>;
+  using Lay = CLayout<(MODE != 0)>;
+  using G = CGeom<(MODE != 0)>;
   constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4;
   constexpr int EBX = G::ebx, XO = G::xo;
   extern __shared__ __align__(128) unsigned char sm_raw[];
@@ -197,7 +202,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   const long long N = p.N, NxNy = p.NxNy;
   const int Nz = p.Nz;
   const int i0 = (FULL ? 0 : 2) + blockIdx.x * cTX, j0 = (FULL ? 0 : 2) + blockIdx.y * cTY;
-  const int k0 = (FULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, FULL ? Nz : Nz - 2);
+  const int k0 = (ZFULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, ZFULL ? Nz : Nz - 2);
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int pstart = k0 - 1;
@@ -344,8 +349,8 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     const float* R = Rw + (pl & 1) * cRow;
     const long long n = nb + (long long)pl * NxNy;
 
-    // plane face flags (FULL): at the plane and of the +z neighbour
-    const bool zf0 = pl == 0 || pl == Nz - 1, zf1 = pl + 1 >= Nz - 1;
+    // plane face flags (MODE 1): at the plane and of the +z neighbour
+    const bool zf0 = ZFULL && (pl == 0 || pl == Nz - 1), zf1 = ZFULL && pl + 1 >= Nz - 1;
     const bool masked = FULL && (warp_face || zf0 || zf1);
 
     // ---- new H of the owned item (tile pairs only in the prologue; FULL:
@@ -358,7 +363,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         Hs[hi] = 0.f; Hs[cExt + hi] = 0.f; Hs[2 * cExt + hi] = 0.f;
       }
     }
-    if (hval && (!prologue || role == 0) && !(FULL && pl < 0)) {
+    if (hval && (!prologue || role == 0) && !(ZFULL && pl < 0)) {
       const float* m0 = mt + id0 * cMatW;
       const float* m1 = mt + id1 * cMatW;
       float2 ex0, ey0, ez0, ey1, ez1, ex2, ez2, ex3, ey3, hx, hy, hz, ya, yb;
@@ -520,16 +525,16 @@ bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int
   return r == CUDA_SUCCESS;
 }
 
-int g_comp_sms[12][64], g_comp_per_sm[12][64];
-bool g_comp_attr[12][64];
+int g_comp_sms[18][64], g_comp_per_sm[18][64];
+bool g_comp_attr[18][64];
 
 }  // namespace
 
-bool tma_comp_full(const FitParams<double>& p) {
-  if (!p.has_pec || p.has_pmc) return false;
-  for (int f = 0; f < 6; f++)
-    if (p.pec_face[f] != 0) return false;
-  return true;
+int tma_comp_mode(const FitParams<double>& p) {
+  if (!p.has_pec || p.has_pmc) return 0;
+  for (int f = 0; f < 4; f++)
+    if (p.pec_face[f] != 0) return 0;
+  return (p.pec_face[4] == 0 && p.pec_face[5] == 0) ? 1 : 2;
 }
 
 bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
@@ -545,7 +550,8 @@ bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
 
 cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, int par,
                             long long step, cudaStream_t st, int KC) {
-  const bool full = tma_comp_full(p);
+  const int mode = tma_comp_mode(p);
+  const bool full = mode != 0;
   CompState cs = comp_state(d, par);
   CompMaps maps;
   const int ebx = full ? CGeom<true>::ebx : CGeom<false>::ebx;
@@ -560,15 +566,18 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   const int ib = p.id_bytes == 1 ? 0 : (p.id_bytes == 2 ? 1 : 2);
   const bool sig = p.j_mode == WK_J_SIGMA_E;
-  const int slot = (full ? 6 : 0) + ib * 2 + (sig ? 1 : 0);
+  const int slot = mode * 6 + ib * 2 + (sig ? 1 : 0);
   using K = void (*)(FitParams<double>, CompState, const CompMaps, long long, int);
-  const K kerns[12] = {
-      k_tma_comp<uint8_t, false, false>,  k_tma_comp<uint8_t, true, false>,
-      k_tma_comp<uint16_t, false, false>, k_tma_comp<uint16_t, true, false>,
-      k_tma_comp<uint32_t, false, false>, k_tma_comp<uint32_t, true, false>,
-      k_tma_comp<uint8_t, false, true>,   k_tma_comp<uint8_t, true, true>,
-      k_tma_comp<uint16_t, false, true>,  k_tma_comp<uint16_t, true, true>,
-      k_tma_comp<uint32_t, false, true>,  k_tma_comp<uint32_t, true, true>};
+  const K kerns[18] = {
+      k_tma_comp<uint8_t, false, 0>,  k_tma_comp<uint8_t, true, 0>,
+      k_tma_comp<uint16_t, false, 0>, k_tma_comp<uint16_t, true, 0>,
+      k_tma_comp<uint32_t, false, 0>, k_tma_comp<uint32_t, true, 0>,
+      k_tma_comp<uint8_t, false, 1>,  k_tma_comp<uint8_t, true, 1>,
+      k_tma_comp<uint16_t, false, 1>, k_tma_comp<uint16_t, true, 1>,
+      k_tma_comp<uint32_t, false, 1>, k_tma_comp<uint32_t, true, 1>,
+      k_tma_comp<uint8_t, false, 2>,  k_tma_comp<uint8_t, true, 2>,
+      k_tma_comp<uint16_t, false, 2>, k_tma_comp<uint16_t, true, 2>,
+      k_tma_comp<uint32_t, false, 2>, k_tma_comp<uint32_t, true, 2>};
   const K kern = kerns[slot];
   const int smem = full ? CLayout<true>::bytes : CLayout<false>::bytes;
   if (!g_comp_attr[slot][dev]) {
@@ -583,7 +592,7 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
     g_comp_attr[slot][dev] = true;
   }
   const int span_x = full ? p.Nx : p.Nx - 4, span_y = full ? p.Ny : p.Ny - 4;
-  const int planes = full ? p.Nz : p.Nz - 4;
+  const int planes = mode == 1 ? p.Nz : p.Nz - 4;
   const int gx = (span_x + cTX - 1) / cTX, gy = (span_y + cTY - 1) / cTY;
   if (KC <= 0)
     KC = tma_auto_kc((long long)gx * gy, planes,
