@@ -138,13 +138,16 @@ class ImpedanceDesign:
     Nt (the wakelength is set so that upstream's Nt formula gives it)."""
 
     def __init__(self, solver, design, f_band=(0.5e9, 3e9), n_steps=4000, segment=None,
-                 samples=1001):
+                 samples=1001, adjoint_dtype=None):
         s = self.s = solver
         if s.precision is not None:
             raise ValueError("ImpedanceDesign needs a plain float32 / float64 solver")
         self.dev = s.device
-        self.tdtype = torch.float64 if s.dtype == np.float64 else torch.float32
-        self.wk = _native.WK_F64 if s.dtype == np.float64 else _native.WK_F32
+        # adjoint state dtype (default: the solver's); the forward states are
+        # converted to it where the parameter adjoints read them
+        adt = adjoint_dtype if adjoint_dtype is not None else s.dtype
+        self.tdtype = torch.float64 if adt == np.float64 else torch.float32
+        self.wk = _native.WK_F64 if adt == np.float64 else _native.WK_F32
         mask = np.asarray(design, bool)
         self.cells_np = np.flatnonzero(mask.ravel(order="F")).astype(np.int64)
         self.cells = torch.as_tensor(self.cells_np, device=self.dev)
@@ -338,9 +341,10 @@ class ImpedanceDesign:
                 incs.append((dt * (-bh - J)).contiguous())
             for n in range(b - 1, a - 1, -1):
                 use_sig = int(cond and n >= 1)
+                E0 = Es[n - a].to(self.tdtype)
                 _native.check(lib.wk_adj_grad(
                     self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(incs[n - a]),
-                    ptr(Es[n - a]), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
+                    ptr(E0), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
                     ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
                 _native.check(lib.wk_adj_h(
                     self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
