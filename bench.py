@@ -257,8 +257,10 @@ def run_adjoint(args):
     """Differentiation form (rank 0 only).  The cavity_40 geometry on
     128x128x256 cells (PEC walls) with a central 64^3 design region of
     per-cell eps_r ~ U[1, 10] and sigma ~ U[0, 10] S/m (seed 1); loss =
-    int_{0.5}^{3 GHz} |Z_par|^2 df; FP64 and FP32 forward + adjoint with
-    sqrt(N)-step checkpoints; 16 random directions checked against central
+    int_{0.5}^{3 GHz} |Z_par|^2 df; forward + adjoint in FP64, FP32,
+    FP32-compensated forward with an FP64 adjoint and FP32-compensated
+    forward with an FP32 adjoint, with sqrt(N)-step checkpoints; 16 random
+    directions checked against central
     differences of FP64 forward runs (Richardson-extrapolated from steps
     1e-3 and 5e-4 along the direction)."""
     ws, rank, local = _dist()
@@ -272,18 +274,22 @@ def run_adjoint(args):
     nsteps = args.adjoint_steps
     rng = np.random.default_rng(1)
 
-    def problem(dtype):
-        _, _, s = workloads.build_b200("cavity_40", dtype=dtype, shape=shape)
+    def problem(dtype, precision=None, adjoint_dtype=None):
+        _, _, s = workloads.build_b200("cavity_40", dtype=dtype, shape=shape,
+                                       precision=precision)
         m = np.zeros(shape, bool)
         c = [n // 2 for n in shape]
         h = [min(32, n // 4) for n in shape]
         m[c[0] - h[0]:c[0] + h[0], c[1] - h[1]:c[1] + h[1], c[2] - h[2]:c[2] + h[2]] = True
-        return ImpedanceDesign(s, m, n_steps=nsteps), int(m.sum())
+        return (ImpedanceDesign(s, m, n_steps=nsteps, adjoint_dtype=adjoint_dtype),
+                int(m.sum()))
 
     runs = {}
-    for name, dt_ in (("f64", np.float64), ("f32", np.float32)):
+    forms = (("f64", np.float64, None, None), ("f32", np.float32, None, None),
+             ("fp32c", np.float64, "fp32c", None), ("fp32c_adj32", np.float64, "fp32c", np.float32))
+    for name, dt_, prec, adt in forms:
         t0 = time.perf_counter()
-        prob, nd = problem(dt_)
+        prob, nd = problem(dt_, prec, adt)
         t_setup = time.perf_counter() - t0
         if name == "f64":
             er = rng.uniform(1.0, 10.0, nd)
@@ -301,12 +307,12 @@ def run_adjoint(args):
         N = prob.s.N
         runs[name] = dict(L=L, ge=ge, gs=gs, forward_s=t_fwd, backward_s=t_bwd,
                           setup_s=t_setup)
-        if name == "f32":
+        if name != "f64":
             del prob
             torch.cuda.empty_cache()
         else:
             p64 = prob
-    errs = {"f64": [], "f32": []}
+    errs = {name: [] for name in runs}
 
     def central(v_e, v_s, h):
         p64.set_params(er + h * v_e, sg + h * v_s)
@@ -386,7 +392,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=4000)
     ap.add_argument("--adjoint", action="store_true",
                     help="differentiation form: 128x128x256 cavity with a 64^3 design region, "
-                         "FP32 forward + adjoint (4000 steps), gradient checked on 16 random "
+                         "FP64 / FP32 / FP32-compensated forward + adjoint (4000 steps), "
+                         "gradient checked on 16 random "
                          "directions against central differences of FP64 forward runs")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--batch-compare", action="store_true",

@@ -357,14 +357,16 @@ def test_fp32c_tma_close_to_twopass(tile):
     assert rel_err(ha.cpu().numpy(), hb.cpu().numpy()) <= 2e-6
 
 
+@pytest.mark.parametrize("shape", [(16, 12, 20), (20, 12, 20)])
 @pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
                                  (["periodic", "pec", "pml"], ["periodic", "pec", "pml"])])
-def test_fp32c_tma_fields_close_to_oracle(bcs):
-    """Compensated TMA path from random fields on a 16x12x20 grid with
-    conductive materials: E and H after 8 steps within 1e-5 relative of the
-    FP64 oracle."""
+def test_fp32c_tma_fields_close_to_oracle(bcs, shape):
+    """Compensated TMA path from random fields on a 16x12x20 grid (row pitch
+    Nx % 8 == 0: compensation words staged by TMA) and a 20x12x20 grid
+    (per-thread loads) with conductive materials: E and H after 8 steps
+    within 1e-5 relative of the FP64 oracle."""
     c = dict(cases.STEP_CASES[2])
-    c.update(shape=(16, 12, 20), dtype="float64", bc_low=bcs[0], bc_high=bcs[1], steps=8,
+    c.update(shape=shape, dtype="float64", bc_low=bcs[0], bc_high=bcs[1], steps=8,
              n_pml=3)
     o = oracle_step_case(c)
     s = b200_step_case(c, precision="fp32c")
@@ -420,12 +422,12 @@ def test_batched_fp32c_close_to_fp64():
         assert rel_err(np.abs(np.asarray(wa.Z)), np.abs(np.asarray(wb_.Z))) <= 1e-4
 
 
-def _design_problem(dtype, n_steps=800, adjoint_dtype=None):
+def _design_problem(dtype, n_steps=800, adjoint_dtype=None, precision=None):
     """cavity_40 geometry with an 8x8x8-cell design region at the centre,
-    PEC walls (dt not clamped), FP32 or FP64."""
+    PEC walls (dt not clamped), FP32, FP64 or FP32-compensated."""
     from wakis_b200 import workloads
     from wakis_b200.adjoint import ImpedanceDesign
-    _, _, s = workloads.build_b200("cavity_40", dtype=dtype)
+    _, _, s = workloads.build_b200("cavity_40", dtype=dtype, precision=precision)
     m = np.zeros((s.Nx, s.Ny, s.Nz), bool)
     m[16:24, 16:24, 36:44] = True
     return ImpedanceDesign(s, m, f_band=(0.5e9, 3e9), n_steps=n_steps, segment=30,
@@ -454,19 +456,23 @@ def test_adjoint_operators_match_step_kernels():
     assert rel_err(s.E.numpy(), E1) <= 1e-13
 
 
-@pytest.mark.parametrize("dtype,adt,tol", [(np.float64, None, 1e-5), (np.float32, None, 5e-2),
-                                           (np.float32, np.float64, 5e-2)])
-def test_adjoint_gradient_matches_central_differences(dtype, adt, tol):
+@pytest.mark.parametrize("dtype,prec,adt,tol", [
+    (np.float64, None, None, 1e-5), (np.float64, "fp32c", None, 1e-5),
+    (np.float64, "fp32c", np.float32, 1e-5),
+    (np.float32, None, None, 5e-2), (np.float32, None, np.float64, 5e-2)])
+def test_adjoint_gradient_matches_central_differences(dtype, prec, adt, tol):
     """dL/d(eps_r, sigma) of L = int_{0.5}^{3 GHz} |Z|^2 df from the adjoint
     against central finite differences of FP64 forward runs along 4 random
-    directions of the 1024 parameters: within 1e-5 with the FP64 forward and
-    adjoint; the float32 forward/adjoint (no compensation) is within a few
-    per cent, the accuracy of its float state over 800 steps."""
+    directions of the 1024 parameters: within 1e-5 with the FP64 adjoint
+    after an FP64 or FP32-compensated forward, and with a float32 adjoint
+    state after the compensated forward; the plain float32 forward (either
+    adjoint dtype) within a few per cent, the accuracy of its float state
+    over 800 steps."""
     rng = np.random.default_rng(1)
     nd = 512
     er = rng.uniform(1.0, 10.0, nd)
     sg = rng.uniform(0.0, 10.0, nd)
-    p = _design_problem(dtype, adjoint_dtype=adt)
+    p = _design_problem(dtype, adjoint_dtype=adt, precision=prec)
     p.set_params(er, sg)
     L = p.forward()
     ge, gs = p.backward()
@@ -486,7 +492,7 @@ def test_adjoint_gradient_matches_central_differences(dtype, adt, tol):
         # Richardson extrapolation of two central differences: O(h^4)
         fd = (4.0 * central(ve, vs, 5e-4) - central(ve, vs, 1e-3)) / 3.0
         ad = ge @ ve + gs @ vs
-        print("adjoint", dtype.__name__, adt, t, abs(ad - fd) / abs(fd))
+        print("adjoint", dtype.__name__, prec, adt, t, abs(ad - fd) / abs(fd))
         assert abs(ad - fd) <= tol * abs(fd), (t, ad, fd)
 
 

@@ -57,25 +57,34 @@ constexpr int R_HXA = 0, R_HXB = 10, R_HYA = 20, R_HYB = 86, R_EXA = 152, R_EXB 
 struct CompMaps {
   CUtensorMap e[3];
   CUtensorMap h[3];
+  CUtensorMap c[6];        // compensation words (CT): Hc x/y/z, then Ec x/y/z
 };
 
 // FULL (every face PEC-masked): tiles from i0 = 64 bx cover the whole grid
 // and both boxes start at i0-4 (16-byte aligned): E 72 wide, H 68 wide.
+// The compensation-word boxes (CT) are 9 rows from j0-1 and start at an x
+// that is a multiple of 8 (16 bytes of bf16 words): i0-8, 80 wide (FULL),
+// or i0-2, 72 wide.
 template <bool FULL>
 struct CGeom {
   static constexpr int ebx = FULL ? cTX + 8 : cBX;   // E box width
   static constexpr int hbx = cBX;                    // H box width (68)
   static constexpr int xo = FULL ? 3 : 1;            // box x of ext column 0
   static constexpr int xs_off = FULL ? 4 : 2;        // box start = i0 - xs_off
+  static constexpr int cbx = FULL ? cTX + 16 : cTX + 8;   // compensation box width
+  static constexpr int cxs_off = FULL ? 8 : 2;            // its start = i0 - cxs_off
+  static constexpr int cxo = cxs_off - 1;                 // its x of ext column 0
 };
 
-template <bool FULL>
+template <bool FULL, bool CT>
 struct CLayout {
   static constexpr int eslot = round128(CGeom<FULL>::ebx * cBY * 4);
   static constexpr int hslot = round128(CGeom<FULL>::hbx * cHBY * 4);
+  static constexpr int cslot = CT ? round128(CGeom<FULL>::cbx * cHBY * 2) : 0;
   static constexpr int e_off = 0;
   static constexpr int h_off = e_off + cES * 3 * eslot;
-  static constexpr int hs_off = h_off + cHS * 3 * hslot;
+  static constexpr int c_off = h_off + cHS * 3 * hslot;      // [cHS][6][cslot]
+  static constexpr int hs_off = c_off + cHS * 6 * cslot;
   static constexpr int row_off = hs_off + round128(3 * cExt * 4);
   static constexpr int mat_off = row_off + round128(2 * cRow * 4);
   static constexpr int bar_off = mat_off + round128(cMat * cMatW * 4);
@@ -169,7 +178,9 @@ __device__ __forceinline__ float row_value(double dt, double f, double g) {
 }
 
 // IdT: material id type; SIG: the J entering a row is sigma * E (the
-// conductive J mode) rather than zero.  MODE 0: interior cells, the shell
+// conductive J mode) rather than zero; CT: the compensation words of plane k
+// arrive by TMA with H(k) (row pitch Nx % 8 == 0) instead of per-thread
+// loads issued one plane ahead.  MODE 0: interior cells, the shell
 // follows in separate launches.  MODE 1: every face carries the PEC column
 // mask (no PMC); the tiles cover the whole grid and the cells on or next to
 // a face use the same rows with the masked entries set to zero (E entries
@@ -178,21 +189,22 @@ __device__ __forceinline__ float row_value(double dt, double f, double g) {
 // masked), so no shell launch follows.  MODE 2: the x/y faces are PEC-masked
 // and the z faces are not; the tiles cover all of x and y for the planes
 // 2 <= k <= Nz-3 and the shell launches cover only the four boundary planes.
-template <typename IdT, bool SIG, int MODE>
+template <typename IdT, bool SIG, int MODE, bool CT>
 __global__ void __launch_bounds__(cThreads, 2)
 k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
            long long step, int KC) {
   constexpr bool FULL = MODE != 0;     // tiles cover x and y entirely
   constexpr bool ZFULL = MODE == 1;    // ... and every plane
   step = step_index(p, step);
-  using Lay = CLayout<(MODE != 0)>;
+  using Lay = CLayout<(MODE != 0), CT>;
   using G = CGeom<(MODE != 0)>;
-  constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4;
+  constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4, SC = Lay::cslot / 2;
   constexpr int EBX = G::ebx, XO = G::xo;
   extern __shared__ __align__(128) unsigned char sm_raw[];
   unsigned char* sm = sm_raw + ((128 - (smem_u32(sm_raw) & 127)) & 127);
   float* Eb = reinterpret_cast<float*>(sm + Lay::e_off);
   float* Hb = reinterpret_cast<float*>(sm + Lay::h_off);
+  uint16_t* Cb = reinterpret_cast<uint16_t*>(sm + Lay::c_off);   // [cHS][6][SC]
   float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][cExt]
   float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][cRow]
   float* mt = reinterpret_cast<float*>(sm + Lay::mat_off);    // [n_mat][16]
@@ -206,7 +218,8 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int pstart = k0 - 1;
-  const uint32_t e_bytes = 3u * EBX * cBY * 4u, h_bytes = 3u * G::hbx * cHBY * 4u;
+  const uint32_t e_bytes = 3u * EBX * cBY * 4u;
+  const uint32_t h_bytes = 3u * G::hbx * cHBY * 4u + (CT ? 6u * G::cbx * cHBY * 2u : 0u);
 
   if (tid == 0) {
     for (int s = 0; s < cES + cHS; s++) mbar_init(&bar[s], 1);
@@ -225,6 +238,12 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
 #pragma unroll
     for (int d = 0; d < 3; d++)
       tma_load_3d(Hb + (slot * 3 + d) * SH, &maps.h[d], xs, ys, q, &bar[cES + slot]);
+    if (CT) {
+#pragma unroll
+      for (int c = 0; c < 6; c++)
+        tma_load_3d(Cb + (slot * 6 + c) * SC, &maps.c[c], i0 - G::cxs_off, ys, q,
+                    &bar[cES + slot]);
+    }
   };
   auto wait_e = [&](int q) {
     return mbar_wait(&bar[(q - pstart) % cES], (uint32_t)(((q - pstart) / cES) & 1));
@@ -259,7 +278,11 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   const bool nearface = hval && (xf0a || xf1a || (pair && (xf0b || xf1b)) || yf0 || yf1);
   const bool warp_face = FULL && __any_sync(0xffffffffu, nearface);
   const int hi = eb * cEW + ea + 1;                       // Hs index
+  const int cix = eb * G::cbx + ea + G::cxo;              // compensation box index
   const long long nb = ci + (long long)cj * Nx;           // flat index at k = 0
+  // the item holds a cell of the Ez capture window (plane-invariant test)
+  const bool cap_item = eval && p.cap_on && cj >= p.cap_j0 && cj < p.cap_j0 + p.cap_nj &&
+                        ci + 1 >= p.cap_i0 && ci < p.cap_i0 + p.cap_ni;
 
   // plane-invariant z-row factors
   float2 hza = bcast(0.f), hzb = bcast(0.f), eza = bcast(0.f), ezb = bcast(0.f);
@@ -302,11 +325,18 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       w[d] = pair ? *reinterpret_cast<const uint32_t*>(base + d * N + n)
                   : (uint32_t)base[d * N + n];
   };
+  // compensation words from the staged box (CT): components c0..c0+2
+  auto read_comp = [&](const uint16_t* Ck, int c0, uint32_t* w) {
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      w[d] = pair ? *reinterpret_cast<const uint32_t*>(Ck + (c0 + d) * SC + cix)
+                  : (uint32_t)Ck[(c0 + d) * SC + cix];
+  };
   int id0 = 0, id1 = 0;
   uint32_t hc[3] = {0, 0, 0}, ec[3] = {0, 0, 0};
   if (hval && pstart >= 0) {
     load_ids(pstart, id0, id1);
-    load_comp(cs.Hc_in, pstart, hc);
+    if (!CT) load_comp(cs.Hc_in, pstart, hc);
   }
   const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
   if (tid < cRow) {
@@ -338,14 +368,15 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     if (more) {
       if (hval) {
         load_ids(pl + 1, nid0, nid1);
-        load_comp(cs.Hc_in, pl + 1, nhc);
+        if (!CT) load_comp(cs.Hc_in, pl + 1, nhc);
       }
-      if (eval) load_comp(cs.Ec_in, pl + 1, nec);
+      if (!CT && eval) load_comp(cs.Ec_in, pl + 1, nec);
       if (tid < cRow) row_load(rsrc, pl + 1, Nz, rf, rg);
     }
     const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
     const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
     const float* Hk = Hb + ((pl - pstart) % cHS) * 3 * SH;
+    const uint16_t* Ck = Cb + ((pl - pstart) % cHS) * 6 * SC;
     const float* R = Rw + (pl & 1) * cRow;
     const long long n = nb + (long long)pl * NxNy;
 
@@ -410,6 +441,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       // S_z = a (ex0 - ex2) + b (ey1 - ey0)   (a = dt iAz Lx imu_z, b = dt iAz Ly imu_z)
       const float2 sz = fma2(mul2(muz, hza), sub2(ex0, ex2), mul2(mul2(muz, hzb), sub2(ey1, ey0)));
       const float2 m1v = bcast(-1.0f);
+      if (CT) read_comp(Ck, 0, hc);
       hx = cadd2(hx, hc[0], mul2(sx, m1v));
       hy = cadd2(hy, hc[1], mul2(sy, m1v));
       hz = cadd2(hz, hc[2], mul2(sz, m1v));
@@ -462,7 +494,8 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         cu[2] = make_float2((xf0a || yf0) ? 0.f : cu[2].x, (xf0b || yf0) ? 0.f : cu[2].y);
       }
       float2 ev[3] = {ld2(Ek + bi), ld2(Ek + SE + bi), ld2(Ek + 2 * SE + bi)};
-      if (p.cap_on) {
+      if (CT) read_comp(Ck, 3, ec);
+      if (cap_item) {
 #pragma unroll
         for (int u = 0; u < 2; u++) {
           Cell c;
@@ -496,10 +529,12 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     hxp = hxn;
     hyp = hyn;
     id0 = nid0; id1 = nid1;
+    if (!CT) {
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      hc[d] = nhc[d];
-      ec[d] = nec[d];
+      for (int d = 0; d < 3; d++) {
+        hc[d] = nhc[d];
+        ec[d] = nec[d];
+      }
     }
     if (more && tid < cRow) Rw[((pl + 1) & 1) * cRow + tid] = row_value(p.dt, rf, rg);
   }
@@ -513,20 +548,26 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   }
 }
 
-bool encode_f32(CUtensorMap* map, const float* base, int Nx, int Ny, int Nz, int bx, int by) {
+// 3-D tensor map of an (Nx, Ny, Nz) array of `esize`-byte elements (float
+// or raw bf16 words) with a bx x by x 1 box
+bool encode_3d(CUtensorMap* map, const void* base, int esize, int Nx, int Ny, int Nz, int bx,
+               int by) {
   cuuint64_t gdim[3] = {(cuuint64_t)Nx, (cuuint64_t)Ny, (cuuint64_t)Nz};
-  cuuint64_t gstr[2] = {(cuuint64_t)Nx * 4, (cuuint64_t)Nx * Ny * 4};
+  cuuint64_t gstr[2] = {(cuuint64_t)Nx * esize, (cuuint64_t)Nx * Ny * esize};
   cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   cuuint32_t est[3] = {1, 1, 1};
-  CUresult r = tma_encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, gdim,
-                               gstr, box, est, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  const CUtensorMapDataType dt =
+      esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+  CUresult r = tma_encode_fn()(map, dt, 3, const_cast<void*>(base), gdim, gstr, box, est,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 
-int g_comp_sms[18][64], g_comp_per_sm[18][64];
-bool g_comp_attr[18][64];
+constexpr int kCompKernels = 36;
+int g_comp_sms[kCompKernels][64], g_comp_per_sm[kCompKernels][64];
+bool g_comp_attr[kCompKernels][64];
 
 }  // namespace
 
@@ -555,9 +596,16 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   CompState cs = comp_state(d, par);
   CompMaps maps;
   const int ebx = full ? CGeom<true>::ebx : CGeom<false>::ebx;
+  const int cbx = full ? CGeom<true>::cbx : CGeom<false>::cbx;
+  // compensation words by TMA: 16-byte row pitch and component bases
+  const bool ct = p.Nx % 8 == 0 && ((uintptr_t)cs.Hc_in % 16) == 0 &&
+                  ((uintptr_t)cs.Ec_in % 16) == 0;
   for (int c = 0; c < 3; c++) {
-    if (!encode_f32(&maps.e[c], cs.E_in + c * p.N, p.Nx, p.Ny, p.Nz, ebx, cBY) ||
-        !encode_f32(&maps.h[c], cs.H_in + c * p.N, p.Nx, p.Ny, p.Nz, cBX, cHBY))
+    if (!encode_3d(&maps.e[c], cs.E_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, ebx, cBY) ||
+        !encode_3d(&maps.h[c], cs.H_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, cBX, cHBY))
+      return cudaErrorInvalidValue;
+    if (ct && (!encode_3d(&maps.c[c], cs.Hc_in + c * p.N, 2, p.Nx, p.Ny, p.Nz, cbx, cHBY) ||
+               !encode_3d(&maps.c[3 + c], cs.Ec_in + c * p.N, 2, p.Nx, p.Ny, p.Nz, cbx, cHBY)))
       return cudaErrorInvalidValue;
   }
   int dev = 0;
@@ -566,20 +614,23 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   const int ib = p.id_bytes == 1 ? 0 : (p.id_bytes == 2 ? 1 : 2);
   const bool sig = p.j_mode == WK_J_SIGMA_E;
-  const int slot = mode * 6 + ib * 2 + (sig ? 1 : 0);
+  const int slot = (ct ? 18 : 0) + mode * 6 + ib * 2 + (sig ? 1 : 0);
   using K = void (*)(FitParams<double>, CompState, const CompMaps, long long, int);
-  const K kerns[18] = {
-      k_tma_comp<uint8_t, false, 0>,  k_tma_comp<uint8_t, true, 0>,
-      k_tma_comp<uint16_t, false, 0>, k_tma_comp<uint16_t, true, 0>,
-      k_tma_comp<uint32_t, false, 0>, k_tma_comp<uint32_t, true, 0>,
-      k_tma_comp<uint8_t, false, 1>,  k_tma_comp<uint8_t, true, 1>,
-      k_tma_comp<uint16_t, false, 1>, k_tma_comp<uint16_t, true, 1>,
-      k_tma_comp<uint32_t, false, 1>, k_tma_comp<uint32_t, true, 1>,
-      k_tma_comp<uint8_t, false, 2>,  k_tma_comp<uint8_t, true, 2>,
-      k_tma_comp<uint16_t, false, 2>, k_tma_comp<uint16_t, true, 2>,
-      k_tma_comp<uint32_t, false, 2>, k_tma_comp<uint32_t, true, 2>};
+#define WK_COMP_KERNS(CT)                                                          \
+  k_tma_comp<uint8_t, false, 0, CT>, k_tma_comp<uint8_t, true, 0, CT>,             \
+      k_tma_comp<uint16_t, false, 0, CT>, k_tma_comp<uint16_t, true, 0, CT>,       \
+      k_tma_comp<uint32_t, false, 0, CT>, k_tma_comp<uint32_t, true, 0, CT>,       \
+      k_tma_comp<uint8_t, false, 1, CT>, k_tma_comp<uint8_t, true, 1, CT>,         \
+      k_tma_comp<uint16_t, false, 1, CT>, k_tma_comp<uint16_t, true, 1, CT>,       \
+      k_tma_comp<uint32_t, false, 1, CT>, k_tma_comp<uint32_t, true, 1, CT>,       \
+      k_tma_comp<uint8_t, false, 2, CT>, k_tma_comp<uint8_t, true, 2, CT>,         \
+      k_tma_comp<uint16_t, false, 2, CT>, k_tma_comp<uint16_t, true, 2, CT>,       \
+      k_tma_comp<uint32_t, false, 2, CT>, k_tma_comp<uint32_t, true, 2, CT>
+  const K kerns[kCompKernels] = {WK_COMP_KERNS(false), WK_COMP_KERNS(true)};
+#undef WK_COMP_KERNS
   const K kern = kerns[slot];
-  const int smem = full ? CLayout<true>::bytes : CLayout<false>::bytes;
+  const int smem = full ? (ct ? CLayout<true, true>::bytes : CLayout<true, false>::bytes)
+                        : (ct ? CLayout<false, true>::bytes : CLayout<false, false>::bytes);
   if (!g_comp_attr[slot][dev]) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
