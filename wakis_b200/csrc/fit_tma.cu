@@ -16,10 +16,10 @@
 // Per plane the block computes the new H on the tile plus its low halo row
 // and column (single-coefficient rows; the halo is recomputed so that no
 // block waits for another), a barrier, then the new E of the tile.  Each
-// thread owns the same tile cells in both phases (320 threads: cells t and
-// t+320 of the 512-cell tile; threads 192..264 also own one halo cell), so
-// the new Hx, Hy of its tile cells stay in registers as H(k-1) of the next
-// plane.  Material ids of the owned cells and the per-plane metric rows
+// thread owns the same cells in both phases (warps 0-7: row j0+w of the
+// tile, cells i0+lane and i0+32+lane; warp 8: the halo row; warp 9: the halo
+// column and the last cell of the halo row), so the new Hx, Hy of its tile
+// cells stay in registers as H(k-1) of the next plane.  Material ids of the owned cells and the per-plane metric rows
 // (iAx, iAy, itAx, itAy, Lz, tLz) of plane k+1 are loaded while plane k is
 // computed; the plane-invariant metrics (Lx, Ly, iAz, ...) are loaded once.
 // A chunk starting at k0 first forms the new H of plane k0-1 on its tile.
@@ -42,10 +42,8 @@ constexpr int kBX = kTX + 4, kBY = kTY + 2;          // E box
 constexpr int kHBY = kTY + 1;                        // H box rows
 constexpr int kES = 3, kHS = 2;                      // ring slots
 constexpr int kTmaThreads = 320;
-constexpr int kTile = kTX * kTY;                     // 512
 constexpr int kEW = kTX + 1;                         // ext tile row width
 constexpr int kExt = kEW * (kTY + 1);                // 585
-constexpr int kHalo = kEW + kTY;                     // 73
 constexpr int kRow = 148;                            // per-plane metric values
 constexpr int kMatSmem = 32;                         // materials staged in smem
 
@@ -86,10 +84,6 @@ struct TmaLayout {
   static constexpr int bytes = bar_off + (kES + kHS) * 8 + 128;   // + base alignment
 };
 
-// Ext-tile index (row width 65, origin at (i0-1, j0-1)) of tile cell o.
-__device__ __forceinline__ int ext_of_tile(int o) { return (o / kTX + 1) * kEW + o % kTX + 1; }
-// Ext-tile index of halo cell h: row j0-1 (h < 65), then column i0-1.
-__device__ __forceinline__ int ext_of_halo(int h) { return h < kEW ? h : (h - kEW + 1) * kEW; }
 
 // Per-plane metric row of plane q: [0,9) iAx(j0-1..j0+7), [9,74) iAy(i0-1..i0+63),
 // [74,82) itAx(j0..j0+7), [82,146) itAy(i0..i0+63), 146 Lz, 147 tLz.
@@ -195,22 +189,27 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     for (int q = pstart; q <= min(pstart + kHS - 1, k1 - 1); q++) { issue_h(q); h_hi = q; }
   }
 
-  // owned cells: tile cells t and t+320 (t < 192); threads 192..264 also
-  // compute the H of halo cell t-192
-  const bool two = tid < kTile - kTmaThreads;
-  const bool halo = !two && tid < kTile - kTmaThreads + kHalo;
-  int ext[2], ci[2], cj[2];
+  // owned cells, in ext-tile coordinates (ea, eb) with the origin at
+  // (i0-1, j0-1): warps 0-7 the tile cells (lane+1, w+1) and (lane+33, w+1);
+  // warp 8 the halo-row cells (lane, 0) and (lane+32, 0); warp 9 lanes 0-7
+  // the halo-column cells (0, lane+1) and lane 8 the halo-row cell (64, 0).
+  // The second cell of a thread is its first one 32 columns on.
+  const int warp = tid >> 5, lane = tid & 31;
+  const bool tile = warp < 8;
+  const int ea0 = tile ? lane + 1 : (warp == 8 ? lane : (lane < 8 ? 0 : 64));
+  const int eb0 = tile ? warp + 1 : (warp == 8 ? 0 : (lane < 8 ? lane + 1 : 0));
+  const bool owns[2] = {warp < 9 || lane < 9, warp < 9};
+  const int ext0 = eb0 * kEW + ea0;
+  int ci[2], cj[2];
   bool hval[2], eval[2];
-  ext[0] = ext_of_tile(tid);
-  ext[1] = two ? ext_of_tile(tid + kTmaThreads) : (halo ? ext_of_halo(tid - (kTile - kTmaThreads)) : 0);
 #pragma unroll
   for (int r = 0; r < 2; r++) {
-    ci[r] = i0 - 1 + ext[r] % kEW;
-    cj[r] = j0 - 1 + ext[r] / kEW;
-    const bool own = r == 0 || two || halo;
+    ci[r] = i0 - 1 + ea0 + 32 * r;
+    cj[r] = j0 - 1 + eb0;
+    const bool own = owns[r];
     hval[r] = FULL ? (own && ci[r] >= 0 && ci[r] <= Nx - 1 && cj[r] >= 0 && cj[r] <= Ny - 1)
                    : (own && ci[r] <= Nx - 3 && cj[r] <= Ny - 3);
-    eval[r] = (r == 0 || two) && hval[r];
+    eval[r] = tile && hval[r];
   }
   // face flags of the owned cells (FULL): at the cell, and of the +x / +y
   // neighbour (a wrapped neighbour counts as on the face)
@@ -226,6 +225,17 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   }
   const bool warp_face = FULL && __any_sync(0xffffffffu, nearface);
   const bool desc = p.h_desc != 0;
+  // plane-invariant tests of the owned cells, one bit each: cell r in the
+  // Ez capture window (bit r), on the source line (bit 2 + r)
+  int cell_bits = 0;
+#pragma unroll
+  for (int r = 0; r < 2; r++) {
+    if (eval[r] && p.cap_on && ci[r] >= p.cap_i0 && ci[r] < p.cap_i0 + p.cap_ni &&
+        cj[r] >= p.cap_j0 && cj[r] < p.cap_j0 + p.cap_nj)
+      cell_bits |= 1 << r;
+    if (eval[r] && (p.line_on || p.beam_on) && ci[r] == p.ixs && cj[r] == p.iys)
+      cell_bits |= 4 << r;
+  }
   // plane-invariant metrics
   T iAz[2], itAz[2];
 #pragma unroll
@@ -291,16 +301,15 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 #pragma unroll
     for (int r = 0; r < 2; r++) {
       hxn[r] = hyn[r] = T(0);
-      const bool tile_cell = r == 0 || two;
-      if (FULL && (r == 0 || two || halo) && !hval[r]) {
-        const int e = ext[r];
+      const bool tile_cell = tile;
+      const int e = ext0 + 32 * r;
+      if (FULL && owns[r] && !hval[r]) {
         Hs[e] = T(0);
         Hs[kExt + e] = T(0);
         Hs[2 * kExt + e] = T(0);
       }
       if (!hval[r] || (prologue && !tile_cell) || (ZFULL && pl < 0)) continue;
-      const int e = ext[r];
-      const int ea = e % kEW, eb = e / kEW;
+      const int ea = ea0 + 32 * r, eb = eb0;
       const int bi = eb * EBX + ea + XO;
       const int hb = eb * HBX + ea + XO;
       const T* m0 = mat + 9 * id[r];
@@ -346,8 +355,8 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 #pragma unroll
       for (int r = 0; r < 2; r++) {
         if (!eval[r]) continue;
-        const int e = ext[r];
-        const int a = e % kEW - 1, b = e / kEW - 1;
+        const int e = ext0 + 32 * r;
+        const int a = ea0 + 32 * r - 1, b = eb0 - 1;
         const int bi = (b + 1) * EBX + a + 1 + XO;
         const long long n = ci[r] + (long long)cj[r] * Nx + off;
         const T* m0 = mat + 9 * id[r];
@@ -367,8 +376,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         const T eold[3] = {Ek[bi], Ek[SE + bi], Ek[2 * SE + bi]};
         Cell cc;
         cc.i = ci[r]; cc.j = cj[r]; cc.k = pl;
-        if (p.cap_on) capture(p, cc, n, step, eold[2]);
-        const bool src = (p.line_on || p.beam_on) && cc.i == p.ixs && cc.j == p.iys;
+        if (cell_bits & (1 << r)) capture(p, cc, n, step, eold[2]);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const T ieps = m0[d], sigma = m0[6 + d];
@@ -376,7 +384,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
           T jv = T(0);
           if (JM == WK_J_SIGMA_E) jv = mul(sigma, eold[d]);
           if (JM == WK_J_ARRAY) jv = p.J[d * N + n];
-          if (d == 2 && src) jv = j_in(p, d, cc, n, step, eold[d], sigma);
+          if (d == 2 && (cell_bits & (4 << r))) jv = j_in(p, d, cc, n, step, eold[d], sigma);
           const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
           p.E_out[d * N + n] = enew;
           if (JM == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);

@@ -86,7 +86,9 @@ struct CLayout {
   static constexpr int c_off = h_off + cHS * 3 * hslot;      // [cHS][6][cslot]
   static constexpr int hs_off = c_off + cHS * 6 * cslot;
   static constexpr int row_off = hs_off + round128(3 * cExt * 4);
-  static constexpr int mat_off = row_off + round128(2 * cRow * 4);
+  static constexpr int raw_off = row_off + round128(2 * cRow * 4);     // [3][cRow][2] doubles
+  static constexpr int id_off = raw_off + round128(3 * cRow * 16);     // [3][threads] u64
+  static constexpr int mat_off = id_off + round128(3 * cThreads * 8);
   static constexpr int bar_off = mat_off + round128(cMat * cMatW * 4);
   static constexpr int bytes = bar_off + (cES + cHS) * 8 + 128;
 };
@@ -164,14 +166,13 @@ __device__ __forceinline__ RowSrc row_src(const FitParams<double>& p, int r, int
   }
   return s;
 }
-__device__ __forceinline__ void row_load(const RowSrc& s, int q, int Nz, double& f, double& g) {
-  if (s.f && q >= 0 && q < Nz) {
-    f = s.f[(long long)q * s.fs];
-    g = s.g[(long long)q * s.gs];
-  } else {
-    f = 0.0;
-    g = 0.0;
-  }
+// f and g of plane q into two shared-memory doubles by cp.async (zeros
+// outside the grid; `any` is a valid address that is then not read)
+__device__ __forceinline__ void row_stage(const RowSrc& s, int q, int Nz, const double* any,
+                                          double* dst) {
+  const bool v = s.f && q >= 0 && q < Nz;
+  cp_async<8>(dst, v ? s.f + (long long)q * s.fs : any, v);
+  cp_async<8>(dst + 1, v ? s.g + (long long)q * s.gs : any, v);
 }
 __device__ __forceinline__ float row_value(double dt, double f, double g) {
   return (float)((dt * f) * g);
@@ -207,6 +208,8 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   uint16_t* Cb = reinterpret_cast<uint16_t*>(sm + Lay::c_off);   // [cHS][6][SC]
   float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][cExt]
   float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][cRow]
+  double* Rraw = reinterpret_cast<double*>(sm + Lay::raw_off); // [3][cRow][2] f, g
+  uint64_t* sidw = reinterpret_cast<uint64_t*>(sm + Lay::id_off);  // [3][threads] id words
   float* mt = reinterpret_cast<float*>(sm + Lay::mat_off);    // [n_mat][16]
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Lay::bar_off);
 
@@ -312,11 +315,40 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     mt[m * cMatW + 12 + d] = (float)((p.dt * m0[d]) * m0[6 + d]);
   }
   // ids, compensation words and factor row of the first plane
-  auto load_ids = [&](int q, int& a0, int& a1) {
+  // The material ids of the item at plane q, staged by cp.async as the
+  // aligned word(s) that hold them (a pair starts at an even cell, so both
+  // ids share one 4-byte word, or one 8-byte word for 4-byte ids); a word
+  // that would reach past the id array is composed from direct loads.
+  const IdT* ids = static_cast<const IdT*>(p.mat_id);
+  auto stage_ids = [&](int q, uint64_t* dst) {
     const long long n = nb + (long long)q * NxNy;
-    const IdT* ids = static_cast<const IdT*>(p.mat_id);
-    a0 = (int)ids[n];
-    a1 = pair ? (int)ids[n + 1] : a0;
+    if (q < 0) {
+      *dst = 0ull;
+    } else if (sizeof(IdT) == 4 && pair) {
+      cp_async<8>(dst, ids + n, true);
+    } else {
+      const long long byte = n * (long long)sizeof(IdT);
+      if ((byte | 3) < N * (long long)sizeof(IdT)) {
+        cp_async<4>(dst, reinterpret_cast<const uint32_t*>(ids) + (byte >> 2), true);
+      } else {
+        uint32_t w = (uint32_t)ids[n] << (8 * (int)(byte & 3));
+        if (pair) w |= (uint32_t)ids[n + 1] << (8 * (int)((byte + sizeof(IdT)) & 3));
+        *dst = w;
+      }
+    }
+  };
+  auto read_ids = [&](int q, const uint64_t* src, int& a0, int& a1) {
+    const long long n = nb + (long long)q * NxNy;
+    const uint64_t w = *src;
+    if (sizeof(IdT) == 4) {
+      a0 = (int)(uint32_t)w;
+      a1 = pair ? (int)(uint32_t)(w >> 32) : a0;
+    } else {
+      const int sh = (int)((n * (long long)sizeof(IdT)) & 3) * 8;
+      const uint32_t m = sizeof(IdT) == 1 ? 0xffu : 0xffffu;
+      a0 = (int)(((uint32_t)w >> sh) & m);
+      a1 = pair ? (int)(((uint32_t)w >> (sh + 8 * (int)sizeof(IdT))) & m) : a0;
+    }
   };
   auto load_comp = [&](const comp_t* base, int q, uint32_t* w) {
     const long long n = nb + (long long)q * NxNy;
@@ -332,18 +364,30 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       w[d] = pair ? *reinterpret_cast<const uint32_t*>(Ck + (c0 + d) * SC + cix)
                   : (uint32_t)Ck[(c0 + d) * SC + cix];
   };
-  int id0 = 0, id1 = 0;
   uint32_t hc[3] = {0, 0, 0}, ec[3] = {0, 0, 0};
-  if (hval && pstart >= 0) {
-    load_ids(pstart, id0, id1);
-    if (!CT) load_comp(cs.Hc_in, pstart, hc);
-  }
+  if (!CT && hval && pstart >= 0) load_comp(cs.Hc_in, pstart, hc);
   const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
-  if (tid < cRow) {
-    double f, g;
-    row_load(rsrc, pstart, Nz, f, g);
-    Rw[(pstart & 1) * cRow + tid] = row_value(p.dt, f, g);
-  }
+  // the factor-row inputs and the ids of plane q go into ring slot
+  // (q - pstart) % 3 two planes ahead (one cp.async group per plane); the
+  // float row of plane q is formed at the end of plane q-1
+  auto stage = [&](int q) {
+    if (q < k1) {
+      const int b = (q - pstart) % 3;
+      if (tid < cRow) row_stage(rsrc, q, Nz, p.Lz, Rraw + (b * cRow + tid) * 2);
+      if (hval) stage_ids(q, sidw + b * cThreads + tid);
+    }
+    cp_async_commit();
+  };
+  auto form_row = [&](int q) {
+    if (tid < cRow) {
+      const double* r = Rraw + (((q - pstart) % 3) * cRow + tid) * 2;
+      Rw[(q & 1) * cRow + tid] = row_value(p.dt, r[0], r[1]);
+    }
+  };
+  stage(pstart);
+  stage(pstart + 1);
+  cp_async_wait<1>();
+  form_row(pstart);
   float2 hxp = bcast(0.f), hyp = bcast(0.f);
   const float2 zero2 = bcast(0.f);
 
@@ -360,18 +404,15 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       if (pl + cES - 1 <= k1) { issue_e(pl + cES - 1); e_hi = pl + cES - 1; }
       if (pl + cHS - 1 <= k1 - 1) { issue_h(pl + cHS - 1); h_hi = pl + cHS - 1; }
     }
-    // prefetch plane pl+1: ids, compensation words, factor-row inputs
+    int id0 = 0, id1 = 0;
+    if (hval) read_ids(pl, sidw + ((pl - pstart) % 3) * cThreads + tid, id0, id1);
+    stage(pl + 2);               // the ring slot of plane pl-1 is free
+    // prefetch the compensation words of plane pl+1 (per-thread loads)
     const bool more = pl + 1 < k1;
-    int nid0 = 0, nid1 = 0;
     uint32_t nhc[3] = {0, 0, 0}, nec[3] = {0, 0, 0};
-    double rf = 0.0, rg = 0.0;
-    if (more) {
-      if (hval) {
-        load_ids(pl + 1, nid0, nid1);
-        if (!CT) load_comp(cs.Hc_in, pl + 1, nhc);
-      }
-      if (!CT && eval) load_comp(cs.Ec_in, pl + 1, nec);
-      if (tid < cRow) row_load(rsrc, pl + 1, Nz, rf, rg);
+    if (!CT && more) {
+      if (hval) load_comp(cs.Hc_in, pl + 1, nhc);
+      if (eval) load_comp(cs.Ec_in, pl + 1, nec);
     }
     const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
     const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
@@ -528,7 +569,6 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     }
     hxp = hxn;
     hyp = hyn;
-    id0 = nid0; id1 = nid1;
     if (!CT) {
 #pragma unroll
       for (int d = 0; d < 3; d++) {
@@ -536,8 +576,12 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         ec[d] = nec[d];
       }
     }
-    if (more && tid < cRow) Rw[((pl + 1) & 1) * cRow + tid] = row_value(p.dt, rf, rg);
+    if (more) {
+      cp_async_wait<1>();        // this thread's row inputs and ids of plane pl+1
+      form_row(pl + 1);
+    }
   }
+  cp_async_wait<0>();
   if (!ok) {
     if (tid == 0) {
       if (p.status) atomicExch(p.status, 1);

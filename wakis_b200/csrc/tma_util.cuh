@@ -50,6 +50,36 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// cp.async (LDGSTS) of one 4- or 8-byte word into shared memory; with
+// valid == false nothing is read and the word is zero-filled.  Completion is
+// per thread: cp_async_commit() closes a group, cp_async_wait<N>() waits
+// until at most N of this thread's groups are still in flight.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid) {
+  static_assert(BYTES == 4 || BYTES == 8, "cp.async word size");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src),
+               "n"(BYTES), "r"(valid ? BYTES : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Material id n of an id array of `bytes`-byte entries (1, 2 or 4) held in
+// the 4-byte word that contains it: the word's index and the id's position.
+__device__ __forceinline__ long long id_word_index(int bytes, long long n) {
+  return (n * bytes) >> 2;
+}
+__device__ __forceinline__ int id_from_word(uint32_t w, int bytes, long long n) {
+  if (bytes == 4) return (int)w;
+  const int sh = (int)((n * bytes) & 3) * 8;
+  return (int)((w >> sh) & (bytes == 1 ? 0xffu : 0xffffu));
+}
+
 // cuTensorMapEncodeTiled from the driver, fetched once through the runtime
 // (the library links only the CUDA runtime); nullptr when unavailable.
 inline PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn() {
