@@ -78,7 +78,7 @@ struct TmaLayout {
   static constexpr int h_off = e_off + kES * 3 * eslot;
   static constexpr int hs_off = h_off + kHS * 3 * hslot;
   static constexpr int row_off = hs_off + round128(3 * kExt * (int)sizeof(T));
-  static constexpr int l_off = row_off + round128(2 * kRow * (int)sizeof(T));
+  static constexpr int l_off = row_off + round128(3 * kRow * (int)sizeof(T));
   static constexpr int mat_off = l_off + round128((kEW + kTY + 1 + kTX + kTY) * (int)sizeof(T));
   static constexpr int bar_off = mat_off + round128(9 * kMatSmem * (int)sizeof(T));
   static constexpr int bytes = bar_off + (kES + kHS) * 8 + 128;   // + base alignment
@@ -87,24 +87,28 @@ struct TmaLayout {
 
 // Per-plane metric row of plane q: [0,9) iAx(j0-1..j0+7), [9,74) iAy(i0-1..i0+63),
 // [74,82) itAx(j0..j0+7), [82,146) itAy(i0..i0+63), 146 Lz, 147 tLz.
-// Entries outside the grid (index < 0 or beyond the last cell, plane q
-// outside [0, Nz)) read as 0.
+// Entry r of plane q is a[q * stride] (RowEntry); entries outside the grid
+// (index < 0 or beyond the last cell, a == nullptr) and planes outside
+// [0, Nz) read as 0.
 template <typename T>
-__device__ __forceinline__ T row_value(const FitParams<T>& p, int r, int q, int i0, int j0) {
-  if (q < 0 || q >= p.Nz) return T(0);
-  int idx;
+struct RowEntry {
   const T* a;
-  if (r < 9) { idx = j0 - 1 + r; a = p.iAx; if (idx < 0 || idx >= p.Ny) return T(0); idx += q * p.Ny; }
-  else if (r < 74) { idx = i0 - 10 + r; a = p.iAy; if (idx < 0 || idx >= p.Nx) return T(0); idx += q * p.Nx; }
-  else if (r < 82) { idx = j0 - 74 + r; a = p.itAx; if (idx < 0 || idx >= p.Ny) return T(0); idx += q * p.Ny; }
-  else if (r < 146) { idx = i0 - 82 + r; a = p.itAy; if (idx < 0 || idx >= p.Nx) return T(0); idx += q * p.Nx; }
-  else if (r == 146) return p.Lz[q];
-  else return p.tLz[q];
-  return a[idx];
+  int stride;
+};
+template <typename T>
+__device__ __forceinline__ RowEntry<T> row_entry(const FitParams<T>& p, int r, int i0, int j0) {
+  int idx;
+  if (r < 9) { idx = j0 - 1 + r; if (idx < 0 || idx >= p.Ny) return {nullptr, 0}; return {p.iAx + idx, p.Ny}; }
+  if (r < 74) { idx = i0 - 10 + r; if (idx < 0 || idx >= p.Nx) return {nullptr, 0}; return {p.iAy + idx, p.Nx}; }
+  if (r < 82) { idx = j0 - 74 + r; if (idx < 0 || idx >= p.Ny) return {nullptr, 0}; return {p.itAx + idx, p.Ny}; }
+  if (r < 146) { idx = i0 - 82 + r; if (idx < 0 || idx >= p.Nx) return {nullptr, 0}; return {p.itAy + idx, p.Nx}; }
+  if (r == 146) return {p.Lz, 1};
+  if (r == 147) return {p.tLz, 1};
+  return {nullptr, 0};
 }
 
-// SM: the material table fits in shared memory (n_mat <= kMatSmem); the
-// table reads are then shared-memory loads.  JM: the J mode of the launch
+// SM: the material table fits in shared memory (n_mat <= kMatSmem) and the
+// ids are one byte each; the table reads are then shared-memory loads.  JM: the J mode of the launch
 // (WK_J_ZERO, WK_J_SIGMA_E or WK_J_ARRAY), fixed at compile time.
 // MODE 0: interior cells only (2 <= i, j, k <= N-3), the two-cell shell runs
 // in separate launches.  MODE 1: every face of the grid carries the PEC
@@ -138,7 +142,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   T* Eb = reinterpret_cast<T*>(sm + Lay::e_off);     // [kES][3][SE]
   T* Hb = reinterpret_cast<T*>(sm + Lay::h_off);     // [kHS][3][SH]
   T* Hs = reinterpret_cast<T*>(sm + Lay::hs_off);    // [3][kExt] new H of the plane
-  T* Rw = reinterpret_cast<T*>(sm + Lay::row_off);   // [2][kRow] per-plane metrics
+  T* Rw = reinterpret_cast<T*>(sm + Lay::row_off);   // [3][kRow] per-plane metrics
   T* sLx = reinterpret_cast<T*>(sm + Lay::l_off);    // Lx(i0-1..i0+63)
   T* sLy = sLx + kEW;                                // Ly(j0-1..j0+7)
   T* stLx = sLy + kTY + 1;                           // tLx(i0..i0+63)
@@ -251,19 +255,40 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   if (SM)
     for (int q = tid; q < 9 * p.n_mat; q += kTmaThreads) smat[q] = p.mat[q];
   const T* mat = SM ? smat : p.mat;
-  // ids and metric row of the first plane
+  // The metric row of plane q goes into ring slot (q - pstart) % 3 by
+  // cp.async two planes ahead (one group per plane and thread).
+  const RowEntry<T> rent = row_entry(p, tid < kRow ? tid : kRow, i0, j0);
+  auto stage_row = [&](int q) {
+    if (tid < kRow && q < k1) {
+      const bool v = rent.a != nullptr && q >= 0 && q < Nz;
+      cp_async<sizeof(T)>(Rw + ((q - pstart) % 3) * kRow + tid,
+                          v ? rent.a + (long long)q * rent.stride : p.Lz, v);
+    }
+    cp_async_commit();
+  };
+  stage_row(pstart);
+  stage_row(pstart + 1);
+  // material ids: one byte each with the table in shared memory (SM),
+  // else id_bytes wide; the pointer of cell 0 advances one plane per step
+  const unsigned char* idp = static_cast<const unsigned char*>(p.mat_id) +
+                             (ci[0] + (long long)cj[0] * Nx) * p.id_bytes;
+  const long long id_plane = NxNy * p.id_bytes;
+  auto id_at = [&](int r, int q) -> int {
+    const unsigned char* a = idp + (long long)q * id_plane + 32 * r * (SM ? 1 : p.id_bytes);
+    if (SM) return a[0];
+    if (p.id_bytes == 1) return a[0];
+    if (p.id_bytes == 2) return *reinterpret_cast<const uint16_t*>(a);
+    return (int)*reinterpret_cast<const uint32_t*>(a);
+  };
   int id[2];
 #pragma unroll
-  for (int r = 0; r < 2; r++)
-    id[r] = (hval[r] && pstart >= 0)
-                ? load_id(p.mat_id, p.id_bytes, ci[r] + (long long)cj[r] * Nx + (long long)pstart * NxNy)
-                : 0;
-  if (tid < kRow) Rw[(pstart & 1) * kRow + tid] = row_value(p, tid, pstart, i0, j0);
+  for (int r = 0; r < 2; r++) id[r] = (hval[r] && pstart >= 0) ? id_at(r, pstart) : 0;
   T hxp[2] = {T(0), T(0)}, hyp[2] = {T(0), T(0)};
 
   bool ok = true;
   int pl = pstart;
   for (; pl < k1; pl++) {
+    cp_async_wait<1>();          // this thread's row entry of plane pl
     bool got = true;
     if (tid == 0) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
     ok = __syncthreads_and(got);
@@ -275,20 +300,19 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
       if (pl + kES - 1 <= k1) { issue_e(pl + kES - 1); e_hi = pl + kES - 1; }
       if (pl + kHS - 1 <= k1 - 1) { issue_h(pl + kHS - 1); h_hi = pl + kHS - 1; }
     }
-    // prefetch the ids and metric row of plane pl+1
+    stage_row(pl + 2);           // the row slot of plane pl-1 is free
+    // prefetch the ids of plane pl+1
     const bool more = pl + 1 < k1;
     int idn[2] = {0, 0};
-    T rn = T(0);
     if (more) {
 #pragma unroll
       for (int r = 0; r < 2; r++)
-        if (hval[r]) idn[r] = load_id(p.mat_id, p.id_bytes, ci[r] + (long long)cj[r] * Nx + (long long)(pl + 1) * NxNy);
-      if (tid < kRow) rn = row_value(p, tid, pl + 1, i0, j0);
+        if (hval[r]) idn[r] = id_at(r, pl + 1);
     }
     const T* Ek = Eb + ((pl - pstart) % kES) * 3 * SE;
     const T* Ek1 = Eb + ((pl + 1 - pstart) % kES) * 3 * SE;
     const T* Hk = Hb + ((pl - pstart) % kHS) * 3 * SH;
-    const T* R = Rw + (pl & 1) * kRow;
+    const T* R = Rw + ((pl - pstart) % 3) * kRow;
     const long long off = (long long)pl * NxNy;
 
     // plane face flags (MODE 1): at the plane and of the +z neighbour
@@ -397,8 +421,8 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
       hyp[r] = hyn[r];
       id[r] = idn[r];
     }
-    if (more && tid < kRow) Rw[((pl + 1) & 1) * kRow + tid] = rn;
   }
+  cp_async_wait<0>();
   if (!ok) {
     // a load did not complete in time: record it, wait (bounded) for the
     // loads this block issued, then return
@@ -512,7 +536,7 @@ static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cud
 // One step with the TMA kernel in the mode the faces allow (see k_tma).
 template <typename T>
 cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC) {
-  const bool sm_table = p.n_mat <= kMatSmem;
+  const bool sm_table = p.n_mat <= kMatSmem && p.id_bytes == 1;
   const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
   const int mode = tma_mode(p);
 #define WK_TMA_CASE(SMV, JMV)                                                         \
