@@ -157,11 +157,14 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   const int k0 = (ZFULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, ZFULL ? Nz : Nz - 2);
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x;
+  // the producer (mbarrier set-up, TMA issue and waits) is the last lane of
+  // warp 9, which owns no cell
+  const bool prod = tid == kTmaThreads - 1;
   const int pstart = k0 - 1;
   const uint32_t e_bytes = (uint32_t)(3 * EBX * kBY * sizeof(T));
   const uint32_t h_bytes = (uint32_t)(3 * HBX * kHBY * sizeof(T));
 
-  if (tid == 0) {
+  if (prod) {
     for (int s = 0; s < kES + kHS; s++) mbar_init(&bar[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -186,9 +189,9 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     return mbar_wait(&bar[kES + (q - pstart) % kHS], (uint32_t)(((q - pstart) / kHS) & 1));
   };
   // E planes pstart..k1 and H planes pstart..k1-1 are loaded, each exactly
-  // once; e_hi / h_hi (thread 0) track the last plane issued
+  // once; e_hi / h_hi (producer) track the last plane issued
   int e_hi = pstart - 1, h_hi = pstart - 1;
-  if (tid == 0) {
+  if (prod) {
     for (int q = pstart; q <= min(pstart + kES - 1, k1); q++) { issue_e(q); e_hi = q; }
     for (int q = pstart; q <= min(pstart + kHS - 1, k1 - 1); q++) { issue_h(q); h_hi = q; }
   }
@@ -256,13 +259,21 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     for (int q = tid; q < 9 * p.n_mat; q += kTmaThreads) smat[q] = p.mat[q];
   const T* mat = SM ? smat : p.mat;
   // The metric row of plane q goes into ring slot (q - pstart) % 3 by
-  // cp.async two planes ahead (one group per plane and thread).
-  const RowEntry<T> rent = row_entry(p, tid < kRow ? tid : kRow, i0, j0);
+  // cp.async two planes ahead, issued by warps 8 and 9 (entries t, t+64,
+  // t+128 for t = tid - 256) while the tile warps compute the E of the
+  // plane before; one group per plane and thread.
   auto stage_row = [&](int q) {
-    if (tid < kRow && q < k1) {
-      const bool v = rent.a != nullptr && q >= 0 && q < Nz;
-      cp_async<sizeof(T)>(Rw + ((q - pstart) % 3) * kRow + tid,
-                          v ? rent.a + (long long)q * rent.stride : p.Lz, v);
+    if (tid >= 256 && q < k1) {
+#pragma unroll
+      for (int u = 0; u < 3; u++) {
+        const int r = tid - 256 + 64 * u;
+        if (r < kRow) {
+          const RowEntry<T> e = row_entry(p, r, i0, j0);
+          const bool v = e.a != nullptr && q >= 0 && q < Nz;
+          cp_async<sizeof(T)>(Rw + ((q - pstart) % 3) * kRow + r,
+                              v ? e.a + (long long)q * e.stride : p.Lz, v);
+        }
+      }
     }
     cp_async_commit();
   };
@@ -290,17 +301,16 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   for (; pl < k1; pl++) {
     cp_async_wait<1>();          // this thread's row entry of plane pl
     bool got = true;
-    if (tid == 0) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
+    if (prod) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
     ok = __syncthreads_and(got);
     if (!ok) break;
     const bool prologue = pl == pstart;
-    if (tid == 0 && !prologue) {
+    if (prod && !prologue) {
       // the slots of E(pl-1) and H(pl-1) are free: every thread finished plane pl-1
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       if (pl + kES - 1 <= k1) { issue_e(pl + kES - 1); e_hi = pl + kES - 1; }
       if (pl + kHS - 1 <= k1 - 1) { issue_h(pl + kHS - 1); h_hi = pl + kHS - 1; }
     }
-    stage_row(pl + 2);           // the row slot of plane pl-1 is free
     // prefetch the ids of plane pl+1
     const bool more = pl + 1 < k1;
     int idn[2] = {0, 0};
@@ -374,6 +384,9 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     }
     __syncthreads();
 
+    // warps 8 and 9 own no E row: the row slot of plane pl-1 is free (every
+    // thread passed the top barrier of plane pl), stage the row of pl+2
+    if (warp >= 8) stage_row(pl + 2);
     if (!prologue) {
       const T tLz = R[147];
 #pragma unroll
@@ -426,7 +439,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   if (!ok) {
     // a load did not complete in time: record it, wait (bounded) for the
     // loads this block issued, then return
-    if (tid == 0) {
+    if (prod) {
       if (p.status) atomicExch(p.status, 1);
       for (int q = pl; q <= e_hi; q++) wait_e(q);
       for (int q = pl; q <= h_hi; q++) wait_h(q);
