@@ -87,8 +87,7 @@ struct CLayout {
   static constexpr int hs_off = c_off + cHS * 6 * cslot;
   static constexpr int row_off = hs_off + round128(3 * cExt * 4);
   static constexpr int raw_off = row_off + round128(2 * cRow * 4);     // [3][cRow][2] doubles
-  static constexpr int id_off = raw_off + round128(3 * cRow * 16);     // [3][threads] u64
-  static constexpr int mat_off = id_off + round128(3 * cThreads * 8);
+  static constexpr int mat_off = raw_off + round128(3 * cRow * 16);
   static constexpr int bar_off = mat_off + round128(cMat * cMatW * 4);
   static constexpr int bytes = bar_off + (cES + cHS) * 8 + 128;
 };
@@ -209,7 +208,6 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][cExt]
   float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][cRow]
   double* Rraw = reinterpret_cast<double*>(sm + Lay::raw_off); // [3][cRow][2] f, g
-  uint64_t* sidw = reinterpret_cast<uint64_t*>(sm + Lay::id_off);  // [3][threads] id words
   float* mt = reinterpret_cast<float*>(sm + Lay::mat_off);    // [n_mat][16]
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Lay::bar_off);
 
@@ -220,11 +218,14 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   const int k0 = (ZFULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, ZFULL ? Nz : Nz - 2);
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the producer (mbarrier set-up, TMA issue and waits) is the last lane of
+  // warp 9, which owns no item
+  const bool prod = tid == cThreads - 1;
   const int pstart = k0 - 1;
   const uint32_t e_bytes = 3u * EBX * cBY * 4u;
   const uint32_t h_bytes = 3u * G::hbx * cHBY * 4u + (CT ? 6u * G::cbx * cHBY * 2u : 0u);
 
-  if (tid == 0) {
+  if (prod) {
     for (int s = 0; s < cES + cHS; s++) mbar_init(&bar[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -255,7 +256,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     return mbar_wait(&bar[cES + (q - pstart) % cHS], (uint32_t)(((q - pstart) / cHS) & 1));
   };
   int e_hi = pstart - 1, h_hi = pstart - 1;
-  if (tid == 0) {
+  if (prod) {
     for (int q = pstart; q <= min(pstart + cES - 1, k1); q++) { issue_e(q); e_hi = q; }
     for (int q = pstart; q <= min(pstart + cHS - 1, k1 - 1); q++) { issue_h(q); h_hi = q; }
   }
@@ -314,40 +315,22 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     mt[m * cMatW + 8 + d] = (float)(p.dt * m0[d]);
     mt[m * cMatW + 12 + d] = (float)((p.dt * m0[d]) * m0[6 + d]);
   }
-  // ids, compensation words and factor row of the first plane
-  // The material ids of the item at plane q, staged by cp.async as the
-  // aligned word(s) that hold them (a pair starts at an even cell, so both
-  // ids share one 4-byte word, or one 8-byte word for 4-byte ids); a word
-  // that would reach past the id array is composed from direct loads.
-  const IdT* ids = static_cast<const IdT*>(p.mat_id);
-  auto stage_ids = [&](int q, uint64_t* dst) {
-    const long long n = nb + (long long)q * NxNy;
-    if (q < 0) {
-      *dst = 0ull;
-    } else if (sizeof(IdT) == 4 && pair) {
-      cp_async<8>(dst, ids + n, true);
+  // material ids of the item at plane q: a pair starts at an even cell, so
+  // both ids come in one aligned load of twice the id width
+  const IdT* idp = static_cast<const IdT*>(p.mat_id) + nb;
+  auto load_ids = [&](int q, int& a0, int& a1) {
+    const IdT* a = idp + (long long)q * NxNy;
+    if (!pair) {
+      a0 = a1 = (int)a[0];
+    } else if (sizeof(IdT) == 1) {
+      const uint32_t w = *reinterpret_cast<const uint16_t*>(a);
+      a0 = (int)(w & 0xffu); a1 = (int)(w >> 8);
+    } else if (sizeof(IdT) == 2) {
+      const uint32_t w = *reinterpret_cast<const uint32_t*>(a);
+      a0 = (int)(w & 0xffffu); a1 = (int)(w >> 16);
     } else {
-      const long long byte = n * (long long)sizeof(IdT);
-      if ((byte | 3) < N * (long long)sizeof(IdT)) {
-        cp_async<4>(dst, reinterpret_cast<const uint32_t*>(ids) + (byte >> 2), true);
-      } else {
-        uint32_t w = (uint32_t)ids[n] << (8 * (int)(byte & 3));
-        if (pair) w |= (uint32_t)ids[n + 1] << (8 * (int)((byte + sizeof(IdT)) & 3));
-        *dst = w;
-      }
-    }
-  };
-  auto read_ids = [&](int q, const uint64_t* src, int& a0, int& a1) {
-    const long long n = nb + (long long)q * NxNy;
-    const uint64_t w = *src;
-    if (sizeof(IdT) == 4) {
-      a0 = (int)(uint32_t)w;
-      a1 = pair ? (int)(uint32_t)(w >> 32) : a0;
-    } else {
-      const int sh = (int)((n * (long long)sizeof(IdT)) & 3) * 8;
-      const uint32_t m = sizeof(IdT) == 1 ? 0xffu : 0xffffu;
-      a0 = (int)(((uint32_t)w >> sh) & m);
-      a1 = pair ? (int)(((uint32_t)w >> (sh + 8 * (int)sizeof(IdT))) & m) : a0;
+      const uint2 w = *reinterpret_cast<const uint2*>(a);
+      a0 = (int)w.x; a1 = (int)w.y;
     }
   };
   auto load_comp = [&](const comp_t* base, int q, uint32_t* w) {
@@ -366,28 +349,27 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   };
   uint32_t hc[3] = {0, 0, 0}, ec[3] = {0, 0, 0};
   if (!CT && hval && pstart >= 0) load_comp(cs.Hc_in, pstart, hc);
+  // The f, g inputs of factor-row entry tid of plane q go into ring slot
+  // (q - pstart) % 3 by cp.async two planes ahead (one group per plane and
+  // thread); the float row of plane q is formed at the end of plane q-1.
   const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
-  // the factor-row inputs and the ids of plane q go into ring slot
-  // (q - pstart) % 3 two planes ahead (one cp.async group per plane); the
-  // float row of plane q is formed at the end of plane q-1
-  auto stage = [&](int q) {
-    if (q < k1) {
-      const int b = (q - pstart) % 3;
-      if (tid < cRow) row_stage(rsrc, q, Nz, p.Lz, Rraw + (b * cRow + tid) * 2);
-      if (hval) stage_ids(q, sidw + b * cThreads + tid);
-    }
+  auto stage_rows = [&](int q) {
+    if (tid < cRow && q < k1)
+      row_stage(rsrc, q, Nz, p.Lz, Rraw + (((q - pstart) % 3) * cRow + tid) * 2);
     cp_async_commit();
   };
   auto form_row = [&](int q) {
     if (tid < cRow) {
-      const double* r = Rraw + (((q - pstart) % 3) * cRow + tid) * 2;
-      Rw[(q & 1) * cRow + tid] = row_value(p.dt, r[0], r[1]);
+      const double* v = Rraw + (((q - pstart) % 3) * cRow + tid) * 2;
+      Rw[(q & 1) * cRow + tid] = row_value(p.dt, v[0], v[1]);
     }
   };
-  stage(pstart);
-  stage(pstart + 1);
+  stage_rows(pstart);
+  stage_rows(pstart + 1);
   cp_async_wait<1>();
   form_row(pstart);
+  int id0 = 0, id1 = 0;
+  if (hval && pstart >= 0) load_ids(pstart, id0, id1);
   float2 hxp = bcast(0.f), hyp = bcast(0.f);
   const float2 zero2 = bcast(0.f);
 
@@ -395,24 +377,24 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   int pl = pstart;
   for (; pl < k1; pl++) {
     bool got = true;
-    if (tid == 0) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
+    if (prod) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
     ok = __syncthreads_and(got);
     if (!ok) break;
     const bool prologue = pl == pstart;
-    if (tid == 0 && !prologue) {
+    if (prod && !prologue) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       if (pl + cES - 1 <= k1) { issue_e(pl + cES - 1); e_hi = pl + cES - 1; }
       if (pl + cHS - 1 <= k1 - 1) { issue_h(pl + cHS - 1); h_hi = pl + cHS - 1; }
     }
-    int id0 = 0, id1 = 0;
-    if (hval) read_ids(pl, sidw + ((pl - pstart) % 3) * cThreads + tid, id0, id1);
-    stage(pl + 2);               // the ring slot of plane pl-1 is free
-    // prefetch the compensation words of plane pl+1 (per-thread loads)
+    stage_rows(pl + 2);          // the ring slot of plane pl-1 is free
+    // prefetch the ids (and without CT the compensation words) of plane pl+1
     const bool more = pl + 1 < k1;
+    int nid0 = 0, nid1 = 0;
     uint32_t nhc[3] = {0, 0, 0}, nec[3] = {0, 0, 0};
-    if (!CT && more) {
-      if (hval) load_comp(cs.Hc_in, pl + 1, nhc);
-      if (eval) load_comp(cs.Ec_in, pl + 1, nec);
+    if (more) {
+      if (hval) load_ids(pl + 1, nid0, nid1);
+      if (!CT && hval) load_comp(cs.Hc_in, pl + 1, nhc);
+      if (!CT && eval) load_comp(cs.Ec_in, pl + 1, nec);
     }
     const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
     const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
@@ -569,6 +551,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     }
     hxp = hxn;
     hyp = hyn;
+    id0 = nid0; id1 = nid1;
     if (!CT) {
 #pragma unroll
       for (int d = 0; d < 3; d++) {
@@ -577,13 +560,13 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       }
     }
     if (more) {
-      cp_async_wait<1>();        // this thread's row inputs and ids of plane pl+1
+      cp_async_wait<1>();        // this thread's row inputs of plane pl+1
       form_row(pl + 1);
     }
   }
   cp_async_wait<0>();
   if (!ok) {
-    if (tid == 0) {
+    if (prod) {
       if (p.status) atomicExch(p.status, 1);
       for (int q = pl; q <= e_hi; q++) wait_e(q);
       for (int q = pl; q <= h_hi; q++) wait_h(q);
@@ -626,6 +609,8 @@ bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
   if (p.Nx < 5 || p.Ny < 5 || p.Nz < 5) return false;
   if (p.N >= (1LL << 30)) return false;
   if (p.Nx % 4 != 0 || p.n_mat > cMat) return false;
+  // a cell pair's two ids are read as one word of twice the id width
+  if ((uintptr_t)p.mat_id % (2 * p.id_bytes) != 0) return false;
   for (int q = 0; q < 2; q++)
     if (((uintptr_t)d->E[q] % 16) || ((uintptr_t)d->H[q] % 16) || ((uintptr_t)d->Ec[q] % 4) ||
         ((uintptr_t)d->Hc[q] % 4))
