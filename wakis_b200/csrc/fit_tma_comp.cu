@@ -87,7 +87,8 @@ struct CLayout {
   static constexpr int hs_off = c_off + cHS * 6 * cslot;
   static constexpr int row_off = hs_off + round128(3 * cExt * 4);
   static constexpr int raw_off = row_off + round128(2 * cRow * 4);     // [3][cRow][2] doubles
-  static constexpr int mat_off = raw_off + round128(3 * cRow * 16);
+  static constexpr int id_off = raw_off + round128(3 * cRow * 16);     // [3][threads] u64
+  static constexpr int mat_off = id_off + round128(3 * cThreads * 8);
   static constexpr int bar_off = mat_off + round128(cMat * cMatW * 4);
   static constexpr int bytes = bar_off + (cES + cHS) * 8 + 128;
 };
@@ -208,6 +209,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][cExt]
   float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][cRow]
   double* Rraw = reinterpret_cast<double*>(sm + Lay::raw_off); // [3][cRow][2] f, g
+  uint64_t* sidw = reinterpret_cast<uint64_t*>(sm + Lay::id_off);  // [3][threads] id words
   float* mt = reinterpret_cast<float*>(sm + Lay::mat_off);    // [n_mat][16]
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Lay::bar_off);
 
@@ -315,22 +317,31 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     mt[m * cMatW + 8 + d] = (float)(p.dt * m0[d]);
     mt[m * cMatW + 12 + d] = (float)((p.dt * m0[d]) * m0[6 + d]);
   }
-  // material ids of the item at plane q: a pair starts at an even cell, so
-  // both ids come in one aligned load of twice the id width
+  // material ids of the item at plane q, staged by cp.async (with the
+  // factor-row inputs, two planes ahead) as the aligned 4-byte word that
+  // holds them (8 bytes for a pair of 4-byte ids).  A pair starts at an even
+  // cell, so its ids share the word.  With Nx % 4 == 0 the array length in
+  // bytes is a multiple of 4 (every word lies inside it) and the position
+  // of the ids in their word is the same on every plane.
   const IdT* idp = static_cast<const IdT*>(p.mat_id) + nb;
-  auto load_ids = [&](int q, int& a0, int& a1) {
+  const int id_sh = 8 * (int)((nb * (long long)sizeof(IdT)) & 3);
+  auto stage_ids = [&](int q, uint64_t* dst) {
     const IdT* a = idp + (long long)q * NxNy;
-    if (!pair) {
-      a0 = a1 = (int)a[0];
-    } else if (sizeof(IdT) == 1) {
-      const uint32_t w = *reinterpret_cast<const uint16_t*>(a);
-      a0 = (int)(w & 0xffu); a1 = (int)(w >> 8);
-    } else if (sizeof(IdT) == 2) {
-      const uint32_t w = *reinterpret_cast<const uint32_t*>(a);
-      a0 = (int)(w & 0xffffu); a1 = (int)(w >> 16);
+    if (q < 0) *dst = 0ull;
+    else if (pair && sizeof(IdT) == 4) cp_async<8>(dst, a, true);
+    else cp_async<4>(dst, reinterpret_cast<const void*>((uintptr_t)a & ~(uintptr_t)3), true);
+  };
+  auto read_ids = [&](const uint64_t* src, int& a0, int& a1) {
+    const uint64_t w = *src;
+    if constexpr (sizeof(IdT) == 4) {
+      a0 = (int)(uint32_t)w;
+      a1 = pair ? (int)(uint32_t)(w >> 32) : a0;
     } else {
-      const uint2 w = *reinterpret_cast<const uint2*>(a);
-      a0 = (int)w.x; a1 = (int)w.y;
+      constexpr int bits = 8 * (int)sizeof(IdT);
+      constexpr uint32_t m = (1u << bits) - 1u;
+      const uint32_t x = (uint32_t)w >> id_sh;
+      a0 = (int)(x & m);
+      a1 = pair ? (int)((x >> bits) & m) : a0;
     }
   };
   auto load_comp = [&](const comp_t* base, int q, uint32_t* w) {
@@ -354,8 +365,10 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   // thread); the float row of plane q is formed at the end of plane q-1.
   const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
   auto stage_rows = [&](int q) {
-    if (tid < cRow && q < k1)
-      row_stage(rsrc, q, Nz, p.Lz, Rraw + (((q - pstart) % 3) * cRow + tid) * 2);
+    if (q < k1) {
+      if (tid < cRow) row_stage(rsrc, q, Nz, p.Lz, Rraw + (((q - pstart) % 3) * cRow + tid) * 2);
+      if (hval) stage_ids(q, sidw + ((q - pstart) % 3) * cThreads + tid);
+    }
     cp_async_commit();
   };
   auto form_row = [&](int q) {
@@ -368,8 +381,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   stage_rows(pstart + 1);
   cp_async_wait<1>();
   form_row(pstart);
-  int id0 = 0, id1 = 0;
-  if (hval && pstart >= 0) load_ids(pstart, id0, id1);
+
   float2 hxp = bcast(0.f), hyp = bcast(0.f);
   const float2 zero2 = bcast(0.f);
 
@@ -387,14 +399,14 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       if (pl + cHS - 1 <= k1 - 1) { issue_h(pl + cHS - 1); h_hi = pl + cHS - 1; }
     }
     stage_rows(pl + 2);          // the ring slot of plane pl-1 is free
-    // prefetch the ids (and without CT the compensation words) of plane pl+1
+    int id0 = 0, id1 = 0;
+    if (hval) read_ids(sidw + ((pl - pstart) % 3) * cThreads + tid, id0, id1);
+    // prefetch the compensation words of plane pl+1 (without CT)
     const bool more = pl + 1 < k1;
-    int nid0 = 0, nid1 = 0;
     uint32_t nhc[3] = {0, 0, 0}, nec[3] = {0, 0, 0};
-    if (more) {
-      if (hval) load_ids(pl + 1, nid0, nid1);
-      if (!CT && hval) load_comp(cs.Hc_in, pl + 1, nhc);
-      if (!CT && eval) load_comp(cs.Ec_in, pl + 1, nec);
+    if (!CT && more) {
+      if (hval) load_comp(cs.Hc_in, pl + 1, nhc);
+      if (eval) load_comp(cs.Ec_in, pl + 1, nec);
     }
     const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
     const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
@@ -551,7 +563,6 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     }
     hxp = hxn;
     hyp = hyn;
-    id0 = nid0; id1 = nid1;
     if (!CT) {
 #pragma unroll
       for (int d = 0; d < 3; d++) {
@@ -560,7 +571,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       }
     }
     if (more) {
-      cp_async_wait<1>();        // this thread's row inputs of plane pl+1
+      cp_async_wait<1>();        // this thread's row inputs and ids of plane pl+1
       form_row(pl + 1);
     }
   }
@@ -609,8 +620,8 @@ bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
   if (p.Nx < 5 || p.Ny < 5 || p.Nz < 5) return false;
   if (p.N >= (1LL << 30)) return false;
   if (p.Nx % 4 != 0 || p.n_mat > cMat) return false;
-  // a cell pair's two ids are read as one word of twice the id width
-  if ((uintptr_t)p.mat_id % (2 * p.id_bytes) != 0) return false;
+  // ids are copied as aligned 4- or 8-byte words
+  if ((uintptr_t)p.mat_id % 8 != 0) return false;
   for (int q = 0; q < 2; q++)
     if (((uintptr_t)d->E[q] % 16) || ((uintptr_t)d->H[q] % 16) || ((uintptr_t)d->Ec[q] % 4) ||
         ((uintptr_t)d->Hc[q] % 4))
