@@ -342,6 +342,160 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_slab(args):
+    """z-slab decomposition (wakis_b200/slab.py).  With --slabs K (one GPU):
+    the workload split into K z-slabs in this process, ghost planes copied on
+    the device after every step; the rate against the single-domain run is
+    the cost of the ghost planes and the exchange.  Under torchrun with
+    --decomp slab: a chain of N workload blocks along z, one block per rank
+    (weak scaling), ghost planes exchanged with the neighbouring ranks through
+    NCCL point-to-point messages every step; value = all cells x steps / max
+    over ranks of the CUDA-event time."""
+    import datetime
+    from types import SimpleNamespace
+
+    import torch
+    import torch.distributed as dist
+
+    from wakis_b200 import slab, workloads
+    from wakis_b200.sources import Beam
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    sp = workloads.spec(args.workload)
+    shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else sp["shape"]
+    dtype = np.float64 if args.dtype == "fp32c" else np.dtype(args.dtype).type
+    precision = "fp32c" if args.dtype == "fp32c" else None
+    if ws > 1:
+        n_blocks, n, mine, ex = ws, ws, [rank], slab.DistExchange()
+    else:
+        n_blocks, n, mine, ex = 1, max(args.slabs, 1), list(range(max(args.slabs, 1))), \
+            slab.LocalExchange()
+    x, y, z = workloads.stacked_edges(args.workload, n_blocks, shape)
+    Nx, Ny, Nz = len(x) - 1, len(y) - 1, len(z) - 1
+    N = Nx * Ny * Nz
+    lay = slab.layout(Nz, n)
+    solvers = {r: workloads.build_stacked(args.workload, n_blocks, shape=shape,
+                                          planes=(lay[r].lo, lay[r].hi), dtype=dtype,
+                                          precision=precision, device=dev)[2] for r in mine}
+    dts = [float(so.dt) for so in solvers.values()]
+    if ws > 1:
+        allg = [None] * ws
+        dist.all_gather_object(allg, dts)
+        dts = [v for part in allg for v in part]
+    if len(set(dts)) != 1:
+        raise RuntimeError(f"slabs disagree on the time step: {sorted(set(dts))}")
+    so0 = solvers[mine[0]]
+    cen = lambda e: e[:-1] + np.diff(e) / 2
+    view = SimpleNamespace(x=cen(x), y=cen(y), z=cen(z), dx=np.diff(x), dy=np.diff(y))
+    beam = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
+    bp = beam.params(view)
+    ixt = int(np.abs(view.x - sp["wake"]["xtest"]).argmin())
+    iyt = int(np.abs(view.y - sp["wake"]["ytest"]).argmin())
+    total = args.warmup + args.steps
+    caps = {r: (torch.zeros((9, solvers[r].Nz, total), dtype=solvers[r]._cap_dtype, device=dev),
+                ixt - 1, iyt - 1, 3, 3) for r in mine}
+
+    def steps(n0, k):
+        for m in range(n0, n0 + k):
+            for r in mine:
+                solvers[r]._advance(1, m, beam=bp, capture=caps[r])
+            ex(lay, solvers)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    steps(0, args.warmup)
+    torch.cuda.synchronize()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clk = Clocks(uuid)
+    time.sleep(0.3)
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(st)
+    steps(args.warmup, args.steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    # step kernels per slab and step (one timed step per slab)
+    launches = 0
+    for r in mine:
+        tm = []
+        solvers[r]._advance(1, total, timing=tm)
+        launches += sum(t[1] for t in tm)
+    ex(lay, solvers)
+    launches *= args.steps
+    # end to end: per step and slab the beam line of its planes from pinned
+    # host memory and its 3x3 Ez window back (SolverFIT3D.run_with_io), then
+    # the exchange
+    t_line = lambda m: (beam.q * beam.v * beam.profile(view, m * so0.dt) / view.dx[bp[0]]
+                        / view.dy[bp[1]])
+    step0 = total + 1
+    lines = np.stack([t_line(m) for m in range(step0, step0 + args.steps)]).astype(
+        np.float64 if args.dtype == "fp32c" else dtype)
+    jz = {r: torch.from_numpy(np.ascontiguousarray(lines[:, lay[r].lo:lay[r].hi])).pin_memory()
+          for r in mine}
+    ez = {r: torch.empty((args.steps, 9, solvers[r].Nz), dtype=solvers[r]._cap_dtype
+                         ).pin_memory() for r in mine}
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m in range(args.steps):
+        for r in mine:
+            solvers[r].run_with_io(jz[r][m:m + 1], ez[r][m:m + 1], step0=step0 + m)
+        ex(lay, solvers)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    clocks = clk.stop()
+    ms, t_e2e = max_over_ranks([ms, t_e2e], ws, dev)
+    if rank == 0:
+        bpc = BYTES_PER_CELL[args.dtype]
+        peak, src = _peaks()
+        per_gpu = bpc * (N / ws) / (ms / 1e3 / args.steps) / 1e9
+        line = {
+            "metric": METRIC, "value": N * args.steps / (ms / 1e3) / 1e9,
+            "unit": "Gcell-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"float64": "f64", "float32": "f32",
+                      "fp32c": "f32+bf16 comp (f64-formed coef)"}[args.dtype],
+            "data": "synthetic",
+            "config": {"workload": f"{args.workload} chain of {n_blocks} block(s) along z",
+                       "cells": N, "grid": [Nx, Ny, Nz],
+                       "parallelism": f"zslab{ws}" if ws > 1 else f"zslab{n}-on-1gpu",
+                       "slabs": [[s.k0, s.k1] for s in lay],
+                       "exchange": "NCCL point-to-point" if ws > 1 else "device copies",
+                       "l2": "state above L2, no flush",
+                       "step": "fused beam + Ez 3x3 capture + H and E half-steps + ghost "
+                               "exchange"},
+            "roofline": {"bound": "hbm", "achieved": per_gpu, "peak": peak, "unit": "GB/s",
+                         "frac": per_gpu / peak, "peak_source": src, "bytes_per_cell_step": bpc,
+                         "kernel": "whole step per GPU (owned cells; ghost and padding "
+                                   "planes and the exchange are overhead)",
+                         "traffic": None},
+            "e2e": {"value": N * args.steps / t_e2e / 1e9, "unit": "Gcell-steps/s",
+                    "h2d_bytes_per_step": int(sum(jz[r][0].numel() * jz[r].element_size()
+                                                  for r in mine)) * ws,
+                    "d2h_bytes_per_step": int(sum(ez[r][0].numel() * ez[r].element_size()
+                                                  for r in mine)) * ws},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
 def cpu_baseline(args, budget_s=20.0):
     """Single-thread oracle on a bounded sample (rank 0, N=1 only)."""
     from oracle import fit as ofit
@@ -396,6 +550,13 @@ def main():
                          "gradient checked on 16 random "
                          "directions against central differences of FP64 forward runs")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="z-slab decomposition on one GPU: the workload split into this many "
+                         "z-slabs in one process (ghost planes copied every step)")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="with torchrun (N > 1): independent replicas (default) or one block "
+                         "of a chain of N workload blocks per rank with the z-slab ghost "
+                         "exchange over NCCL")
     ap.add_argument("--batch-compare", action="store_true",
                     help="also run the batch in FP64 and report per-instance WP/|Z| errors")
     args = ap.parse_args()
@@ -413,6 +574,9 @@ def main():
         return
     if args.adjoint:
         run_adjoint(args)
+        return
+    if args.slabs > 1 or (args.decomp == "slab" and int(os.environ.get("WORLD_SIZE", "1")) > 1):
+        run_slab(args)
         return
 
     import torch

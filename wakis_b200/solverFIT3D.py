@@ -51,15 +51,20 @@ class SolverFIT3D(RoutinesMixin):
                  bc_high=("Periodic", "Periodic", "Periodic"),
                  use_stl=False, use_conductors=False, use_gpu=True, use_mpi=False,
                  use_sibc=True, fmax=1e9, dtype=np.float64, n_pml=10, bg=(1.0, 1.0),
-                 verbose=1, device=None, backend="b200", precision=None):
+                 verbose=1, device=None, backend="b200", precision=None, coefficients=None):
         """``precision="fp32c"`` keeps E and H as FP32 values plus bf16
         compensation words (Kahan-style updates) while the coefficients, the
         time step, the Ez history and the wake integration stay FP64; it
-        requires dtype=np.float64 and every grid dimension >= 5."""
+        requires dtype=np.float64 and every grid dimension >= 5.
+
+        ``coefficients``: a compact coefficient set already built for this
+        grid (``coefficients.build``, or a z-slab of one, ``slab.py``); the
+        boundary, material and time-step arguments are then not re-applied."""
         if backend != "b200":
             raise ValueError(f"backend {backend!r}: this package only provides 'b200'")
         if use_mpi:
-            raise ValueError("use_mpi: see wakis_b200.slab for z-slab decomposition")
+            raise ValueError("use_mpi: use wakis_b200.slab.SlabWakeSolve (z-slab "
+                             "decomposition over GPUs) instead")
         if not torch.cuda.is_available():
             raise RuntimeError("wakis_b200.SolverFIT3D needs a CUDA device (no CPU fallback)")
         self._lib = _native.lib()
@@ -98,9 +103,14 @@ class SolverFIT3D(RoutinesMixin):
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
 
-        c = build_coefficients(grid, self.bc_low, self.bc_high, dtype=self.dtype, bg=bg,
-                               use_stl=use_stl, use_sibc=use_sibc, fmax=self.fmax,
-                               n_pml=n_pml, cfln=cfln, dt=dt, verbose=verbose)
+        if coefficients is not None:
+            c = coefficients
+            if tuple(c.shape) != (self.Nx, self.Ny, self.Nz) or c.dtype != self.dtype:
+                raise ValueError("coefficients were built for another grid shape or dtype")
+        else:
+            c = build_coefficients(grid, self.bc_low, self.bc_high, dtype=self.dtype, bg=bg,
+                                   use_stl=use_stl, use_sibc=use_sibc, fmax=self.fmax,
+                                   n_pml=n_pml, cfln=cfln, dt=dt, verbose=verbose)
         self._coef = c
         self.use_conductivity = c.use_conductivity
         self.activate_pml = c.activate_pml

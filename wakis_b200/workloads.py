@@ -76,6 +76,71 @@ def build_b200(name, dtype=np.float64, shape=None, precision=None):
     return g, w, s
 
 
+def stacked_edges(name, n_blocks, shape=None):
+    """Edges of a chain of n_blocks copies of a workload grid stacked along
+    z (block b spans z in [-50 + 100 b, 50 + 100 b] mm); one block is the
+    workload's own grid."""
+    Nx, Ny, Nz = shape or spec(name)["shape"]
+    x0, x1, y0, y1, z0, z1 = BOUNDS
+    return (np.linspace(x0, x1, Nx + 1), np.linspace(y0, y1, Ny + 1),
+            np.linspace(z0, z0 + n_blocks * (z1 - z0), n_blocks * Nz + 1))
+
+
+def build_stacked(name, n_blocks, shape=None, planes=None, dtype=np.float64, precision=None,
+                  device=None):
+    """(grid, wake, solver) of a chain of n_blocks copies of a workload
+    stacked along z: the beam pipe runs through all of them, every block
+    holds its own cavity (and insert), the workload's z boundaries (PML,
+    ABC, PEC) close the two ends of the chain.  With planes = (lo, hi) only
+    the planes [lo, hi) of the chain are built, on the chain's own edges, as
+    one z-slab for ``slab.py``: an end of the slab inside the chain is an
+    internal face (no PML; the PEC mask there touches only the padding).  Weak-scaling workload of the slab
+    decomposition: each GPU steps one block."""
+    from .gridFIT3D import GridFIT3D
+    from .solverFIT3D import SolverFIT3D
+    from .wakeSolver import WakeSolver
+    sp = spec(name)
+    x, y, z = stacked_edges(name, n_blocks, shape)
+    Nz = len(z) - 1
+    lo, hi = planes if planes is not None else (0, Nz)
+    zl = z[lo:hi + 1]
+    Lz = BOUNDS[5] - BOUNDS[4]
+    cav = geometry.CylinderZ(0.005)
+    ins = None
+    for b in range(n_blocks):
+        cav = cav | geometry.Box(-0.015, 0.015, -0.015, 0.015, -0.015 + b * Lz,
+                                 0.015 + b * Lz, tol=1e-12)
+        if "insert" in sp:
+            bx = list(sp["insert"]["box"])
+            box = geometry.Box(*bx[:4], bx[4] + b * Lz, bx[5] + b * Lz, tol=1e-12)
+            ins = box if ins is None else ins | box
+    # the CFL step of the whole chain (the builder's expression on the global
+    # edges: a slab's own minimum spacing can differ in the last bit)
+    from .coefficients import C_LIGHT
+    dt = 0.5 / (C_LIGHT * np.sqrt(1 / np.min(np.diff(x)) ** 2 + 1 / np.min(np.diff(y)) ** 2
+                                  + 1 / np.min(np.diff(z)) ** 2))
+    g = GridFIT3D(x=x, y=y, z=zl, verbose=0)
+    g.add_solid("cavity", geometry.cell_mask(cav, g.x, g.y, g.z), "vacuum")
+    if ins is not None:
+        g.add_solid("insert", geometry.cell_mask(ins, g.x, g.y, g.z), sp["insert"]["material"])
+    # an end of the slab inside the chain: the PEC column mask (it reaches
+    # only the slab's padding plane, slab.py) when the grid has a PEC-like
+    # face already, so the slab keeps the full-domain kernel and the H-row
+    # summation order; else no mask
+    bc_low, bc_high = list(sp["bc_low"]), list(sp["bc_high"])
+    pec_like = any(b.lower() in ("pec", "electric", "pml") for b in bc_low + bc_high)
+    inner = "pec" if pec_like else "abc"
+    if lo > 0:
+        bc_low[2] = inner
+    if hi < Nz:
+        bc_high[2] = inner
+    w = WakeSolver(save=False, verbose=0, **sp["wake"])
+    s = SolverFIT3D(g, w, dt=dt, bc_low=bc_low, bc_high=bc_high, use_stl=True, bg=sp["bg"],
+                    dtype=dtype, n_pml=sp["n_pml"], verbose=0, precision=precision,
+                    device=device)
+    return g, w, s
+
+
 def precision_compare(name="precision_448", shape=None, wakelength=None, max_steps=None):
     """Run wakesolve twice on the same grid, FP64 and FP32-compensated, and
     return the relative errors (max|a-b| / max|b|) of the FP32c results
