@@ -17,7 +17,10 @@ e2e    = the same through SolverFIT3D.run_with_io: every step copies the
          device->host (pinned buffers), wall clock around the K steps.
 Multi-GPU (torchrun): every rank runs an independent replica of the
 workload (weak scaling, no data-path collective); NCCL only carries the
-barrier and the max of the timings.
+barrier and the max of the timings.  --decomp slab instead steps a chain of
+N workload blocks along z, one per rank, exchanging ghost planes with the
+neighbouring ranks every step (wakis_b200/slab.py); --slabs K splits the
+workload into K z-slabs on one GPU.
 
 --impl reference times the CPU oracle (a restatement of upstream's scipy
 solver) on the host cores with all threads, on a bounded sample of the
