@@ -194,6 +194,23 @@ int wk_adj_grad(int dtype, const long long* cells, long long ncell, long long N,
                 void* stream);
 
 /*
+ * The same two transposes without assembled matrices: stencils over the
+ * compact coefficient tables of a solver descriptor (material ids and
+ * table, separable metrics, PEC/PMC face masks, dt; the state buffers of
+ * the descriptor are not read or written).  No counterpart in the
+ * reference (transposes of SolverFIT3D._one_step, solverFIT3D.py:482-503).
+ * dtype (WK_F64 / WK_F32) is the type of the adjoint vectors (3N entries
+ * each); the coefficient tables keep the descriptor's type.
+ *   wk_adj_h_fit: lH_out = lH_in + dt * B0^T (ieps .* lE)
+ *   wk_adj_e_fit: lE_out = decay .* lE_in - A^T lH      (decay may be NULL: 1)
+ * lH_in may equal lH_out and lE_in may equal lE_out.  Fewer than 2^31 cells.
+ */
+int wk_adj_h_fit(const wk_fit_desc* d, int dtype, const void* lamE, const void* lamH_in,
+                 void* lamH_out, void* stream);
+int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* lamH, const void* lamE_in,
+                 const void* decay, void* lamE_out, void* stream);
+
+/*
  * Frequency-domain monitor update: for f < nf and d < 3,
  * acc[f][d][n] += E_d[n] * phases[f] (complex double, interleaved re/im,
  * acc laid out [nf][3][N] in the flat field order).  Replaces the loop of

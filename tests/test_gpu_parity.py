@@ -422,7 +422,8 @@ def test_batched_fp32c_close_to_fp64():
         assert rel_err(np.abs(np.asarray(wa.Z)), np.abs(np.asarray(wb_.Z))) <= 1e-4
 
 
-def _design_problem(dtype, n_steps=800, adjoint_dtype=None, precision=None):
+def _design_problem(dtype, n_steps=800, adjoint_dtype=None, precision=None,
+                    operators="stencil"):
     """cavity_40 geometry with an 8x8x8-cell design region at the centre,
     PEC walls (dt not clamped), FP32, FP64 or FP32-compensated."""
     from wakis_b200 import workloads
@@ -431,7 +432,27 @@ def _design_problem(dtype, n_steps=800, adjoint_dtype=None, precision=None):
     m = np.zeros((s.Nx, s.Ny, s.Nz), bool)
     m[16:24, 16:24, 36:44] = True
     return ImpedanceDesign(s, m, f_band=(0.5e9, 3e9), n_steps=n_steps, segment=30,
-                           adjoint_dtype=adjoint_dtype)
+                           adjoint_dtype=adjoint_dtype, operators=operators)
+
+
+@pytest.mark.parametrize("dtype,adt", [(np.float64, None), (np.float32, None),
+                                       (np.float32, np.float64)])
+def test_adjoint_stencil_transposes_equal_csr(dtype, adt):
+    """The matrix-free transposes (wk_adj_h_fit / wk_adj_e_fit, stencils over
+    the compact coefficient tables) give the gradient of the CSR products of
+    the host-assembled A^T, B0^T to rounding (same parameters, 300 steps)."""
+    rng = np.random.default_rng(2)
+    er = rng.uniform(1.0, 10.0, 512)
+    sg = rng.uniform(0.0, 10.0, 512)
+    out = {}
+    for op in ("csr", "stencil"):
+        p = _design_problem(dtype, n_steps=300, adjoint_dtype=adt, operators=op)
+        p.set_params(er, sg)
+        p.forward()
+        out[op] = p.backward()
+    tol = 1e-10 if (adt or dtype) == np.float64 else 1e-4
+    for a, b in zip(out["stencil"], out["csr"]):
+        assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b))
 
 
 def test_adjoint_operators_match_step_kernels():

@@ -18,9 +18,11 @@ time step (the relaxation-time clamp of the constructor is not re-evaluated).
   index wrap as the wake kernel), so torch autograd gives dL/dEz(k, n).
 * Backward: segment by segment from the end, the forward states of the
   segment are recomputed from its checkpoint, then the adjoint steps
-  (``wk_adj_h``, ``wk_adj_e``: CSR products with A^T and B0^T assembled on
-  the host from the same coefficient tables the step kernels read) run
-  backwards with dL/dEz injected at the test line, and ``wk_adj_grad``
+  (``wk_adj_h_fit``, ``wk_adj_e_fit``: A^T and B0^T applied as stencils over
+  the compact coefficient tables the step kernels read; ``operators="csr"``
+  uses ``wk_adj_h`` / ``wk_adj_e`` with CSR matrices assembled on the host
+  instead) run backwards with dL/dEz injected at the test line, and
+  ``wk_adj_grad``
   accumulates the parameter adjoints of every step (the eps increment
   dt (B0 H' - J) of the design entries is re-formed in FP64 from the
   recomputed H', so a float state loses nothing to E' - E cancellation).
@@ -145,7 +147,7 @@ class ImpedanceDesign:
     dtype of the adjoint state, by default the solver's coefficient dtype."""
 
     def __init__(self, solver, design, f_band=(0.5e9, 3e9), n_steps=4000, segment=None,
-                 samples=1001, adjoint_dtype=None):
+                 samples=1001, adjoint_dtype=None, operators="stencil"):
         s = self.s = solver
         if s.precision not in (None, "fp32c"):
             raise ValueError(f"ImpedanceDesign: precision {s.precision!r} not supported")
@@ -163,9 +165,13 @@ class ImpedanceDesign:
         self.segment = int(segment) if segment else max(1, int(round(np.sqrt(self.n_steps))))
         self.f_band = f_band
         self.samples = samples
+        if operators not in ("stencil", "csr"):
+            raise ValueError(f"operators {operators!r}: 'stencil' or 'csr'")
+        self.operators = operators
         A, B0 = assemble_operators(s)
-        self.AT = _DevCSR(A.T, self.tdtype, self.dev)
-        self.B0T = _DevCSR(B0.T, self.tdtype, self.dev)
+        if operators == "csr":
+            self.AT = _DevCSR(A.T, self.tdtype, self.dev)
+            self.B0T = _DevCSR(B0.T, self.tdtype, self.dev)
         N = s.N
         nc = len(self.cells_np)
         # rows of B0 at the design entries (FP64): the E increment there is
@@ -310,6 +316,26 @@ class ImpedanceDesign:
         s.nstep = n
         s._j_state = 1 if (n >= 1 and s.use_conductivity) else 0   # WK_J_SIGMA_E / ZERO
 
+    def _beam_rows_J(self, bp):
+        """Jz of the fused beam at the design entries on the beam line, for
+        every step (n_steps x entries, FP64 device tensor; None without such
+        entries): the expressions of ``sources.beam_line_values`` evaluated
+        for all steps at once (float32 time arithmetic with a float32 dt)."""
+        if not len(self.beam_rows):
+            return None
+        s = self.s
+        _, _, qv, v, s0, c0, two_sig2, bdx, bdy = bp
+        steps = np.arange(self.n_steps)
+        if isinstance(s.dt, np.float32):
+            vt = v * (steps.astype(np.float32) * s.dt)
+        else:
+            vt = v * (steps * np.float64(s.dt))
+        z = np.asarray(s.z)[self.beam_k.cpu().numpy()]
+        sz = z[None, :] - vt[:, None]
+        prof = c0 * np.exp(-((sz - s0) ** 2) / two_sig2)
+        vals = (qv * prof / bdx / bdy).astype(s.dtype).astype(np.float64)
+        return torch.as_tensor(vals, device=self.dev)
+
     def backward(self):
         """(dL/d eps_r, dL/d sigma) of the design cells (numpy float64)."""
         s, N, lib = self.s, self.s.N, self.lib
@@ -333,7 +359,7 @@ class ImpedanceDesign:
         ptr = lambda t: ctypes.c_void_p(t.data_ptr())
         bp = self._ws["beam_params"]
         starts = sorted(self.ckpt)
-        from .sources import beam_line_values
+        beam_J = self._beam_rows_J(bp)
         for a in reversed(starts):
             b = min(a + self.segment, self.n_steps)
             self._restore(a)
@@ -350,12 +376,14 @@ class ImpedanceDesign:
                     _native.WK_F64, ptr(self.Bd.rowptr), ptr(self.Bd.col), ptr(self.Bd.val),
                     self.Bd.n, ptr(Hd), ptr(self.zd), ptr(self.zd), ptr(bh),
                     ctypes.c_void_p(st)), "wk_adj_e")
-                J = (self.sig_d * Es[n - a].double()[self.rows] if (cond and n >= 1)
-                     else torch.zeros_like(self.zd))
-                if len(self.beam_rows):
-                    jb = beam_line_values(s, bp, n).double()
-                    J[self.beam_rows] = jb[self.beam_k]
-                incs.append((dt * (-bh - J)).contiguous())
+                if cond and n >= 1:
+                    J = self.sig_d * Es[n - a][self.rows].double()
+                    if beam_J is not None:
+                        J[self.beam_rows] = beam_J[n]
+                    bh.add_(J)
+                elif beam_J is not None:
+                    bh.index_add_(0, self.beam_rows, beam_J[n])
+                incs.append(bh.mul_(-dt))
             for n in range(b - 1, a - 1, -1):
                 use_sig = int(cond and n >= 1)
                 E0 = Es[n - a].to(self.tdtype)
@@ -363,14 +391,22 @@ class ImpedanceDesign:
                     self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(incs[n - a]),
                     ptr(E0), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
                     ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
-                _native.check(lib.wk_adj_h(
-                    self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
-                    self.B0T.n, ptr(lE), ptr(self.ieps), dt, ptr(lH), ptr(lH),
-                    ctypes.c_void_p(st)), "wk_adj_h")
-                _native.check(lib.wk_adj_e(
-                    self.wk, ptr(self.AT.rowptr), ptr(self.AT.col), ptr(self.AT.val), self.AT.n,
-                    ptr(lH), ptr(lE), ptr(decay if use_sig else ones), ptr(lE),
-                    ctypes.c_void_p(st)), "wk_adj_e")
+                if self.operators == "stencil":
+                    d = s._sync_desc()
+                    _native.check(lib.wk_adj_h_fit(d, self.wk, ptr(lE), ptr(lH), ptr(lH),
+                                                   ctypes.c_void_p(st)), "wk_adj_h_fit")
+                    _native.check(lib.wk_adj_e_fit(
+                        d, self.wk, ptr(lH), ptr(lE), ptr(decay) if use_sig else None,
+                        ptr(lE), ctypes.c_void_p(st)), "wk_adj_e_fit")
+                else:
+                    _native.check(lib.wk_adj_h(
+                        self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
+                        self.B0T.n, ptr(lE), ptr(self.ieps), dt, ptr(lH), ptr(lH),
+                        ctypes.c_void_p(st)), "wk_adj_h")
+                    _native.check(lib.wk_adj_e(
+                        self.wk, ptr(self.AT.rowptr), ptr(self.AT.col), ptr(self.AT.val),
+                        self.AT.n, ptr(lH), ptr(lE), ptr(decay if use_sig else ones), ptr(lE),
+                        ctypes.c_void_p(st)), "wk_adj_e")
                 lE[zidx] += g_hist[:, n]
         er = self.eps_r
         g_eps = gI * (-1.0 / (EPS_0 * er * er))

@@ -21,6 +21,10 @@
 
 #include "../../include/wakis_b200.h"
 #include "abi_internal.h"
+#include "fit_common.cuh"
+#include "fit_kernels.cuh"
+
+using namespace wk;
 
 namespace {
 
@@ -72,6 +76,91 @@ k_adj_grad(const long long* __restrict__ cells, long long ncell, long long N,
   }
   gI[q] += gi;
   gS[q] += gs;
+}
+
+// Matrix-free transposes (wk_adj_h_fit / wk_adj_e_fit), one thread per
+// cell m and all three components, from the compact coefficient tables the
+// step kernels read (T: their type; L: the adjoint state type, the
+// arithmetic type).  With B0 row (d, n) factor itA_d(n) pec_d(n), column
+// (e, n - off) factor tL_e pmc_e, and A row (d, n) factor
+// dt iA_d(n) imu_d(n) pmc_d(n), column (e, n + off) factor L_e pec_e:
+//   lamH'[e, m] = lamH[e, m] + dt tL_e(m) pmc_e(m) sum sg u_d(m + off),
+//       u_d(n) = itA_d(n) pec_d(n) ieps_d(n) lamE[d, n]            (n < N)
+//   lamE'[e, m] = decay[e, m] lamE[e, m] - L_e(m) pec_e(m) sum sg w_d(m - off),
+//       w_d(n) = dt iA_d(n) imu_d(n) pmc_d(n) lamH'[d, n]          (n >= 0)
+// with the signs and offsets of the curl (x: +1, y: +Nx, z: +Nx*Ny).
+template <typename T, typename L>
+__device__ __forceinline__ L adj_u(const FitParams<T>& p, const L* lamE, int d, Cell c,
+                                   long long n) {
+  const int id = load_id(p.mat_id, p.id_bytes, n);
+  T f = d == 0 ? p.itAx[c.j + (long long)c.k * p.Ny]
+               : (d == 1 ? p.itAy[c.i + (long long)c.k * p.Nx] : p.itAz[c.i + (long long)c.j * p.Nx]);
+  if (p.has_pec && !face_val(p.pec_face, d, c.i, c.j, c.k, p.Nx, p.Ny, p.Nz)) f = T(0);
+  return (L)f * (L)p.mat[9 * id + d] * lamE[d * p.N + n];
+}
+
+template <typename T, typename L>
+__device__ __forceinline__ L adj_w(const FitParams<T>& p, const L* lamH, int d, Cell c,
+                                   long long n) {
+  const int id = load_id(p.mat_id, p.id_bytes, n);
+  T f = d == 0 ? p.iAx[c.j + (long long)c.k * p.Ny]
+               : (d == 1 ? p.iAy[c.i + (long long)c.k * p.Nx] : p.iAz[c.i + (long long)c.j * p.Nx]);
+  if (p.has_pmc && !face_val(p.pmc_face, d, c.i, c.j, c.k, p.Nx, p.Ny, p.Nz)) f = T(0);
+  return (L)p.dt * (L)f * (L)p.mat[9 * id + 3 + d] * lamH[d * p.N + n];
+}
+
+template <typename T, typename L>
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_h_fit(FitParams<T> p, const L* __restrict__ lamE, const L* lamH_in, L* lamH_out) {
+  const long long m = blockIdx.x * (long long)kAdjThreads + threadIdx.x;
+  if (m >= p.N) return;
+  const Cell c = cell_of(m, p.Nx, p.Ny);
+  const long long N = p.N;
+  const bool vx = m + 1 < N, vy = m + p.Nx < N, vz = m + p.NxNy < N;
+  const Cell cx = plus_x(c, p.Nx, p.Ny), cy = plus_y(c, p.Ny);
+  Cell cz = c;
+  cz.k++;
+  const L u0 = adj_u<T, L>(p, lamE, 0, c, m), u1 = adj_u<T, L>(p, lamE, 1, c, m),
+          u2 = adj_u<T, L>(p, lamE, 2, c, m);
+  const L u0y = vy ? adj_u<T, L>(p, lamE, 0, cy, m + p.Nx) : L(0);
+  const L u0z = vz ? adj_u<T, L>(p, lamE, 0, cz, m + p.NxNy) : L(0);
+  const L u1x = vx ? adj_u<T, L>(p, lamE, 1, cx, m + 1) : L(0);
+  const L u1z = vz ? adj_u<T, L>(p, lamE, 1, cz, m + p.NxNy) : L(0);
+  const L u2x = vx ? adj_u<T, L>(p, lamE, 2, cx, m + 1) : L(0);
+  const L u2y = vy ? adj_u<T, L>(p, lamE, 2, cy, m + p.Nx) : L(0);
+  const L acc[3] = {u1 - u1z + u2y - u2, u0z - u0 - u2x + u2, u0 - u0y + u1x - u1};
+  const L dt = (L)p.dt;
+#pragma unroll
+  for (int e = 0; e < 3; e++)
+    lamH_out[e * N + m] = lamH_in[e * N + m] + dt * (L)coltL(p, e, c.i, c.j, c.k) * acc[e];
+}
+
+template <typename T, typename L>
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_e_fit(FitParams<T> p, const L* __restrict__ lamH, const L* lamE_in,
+            const L* __restrict__ decay, L* lamE_out) {
+  const long long m = blockIdx.x * (long long)kAdjThreads + threadIdx.x;
+  if (m >= p.N) return;
+  const Cell c = cell_of(m, p.Nx, p.Ny);
+  const long long N = p.N;
+  const bool vx = m >= 1, vy = m >= p.Nx, vz = m >= p.NxNy;
+  const Cell cx = minus_x(c, p.Nx, p.Ny), cy = minus_y(c, p.Ny);
+  Cell cz = c;
+  cz.k--;
+  const L w0 = adj_w<T, L>(p, lamH, 0, c, m), w1 = adj_w<T, L>(p, lamH, 1, c, m),
+          w2 = adj_w<T, L>(p, lamH, 2, c, m);
+  const L w0y = vy ? adj_w<T, L>(p, lamH, 0, cy, m - p.Nx) : L(0);
+  const L w0z = vz ? adj_w<T, L>(p, lamH, 0, cz, m - p.NxNy) : L(0);
+  const L w1x = vx ? adj_w<T, L>(p, lamH, 1, cx, m - 1) : L(0);
+  const L w1z = vz ? adj_w<T, L>(p, lamH, 1, cz, m - p.NxNy) : L(0);
+  const L w2x = vx ? adj_w<T, L>(p, lamH, 2, cx, m - 1) : L(0);
+  const L w2y = vy ? adj_w<T, L>(p, lamH, 2, cy, m - p.Nx) : L(0);
+  const L acc[3] = {w1z - w1 + w2 - w2y, w0 - w0z - w2 + w2x, w0y - w0 + w1 - w1x};
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    const L dec = decay ? decay[e * N + m] : L(1);
+    lamE_out[e * N + m] = dec * lamE_in[e * N + m] - (L)colL(p, e, c.i, c.j, c.k) * acc[e];
+  }
 }
 
 int check_common(int dtype, const void* a, const void* b, long long n, const char* where) {
@@ -144,4 +233,57 @@ extern "C" int wk_adj_grad(int dtype, const long long* cells, long long ncell, l
         cells, ncell, N, (const float*)lamE1, inc, (const float*)E0, (const float*)ieps,
         (const float*)smask, use_sigma, dt, gI, gS);
   return wk_check_launch("wk_adj_grad");
+}
+
+// ---------------------------------------------------------------------------
+// Matrix-free reverse step from the solver descriptor (coefficient tables of
+// wk_fit_desc; the state buffers of the descriptor are not touched).
+namespace {
+template <typename L>
+int adj_fit_launch(const wk_fit_desc* d, int which, const void* a, const void* b,
+                   const void* decay, void* out, cudaStream_t st) {
+  const long long N = (long long)d->Nx * d->Ny * d->Nz;
+  const bool coef64 = d->dtype == WK_F64 || d->dtype == WK_F32C;
+  if (coef64) {
+    FitParams<double> p = make_params<double>(d, d->par);
+    if (which == 0)
+      k_adj_h_fit<double, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b, (L*)out);
+    else
+      k_adj_e_fit<double, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b,
+                                                                  (const L*)decay, (L*)out);
+  } else {
+    FitParams<float> p = make_params<float>(d, d->par);
+    if (which == 0)
+      k_adj_h_fit<float, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b, (L*)out);
+    else
+      k_adj_e_fit<float, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b,
+                                                                 (const L*)decay, (L*)out);
+  }
+  return WK_OK;
+}
+
+int adj_fit(const wk_fit_desc* d, int dtype, int which, const void* a, const void* b,
+            const void* decay, void* out, void* stream, const char* where) {
+  int rc = wk_validate_fit(d, where);
+  if (rc) return rc;
+  if (dtype != WK_F64 && dtype != WK_F32) return wk_fail(WK_E_DTYPE, "%s: dtype", where);
+  if (!a || !b || !out) return wk_fail(WK_E_NULL, "%s: NULL pointer", where);
+  if ((long long)d->Nx * d->Ny * d->Nz >= (1LL << 31))
+    return wk_fail(WK_E_SHAPE, "%s: more than 2^31 cells", where);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == WK_F64) adj_fit_launch<double>(d, which, a, b, decay, out, st);
+  else adj_fit_launch<float>(d, which, a, b, decay, out, st);
+  return wk_check_launch(where);
+}
+}  // namespace
+
+extern "C" int wk_adj_h_fit(const wk_fit_desc* d, int dtype, const void* lamE,
+                            const void* lamH_in, void* lamH_out, void* stream) {
+  return adj_fit(d, dtype, 0, lamE, lamH_in, nullptr, lamH_out, stream, "wk_adj_h_fit");
+}
+
+extern "C" int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* lamH,
+                            const void* lamE_in, const void* decay, void* lamE_out,
+                            void* stream) {
+  return adj_fit(d, dtype, 1, lamH, lamE_in, decay, lamE_out, stream, "wk_adj_e_fit");
 }

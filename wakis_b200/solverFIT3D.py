@@ -394,6 +394,15 @@ class SolverFIT3D(RoutinesMixin):
                             sg[0:N], sg[N:2 * N], sg[2 * N:]], dim=1)
         table, inv = torch.unique(rows, dim=0, return_inverse=True)
         n_mat = table.shape[0]
+        # number the materials in the order of their first cell, so that
+        # neighbouring cells with distinct materials (a design region) read
+        # neighbouring table rows
+        first = torch.full((n_mat,), N, dtype=torch.int64, device=inv.device)
+        first.scatter_reduce_(0, inv, torch.arange(N, device=inv.device), "amin")
+        order = torch.argsort(first)
+        relabel = torch.empty_like(order)
+        relabel[order] = torch.arange(n_mat, device=order.device)
+        table, inv = table[order], relabel[inv]
         id_t = torch.uint8 if n_mat <= 256 else (torch.int16 if n_mat <= 32768 else torch.int32)
         self._ids = inv.to(id_t).contiguous()
         self._table = table.contiguous().view(-1)
