@@ -128,6 +128,12 @@ typedef struct wk_fit_desc {
    * columns and line rows outside their buffers.  Only the TMA and two-pass
    * schedules (and WK_F32C) take it; every dimension must be >= 5.          */
   const long long* step_dev;
+  /* 1 when the caller knows that every E entry tangential to a PEC-masked
+   * face (and its WK_F32C compensation word) is +0 and stays +0 through the
+   * steps of the call (no source and no stored J on such entries): the
+   * full-domain TMA kernels then skip the PEC column masks of the H rows,
+   * which would only replace +0 by +0.  0 (the default) always masks.      */
+  int faces_clean;
 } wk_fit_desc;
 
 #define WK_KERNEL_AUTO 0   /* WK_KERNEL_TMA when its conditions hold, else

@@ -602,3 +602,41 @@ def test_field_monitor_equals_numpy_dft_during_emsolve():
     got = m.get_components()
     for k in "xyz":
         assert np.array_equal(got["E" + k].cpu().numpy(), ref[k])
+
+
+@pytest.mark.parametrize("name,shape,prec", [("cavity_40", None, None),
+                                             ("lossy_256", (64, 64, 128), None),
+                                             ("lossy_256", (64, 64, 128), "fp32c")])
+def test_clean_faces_skip_equals_masked_step(name, shape, prec):
+    """With fields written only by the steps, the tangential E on the PEC
+    faces stays +0 and the full-domain kernels skip the H-row column masks
+    (faces_clean).  The same 300 steps (beam, Ez capture) after E is
+    rewritten with its own zero values (which marks the faces as not clean,
+    so every mask is applied) give the same fields and history value for
+    value."""
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    sp = workloads.spec(name)
+    runs = []
+    for dirty in (False, True):
+        _, _, s = workloads.build_b200(name, shape=shape, precision=prec)
+        if dirty:
+            s._first_step()
+            s.E.fromarray(np.zeros(3 * s.N))
+            assert not s._faces_clean
+        else:
+            assert s._faces_clean
+        bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
+                  ).params(s)
+        ixt = int(np.abs(s.x).argmin())
+        iyt = int(np.abs(s.y).argmin())
+        hist = torch.zeros((9, s.Nz, 300), dtype=s._cap_dtype, device="cuda")
+        s._advance(300, 0, beam=bp, capture=(hist, ixt - 1, iyt - 1, 3, 3))
+        assert int(s._status.item()) == 0
+        assert s._faces_clean == (not dirty)
+        E = s.E.numpy() if prec is None else _decoded(s, "E")
+        H = s.H.numpy() if prec is None else _decoded(s, "H")
+        runs.append((E, H, hist.cpu().numpy()))
+    assert np.abs(runs[0][0]).max() > 0
+    for a, b in zip(runs[0], runs[1]):
+        assert np.array_equal(a, b)

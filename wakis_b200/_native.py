@@ -43,6 +43,7 @@ class FitDesc(ctypes.Structure):
         ("kernel", _i), ("tile_rows", _i), ("tile_planes", _i),
         ("Ec", _vp * 2), ("Hc", _vp * 2),
         ("step_dev", _vp),
+        ("faces_clean", _i),
     ]
 
 

@@ -51,6 +51,7 @@ struct FitParams {
   T* cap;
   int* status;
   const long long* step_dev;   // optional device step counter
+  int faces_clean;             // tangential E on PEC faces is +0 (wk_fit_desc)
   unsigned nx_mul;   // fast division by Nx: q = umulhi(n, nx_mul) >> nx_shift
   int nx_shift;
 };

@@ -120,6 +120,7 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
   fast_div_magic((unsigned)d->Nx, &p.nx_mul, &p.nx_shift);
   p.status = d->status;
   p.step_dev = d->step_dev;
+  p.faces_clean = d->faces_clean;
   return p;
 }
 

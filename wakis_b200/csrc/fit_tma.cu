@@ -355,8 +355,9 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
       T ey1 = Ek[SE + bi + 1], ez1 = Ek[2 * SE + bi + 1];
       T ex2 = Ek[bi + EBX], ez2 = Ek[2 * SE + bi + EBX];
       T ex3 = Ek1[bi], ey3 = Ek1[SE + bi];
-      if (masked) {
+      if (masked && !p.faces_clean) {
         // E column entries tangential to a face they lie on are masked
+        // (with faces_clean those entries are +0 already)
         const T z = T(0);
         ex0 = (yf0[r] || zf0) ? z : ex0;
         ey0 = (xf0[r] || zf0) ? z : ey0;

@@ -449,8 +449,9 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         hx = bcast(Hk[hbi]); hy = bcast(Hk[SH + hbi]); hz = bcast(Hk[2 * SH + hbi]);
         ya = bcast(R[R_HYA + ea + 1]); yb = bcast(R[R_HYB + ea + 1]);
       }
-      if (masked) {
+      if (masked && !p.faces_clean) {
         // E column entries tangential to a face they lie on are masked
+        // (with faces_clean those entries are +0 already)
         auto m2 = [](float2 v, bool ma, bool mb) {
           return make_float2(ma ? 0.f : v.x, mb ? 0.f : v.y);
         };

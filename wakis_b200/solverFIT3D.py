@@ -140,6 +140,10 @@ class SolverFIT3D(RoutinesMixin):
             self._Ec = [torch.zeros(N3, dtype=torch.bfloat16, device=dev) for _ in range(2)]
             self._Hc = [torch.zeros(N3, dtype=torch.bfloat16, device=dev) for _ in range(2)]
         self._par = 0
+        # tangential E on every PEC-masked face is +0 (true for zero fields;
+        # lost on a write to E, a stored J or a source line on an x/y face):
+        # the full-domain TMA kernels then skip the H-row column masks
+        self._faces_clean = True
         self._j_state = _J_ZERO
         self._j_line = None          # (values tensor) of the last fused beam step
         self._ids = t(c.ids)
@@ -206,6 +210,8 @@ class SolverFIT3D(RoutinesMixin):
         """E is about to change between steps: upstream's stored J = sigma*E
         must keep the old E, so materialise it first.  With precision
         'fp32c' the compensation words of a written field are reset."""
+        if fld is self.E:
+            self._faces_clean = False
         if fld is self.E and self._j_state == _J_SIGMA_E:
             if self.precision == "fp32c":
                 raise RuntimeError("precision='fp32c': E cannot be written between "
@@ -265,6 +271,12 @@ class SolverFIT3D(RoutinesMixin):
                                "use the fused beam / line source")
         d = self._sync_desc()
         d.step_dev = None
+        src_line = (beam[0], beam[1]) if beam is not None else (
+            (line[2], line[3]) if line is not None else None)
+        if self._j_state == _J_ARRAY or (src_line is not None and (
+                src_line[0] in (0, self.Nx - 1) or src_line[1] in (0, self.Ny - 1))):
+            self._faces_clean = False
+        d.faces_clean = int(self._faces_clean)
         if beam is not None:
             d.beam_on = 1
             (d.ixs, d.iys, d.b_qv, d.b_v, d.b_s0, d.b_c0, d.b_two_sig2,
@@ -417,6 +429,7 @@ class SolverFIT3D(RoutinesMixin):
     def reset_fields(self):
         for b in self._E + self._H:
             b.zero_()
+        self._faces_clean = True
         if self.precision == "fp32c":
             for b in self._Ec + self._Hc:
                 b.zero_()
