@@ -220,3 +220,69 @@ class WakeSolver:
         self.Zx = (1j * (X[1] * ds) / lambdaf).cpu().numpy()
         self.Zy = (1j * (X[2] * ds) / lambdaf).cpu().numpy()
         self.fx = self.fy = f
+
+    # --------------------------------------------------- static FFT helpers
+    @staticmethod
+    def calc_impedance_from_wake(wake, s=None, t=None, fmax=None, samples=None, verbose=True):
+        """Impedance of a wake function by FFT (upstream wakeSolver.py:
+        1182-1250), on the host.  ``wake`` is the wake or a list [t, wake];
+        the time axis may also come as ``s`` (m, t = s/c) or ``t`` (s).  With
+        ``fmax`` the wake is first resampled on a 1/(2 fmax) grid, else fmax
+        = 1/dt.  Returns [f, Z]: the bins 0 <= f < fmax of the DFT (2*samples
+        points when ``samples`` is given) scaled by 2/len(wake)."""
+        if type(wake) is list:
+            t, wake = wake[0], wake[1]
+        if s is not None:
+            t = s / c_light
+        elif t is None:
+            raise AttributeError('Provide time data through parameter "t" [s] or "s" [m]')
+        t = np.asarray(t)
+        wake = np.asarray(wake)
+        dt = np.mean(t[1:] - t[:-1])
+        if fmax is not None:
+            grid = np.arange(t.min(), t.max(), 1 / fmax / 2)
+            wake = np.interp(grid, t, wake)
+            dt = np.mean(grid[1:] - grid[:-1])
+        else:
+            fmax = 1 / dt
+        spec = np.fft.fft(wake, n=2 * samples) if samples is not None else np.fft.fft(wake)
+        freqs = np.fft.fftfreq(len(spec), dt)
+        keep = np.logical_and(freqs >= 0, freqs < fmax)
+        f = freqs[keep]
+        Z = spec[keep] / len(wake) * 2
+        if verbose:
+            print(f"* Number of samples = {len(f)}")
+            print(f"* Maximum frequency = {f.max()} Hz")
+            print(f"* Maximum resolution = {np.mean(f[1:] - f[:-1])} Hz")
+        return [f, Z]
+
+    @staticmethod
+    def calc_wake_from_impedance(impedance, f=None, tmax=None, samples=None, pad=0,
+                                 verbose=True):
+        """Wake function of an impedance (upstream wakeSolver.py:1252-1311),
+        on the host.  ``impedance`` is Z or a list [f, Z] (a length-2 argument
+        is read as the list, as upstream does).  With ``tmax`` Z is resampled
+        on a 1/tmax frequency grid, else tmax = 1/df.  The wake is the real
+        part of -FFT(Z) (``samples`` points) rolled back by one sample, on
+        t = linspace(0, tmax, len(wake)); ``pad`` is accepted and unused, as
+        upstream.  Returns [t, wake]."""
+        if len(impedance) == 2:
+            f, Z = impedance[0], impedance[1]
+        elif f is None:
+            raise AttributeError('Provide frequency data through parameter "f"')
+        else:
+            Z = impedance
+        f = np.asarray(f)
+        Z = np.asarray(Z)
+        df = np.mean(f[1:] - f[:-1])
+        if tmax is not None:
+            Z = np.interp(np.arange(f.min(), f.max(), 1 / tmax), f, Z)
+        else:
+            tmax = 1 / df
+        wake = np.roll(np.real(-1 * np.fft.fft(Z, n=samples)), -1)
+        t = np.linspace(0, tmax, len(wake))
+        if verbose:
+            print(f"* Number of samples = {len(t)}")
+            print(f"* Maximum time = {t.max()} s")
+            print(f"* Maximum resolution = {np.mean(t[1:] - t[:-1])} s")
+        return [t, wake]
