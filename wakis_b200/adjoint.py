@@ -336,81 +336,197 @@ class ImpedanceDesign:
         vals = (qv * prof / bdx / bdy).astype(s.dtype).astype(np.float64)
         return torch.as_tensor(vals, device=self.dev)
 
-    def backward(self):
-        """(dL/d eps_r, dL/d sigma) of the design cells (numpy float64)."""
-        s, N, lib = self.s, self.s.N, self.lib
+    def _values_into(self, out, which):
+        """E (which = 0) or H (1) of the live state into `out` (the state
+        values, or the FP64 sums v + c of the compensated state)."""
+        st = self._live()
+        out.copy_(st[which])
+        if self.comp:
+            out.add_(st[2 + which])
+
+    def _segment(self, a, m, B, graph_descs=None):
+        """Recompute steps a .. a+m-1 from the restored state and run their
+        reverse steps.  With graph_descs (one step descriptor per step, the
+        step index read from the device counter B['ctr']) the steps are
+        launched directly, as inside a captured CUDA graph; else through
+        the solver.  All per-step data live in the buffers B."""
+        s, lib, N = self.s, self.lib, self.s.N
+        st = torch.cuda.current_stream(self.dev).cuda_stream
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+        dt = float(s.dt)
+        cond = bool(s.use_conductivity)
+        bp = self._ws["beam_params"]
+        Es, incs, J = B["Es"], B["incs"], B["J"]
+        self._values_into(Es[0], 0)
+        par0 = s._par
+        for q in range(m):
+            n = a + q
+            if graph_descs is None:
+                s._advance(1, n, beam=bp)
+            else:
+                _native.check(lib.wk_fit_step(graph_descs[q], 1, 0, ctypes.c_void_p(st)),
+                              "wk_fit_step")
+                _native.check(lib.wk_counter_add(ptr(B["ctr"]), 1, ctypes.c_void_p(st)),
+                              "wk_counter_add")
+                s._par = par0 ^ ((q + 1) & 1)
+            self._values_into(Es[q + 1], 0)
+            # dt (B0 H' - J) at the design entries, FP64
+            if B["Hd"] is None:
+                Hd = self._live()[1]
+            else:
+                Hd = B["Hd"]
+                self._values_into(Hd, 1)
+            _native.check(lib.wk_adj_e(
+                _native.WK_F64, ptr(self.Bd.rowptr), ptr(self.Bd.col), ptr(self.Bd.val),
+                self.Bd.n, ptr(Hd), ptr(self.zd), ptr(self.zd), ptr(incs[q]),
+                ctypes.c_void_p(st)), "wk_adj_e")
+            if cond and n >= 1:
+                J.copy_(Es[q].index_select(0, self.rows))
+                J.mul_(self.sig_d)
+                if B["bJ"] is not None:
+                    J.index_copy_(0, self.beam_rows, B["bJ"][q])
+                incs[q].add_(J)
+            elif B["bJ"] is not None:
+                incs[q].index_add_(0, self.beam_rows, B["bJ"][q])
+            incs[q].mul_(-dt)
+        lE, lH, gI, gS = B["lE"], B["lH"], B["gI"], B["gS"]
+        for q in range(m - 1, -1, -1):
+            n = a + q
+            use_sig = int(cond and n >= 1)
+            if B["E0"] is None:
+                E0 = Es[q]
+            else:
+                E0 = B["E0"]
+                E0.copy_(Es[q])
+            _native.check(lib.wk_adj_grad(
+                self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(incs[q]),
+                ptr(E0), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
+                ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
+            if self.operators == "stencil":
+                d = B["coef_desc"]
+                _native.check(lib.wk_adj_h_fit(d, self.wk, ptr(lE), ptr(lH), ptr(lH),
+                                               ctypes.c_void_p(st)), "wk_adj_h_fit")
+                _native.check(lib.wk_adj_e_fit(
+                    d, self.wk, ptr(lH), ptr(lE), ptr(B["decay"]) if use_sig else None,
+                    ptr(lE), ctypes.c_void_p(st)), "wk_adj_e_fit")
+            else:
+                _native.check(lib.wk_adj_h(
+                    self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
+                    self.B0T.n, ptr(lE), ptr(self.ieps), dt, ptr(lH), ptr(lH),
+                    ctypes.c_void_p(st)), "wk_adj_h")
+                _native.check(lib.wk_adj_e(
+                    self.wk, ptr(self.AT.rowptr), ptr(self.AT.col), ptr(self.AT.val),
+                    self.AT.n, ptr(lH), ptr(lE), ptr(B["decay"] if use_sig else B["ones"]),
+                    ptr(lE), ctypes.c_void_p(st)), "wk_adj_e")
+            lE.index_add_(0, B["zidx"], B["gh"][:, q])
+
+    def backward(self, graph=True):
+        """(dL/d eps_r, dL/d sigma) of the design cells (numpy float64).
+
+        Segment by segment from the end: restore the checkpoint, recompute
+        the segment's steps, run their reverse steps.  With ``graph`` the
+        full-length segments after the first run as one captured CUDA graph
+        (captured on the first of them, replayed for the others: the step
+        kernels read their step index from a device counter, the beam
+        current and dL/dEz of the segment are staged into static buffers);
+        the first segment, a shorter last one and the CSR operators run
+        step by step."""
+        s, N = self.s, self.s.N
         ez = self.hist.clone().requires_grad_(True)
         L = self.loss_from_history(ez)
         (g_hist,) = torch.autograd.grad(L, ez)
         g_hist = g_hist.to(self.tdtype)
         ixt = int(np.abs(s.x - s.wake.xtest).argmin())
         iyt = int(np.abs(s.y - s.wake.ytest).argmin())
-        zidx = 2 * N + ixt + iyt * s.Nx + torch.arange(s.Nz, device=self.dev) * s.Nx * s.Ny
-        lE = torch.zeros(3 * N, dtype=self.tdtype, device=self.dev)
-        lH = torch.zeros(3 * N, dtype=self.tdtype, device=self.dev)
-        gI = torch.zeros(len(self.cells_np), dtype=torch.float64, device=self.dev)
-        gS = torch.zeros_like(gI)
+        dev, K = self.dev, self.segment
         dt = float(s.dt)
         cond = bool(s.use_conductivity)
-        decay = (1.0 - dt * self.ieps.double() * self.sig.double() * self.smask.double()
-                 ).to(self.tdtype) if cond else torch.ones_like(lE)
-        ones = torch.ones_like(lE)
-        st = torch.cuda.current_stream(self.dev).cuda_stream
-        ptr = lambda t: ctypes.c_void_p(t.data_ptr())
-        bp = self._ws["beam_params"]
-        starts = sorted(self.ckpt)
-        beam_J = self._beam_rows_J(bp)
-        for a in reversed(starts):
-            b = min(a + self.segment, self.n_steps)
+        vdt = torch.float64 if self.comp else self._live()[0].dtype
+        beam_J = self._beam_rows_J(self._ws["beam_params"])
+        B = {
+            "Es": torch.empty((K + 1, 3 * N), dtype=vdt, device=dev),
+            "incs": torch.empty((K, len(self.zd)), dtype=torch.float64, device=dev),
+            # FP64 H' for the B0 rows: the live buffer itself only for a
+            # plain FP64 state
+            "Hd": None if (not self.comp and vdt == torch.float64) else torch.empty(
+                3 * N, dtype=torch.float64, device=dev),
+            "E0": None if vdt == self.tdtype else torch.empty(3 * N, dtype=self.tdtype,
+                                                              device=dev),
+            "J": torch.empty_like(self.zd),
+            "bJ": None if beam_J is None else torch.empty((K, beam_J.shape[1]),
+                                                          dtype=torch.float64, device=dev),
+            "gh": torch.empty((s.Nz, K), dtype=self.tdtype, device=dev),
+            "ctr": torch.zeros(1, dtype=torch.int64, device=dev),
+            "zidx": 2 * N + ixt + iyt * s.Nx + torch.arange(s.Nz, device=dev) * s.Nx * s.Ny,
+            "lE": torch.zeros(3 * N, dtype=self.tdtype, device=dev),
+            "lH": torch.zeros(3 * N, dtype=self.tdtype, device=dev),
+            "gI": torch.zeros(len(self.cells_np), dtype=torch.float64, device=dev),
+            "gS": torch.zeros(len(self.cells_np), dtype=torch.float64, device=dev),
+            "decay": (1.0 - dt * self.ieps.double() * self.sig.double() * self.smask.double()
+                      ).to(self.tdtype) if cond else None,
+            "ones": torch.ones(3 * N, dtype=self.tdtype, device=dev),
+        }
+        B["coef_desc"] = _native.FitDesc.from_buffer_copy(s._sync_desc())
+
+        def stage(a, m):
+            if B["bJ"] is not None:
+                B["bJ"][:m].copy_(beam_J[a:a + m])
+            B["gh"][:, :m].copy_(g_hist[:, a:a + m])
+
+        use_graph = graph and self.operators == "stencil" and cond
+        cg, cg_par, descs = None, None, None
+        for a in reversed(sorted(self.ckpt)):
+            m = min(K, self.n_steps - a)
+            stage(a, m)
+            full = use_graph and m == K and a >= 1
+            if full and cg is not None:
+                # replay: restore into the buffers the graph was captured on
+                s._par = cg_par
+                self._restore(a)
+                B["ctr"].fill_(a)
+                cg.replay()
+                s._par = cg_par ^ (K & 1)
+                continue
             self._restore(a)
-            Es = [self._values()[0].clone()]
-            incs = []
-            for n in range(a, b):
-                s._advance(1, n, beam=bp)
-                E1, H1 = self._values()
-                Es.append(E1.clone())
-                # dt (B0 H' - J) at the design entries, FP64
-                bh = torch.empty_like(self.zd)
-                Hd = H1.double().contiguous()
-                _native.check(lib.wk_adj_e(
-                    _native.WK_F64, ptr(self.Bd.rowptr), ptr(self.Bd.col), ptr(self.Bd.val),
-                    self.Bd.n, ptr(Hd), ptr(self.zd), ptr(self.zd), ptr(bh),
-                    ctypes.c_void_p(st)), "wk_adj_e")
-                if cond and n >= 1:
-                    J = self.sig_d * Es[n - a][self.rows].double()
-                    if beam_J is not None:
-                        J[self.beam_rows] = beam_J[n]
-                    bh.add_(J)
-                elif beam_J is not None:
-                    bh.index_add_(0, self.beam_rows, beam_J[n])
-                incs.append(bh.mul_(-dt))
-            for n in range(b - 1, a - 1, -1):
-                use_sig = int(cond and n >= 1)
-                E0 = Es[n - a].to(self.tdtype)
-                _native.check(lib.wk_adj_grad(
-                    self.wk, ptr(self.cells), len(self.cells_np), N, ptr(lE), ptr(incs[n - a]),
-                    ptr(E0), ptr(self.ieps), ptr(self.smask), use_sig, dt, ptr(gI),
-                    ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
-                if self.operators == "stencil":
-                    d = s._sync_desc()
-                    _native.check(lib.wk_adj_h_fit(d, self.wk, ptr(lE), ptr(lH), ptr(lH),
-                                                   ctypes.c_void_p(st)), "wk_adj_h_fit")
-                    _native.check(lib.wk_adj_e_fit(
-                        d, self.wk, ptr(lH), ptr(lE), ptr(decay) if use_sig else None,
-                        ptr(lE), ctypes.c_void_p(st)), "wk_adj_e_fit")
-                else:
-                    _native.check(lib.wk_adj_h(
-                        self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
-                        self.B0T.n, ptr(lE), ptr(self.ieps), dt, ptr(lH), ptr(lH),
-                        ctypes.c_void_p(st)), "wk_adj_h")
-                    _native.check(lib.wk_adj_e(
-                        self.wk, ptr(self.AT.rowptr), ptr(self.AT.col), ptr(self.AT.val),
-                        self.AT.n, ptr(lH), ptr(lE), ptr(decay if use_sig else ones), ptr(lE),
-                        ctypes.c_void_p(st)), "wk_adj_e")
-                lE[zidx] += g_hist[:, n]
+            if full:
+                # capture on this segment (every kernel of the segment ran
+                # eagerly at least once before, on an earlier segment)
+                if descs is None and getattr(self, "_warm", False):
+                    cg_par = s._par
+                    base = s._step_desc(self._ws["beam_params"], None)
+                    descs = []
+                    for q in range(K):
+                        c = _native.FitDesc.from_buffer_copy(base)
+                        c.par = cg_par ^ (q & 1)
+                        c.step_dev = B["ctr"].data_ptr()
+                        descs.append(c)
+                    # every kernel the graph holds has run before capture
+                    _native.check(self.lib.wk_counter_add(
+                        ctypes.c_void_p(B["ctr"].data_ptr()), 0,
+                        ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
+                        "wk_counter_add")
+                    B["ctr"].fill_(a)
+                    torch.cuda.synchronize(dev)
+                    cg = torch.cuda.CUDAGraph()
+                    cap = torch.cuda.Stream(dev)
+                    cap.wait_stream(torch.cuda.current_stream(dev))
+                    with torch.cuda.graph(cg, stream=cap):
+                        self._segment(a, K, B, graph_descs=descs)
+                    torch.cuda.current_stream(dev).wait_stream(cap)
+                    s._par = cg_par
+                    self._restore(a)
+                    B["ctr"].fill_(a)
+                    # capture ran nothing: replay for this segment as well
+                    cg.replay()
+                    s._par = cg_par ^ (K & 1)
+                    continue
+                self._warm = True
+            self._segment(a, m, B)
+        self._warm = False
+        del cg
         er = self.eps_r
-        g_eps = gI * (-1.0 / (EPS_0 * er * er))
-        return g_eps.cpu().numpy(), gS.cpu().numpy()
+        g_eps = B["gI"] * (-1.0 / (EPS_0 * er * er))
+        return g_eps.cpu().numpy(), B["gS"].cpu().numpy()
 
 
 class ImpedanceLoss(torch.autograd.Function):
