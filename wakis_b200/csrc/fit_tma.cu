@@ -1,17 +1,18 @@
 // Fused FIT step with TMA-staged plane tiles (sm_100a).
 //
-// Interior cells only (2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3); the
-// two-cell shell runs afterwards in an H launch and an E launch.  Block
-// (bx, by, bz) owns the tile
+// Which cells a launch covers depends on the face mode (MODE, see k_tma): the
+// interior (2 <= i, j, k <= N-3, the two-cell shell in separate launches),
+// all of x and y for 2 <= k <= Nz-3 (x/y faces PEC-masked), or the whole grid
+// (every face PEC-masked).  Block (bx, by, bz) owns the tile
 // i in [i0, i0+64), j in [j0, j0+8) of planes [k0, k0+KC) and marches in z.
-// For plane k it needs E_old of planes k and k+1 on the box
-// x in [i0-2, i0+66), y in [j0-1, j0+9) and H_old of plane k on
-// x in [i0-2, i0+64), y in [j0-1, j0+8) (the boxes start at an even x, so
-// the TMA x offset is 16-byte aligned).  Thread 0 issues cp.async.bulk.tensor
-// loads of those boxes (one per field component, no multicast) into a ring of
-// shared-memory slots, three planes of E and two of H, each slot completing
-// on its own mbarrier; at the start of plane k the loads of E(k+2) and
-// H(k+1) go out into the slots plane k-1 released.
+// For plane k it needs E_old of planes k and k+1 on a box from (i0-2, j0-1)
+// (interior) or (i0-4, j0-1) (full-domain modes; x offsets stay 16-byte
+// aligned) and H_old of plane k on a box one row shorter.  An idle lane of
+// warp 9 issues the cp.async.bulk.tensor loads of those boxes (one per field
+// component, no multicast) into a ring of shared-memory slots, three planes
+// of E and two of H, each slot completing on its own mbarrier; at the start
+// of plane k the loads of E(k+2) and H(k+1) go out into the slots plane k-1
+// released.
 //
 // Per plane the block computes the new H on the tile plus its low halo row
 // and column (single-coefficient rows; the halo is recomputed so that no
@@ -19,12 +20,14 @@
 // thread owns the same cells in both phases (warps 0-7: row j0+w of the
 // tile, cells i0+lane and i0+32+lane; warp 8: the halo row; warp 9: the halo
 // column and the last cell of the halo row), so the new Hx, Hy of its tile
-// cells stay in registers as H(k-1) of the next plane.  Material ids of the owned cells and the per-plane metric rows
-// (iAx, iAy, itAx, itAy, Lz, tLz) of plane k+1 are loaded while plane k is
-// computed; the plane-invariant metrics (Lx, Ly, iAz, ...) are loaded once.
-// A chunk starting at k0 first forms the new H of plane k0-1 on its tile.
-// Every mbarrier wait is bounded: on timeout the block records the failure
-// in the status word, waits (bounded) for its loads in flight and returns.
+// cells stay in registers as H(k-1) of the next plane.  The per-plane metric
+// rows (iAx, iAy, itAx, itAy, Lz, tLz) go into a 3-slot ring by cp.async two
+// planes ahead, issued by warps 8 and 9 while the tile warps compute E; the
+// material ids of plane k+1 are loaded during plane k; the plane-invariant
+// metrics (Lx, Ly, iAz, ...) are loaded once.  A chunk starting at k0 first
+// forms the new H of plane k0-1 on its tile.  Every mbarrier wait is
+// bounded: on timeout the block records the failure in the status word,
+// waits (bounded) for its loads in flight and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>

@@ -6,14 +6,14 @@
 // from the FP64 metric and material tables and rounded once to float
 // (dt folded in); the rows then run in float.
 //
-// Interior cells only (2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3); the
-// shell runs afterwards in the compensated shell launches.  Block
-// (bx, by, bz) owns the tile i in [i0, i0+64), j in [j0, j0+8) of planes
-// [k0, k0+KC) and marches in z.  Thread 0 issues cp.async.bulk.tensor loads
-// (no multicast) of E (68x10 floats from (i0-2, j0-1), three planes in a
-// ring) and H (68x9 floats, two planes) into shared memory, each slot
-// completing on its own mbarrier; the loads of E(k+2) and H(k+1) go out at
-// the start of plane k.
+// The face modes are those of the FP64 kernel (k_tma): the interior with
+// shell launches, all of x and y, or the whole grid.  Block (bx, by, bz) owns
+// the tile i in [i0, i0+64), j in [j0, j0+8) of planes [k0, k0+KC) and
+// marches in z.  An idle lane of warp 9 issues cp.async.bulk.tensor loads (no
+// multicast) of E (three planes in a ring), H (two planes) and, with
+// Nx % 8 == 0, the bf16 compensation words of plane k with H(k), into shared
+// memory, each slot completing on its own mbarrier; the loads of E(k+2) and
+// H(k+1) go out at the start of plane k.
 //
 // Threads work on pairs of cells (i, i+1) with packed f32x2 arithmetic:
 // warps 0-7 own the 256 pairs of the tile (row = warp, pair = lane) in both
@@ -21,10 +21,11 @@
 // 9 the halo column i0-1 (single cells).  The halo H is recomputed with the
 // same compensated update as its owner's, so it is the value the owner
 // stores.  The new Hx, Hy of a tile pair stay in registers as H(k-1) of the
-// next plane.  Material ids, compensation words and the per-plane factor
-// rows of plane k+1 are loaded while plane k is computed.  Every mbarrier
-// wait is bounded: on timeout the block sets the status word, waits
-// (bounded) for its loads in flight and returns.
+// next plane.  The material ids and the FP64 inputs of the per-plane factor
+// rows go into a 3-slot ring by cp.async two planes ahead; the float rows of
+// plane k+1 are formed at the end of plane k.  Every mbarrier wait is
+// bounded: on timeout the block sets the status word, waits (bounded) for
+// its loads in flight and returns.
 #include <cuda_bf16.h>
 #include <stdint.h>
 
