@@ -658,3 +658,63 @@ def test_clean_faces_skip_equals_masked_step(name, shape, prec):
     assert np.abs(runs[0][0]).max() > 0
     for a, b in zip(runs[0], runs[1]):
         assert np.array_equal(a, b)
+
+
+def _full_size_pair(kernels):
+    from wakis_b200 import workloads
+    out = []
+    for k in kernels:
+        _, _, s = workloads.build_b200("lossy_256")
+        s.kernel = k
+        out.append(s)
+    return out
+
+
+def test_full_size_tma_equals_twopass():
+    """lossy_256 at its benchmark size (256x256x512): the full-domain TMA
+    step equals the two-pass step value for value, from random fields (H-row
+    face masks applied) and from zero fields with the fused beam and the Ez
+    capture (faces clean, masks skipped), 8 steps each."""
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    a, b = _full_size_pair(["tma", "twopass"])
+    g = torch.Generator(device="cuda").manual_seed(7)
+    E0 = torch.randn(3 * a.N, generator=g, device="cuda", dtype=torch.float64)
+    H0 = torch.randn(3 * a.N, generator=g, device="cuda", dtype=torch.float64)
+    for s in (a, b):
+        s._first_step()
+        s.E.fromarray(E0)
+        s.H.fromarray(H0)
+        s._advance(8, 0)
+    assert int(a._status.item()) == 0
+    assert torch.equal(a.E.array, b.E.array) and torch.equal(a.H.array, b.H.array)
+    sp = workloads.spec("lossy_256")
+    bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
+              ).params(a)
+    hists = []
+    for s in (a, b):
+        s.reset_fields()
+        s.step_0, s.nstep = True, 0
+        h = torch.zeros((9, s.Nz, 8), dtype=torch.float64, device="cuda")
+        s._advance(8, 0, beam=bp, capture=(h, 127, 127, 3, 3))
+        hists.append(h)
+    assert a._faces_clean
+    assert torch.equal(a.E.array, b.E.array) and torch.equal(a.H.array, b.H.array)
+    assert torch.equal(hists[0], hists[1])
+
+
+def test_full_size_step_is_linear():
+    """At the benchmark size, 8 source-free steps from 2x a random state give
+    exactly twice the steps from the state (scaling by a power of two is
+    exact in every product and sum of the update)."""
+    a, b = _full_size_pair(["auto", "auto"])
+    g = torch.Generator(device="cuda").manual_seed(8)
+    E0 = torch.randn(3 * a.N, generator=g, device="cuda", dtype=torch.float64)
+    H0 = torch.randn(3 * a.N, generator=g, device="cuda", dtype=torch.float64)
+    for s, f in ((a, 1.0), (b, 2.0)):
+        s._first_step()
+        s.E.fromarray(E0 * f)
+        s.H.fromarray(H0 * f)
+        s._advance(8, 0)
+    assert torch.equal(b.E.array, 2.0 * a.E.array)
+    assert torch.equal(b.H.array, 2.0 * a.H.array)
