@@ -65,6 +65,69 @@ def _traffic(workload, dtype, schedule):
         return None
 
 
+class RegionClocks:
+    """SM clock and clock-event reasons read through NVML every 2 ms by a
+    thread, from start() to stop(): the samples of the timed region itself
+    (read-only queries; None when NVML is unavailable)."""
+
+    def __init__(self, uuid, device_index):
+        self.samples, self.reasons, self.smax = [], set(), None
+        self.h, self.t, self.run = None, None, False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            h = None
+            if uuid:
+                u = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+                try:
+                    h = pynvml.nvmlDeviceGetHandleByUUID(u)
+                except Exception:
+                    h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.h = h
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.h = None
+
+    def _poll(self):
+        nv = self.nv
+        names = {nv.nvmlClocksEventReasonHwSlowdown: "hw_slowdown",
+                 nv.nvmlClocksEventReasonHwThermalSlowdown: "hw_thermal_slowdown",
+                 nv.nvmlClocksEventReasonSwThermalSlowdown: "sw_thermal_slowdown",
+                 nv.nvmlClocksEventReasonSwPowerCap: "sw_power_cap"}
+        while self.run:
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for b, nm in names.items():
+                    if bits & b:
+                        self.reasons.add(nm)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def start(self):
+        if self.h is None:
+            return
+        import threading
+        self.run = True
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
+
+    def stop(self):
+        if self.t is None:
+            return None
+        self.run = False
+        self.t.join(timeout=5)
+        if not self.samples:
+            return None
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "source": "NVML, every 2 ms inside the timed region"}
+
+
 class Clocks:
     """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
 
@@ -419,15 +482,18 @@ def run_slab(args):
     except Exception:
         pass
     clk = Clocks(uuid)
+    rclk = RegionClocks(uuid, local)
     time.sleep(0.3)
     st = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    rclk.start()
     e0.record(st)
     steps(args.warmup, args.steps)
     e1.record(st)
     torch.cuda.synchronize()
+    region_clocks = rclk.stop()
     barrier()
     ms = e0.elapsed_time(e1)
     # step kernels per slab and step (one timed step per slab)
@@ -459,7 +525,9 @@ def run_slab(args):
         ex(lay, solvers)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
-    clocks = clk.stop()
+    clocks = region_clocks or clk.stop()
+    if region_clocks is not None:
+        clk.stop()
     ms, t_e2e = max_over_ranks([ms, t_e2e], ws, dev)
     if rank == 0:
         bpc = BYTES_PER_CELL[args.dtype]
@@ -625,15 +693,18 @@ def main():
     except Exception:
         pass
     clk = Clocks(uuid)
+    rclk = RegionClocks(uuid, local)
     time.sleep(0.3)
     st = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    rclk.start()
     e0.record(st)
     s._advance(args.steps, args.warmup, beam=bp, capture=cap, split=split)
     e1.record(st)
     torch.cuda.synchronize()
+    region_clocks = rclk.stop()
     barrier()
     ms = e0.elapsed_time(e1)
     # interior-kernel time of the same K steps, CUDA events around each
@@ -681,7 +752,9 @@ def main():
     s.run_with_io(jz, ez, step0=total + args.steps)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
-    clocks = clk.stop()
+    clocks = region_clocks or clk.stop()
+    if region_clocks is not None:
+        clk.stop()
     # device times and the end-to-end wall time: max over ranks
     ms, ms_int, t_e2e = max_over_ranks([ms, ms_int, t_e2e], ws, dev)
 
