@@ -127,7 +127,7 @@ __device__ __forceinline__ RowEntry<T> row_entry(const FitParams<T>& p, int r, i
 // 2 <= k <= Nz-3 (no z face is involved there), and the shell launches
 // cover only the planes k in {0, 1, Nz-2, Nz-1}.  Warps with no cell on or
 // next to a face take the unmasked rows.
-template <typename T, bool SM, int JM, int MODE>
+template <typename T, bool SM, int JM, int MODE, bool DESC>
 __global__ void __launch_bounds__(kTmaThreads, sizeof(T) == 8 ? 2 : 3)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
   constexpr bool FULL = MODE != 0;     // tiles cover x and y entirely
@@ -234,7 +234,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     if (hval[r]) nearface |= xf0[r] || xf1[r] || yf0[r] || yf1[r];
   }
   const bool warp_face = FULL && __any_sync(0xffffffffu, nearface);
-  const bool desc = p.h_desc != 0;
+  constexpr bool desc = DESC;   // H-row summation order (wk_fit_desc.h_sum_desc)
   // plane-invariant tests of the owned cells, one bit each: cell r in the
   // Ez capture window (bit r), on the source line (bit 2 + r)
   int cell_bits = 0;
@@ -482,23 +482,23 @@ bool tma_supported(const FitParams<T>& p) {
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
 struct TmaOcc { int sms = 0, per_sm = 0; bool attr = false; };
-static TmaOcc g_occ[2][2][3][3][64];
+static TmaOcc g_occ[2][2][3][3][2][64];
 
-template <typename T, bool SM, int JM, int MODE>
+template <typename T, bool SM, int JM, int MODE, bool DESC>
 static cudaError_t tma_occupancy(TmaOcc** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][MODE][dev];
+  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][MODE][DESC ? 1 : 0][dev];
   if (!o.attr) {
     const int smem = TmaLayout<T, (MODE != 0)>::bytes;
-    e = cudaFuncSetAttribute(k_tma<T, SM, JM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_tma<T, SM, JM, MODE, DESC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, MODE>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, MODE, DESC>,
                                                       kTmaThreads, smem);
     if (e != cudaSuccess) return e;
     if (o.per_sm < 1) o.per_sm = 1;
@@ -518,7 +518,7 @@ static int tma_mode(const FitParams<T>& p) {
   return (p.pec_face[4] == 0 && p.pec_face[5] == 0) ? 1 : 2;
 }
 
-template <typename T, bool SM, int JM, int MODE>
+template <typename T, bool SM, int JM, int MODE, bool DESC>
 static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cudaStream_t st,
                                       int KC) {
   using G = TmaGeom<T, (MODE != 0)>;
@@ -529,7 +529,7 @@ static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cud
       return cudaErrorInvalidValue;
   }
   TmaOcc* occ = nullptr;
-  cudaError_t e = tma_occupancy<T, SM, JM, MODE>(&occ);
+  cudaError_t e = tma_occupancy<T, SM, JM, MODE, DESC>(&occ);
   if (e != cudaSuccess) return e;
   const int span_x = MODE ? p.Nx : p.Nx - 4, span_y = MODE ? p.Ny : p.Ny - 4;
   const int planes = MODE == 1 ? p.Nz : p.Nz - 4;
@@ -538,7 +538,7 @@ static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cud
     KC = tma_auto_kc((long long)gx * gy, planes, (long long)occ->sms * occ->per_sm);
   const int gz = (planes + KC - 1) / KC;
   timer_begin(st);
-  k_tma<T, SM, JM, MODE><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T, (MODE != 0)>::bytes,
+  k_tma<T, SM, JM, MODE, DESC><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T, (MODE != 0)>::bytes,
                            st>>>(p, maps, step, KC);
   timer_end(st);
   e = cudaGetLastError();
@@ -556,15 +556,22 @@ cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, i
   const bool sm_table = p.n_mat <= kMatSmem && p.id_bytes == 1;
   const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
   const int mode = tma_mode(p);
+  const bool desc = p.h_desc != 0;
+#define WK_TMA_MODES(SMV, JMV, DV)                                                    \
+  {                                                                                   \
+    if (mode == 1) return launch_tma_variant<T, SMV, JMV, 1, DV>(p, step, st, KC);    \
+    if (mode == 2) return launch_tma_variant<T, SMV, JMV, 2, DV>(p, step, st, KC);    \
+    return launch_tma_variant<T, SMV, JMV, 0, DV>(p, step, st, KC);                   \
+  }
 #define WK_TMA_CASE(SMV, JMV)                                                         \
   if (sm_table == SMV && jm == JMV) {                                                 \
-    if (mode == 1) return launch_tma_variant<T, SMV, JMV, 1>(p, step, st, KC);        \
-    if (mode == 2) return launch_tma_variant<T, SMV, JMV, 2>(p, step, st, KC);        \
-    return launch_tma_variant<T, SMV, JMV, 0>(p, step, st, KC);                       \
+    if (desc) WK_TMA_MODES(SMV, JMV, true)                                            \
+    WK_TMA_MODES(SMV, JMV, false)                                                     \
   }
   WK_TMA_CASE(true, 0) WK_TMA_CASE(true, 1) WK_TMA_CASE(true, 2)
   WK_TMA_CASE(false, 0) WK_TMA_CASE(false, 1) WK_TMA_CASE(false, 2)
 #undef WK_TMA_CASE
+#undef WK_TMA_MODES
   return cudaErrorInvalidValue;
 }
 
