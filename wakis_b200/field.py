@@ -204,7 +204,11 @@ class StateField(Field):
     """Field whose storage alternates between two buffers.
 
     The fused step kernel reads one buffer and writes the other; ``owner``
-    holds the parity, so ``array`` always returns the live buffer.
+    holds the parity, so ``array`` always returns the live buffer.  Writes
+    go through ``fromarray``, ``from_matrix`` or item assignment, which tell
+    the owner first (it keeps J = sigma*E and the state of the PEC faces in
+    step with E); an in-place change of the tensor ``array`` returns is not
+    seen by the solver.
     """
 
     def __init__(self, owner, bufs, Nx, Ny, Nz, dtype):
