@@ -44,6 +44,7 @@ constexpr int kTX = 64, kTY = 8;
 constexpr int kBX = kTX + 4, kBY = kTY + 2;          // E box
 constexpr int kHBY = kTY + 1;                        // H box rows
 constexpr int kES = 3, kHS = 2;                      // ring slots
+static_assert(kES == 3 && kHS == 2, "the step loop counts the ring slots for 3 E and 2 H slots");
 constexpr int kTmaThreads = 320;
 constexpr int kEW = kTX + 1;                         // ext tile row width
 constexpr int kExt = kEW * (kTY + 1);                // 585
@@ -261,11 +262,11 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   if (SM)
     for (int q = tid; q < 9 * p.n_mat; q += kTmaThreads) smat[q] = p.mat[q];
   const T* mat = SM ? smat : p.mat;
-  // The metric row of plane q goes into ring slot (q - pstart) % 3 by
-  // cp.async two planes ahead, issued by warps 8 and 9 (entries t, t+64,
-  // t+128 for t = tid - 256) while the tile warps compute the E of the
-  // plane before; one group per plane and thread.
-  auto stage_row = [&](int q) {
+  // The metric row of plane q goes into ring slot (q - pstart) % 3 (passed
+  // as `slot`) by cp.async two planes ahead, issued by warps 8 and 9
+  // (entries t, t+64, t+128 for t = tid - 256) while the tile warps compute
+  // the E of the plane before; one group per plane and thread.
+  auto stage_row = [&](int q, int slot) {
     if (tid >= 256 && q < k1) {
 #pragma unroll
       for (int u = 0; u < 3; u++) {
@@ -273,15 +274,14 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         if (r < kRow) {
           const RowEntry<T> e = row_entry(p, r, i0, j0);
           const bool v = e.a != nullptr && q >= 0 && q < Nz;
-          cp_async<sizeof(T)>(Rw + ((q - pstart) % 3) * kRow + r,
-                              v ? e.a + (long long)q * e.stride : p.Lz, v);
+          cp_async<sizeof(T)>(Rw + slot * kRow + r, v ? e.a + (long long)q * e.stride : p.Lz, v);
         }
       }
     }
     cp_async_commit();
   };
-  stage_row(pstart);
-  stage_row(pstart + 1);
+  stage_row(pstart, 0);
+  stage_row(pstart + 1, 1);
   // material ids: one byte each with the table in shared memory (SM),
   // else id_bytes wide; the pointer of cell 0 advances one plane per step
   const unsigned char* idp = static_cast<const unsigned char*>(p.mat_id) +
@@ -298,6 +298,14 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 #pragma unroll
   for (int r = 0; r < 2; r++) id[r] = (hval[r] && pstart >= 0) ? id_at(r, pstart) : 0;
   T hxp[2] = {T(0), T(0)}, hyp[2] = {T(0), T(0)};
+  // per-plane cursors: the ids of plane pl+1, the outputs of cell 0 of
+  // plane pl (the second cell is 32 entries on); ring slots of E(pl), H(pl)
+  // and of the metric row of pl, counted instead of taken modulo
+  const unsigned char* idq = idp + (long long)(pstart + 1) * id_plane;
+  const long long cn0 = ci[0] + (long long)cj[0] * Nx + (long long)pstart * NxNy;
+  T* hq = p.H_out + cn0;
+  T* eq = p.E_out + cn0;
+  int se = 0, sh = 0;
 
   bool ok = true;
   int pl = pstart;
@@ -319,14 +327,22 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     int idn[2] = {0, 0};
     if (more) {
 #pragma unroll
-      for (int r = 0; r < 2; r++)
-        if (hval[r]) idn[r] = id_at(r, pl + 1);
+      for (int r = 0; r < 2; r++) {
+        if (!hval[r]) continue;
+        const unsigned char* a = idq + 32 * r * (SM ? 1 : p.id_bytes);
+        if (SM || p.id_bytes == 1) idn[r] = a[0];
+        else if (p.id_bytes == 2) idn[r] = *reinterpret_cast<const uint16_t*>(a);
+        else idn[r] = (int)*reinterpret_cast<const uint32_t*>(a);
+      }
     }
-    const T* Ek = Eb + ((pl - pstart) % kES) * 3 * SE;
-    const T* Ek1 = Eb + ((pl + 1 - pstart) % kES) * 3 * SE;
-    const T* Hk = Hb + ((pl - pstart) % kHS) * 3 * SH;
-    const T* R = Rw + ((pl - pstart) % 3) * kRow;
+    const int se1 = se == kES - 1 ? 0 : se + 1;     // slot of E(pl+1)
+    const T* Ek = Eb + se * 3 * SE;
+    const T* Ek1 = Eb + se1 * 3 * SE;
+    const T* Hk = Hb + sh * 3 * SH;
+    const T* R = Rw + se * kRow;                     // row ring: also 3 slots
     const long long off = (long long)pl * NxNy;
+    T* const hq1 = hq + N;
+    T* const eq1 = eq + N;
 
     // plane face flags (MODE 1): at the plane and of the +z neighbour
     const bool zf0 = ZFULL && (pl == 0 || pl == Nz - 1), zf1 = ZFULL && pl + 1 >= Nz - 1;
@@ -380,17 +396,16 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
       hxn[r] = hx;
       hyn[r] = hy;
       if (!prologue && tile_cell) {
-        const long long n = ci[r] + (long long)cj[r] * Nx + off;
-        p.H_out[n] = hx;
-        p.H_out[N + n] = hy;
-        p.H_out[2 * N + n] = hz;
+        hq[32 * r] = hx;
+        hq1[32 * r] = hy;
+        hq1[N + 32 * r] = hz;
       }
     }
     __syncthreads();
 
     // warps 8 and 9 own no E row: the row slot of plane pl-1 is free (every
     // thread passed the top barrier of plane pl), stage the row of pl+2
-    if (warp >= 8) stage_row(pl + 2);
+    if (warp >= 8) stage_row(pl + 2, se == 0 ? kES - 1 : se - 1);
     if (!prologue) {
       const T tLz = R[147];
 #pragma unroll
@@ -427,7 +442,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
           if (JM == WK_J_ARRAY) jv = p.J[d * N + n];
           if (d == 2 && (cell_bits & (4 << r))) jv = j_in(p, d, cc, n, step, eold[d], sigma);
           const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
-          p.E_out[d * N + n] = enew;
+          (d == 0 ? eq : (d == 1 ? eq1 : eq1 + N))[32 * r] = enew;
           if (JM == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
         }
       }
@@ -438,6 +453,11 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
       hyp[r] = hyn[r];
       id[r] = idn[r];
     }
+    idq += id_plane;
+    hq += NxNy;
+    eq += NxNy;
+    se = se1;
+    sh ^= 1;
   }
   cp_async_wait<0>();
   if (!ok) {
