@@ -44,6 +44,7 @@ constexpr int cTX = 64, cTY = 8;
 constexpr int cBX = 68, cBY = 10;         // E box (floats): x from i0-2, y from j0-1
 constexpr int cHBY = 9;                   // H box rows (68 wide)
 constexpr int cES = 3, cHS = 2;
+static_assert(cES == 3 && cHS == 2, "the step loop counts the ring slots for 3 E and 2 H slots");
 constexpr int cThreads = 320;
 constexpr int cEW = 66;                   // Hs row: index eb*66 + ea + 1
 constexpr int cExt = cEW * (cTY + 1);     // 594
@@ -326,8 +327,7 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   // of the ids in their word is the same on every plane.
   const IdT* idp = static_cast<const IdT*>(p.mat_id) + nb;
   const int id_sh = 8 * (int)((nb * (long long)sizeof(IdT)) & 3);
-  auto stage_ids = [&](int q, uint64_t* dst) {
-    const IdT* a = idp + (long long)q * NxNy;
+  auto stage_ids = [&](int q, const IdT* a, uint64_t* dst) {
     if (q < 0) *dst = 0ull;
     else if (pair && sizeof(IdT) == 4) cp_async<8>(dst, a, true);
     else cp_async<4>(dst, reinterpret_cast<const void*>((uintptr_t)a & ~(uintptr_t)3), true);
@@ -365,23 +365,34 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   // (q - pstart) % 3 by cp.async two planes ahead (one group per plane and
   // thread); the float row of plane q is formed at the end of plane q-1.
   const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
-  auto stage_rows = [&](int q) {
+  // slot = (q - pstart) % 3, ida = the ids of the item at plane q
+  auto stage_rows = [&](int q, int slot, const IdT* ida) {
     if (q < k1) {
-      if (tid < cRow) row_stage(rsrc, q, Nz, p.Lz, Rraw + (((q - pstart) % 3) * cRow + tid) * 2);
-      if (hval) stage_ids(q, sidw + ((q - pstart) % 3) * cThreads + tid);
+      if (tid < cRow) row_stage(rsrc, q, Nz, p.Lz, Rraw + (slot * cRow + tid) * 2);
+      if (hval) stage_ids(q, ida, sidw + slot * cThreads + tid);
     }
     cp_async_commit();
   };
-  auto form_row = [&](int q) {
+  auto form_row = [&](int q, int slot) {
     if (tid < cRow) {
-      const double* v = Rraw + (((q - pstart) % 3) * cRow + tid) * 2;
+      const double* v = Rraw + (slot * cRow + tid) * 2;
       Rw[(q & 1) * cRow + tid] = row_value(p.dt, v[0], v[1]);
     }
   };
-  stage_rows(pstart);
-  stage_rows(pstart + 1);
+  stage_rows(pstart, 0, idp + (long long)pstart * NxNy);
+  stage_rows(pstart + 1, 1, idp + (long long)(pstart + 1) * NxNy);
   cp_async_wait<1>();
-  form_row(pstart);
+  form_row(pstart, 0);
+  // per-plane cursors: the ids of plane pl+2, the outputs of the item at
+  // plane pl; ring slots of E(pl), H(pl) and of the staged inputs of pl,
+  // counted instead of taken modulo
+  const IdT* idq = idp + (long long)(pstart + 2) * NxNy;
+  const long long nq = nb + (long long)pstart * NxNy;
+  float* hq = cs.H_out + nq;
+  float* eq = cs.E_out + nq;
+  comp_t* hcq = cs.Hc_out + nq;
+  comp_t* ecq = cs.Ec_out + nq;
+  int se = 0, sh = 0;
 
   float2 hxp = bcast(0.f), hyp = bcast(0.f);
   const float2 zero2 = bcast(0.f);
@@ -399,9 +410,11 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       if (pl + cES - 1 <= k1) { issue_e(pl + cES - 1); e_hi = pl + cES - 1; }
       if (pl + cHS - 1 <= k1 - 1) { issue_h(pl + cHS - 1); h_hi = pl + cHS - 1; }
     }
-    stage_rows(pl + 2);          // the ring slot of plane pl-1 is free
+    const int se1 = se == cES - 1 ? 0 : se + 1;     // slot of plane pl+1
+    const int se2 = se == 0 ? cES - 1 : se - 1;      // slot of plane pl+2
+    stage_rows(pl + 2, se2, idq);  // the ring slot of plane pl-1 is free
     int id0 = 0, id1 = 0;
-    if (hval) read_ids(sidw + ((pl - pstart) % 3) * cThreads + tid, id0, id1);
+    if (hval) read_ids(sidw + se * cThreads + tid, id0, id1);
     // prefetch the compensation words of plane pl+1 (without CT)
     const bool more = pl + 1 < k1;
     uint32_t nhc[3] = {0, 0, 0}, nec[3] = {0, 0, 0};
@@ -409,10 +422,10 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       if (hval) load_comp(cs.Hc_in, pl + 1, nhc);
       if (eval) load_comp(cs.Ec_in, pl + 1, nec);
     }
-    const float* Ek = Eb + ((pl - pstart) % cES) * 3 * SE;
-    const float* Ek1 = Eb + ((pl + 1 - pstart) % cES) * 3 * SE;
-    const float* Hk = Hb + ((pl - pstart) % cHS) * 3 * SH;
-    const uint16_t* Ck = Cb + ((pl - pstart) % cHS) * 6 * SC;
+    const float* Ek = Eb + se * 3 * SE;
+    const float* Ek1 = Eb + se1 * 3 * SE;
+    const float* Hk = Hb + sh * 3 * SH;
+    const uint16_t* Ck = Cb + sh * 6 * SC;
     const float* R = Rw + (pl & 1) * cRow;
     const long long n = nb + (long long)pl * NxNy;
 
@@ -490,10 +503,12 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
       hxn = hx;
       hyn = hy;
       if (role == 0 && !prologue) {
-        st2(cs.H_out + n, hx); st2(cs.H_out + N + n, hy); st2(cs.H_out + 2 * N + n, hz);
-        *reinterpret_cast<uint32_t*>(cs.Hc_out + n) = hc[0];
-        *reinterpret_cast<uint32_t*>(cs.Hc_out + N + n) = hc[1];
-        *reinterpret_cast<uint32_t*>(cs.Hc_out + 2 * N + n) = hc[2];
+        float* const h1 = hq + N;
+        comp_t* const hc1 = hcq + N;
+        st2(hq, hx); st2(h1, hy); st2(h1 + N, hz);
+        *reinterpret_cast<uint32_t*>(hcq) = hc[0];
+        *reinterpret_cast<uint32_t*>(hc1) = hc[1];
+        *reinterpret_cast<uint32_t*>(hc1 + N) = hc[2];
       }
     }
     __syncthreads();
@@ -558,10 +573,12 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
         }
         ev[d] = cadd2(ev[d], ec[d], sub2(cu[d], jt));
       }
-      st2(cs.E_out + n, ev[0]); st2(cs.E_out + N + n, ev[1]); st2(cs.E_out + 2 * N + n, ev[2]);
-      *reinterpret_cast<uint32_t*>(cs.Ec_out + n) = ec[0];
-      *reinterpret_cast<uint32_t*>(cs.Ec_out + N + n) = ec[1];
-      *reinterpret_cast<uint32_t*>(cs.Ec_out + 2 * N + n) = ec[2];
+      float* const e1 = eq + N;
+      comp_t* const ec1 = ecq + N;
+      st2(eq, ev[0]); st2(e1, ev[1]); st2(e1 + N, ev[2]);
+      *reinterpret_cast<uint32_t*>(ecq) = ec[0];
+      *reinterpret_cast<uint32_t*>(ec1) = ec[1];
+      *reinterpret_cast<uint32_t*>(ec1 + N) = ec[2];
     }
     hxp = hxn;
     hyp = hyn;
@@ -574,8 +591,15 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
     }
     if (more) {
       cp_async_wait<1>();        // this thread's row inputs and ids of plane pl+1
-      form_row(pl + 1);
+      form_row(pl + 1, se1);
     }
+    idq += NxNy;
+    hq += NxNy;
+    eq += NxNy;
+    hcq += NxNy;
+    ecq += NxNy;
+    se = se1;
+    sh ^= 1;
   }
   cp_async_wait<0>();
   if (!ok) {
