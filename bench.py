@@ -53,14 +53,19 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _traffic(workload, dtype, schedule):
-    """DRAM bytes (read + write) per launch of the interior kernel, from the
-    committed ncu summary profiles/traffic.json, if it holds this case."""
+def _traffic(workload, dtype, schedule, cells):
+    """DRAM bytes (read + write) per launch of the interior kernel over
+    `cells` cells: the bytes per cell of the committed ncu summary
+    profiles/traffic.json (one launch on a smaller grid of the same
+    workload) times the cells, if the summary holds this case."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
         e = t.get(f"{workload}:{dtype}:{schedule}")
-        return None if e is None else e["bytes_per_launch"]
+        if e is None:
+            return None
+        per_cell = (e["read_bytes_small"] + e["write_bytes_small"]) / e["cells_small"]
+        return int(round(per_cell * cells))
     except Exception:
         return None
 
@@ -788,7 +793,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": src,
                          "bytes_per_cell_step": bpc, "kernel": kernel_note,
-                         "traffic": _traffic(args.workload, args.dtype, schedule),
+                         "traffic": _traffic(args.workload, args.dtype, schedule, interior),
                          "step_achieved": step_gbs, "step_frac": step_gbs / peak},
             "e2e": {"value": N * args.steps * ws / t_e2e / 1e9, "unit": "Gcell-steps/s",
                     "h2d_bytes_per_step": int(jz[0].numel() * jz.element_size()),
