@@ -68,3 +68,20 @@ def test_single_rank_max_is_identity():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.max_over_ranks([1.5, 2.0], 1) == [1.5, 2.0]
+
+
+def test_traffic_scales_with_the_cells_of_the_launch():
+    """roofline.traffic: the ncu bytes per cell of the committed summary
+    times the cells of the launch; None for a case it does not hold."""
+    import json
+    sys.path.insert(0, ROOT)
+    import bench
+    with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+        e = json.load(f)["lossy_256:float64:tma"]
+    per_cell = (e["read_bytes_small"] + e["write_bytes_small"]) / e["cells_small"]
+    assert 80.0 < per_cell < 96.5
+    assert bench._traffic("lossy_256", "float64", "tma", e["cells_small"]) == \
+        e["read_bytes_small"] + e["write_bytes_small"]
+    assert bench._traffic("lossy_256", "float64", "tma", 256 * 256 * 512) == \
+        int(round(per_cell * 256 * 256 * 512))
+    assert bench._traffic("lossy_256", "float64", "no-such-schedule", 10) is None
