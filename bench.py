@@ -602,7 +602,8 @@ def cpu_baseline(args, budget_s=20.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=200,
+                    help="timed steps (200 FP64 steps at 256x256x512 take about 0.12 s, long enough for\n                    several clock samples inside the timed region)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="lossy_256")
