@@ -200,6 +200,17 @@ def max_over_ranks(vals, ws, device=None):
     return [float(v) for v in t.tolist()]
 
 
+def _status_ok(solver):
+    """True when no step kernel of `solver` timed out since the last check
+    (reads and clears its device status word)."""
+    try:
+        solver.check_status("bench")
+        return True
+    except RuntimeError as e:
+        print(str(e), file=sys.stderr, flush=True)
+        return False
+
+
 def run_reference(args):
     """CPU oracle on the host cores: Gcell-steps/s of upstream's scipy
     algorithm on a bounded sample (same geometry, 128x128x256)."""
@@ -609,7 +620,7 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32", "fp32c"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "slab", "fused", "twopass", "march", "cell", "split"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "twopass", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
@@ -711,6 +722,9 @@ def main():
     e1.record(st)
     torch.cuda.synchronize()
     region_clocks = rclk.stop()
+    # the status word of the step kernels: a timed-out tile load leaves the
+    # steps incomplete, and then no rate is reported
+    status_ok = _status_ok(s)
     barrier()
     ms = e0.elapsed_time(e1)
     # interior-kernel time of the same K steps, CUDA events around each
@@ -722,10 +736,7 @@ def main():
     # kernels launched per step: TMA 1 (every face PEC-masked) or 1 interior
     # + 2 shell launches, two-pass 2 interior + 2 shell launches; the other
     # schedules launch a fixed set
-    planes = s.tile[1] if s.tile[1] > 0 else max(
-        2, (80 * 1024 * 1024) // (9 * np.dtype(dtype).itemsize * s.Nx * s.Ny))
-    nslab = -(-s.Nz // planes)
-    fixed = {"split": 4, "fused": 2, "slab": 2 * nslab, "march": 1, "cell": 1}
+    fixed = {"split": 4, "cell": 1}
     n_per = n_int // max(args.steps, 1)
     # the TMA schedule needs no shell launch when every face is PEC-masked
     pec_faces = all(b.lower() in ("pec", "electric", "pml") for b in s.bc_low + s.bc_high)
@@ -761,8 +772,17 @@ def main():
     clocks = region_clocks or clk.stop()
     if region_clocks is not None:
         clk.stop()
-    # device times and the end-to-end wall time: max over ranks
-    ms, ms_int, t_e2e = max_over_ranks([ms, ms_int, t_e2e], ws, dev)
+    # device times and the end-to-end wall time: max over ranks (and the
+    # status flags: any rank that timed out voids the run)
+    ms, ms_int, t_e2e, bad = max_over_ranks([ms, ms_int, t_e2e, 0.0 if status_ok else 1.0],
+                                            ws, dev)
+    if bad:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "error": "a step kernel timed out waiting for "
+                              "a tile load in the timed region; no rate reported"}), flush=True)
+        if ws > 1:
+            dist.destroy_process_group()
+        sys.exit(3)
 
     if rank == 0:
         value = N * args.steps * ws / (ms / 1e3) / 1e9
@@ -801,6 +821,7 @@ def main():
                     "d2h_bytes_per_step": int(ez[0].numel() * ez.element_size())},
             "gpu_launches": launches,
             "clocks": clocks,
+            "status_word": 0,
         }
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args)

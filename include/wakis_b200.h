@@ -31,10 +31,11 @@ extern "C" {
 #define WK_E_ALIGN 4     /* pointer not aligned to its element size      */
 #define WK_E_RANGE 5     /* index (beam line, capture window) off-grid   */
 #define WK_E_MODE 6      /* inconsistent mode flags                      */
+#define WK_E_TIMEOUT 7   /* a device-side wait ran out (wk_read_status)  */
 
 #define WK_F64 0
 #define WK_F32 1
-#define WK_F32C 2   /* FP32 state with int8 compensation words (Ec, Hc);
+#define WK_F32C 2   /* FP32 state with bf16 compensation words (Ec, Hc);
                        coefficient tables FP64; Ez capture FP64          */
 
 /* J source used by the E half-step (upstream computes E += dt*(B*H - ieps*J)
@@ -111,8 +112,9 @@ typedef struct wk_fit_desc {
   void* cap;               /* dtype elements                                 */
   int* status;             /* device status word (0 = ok), may be NULL       */
   /* Kernel choice for wk_fit_step (WK_KERNEL_* below).
-   * tile_rows / tile_planes (0 = automatic) set the rows per block and the
-   * planes per block of the plane-marching kernel.                         */
+   * tile_planes (0 = automatic) sets the planes per block of the TMA kernel
+   * and the planes per thread of the two-pass kernels; tile_rows is not
+   * read.                                                                  */
   int kernel;
   int tile_rows, tile_planes;
   /* WK_F32C only: per-component compensation words of E and H (bf16 bit
@@ -134,6 +136,13 @@ typedef struct wk_fit_desc {
    * full-domain TMA kernels then skip the PEC column masks of the H rows,
    * which would only replace +0 by +0.  0 (the default) always masks.      */
   int faces_clean;
+  /* Bound of each mbarrier wait in the step loop of the TMA kernels, in
+   * nanoseconds of the GPU's global timer; 0 (the default) = 100 ms.  A
+   * negative value makes the first wait give up at once: the block then
+   * records the timeout in *status, waits with the default bound for the
+   * loads it issued and returns (a test of the timeout path, which leaves
+   * the output of the step incomplete).                                   */
+  long long wait_ns;
 } wk_fit_desc;
 
 #define WK_KERNEL_AUTO 0   /* WK_KERNEL_TMA when its conditions hold, else
@@ -141,12 +150,6 @@ typedef struct wk_fit_desc {
                               WK_KERNEL_CELL                                */
 #define WK_KERNEL_CELL 1   /* one thread per cell, general row code, H of
                               the backward neighbours recomputed            */
-#define WK_KERNEL_MARCH 2  /* plane-marching, E planes staged in shared
-                              memory (WK_E_SHAPE if the tile does not fit)  */
-#define WK_KERNEL_FUSED 3  /* one thread per cell in two launches: interior
-                              cells with single-coefficient rows, then the
-                              two-cell shell with the general row code
-                              (WK_E_SHAPE if a dimension is below 5)        */
 #define WK_KERNEL_TWOPASS 4 /* H pass then E pass, each an interior launch
                               with single-coefficient rows plus a shell
                               launch; tile_planes = planes per thread (1, 2
@@ -159,10 +162,8 @@ typedef struct wk_fit_desc {
                               tile_planes = planes per block (0 = auto).
                               A load that does not arrive within a bounded
                               wait sets *status = 1 and the block returns. */
-#define WK_KERNEL_SLAB 5   /* the two passes slab by slab along z
-                              (tile_planes planes per slab, 0 = sized for
-                              L2) so the E pass re-reads the slab from L2
-                              (WK_E_SHAPE if a dimension is below 5)        */
+/* Kernel values 2, 3 and 5 (earlier schedules) are no longer accepted:
+ * wk_fit_step returns WK_E_MODE for them.                                   */
 
 /*
  * Add `inc` to the device counter *ctr (one thread, on `stream`): advances
@@ -225,6 +226,16 @@ int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* lamH, const void* 
  */
 int wk_field_monitor(const void* E, int dtype, long long N, const double* phases, int nf,
                      double* acc, void* stream);
+
+/*
+ * Wait for `stream`, read the device status word that the step kernels
+ * set (wk_fit_desc.status) and, with reset != 0, clear it.  Returns WK_OK
+ * when it is 0 and WK_E_TIMEOUT when a TMA step kernel gave up waiting for
+ * a tile load (the fields written since the last check are then
+ * incomplete).  No counterpart in the reference (upstream's scipy step
+ * cannot time out).
+ */
+int wk_read_status(int* status, int reset, void* stream);
 
 /* ABI version (WK_ABI_VERSION). */
 int wk_version(void);

@@ -1,10 +1,10 @@
 """Generate the golden fixtures under tests/golden/ from the upstream Wakis
 package (pure Python, loaded through ``refshim``).
 
-Run on a machine that has the upstream source tree (default
-``/root/reference``, override with ``WAKIS_UPSTREAM``):
+Run on a machine that has the upstream source tree, naming its root in
+``WAKIS_UPSTREAM``:
 
-    python tests/golden/make_golden.py
+    WAKIS_UPSTREAM=<upstream tree> python tests/golden/make_golden.py [step|wake|source|test001]
 
 Outputs (all small, committed):
 

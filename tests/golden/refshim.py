@@ -25,7 +25,7 @@ import types
 
 import numpy as np
 
-UPSTREAM = os.environ.get("WAKIS_UPSTREAM", "/root/reference")
+UPSTREAM = os.environ.get("WAKIS_UPSTREAM")
 
 _H5_STORE = {}
 
@@ -73,7 +73,12 @@ class _StructuredGrid(dict):
 
 
 def install():
-    """Install the stand-ins and import upstream ``wakis`` from UPSTREAM."""
+    """Install the stand-ins and import upstream ``wakis`` from UPSTREAM
+    (the environment variable WAKIS_UPSTREAM: the root of the upstream
+    source tree, the directory that holds the ``wakis`` package)."""
+    if not UPSTREAM or not os.path.isdir(os.path.join(UPSTREAM, "wakis")):
+        raise RuntimeError("set WAKIS_UPSTREAM to the root of the upstream Wakis source tree "
+                           f"(got {UPSTREAM!r})")
     if "wakis" in sys.modules and getattr(sys.modules["wakis"], "_refshim", False):
         return sys.modules["wakis"]
     h5 = types.ModuleType("h5py")

@@ -13,8 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libwakis_b200.so")
 
 WK_F64, WK_F32, WK_F32C = 0, 1, 2
 WK_J_ZERO, WK_J_SIGMA_E, WK_J_ARRAY = 0, 1, 2
-WK_KERNEL_AUTO, WK_KERNEL_CELL, WK_KERNEL_MARCH, WK_KERNEL_FUSED, WK_KERNEL_TWOPASS = 0, 1, 2, 3, 4
-WK_KERNEL_SLAB, WK_KERNEL_TMA = 5, 6
+WK_KERNEL_AUTO, WK_KERNEL_CELL, WK_KERNEL_TWOPASS, WK_KERNEL_TMA = 0, 1, 4, 6
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -44,6 +43,7 @@ class FitDesc(ctypes.Structure):
         ("Ec", _vp * 2), ("Hc", _vp * 2),
         ("step_dev", _vp),
         ("faces_clean", _i),
+        ("wait_ns", _ll),
     ]
 
 
@@ -68,6 +68,7 @@ _SIGS = {
                                _vp, _ll, _d, _d, _d, _d, _d, _d, _d, _i, _vp, _vp]),
     "wk_trans_wake": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp]),
     "wk_dft_bins": (_i, [_vp, _i, _ll, _ll, _i, _vp, _vp]),
+    "wk_read_status": (_i, [_vp, _i, _vp]),
 }
 
 EXPORTED = tuple(_SIGS)
@@ -95,6 +96,20 @@ def lib():
 
 class NativeError(RuntimeError):
     pass
+
+
+WK_E_TIMEOUT = 7
+
+
+def read_status(status, stream, what="step", reset=True):
+    """Wait for `stream` and read the device status word ``status`` (a
+    one-element int32 CUDA tensor) that the step kernels set when a tile
+    load did not arrive within its wait bound; raise NativeError naming
+    `what` when it is set (and clear it with ``reset``)."""
+    rc = lib().wk_read_status(status.data_ptr(), int(bool(reset)), stream)
+    if rc != 0:
+        msg = lib().wk_last_error().decode(errors="replace")
+        raise NativeError(f"{what}: {msg}")
 
 
 def check(rc, what):

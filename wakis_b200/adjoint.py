@@ -304,6 +304,7 @@ class ImpedanceDesign:
             m = min(K, self.n_steps - n)
             s._advance(m, n, beam=ws["beam_params"], capture=ws["capture"])
             n += m
+        s.check_status("ImpedanceDesign.forward")
         self.hist = ws["hist"][0].double()
         return float(self.loss_from_history(self.hist).item())
 
@@ -524,6 +525,7 @@ class ImpedanceDesign:
             self._segment(a, m, B)
         self._warm = False
         del cg
+        s.check_status("ImpedanceDesign.backward")
         er = self.eps_r
         g_eps = B["gI"] * (-1.0 / (EPS_0 * er * er))
         return g_eps.cpu().numpy(), B["gS"].cpu().numpy()

@@ -150,6 +150,8 @@ class BatchedWakeSolve:
         ms = ev0.elapsed_time(ev1)
         wall = time.perf_counter() - t0
         del graph
+        for q, s in enumerate(self.solvers):
+            s.check_status(f"BatchedWakeSolve.run (instance {q})")
         cells = sum(s.N for s in self.solvers)
         self.timing = {"ms": ms, "wall_s": wall, "cells": cells, "steps": self.n_steps,
                        "gcell_steps_per_s": cells * self.n_steps / (ms / 1e3) / 1e9}

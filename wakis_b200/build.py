@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwakis_b200.so")
-SOURCES = ["abi.cu", "fit_step.cu", "fit_march.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma_comp.cu",
+SOURCES = ["abi.cu", "fit_step.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma_comp.cu",
            "wake.cu", "adjoint.cu", "monitor.cu"]
 HEADERS = ["abi_internal.h", "fit_common.cuh", "fit_kernels.cuh", "fit_comp.cuh", "tma_util.cuh"]
 
@@ -21,7 +21,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "--expt-relaxed-constexpr", "--extended-lambda",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -42,14 +42,33 @@ def _stale():
 
 
 def build(force=False, verbose=True, extra=()):
+    """Compile every translation unit to an object file (in parallel, one
+    nvcc per source) and link them into the shared library."""
     if not force and not _stale():
         return OUT
-    srcs = [os.path.join(CSRC, f) for f in SOURCES]
-    tmp = OUT + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-o", tmp, *srcs]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+    inc = ["-I", os.path.join(ROOT, "include")]
+    with tempfile.TemporaryDirectory(prefix="wk_build_") as tmpdir:
+        def compile_one(src):
+            obj = os.path.join(tmpdir, os.path.splitext(src)[0] + ".o")
+            cmd = [nvcc(), *NVCC_FLAGS, *extra, *inc, "-c", "-o", obj, os.path.join(CSRC, src)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode:
+                raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}{r.stderr}")
+            if r.stderr and verbose:
+                print(r.stderr, end="", flush=True)
+            return obj
+        with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+            objs = list(ex.map(compile_one, SOURCES))
+        tmp = OUT + ".tmp"
+        cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+               "-Xcompiler", "-fPIC", "-o", tmp, *objs]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
     return OUT
 

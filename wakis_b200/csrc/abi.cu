@@ -77,3 +77,22 @@ int wk_validate_fit(const wk_fit_desc* d, const char* where) {
   }
   return WK_OK;
 }
+
+extern "C" int wk_read_status(int* status, int reset, void* stream) {
+  if (!status) return wk_fail(WK_E_NULL, "wk_read_status: status is NULL");
+  cudaStream_t st = (cudaStream_t)stream;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && h != 0 && reset) {
+    e = cudaMemsetAsync(status, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  if (e != cudaSuccess)
+    return wk_fail(-(int)e, "wk_read_status: %s", cudaGetErrorString(e));
+  if (h != 0)
+    return wk_fail(WK_E_TIMEOUT,
+                   "wk_read_status: a step kernel gave up waiting for a tile load (status %d); "
+                   "the fields of the steps since the last check are incomplete", h);
+  return WK_OK;
+}

@@ -52,6 +52,7 @@ struct FitParams {
   int* status;
   const long long* step_dev;   // optional device step counter
   int faces_clean;             // tangential E on PEC faces is +0 (wk_fit_desc)
+  long long wait_ns;           // bound of the TMA step-loop waits (wk_fit_desc)
   unsigned nx_mul;   // fast division by Nx: q = umulhi(n, nx_mul) >> nx_shift
   int nx_shift;
 };

@@ -1,18 +1,12 @@
-// Fused FIT step without shared memory (sm_100a): interior + shell launches.
+// Two-pass FIT step without shared memory (sm_100a), and the shell launches.
 //
-// One thread per cell reads the old state (E_in, H_in) and writes the new
-// state (E_out, H_out), so no block depends on another.  The E row of cell
-// n needs the new H at n, n-1, n-Nx and n-Nx*Ny; the thread recomputes those
-// H rows itself (3 full rows at n, 2 rows at each backward neighbour), with
-// the neighbour E values served by L1/L2 (each E value is read from DRAM
-// once per step: ~96 B of DRAM traffic per cell for FP64).
-//
-// The grid is split in two launches so that every warp runs one code path:
-// * k_interior: cells with 2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3,
-//   where no flat-offset wrap and no face mask can reach any row the cell
-//   needs; each metric coefficient is formed once (h_lean_* / e_lean).
-// * k_shell: the remaining cells (a shell two cells thick), enumerated
-//   compactly, with the general row code (masks, wraps, grid edges).
+// The two-pass schedule (H pass, then E pass) updates the interior cells
+// (2 <= i <= Nx-3, 2 <= j <= Ny-3, 2 <= k <= Nz-3: no flat-offset wrap and
+// no face mask reaches any row they need) with single-coefficient rows, and
+// the two-cell shell with the general row code (masks, wraps, grid edges).
+// It serves grids the TMA kernel cannot take and is the cross-check of the
+// TMA schedule.  The shell kernels here also close the TMA step when a face
+// is not PEC-masked.
 #include "../../include/wakis_b200.h"
 #include "abi_internal.h"
 #include "fit_common.cuh"
@@ -20,206 +14,7 @@
 
 namespace wk {
 
-constexpr int kInteriorX = 128, kInteriorY = 2, kShellThreads = 256;
-constexpr int kColumnRows = 4;   // warps (rows j) per block of the column kernel
-
-template <typename T>
-__global__ void __launch_bounds__(kInteriorX * kInteriorY)
-k_interior(FitParams<T> p, long long step) {
-  const int i = 2 + blockIdx.x * kInteriorX + threadIdx.x;
-  const int j = 2 + blockIdx.y * kInteriorY + threadIdx.y;
-  const int k = 2 + blockIdx.z;
-  if (i > p.Nx - 3 || j > p.Ny - 3) return;
-  const int Nx = p.Nx, Ny = p.Ny;
-  const long long N = p.N, sy = Nx, sz = p.NxNy;
-  const long long n = i + j * sy + k * sz;
-  const T* __restrict__ ex = p.E_in;
-  const T* __restrict__ ey = p.E_in + N;
-  const T* __restrict__ ez = p.E_in + 2 * N;
-  const T* __restrict__ hx = p.H_in;
-  const T* __restrict__ hy = p.H_in + N;
-  const T* __restrict__ hz = p.H_in + 2 * N;
-  const T dt = p.dt;
-  const bool desc = p.h_desc != 0;
-
-  const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
-  const T* m1 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - 1);
-  const T* m2 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - sy);
-  const T* m3 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - sz);
-  const T Lxi = p.Lx[i], Lxm = p.Lx[i - 1];
-  const T Lyj = p.Ly[j], Lym = p.Ly[j - 1];
-  const T Lzk = p.Lz[k], Lzm = p.Lz[k - 1];
-
-  // E at n and around it
-  const T ex0 = ex[n], ey0 = ey[n], ez0 = ez[n];
-  // new H at n (three rows)
-  T hxn = hx[n], hyn = hy[n], hzn = hz[n];
-  {
-    const T R0 = mul(p.iAx[j + (long long)k * Ny], m0[3]);
-    const T R1 = mul(p.iAy[i + (long long)k * Nx], m0[4]);
-    const T R2 = mul(p.iAz[i + (long long)j * Nx], m0[5]);
-    h_lean(dt, desc, R0, R1, R2, Lxi, Lyj, Lzk, ex0, ey0, ez0, ey[n + 1], ez[n + 1],
-           ex[n + sy], ez[n + sy], ex[n + sz], ey[n + sz], hxn, hyn, hzn);
-  }
-  // new H at n-1: y and z rows of cell (i-1, j, k)
-  const long long a1 = n - 1;
-  const T ex_a1 = ex[a1];
-  const T hy1 = h_lean_y(dt, desc, mul(p.iAy[i - 1 + (long long)k * Nx], m1[4]), Lxm, Lzk,
-                         ex_a1, ex[a1 + sz], ez[a1], ez0, hy[a1]);
-  const T hz1 = h_lean_z(dt, desc, mul(p.iAz[i - 1 + (long long)j * Nx], m1[5]), Lxm, Lyj,
-                         ex_a1, ex[a1 + sy], ey[a1], ey0, hz[a1]);
-  // new H at n-Nx: x and z rows of cell (i, j-1, k)
-  const long long a2 = n - sy;
-  const T ey_a2 = ey[a2];
-  const T hx2 = h_lean_x(dt, desc, mul(p.iAx[j - 1 + (long long)k * Ny], m2[3]), Lym, Lzk,
-                         ey_a2, ey[a2 + sz], ez[a2], ez0, hx[a2]);
-  const T hz2 = h_lean_z(dt, desc, mul(p.iAz[i + (long long)(j - 1) * Nx], m2[5]), Lxi, Lym,
-                         ex[a2], ex0, ey_a2, ey[a2 + 1], hz[a2]);
-  // new H at n-Nx*Ny: x and y rows of cell (i, j, k-1)
-  const long long a3 = n - sz;
-  const T ez_a3 = ez[a3];
-  const T hx3 = h_lean_x(dt, desc, mul(p.iAx[j + (long long)(k - 1) * Ny], m3[3]), Lyj, Lzm,
-                         ey[a3], ey0, ez_a3, ez[a3 + sy], hx[a3]);
-  const T hy3 = h_lean_y(dt, desc, mul(p.iAy[i + (long long)(k - 1) * Nx], m3[4]), Lxi, Lzm,
-                         ex[a3], ex0, ez_a3, ez[a3 + 1], hy[a3]);
-
-  // E at n
-  T curl[3];
-  {
-    const T R0 = mul(m0[0], p.itAx[j + (long long)k * Ny]);
-    const T R1 = mul(m0[1], p.itAy[i + (long long)k * Nx]);
-    const T R2 = mul(m0[2], p.itAz[i + (long long)j * Nx]);
-    e_lean(R0, R1, R2, p.tLx[i], p.tLy[j], p.tLz[k], hxn, hyn, hzn, hy1, hz1, hx2, hz2, hx3,
-           hy3, curl[0], curl[1], curl[2]);
-  }
-  Cell c;
-  c.i = i; c.j = j; c.k = k;
-  const T eold[3] = {ex0, ey0, ez0};
-  if (p.cap_on) capture(p, c, n, step, ez0);
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const T ieps = m0[d], sigma = m0[6 + d];
-    const T jv = j_in(p, d, c, n, step, eold[d], sigma);
-    const T enew = add(eold[d], mul(dt, sub(curl[d], mul(ieps, jv))));
-    p.E_out[d * N + n] = enew;
-    if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
-  }
-  p.H_out[n] = hxn;
-  p.H_out[N + n] = hyn;
-  p.H_out[2 * N + n] = hzn;
-}
-
-// Interior cells, one thread per (i, j) column marching kz planes.  Lane l
-// of a warp sits at i = i0 - 1 + l; lanes 1..31 own their cells, lane 0 only
-// supplies the new H of (i0-1, j) to lane 1 (shuffle).  Carried from plane
-// k-1 to k: E(n) x/y (loaded as E(n+Nx*Ny) one plane earlier), Ey(n-Nx), and
-// the new H(n-Nx*Ny) x/y.  The ±1 neighbours come from the adjacent lanes;
-// the H rows of (i, j-1) are recomputed.
-template <typename T>
-__global__ void __launch_bounds__(32 * kColumnRows)
-k_column(FitParams<T> p, long long step, int kz) {
-  const int lane = threadIdx.x;
-  const int i_raw = 2 + blockIdx.x * 31 - 1 + lane;
-  const int j = 2 + blockIdx.y * kColumnRows + threadIdx.y;
-  const int k0 = 2 + blockIdx.z * kz;
-  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
-  if (j > Ny - 3) return;                 // whole warp
-  const int k1 = min(k0 + kz, Nz - 2);
-  const bool owner = lane >= 1 && i_raw <= Nx - 3;
-  const int i = min(i_raw, Nx - 2);       // lanes past the last owner + 1 only feed shuffles
-  const long long N = p.N, sy = Nx, sz = p.NxNy;
-  const T* __restrict__ ex = p.E_in;
-  const T* __restrict__ ey = p.E_in + N;
-  const T* __restrict__ ez = p.E_in + 2 * N;
-  const T* __restrict__ hx = p.H_in;
-  const T* __restrict__ hy = p.H_in + N;
-  const T* __restrict__ hz = p.H_in + 2 * N;
-  const T dt = p.dt;
-  const bool desc = p.h_desc != 0;
-  const unsigned FULL = 0xffffffffu;
-
-  // per-column metrics
-  const T Lxi = p.Lx[i], Lyj = p.Ly[j], Lym = p.Ly[j - 1];
-  const T tLxi = p.tLx[i], tLyj = p.tLy[j];
-  const T iAz0 = p.iAz[i + (long long)j * Nx], iAzm = p.iAz[i + (long long)(j - 1) * Nx];
-  const T itAz0 = p.itAz[i + (long long)j * Nx];
-
-  // prologue: carried values for plane k0
-  long long n = i + j * sy + k0 * sz;
-  T exc = ex[n], eyc = ey[n], eymc = ey[n - sy];
-  T hxp, hyp;
-  {
-    const long long a = n - sz;
-    const T* m = p.mat + 9 * load_id(p.mat_id, p.id_bytes, a);
-    const T ez_a = ez[a];
-    hxp = h_lean_x(dt, desc, mul(p.iAx[j + (long long)(k0 - 1) * Ny], m[3]), Lyj,
-                   p.Lz[k0 - 1], ey[a], eyc, ez_a, ez[a + sy], hx[a]);
-    hyp = h_lean_y(dt, desc, mul(p.iAy[i + (long long)(k0 - 1) * Nx], m[4]), Lxi,
-                   p.Lz[k0 - 1], ex[a], exc, ez_a, ez[a + 1], hy[a]);
-  }
-
-  for (int k = k0; k < k1; k++, n += sz) {
-    const T* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
-    const T* m2 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n - sy);
-    const T Lzk = p.Lz[k];
-    const T ez0 = ez[n];
-    const T ex_pz = ex[n + sz], ey_pz = ey[n + sz];
-    const T ex_py = ex[n + sy], ez_py = ez[n + sy];
-    const T ex_my = ex[n - sy], ez_my = ez[n - sy];
-    const T ey_mypz = ey[n - sy + sz];
-    // +1 neighbours from lane + 1 (lane 31 loads its own)
-    T ey_p1 = __shfl_down_sync(FULL, eyc, 1);
-    T ez_p1 = __shfl_down_sync(FULL, ez0, 1);
-    T ey_myp1 = __shfl_down_sync(FULL, eymc, 1);
-    if (lane == 31) {
-      ey_p1 = ey[n + 1];
-      ez_p1 = ez[n + 1];
-      ey_myp1 = ey[n - sy + 1];
-    }
-    // new H at n
-    const T hxn = h_lean_x(dt, desc, mul(p.iAx[j + (long long)k * Ny], m0[3]), Lyj, Lzk, eyc,
-                           ey_pz, ez0, ez_py, hx[n]);
-    const T hyn = h_lean_y(dt, desc, mul(p.iAy[i + (long long)k * Nx], m0[4]), Lxi, Lzk, exc,
-                           ex_pz, ez0, ez_p1, hy[n]);
-    const T hzn = h_lean_z(dt, desc, mul(iAz0, m0[5]), Lxi, Lyj, exc, ex_py, eyc, ey_p1, hz[n]);
-    // new H at n - Nx (cell (i, j-1, k)): x and z rows
-    const T hx2 = h_lean_x(dt, desc, mul(p.iAx[j - 1 + (long long)k * Ny], m2[3]), Lym, Lzk,
-                           eymc, ey_mypz, ez_my, ez0, hx[n - sy]);
-    const T hz2 = h_lean_z(dt, desc, mul(iAzm, m2[5]), Lxi, Lym, ex_my, exc, eymc, ey_myp1,
-                           hz[n - sy]);
-    // new H at n - 1 from lane - 1
-    const T hy1 = __shfl_up_sync(FULL, hyn, 1);
-    const T hz1 = __shfl_up_sync(FULL, hzn, 1);
-    if (owner) {
-      T curl[3];
-      const T R0 = mul(m0[0], p.itAx[j + (long long)k * Ny]);
-      const T R1 = mul(m0[1], p.itAy[i + (long long)k * Nx]);
-      const T R2 = mul(m0[2], itAz0);
-      e_lean(R0, R1, R2, tLxi, tLyj, p.tLz[k], hxn, hyn, hzn, hy1, hz1, hx2, hz2, hxp, hyp,
-             curl[0], curl[1], curl[2]);
-      Cell c;
-      c.i = i; c.j = j; c.k = k;
-      const T eold[3] = {exc, eyc, ez0};
-      if (p.cap_on) capture(p, c, n, step, ez0);
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const T ieps = m0[d], sigma = m0[6 + d];
-        const T jv = j_in(p, d, c, n, step, eold[d], sigma);
-        const T enew = add(eold[d], mul(dt, sub(curl[d], mul(ieps, jv))));
-        p.E_out[d * N + n] = enew;
-        if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
-      }
-      p.H_out[n] = hxn;
-      p.H_out[N + n] = hyn;
-      p.H_out[2 * N + n] = hzn;
-    }
-    exc = ex_pz;
-    eyc = ey_pz;
-    eymc = ey_mypz;
-    hxp = hxn;
-    hyp = hyn;
-  }
-}
+constexpr int kShellThreads = 256;
 
 // ------------------------------------------------------------ two passes --
 // H pass then E pass over the interior (lean rows) and the shell (general
@@ -482,220 +277,5 @@ template cudaError_t launch_two_pass<double>(const FitParams<double>&, long long
                                              int);
 template cudaError_t launch_two_pass<float>(const FitParams<float>&, long long, cudaStream_t,
                                             int);
-
-// ------------------------------------------------------------- z slabs ----
-// The two passes run slab by slab along z: H pass of planes [ka, kb), then
-// E pass of the same planes, then the next slab.  H(k) needs E_old at k and
-// k+1 and E(k) needs H_new at k and k-1, so this order gives the same result
-// as two whole-grid passes, while the E pass re-reads the slab's E_in and
-// H_out from L2.  One launch per pass per slab: the first blocks are
-// interior tiles (single-coefficient rows), the remaining blocks cover the
-// slab's shell cells (general rows).
-struct SlabInfo {
-  int k_int0, n_int;         // interior planes [k_int0, k_int0 + n_int)
-  int gx, gy;                // interior tiles per plane (x, y)
-  long long nb_int;          // interior blocks
-  int F[4], nF;              // full shell planes in the slab
-  int lo, n_inner, S_in;     // inner shell planes [lo, lo + n_inner), cells per plane
-  long long shell_count;
-};
-
-__device__ __forceinline__ Cell slab_shell_cell(long long idx, int Nx, int Ny,
-                                                const SlabInfo& s) {
-  Cell c;
-  const long long NxNy = (long long)Nx * Ny;
-  if (idx < s.nF * NxNy) {
-    const int f = (int)(idx / NxNy);
-    const long long rem = idx - f * NxNy;
-    c.k = s.F[f];
-    c.j = (int)(rem / Nx);
-    c.i = (int)(rem - (long long)c.j * Nx);
-    return c;
-  }
-  idx -= s.nF * NxNy;
-  const long long pl = idx / s.S_in;
-  int r = (int)(idx - pl * s.S_in);
-  c.k = s.lo + (int)pl;
-  if (r < 4 * Nx) {
-    const int jj = r / Nx;
-    c.i = r - jj * Nx;
-    c.j = jj < 2 ? jj : Ny - 4 + jj;
-    return c;
-  }
-  r -= 4 * Nx;
-  const int ii = r % 4;
-  c.i = ii < 2 ? ii : Nx - 4 + ii;
-  c.j = 2 + r / 4;
-  return c;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), 1))
-k_h_slab(FitParams<T> p, SlabInfo s, int mat_smem) {
-  extern __shared__ __align__(16) unsigned char pass_smem[];
-  const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
-  const long long b = blockIdx.x;
-  const long long N = p.N;
-  if (b < s.nb_int) {
-    const int bx = (int)(b % s.gx);
-    const long long r = b / s.gx;
-    const int by = (int)(r % s.gy);
-    const int bz = (int)(r / s.gy);
-    const int i = 2 + bx * kPassX + threadIdx.x;
-    const int j = 2 + by * kPassY + threadIdx.y;
-    const int k = s.k_int0 + bz;
-    if (i > p.Nx - 3 || j > p.Ny - 3) return;
-    const int sy = p.Nx, sz = (int)p.NxNy;
-    const long long n = i + (long long)j * sy + (long long)k * sz;
-    const T* ex = p.E_in + n;
-    const T* ey = p.E_in + N + n;
-    const T* ez = p.E_in + 2 * N + n;
-    const T* m0 = mat + 9 * load_id(p.mat_id, p.id_bytes, n);
-    T hx = p.H_in[n], hy = p.H_in[N + n], hz = p.H_in[2 * N + n];
-    const T R0 = mul(p.iAx[j + k * p.Ny], m0[3]);
-    const T R1 = mul(p.iAy[i + k * sy], m0[4]);
-    const T R2 = mul(p.iAz[i + j * sy], m0[5]);
-    h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[i], p.Ly[j], p.Lz[k], ex[0], ey[0], ez[0],
-           ey[1], ez[1], ex[sy], ez[sy], ex[sz], ey[sz], hx, hy, hz);
-    p.H_out[n] = hx;
-    p.H_out[N + n] = hy;
-    p.H_out[2 * N + n] = hz;
-  } else {
-    const long long idx = (b - s.nb_int) * (kPassX * kPassY) + threadIdx.x +
-                          threadIdx.y * kPassX;
-    if (idx >= s.shell_count) return;
-    const Cell c = slab_shell_cell(idx, p.Nx, p.Ny, s);
-    const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
-    const int id = load_id(p.mat_id, p.id_bytes, n);
-    T h[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) h[d] = h_row(p, p.E_in, p.H_in[d * N + n], d, c, n, id);
-#pragma unroll
-    for (int d = 0; d < 3; d++) p.H_out[d * N + n] = h[d];
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kPassX * kPassY, pass_min_blocks(sizeof(T), 1))
-k_e_slab(FitParams<T> p, long long step, SlabInfo s, int mat_smem) {
-  extern __shared__ __align__(16) unsigned char pass_smem[];
-  const T* mat = stage_table(p, mat_smem, reinterpret_cast<T*>(pass_smem));
-  const long long b = blockIdx.x;
-  const long long N = p.N;
-  if (b < s.nb_int) {
-    const int bx = (int)(b % s.gx);
-    const long long r = b / s.gx;
-    const int by = (int)(r % s.gy);
-    const int bz = (int)(r / s.gy);
-    const int i = 2 + bx * kPassX + threadIdx.x;
-    const int j = 2 + by * kPassY + threadIdx.y;
-    const int k = s.k_int0 + bz;
-    if (i > p.Nx - 3 || j > p.Ny - 3) return;
-    const int sy = p.Nx, sz = (int)p.NxNy;
-    const long long n = i + (long long)j * sy + (long long)k * sz;
-    const T* hx = p.H_out + n;
-    const T* hy = p.H_out + N + n;
-    const T* hz = p.H_out + 2 * N + n;
-    const T* m0 = mat + 9 * load_id(p.mat_id, p.id_bytes, n);
-    const T eold[3] = {p.E_in[n], p.E_in[N + n], p.E_in[2 * N + n]};
-    const T R0 = mul(m0[0], p.itAx[j + k * p.Ny]);
-    const T R1 = mul(m0[1], p.itAy[i + k * sy]);
-    const T R2 = mul(m0[2], p.itAz[i + j * sy]);
-    T curl[3];
-    e_lean(R0, R1, R2, p.tLx[i], p.tLy[j], p.tLz[k], hx[0], hy[0], hz[0], hy[-1], hz[-1],
-           hx[-sy], hz[-sy], hx[-sz], hy[-sz], curl[0], curl[1], curl[2]);
-    Cell c;
-    c.i = i; c.j = j; c.k = k;
-    if (p.cap_on) capture(p, c, n, step, eold[2]);
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const T ieps = m0[d], sigma = m0[6 + d];
-      const T jv = j_in(p, d, c, n, step, eold[d], sigma);
-      const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
-      p.E_out[d * N + n] = enew;
-      if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
-    }
-  } else {
-    const long long idx = (b - s.nb_int) * (kPassX * kPassY) + threadIdx.x +
-                          threadIdx.y * kPassX;
-    if (idx >= s.shell_count) return;
-    const Cell c = slab_shell_cell(idx, p.Nx, p.Ny, s);
-    const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
-    const int id = load_id(p.mat_id, p.id_bytes, n);
-    const T* Hn = p.H_out;
-    auto hval = [&](int e, long long m) -> T { return Hn[e * N + m]; };
-    if (p.cap_on) capture(p, c, n, step, p.E_in[2 * N + n]);
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const T ieps = p.mat[9 * id + d], sigma = p.mat[9 * id + 6 + d];
-      const T eold = p.E_in[d * N + n];
-      const T jv = j_in(p, d, c, n, step, eold, sigma);
-      const T curl = e_curl(p, d, c, n, ieps, hval);
-      const T enew = add(eold, mul(p.dt, sub(curl, mul(ieps, jv))));
-      p.E_out[d * N + n] = enew;
-      if (p.j_mode == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
-    }
-  }
-}
-
-template <typename T>
-cudaError_t launch_slabs(const FitParams<T>& p, long long step, cudaStream_t st, int planes) {
-  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
-  const int mat_smem = p.n_mat * 9 <= 1024 ? p.n_mat * 9 : 0;
-  const size_t smem = (size_t)mat_smem * sizeof(T);
-  const int threads = kPassX * kPassY;
-  for (int ka = 0; ka < Nz; ka += planes) {
-    const int kb = min(ka + planes, Nz);
-    SlabInfo s;
-    s.k_int0 = max(ka, 2);
-    s.n_int = max(0, min(kb, Nz - 2) - s.k_int0);
-    s.gx = (Nx - 4 + kPassX - 1) / kPassX;
-    s.gy = (Ny - 4 + kPassY - 1) / kPassY;
-    s.nb_int = (long long)s.gx * s.gy * s.n_int;
-    s.nF = 0;
-    const int full[4] = {0, 1, Nz - 2, Nz - 1};
-    for (int f = 0; f < 4; f++)
-      if (full[f] >= ka && full[f] < kb) s.F[s.nF++] = full[f];
-    s.lo = max(ka, 2);
-    s.n_inner = max(0, min(kb, Nz - 2) - s.lo);
-    s.S_in = 4 * Nx + 4 * (Ny - 4);
-    s.shell_count = (long long)s.nF * Nx * Ny + (long long)s.n_inner * s.S_in;
-    const long long blocks = s.nb_int + (s.shell_count + threads - 1) / threads;
-    if (blocks == 0) continue;
-    dim3 blk(kPassX, kPassY);
-    k_h_slab<T><<<(unsigned)blocks, blk, smem, st>>>(p, s, mat_smem);
-    k_e_slab<T><<<(unsigned)blocks, blk, smem, st>>>(p, step, s, mat_smem);
-  }
-  return cudaGetLastError();
-}
-
-template cudaError_t launch_slabs<double>(const FitParams<double>&, long long, cudaStream_t,
-                                          int);
-template cudaError_t launch_slabs<float>(const FitParams<float>&, long long, cudaStream_t, int);
-
-template <typename T>
-cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,
-                                  int kz) {
-  if (kz <= 0) {
-    dim3 blk(kInteriorX, kInteriorY);
-    dim3 grid((p.Nx - 4 + kInteriorX - 1) / kInteriorX,
-              (p.Ny - 4 + kInteriorY - 1) / kInteriorY, p.Nz - 4);
-    k_interior<T><<<grid, blk, 0, st>>>(p, step);
-  } else {
-    dim3 blk(32, kColumnRows);
-    dim3 grid((p.Nx - 4 + 30) / 31, (p.Ny - 4 + kColumnRows - 1) / kColumnRows,
-              (p.Nz - 4 + kz - 1) / kz);
-    k_column<T><<<grid, blk, 0, st>>>(p, step, kz);
-  }
-  const long long count = p.N - (long long)(p.Nx - 4) * (p.Ny - 4) * (p.Nz - 4);
-  k_shell<T><<<(unsigned)((count + kShellThreads - 1) / kShellThreads), kShellThreads, 0, st>>>(
-      p, step, count);
-  return cudaGetLastError();
-}
-
-template cudaError_t launch_interior_shell<double>(const FitParams<double>&, long long,
-                                                   cudaStream_t, int);
-template cudaError_t launch_interior_shell<float>(const FitParams<float>&, long long,
-                                                  cudaStream_t, int);
 
 }  // namespace wk

@@ -121,6 +121,7 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
   p.status = d->status;
   p.step_dev = d->step_dev;
   p.faces_clean = d->faces_clean;
+  p.wait_ns = d->wait_ns;
   return p;
 }
 
@@ -214,34 +215,11 @@ __device__ __forceinline__ void fused_cell_general(const FitParams<T>& p, long l
   for (int d = 0; d < 3; d++) p.H_out[d * N + n] = hn[d];
 }
 
-// Shell cells (two-cell rim) of one fused step, one thread per cell.
-template <typename T>
-__global__ void __launch_bounds__(256) k_shell(FitParams<T> p, long long step,
-                                                          long long count) {
-  const long long idx = blockIdx.x * 256LL + threadIdx.x;
-  if (idx >= count) return;
-  const Cell c = shell_cell(idx, p.Nx, p.Ny, p.Nz);
-  const long long n = c.i + (long long)c.j * p.Nx + (long long)c.k * p.NxNy;
-  fused_cell_general(p, step_index(p, step), n, c);
-}
-
-// Launch the interior (lean) and shell (general) fused kernels of one step
-// (fit_fused.cu); needs Nx, Ny, Nz >= 5.  kz > 0 selects the column kernel
-// with kz planes per thread, kz = 0 the one-thread-per-cell interior kernel.
-template <typename T>
-cudaError_t launch_interior_shell(const FitParams<T>& p, long long step, cudaStream_t st,
-                                  int kz);
-
 // Launch the two-pass schedule (H pass, then E pass; interior lean kernels
 // and general shell kernels) of one step (fit_fused.cu); needs Nx, Ny, Nz >= 5.
 // kb = planes per thread (1, 2 or 4).
 template <typename T>
 cudaError_t launch_two_pass(const FitParams<T>& p, long long step, cudaStream_t st, int kb);
-
-// Launch the z-slab two-pass schedule of one step (fit_fused.cu): for each
-// slab of `planes` planes, an H launch then an E launch; needs Nx, Ny, Nz >= 5.
-template <typename T>
-cudaError_t launch_slabs(const FitParams<T>& p, long long step, cudaStream_t st, int planes);
 
 // Shell of a step whose interior was stepped by a fused kernel: H of the
 // shell cells from the old state, then E of the shell cells from the new H
@@ -255,11 +233,5 @@ template <typename T>
 bool tma_supported(const FitParams<T>& p);
 template <typename T>
 cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC);
-
-// Launch the plane-marching kernel (defined in fit_march.cu) with TY rows
-// and KC planes per block and `smem` bytes of dynamic shared memory.
-template <typename T>
-cudaError_t launch_march(const FitParams<T>& p, long long step, int TY, int KC, size_t smem,
-                         cudaStream_t st);
 
 }  // namespace wk

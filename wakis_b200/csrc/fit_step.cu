@@ -90,55 +90,9 @@ __global__ void k_sigma_e(FitParams<T> p, T* J) {
 
 int blocks_for(long long N) { return (int)((N + kThreads - 1) / kThreads); }
 
-// Shared memory of the plane-marching kernel for TY rows per block.
-template <typename T>
-size_t march_smem(int Nx, int TY) {
-  return (size_t)(11LL * TY * Nx + 15LL * Nx) * sizeof(T);
-}
-
-struct MarchShape { int TY, KC; size_t smem; };
-
-// Rows per block: the largest count whose tile leaves room for two blocks
-// per SM (else one); planes per block: enough blocks for ~8 per SM.
-template <typename T>
-bool march_shape(const wk_fit_desc* d, MarchShape* ms) {
-  static int max_optin = -1, n_sm = 0;
-  if (max_optin < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  }
-  const size_t two_per_sm = 110 * 1024;
-  int TY = d->tile_rows;
-  if (TY <= 0) {
-    TY = 0;
-    for (int t = 1; t <= d->Ny && (long long)t * d->Nx <= 2048; t++)
-      if (march_smem<T>(d->Nx, t) <= two_per_sm) TY = t;
-    if (TY == 0 && march_smem<T>(d->Nx, 1) <= (size_t)max_optin) TY = 1;
-    if (TY == 0) return false;
-  }
-  if (TY > d->Ny) TY = d->Ny;
-  size_t smem = march_smem<T>(d->Nx, TY);
-  if (smem > (size_t)max_optin) return false;
-  int nseg = (d->Ny + TY - 1) / TY;
-  int KC = d->tile_planes;
-  if (KC <= 0) {
-    long long want = 8LL * (n_sm > 0 ? n_sm : 148);
-    long long nch = (want + nseg - 1) / nseg;
-    KC = (int)((d->Nz + nch - 1) / nch);
-    if (KC < 4) KC = 4;
-  }
-  if (KC > d->Nz) KC = d->Nz;
-  ms->TY = TY; ms->KC = KC; ms->smem = smem;
-  return true;
-}
-
 template <typename T>
 int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t st) {
   int par = d->par;
-  MarchShape ms{0, 0, 0};
-  bool march = false;
   const bool big = d->Nx >= 5 && d->Ny >= 5 && d->Nz >= 5 && d->Nz - 4 <= 65535 &&
                    (d->Ny - 4 + 1) / 2 <= 65535;
   bool use_tma = d->kernel == WK_KERNEL_TMA;
@@ -159,25 +113,8 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
     }
     return wk_check_launch("wk_fit_step");
   }
-  if (d->kernel == WK_KERNEL_SLAB) {
-    if (!big) return wk_fail(WK_E_SHAPE, "wk_fit_step: slab kernels need every dimension >= 5");
-    int planes = d->tile_planes;
-    if (planes <= 0) {
-      // E_in, H_in and H_out of a slab (3 fields) within ~80 MB of L2
-      const long long per_plane = 9LL * sizeof(T) * d->Nx * d->Ny;
-      planes = (int)(80LL * 1024 * 1024 / per_plane);
-      if (planes < 2) planes = 2;
-    }
-    for (int s = 0; s < n_steps; s++) {
-      FitParams<T> p = make_params<T>(d, par);
-      cudaError_t e = launch_slabs<T>(p, step0 + s, st, planes);
-      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
-      par ^= 1;
-    }
-    return wk_check_launch("wk_fit_step");
-  }
-  if ((d->kernel == WK_KERNEL_FUSED || d->kernel == WK_KERNEL_TWOPASS) && !big)
-    return wk_fail(WK_E_SHAPE, "wk_fit_step: interior/shell kernels need every dimension >= 5");
+  if (d->kernel == WK_KERNEL_TWOPASS && !big)
+    return wk_fail(WK_E_SHAPE, "wk_fit_step: two-pass kernels need every dimension >= 5");
   if (d->kernel == WK_KERNEL_TWOPASS || (d->kernel == WK_KERNEL_AUTO && big)) {
     // planes per thread: 1 for FP64, 2 for FP32 (fastest measured on B200)
     const int kb = d->tile_planes > 0 ? d->tile_planes : (sizeof(T) == 8 ? 1 : 2);
@@ -189,45 +126,12 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
     }
     return wk_check_launch("wk_fit_step");
   }
-  if (d->kernel == WK_KERNEL_FUSED) {
-    // tile_planes: planes per thread of the column kernel (0 = automatic,
-    // -1 = one-thread-per-cell interior kernel)
-    int kz = d->tile_planes;
-    if (kz == 0) {
-      long long cols = (long long)((d->Nx - 4 + 30) / 31) * 32 * (d->Ny - 4);
-      long long want = 148LL * 2048 * 2;       // threads for ~2 waves
-      long long chunks = (want + cols - 1) / cols;
-      kz = (int)((d->Nz - 4 + chunks - 1) / chunks);
-      if (kz < 8) kz = 8;
-    }
-    if (kz < 0) kz = 0;
-    if (kz > 0 && (d->Nz - 4 + kz - 1) / kz > 65535) kz = (d->Nz - 4 + 65534) / 65535;
-    for (int s = 0; s < n_steps; s++) {
-      FitParams<T> p = make_params<T>(d, par);
-      cudaError_t e = launch_interior_shell<T>(p, step0 + s, st, kz);
-      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
-      par ^= 1;
-    }
-    return wk_check_launch("wk_fit_step");
-  }
-  if (d->kernel == WK_KERNEL_MARCH) {
-    march = march_shape<T>(d, &ms);
-    if (!march)
-      return wk_fail(WK_E_SHAPE, "wk_fit_step: plane-marching tile does not fit (Nx=%d)", d->Nx);
-  }
-  if (march) {
-    for (int s = 0; s < n_steps; s++) {
-      FitParams<T> p = make_params<T>(d, par);
-      cudaError_t e = launch_march<T>(p, step0 + s, ms.TY, ms.KC, ms.smem, st);
-      if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
-      par ^= 1;
-    }
-  } else {
-    for (int s = 0; s < n_steps; s++) {
-      FitParams<T> p = make_params<T>(d, par);
-      k_fused<T><<<blocks_for(p.N), kThreads, 0, st>>>(p, step0 + s);
-      par ^= 1;
-    }
+  if (d->kernel != WK_KERNEL_AUTO && d->kernel != WK_KERNEL_CELL)
+    return wk_fail(WK_E_MODE, "wk_fit_step: unknown kernel %d", d->kernel);
+  for (int s = 0; s < n_steps; s++) {
+    FitParams<T> p = make_params<T>(d, par);
+    k_fused<T><<<blocks_for(p.N), kThreads, 0, st>>>(p, step0 + s);
+    par ^= 1;
   }
   return wk_check_launch("wk_fit_step");
 }

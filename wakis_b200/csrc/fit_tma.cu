@@ -186,11 +186,11 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     for (int d = 0; d < 3; d++)
       tma_load_3d(Hb + (slot * 3 + d) * SH, &maps.h[d], xs, ys, q, &bar[kES + slot]);
   };
-  auto wait_e = [&](int q) {
-    return mbar_wait(&bar[(q - pstart) % kES], (uint32_t)(((q - pstart) / kES) & 1));
+  auto wait_e = [&](int q, long long lim) {
+    return mbar_wait(&bar[(q - pstart) % kES], (uint32_t)(((q - pstart) / kES) & 1), lim);
   };
-  auto wait_h = [&](int q) {
-    return mbar_wait(&bar[kES + (q - pstart) % kHS], (uint32_t)(((q - pstart) / kHS) & 1));
+  auto wait_h = [&](int q, long long lim) {
+    return mbar_wait(&bar[kES + (q - pstart) % kHS], (uint32_t)(((q - pstart) / kHS) & 1), lim);
   };
   // E planes pstart..k1 and H planes pstart..k1-1 are loaded, each exactly
   // once; e_hi / h_hi (producer) track the last plane issued
@@ -309,10 +309,11 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 
   bool ok = true;
   int pl = pstart;
+  const long long lim = loop_wait_ns(p.wait_ns);   // step-loop waits; the drain keeps kWaitNs
   for (; pl < k1; pl++) {
     cp_async_wait<1>();          // this thread's row entry of plane pl
     bool got = true;
-    if (prod) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
+    if (prod) got = wait_e(pl, lim) && wait_e(pl + 1, lim) && wait_h(pl, lim);
     ok = __syncthreads_and(got);
     if (!ok) break;
     const bool prologue = pl == pstart;
@@ -465,8 +466,8 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     // loads this block issued, then return
     if (prod) {
       if (p.status) atomicExch(p.status, 1);
-      for (int q = pl; q <= e_hi; q++) wait_e(q);
-      for (int q = pl; q <= h_hi; q++) wait_h(q);
+      for (int q = pl; q <= e_hi; q++) wait_e(q, kWaitNs);
+      for (int q = pl; q <= h_hi; q++) wait_h(q, kWaitNs);
     }
     __syncthreads();
   }

@@ -253,11 +253,11 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
                     &bar[cES + slot]);
     }
   };
-  auto wait_e = [&](int q) {
-    return mbar_wait(&bar[(q - pstart) % cES], (uint32_t)(((q - pstart) / cES) & 1));
+  auto wait_e = [&](int q, long long lim) {
+    return mbar_wait(&bar[(q - pstart) % cES], (uint32_t)(((q - pstart) / cES) & 1), lim);
   };
-  auto wait_h = [&](int q) {
-    return mbar_wait(&bar[cES + (q - pstart) % cHS], (uint32_t)(((q - pstart) / cHS) & 1));
+  auto wait_h = [&](int q, long long lim) {
+    return mbar_wait(&bar[cES + (q - pstart) % cHS], (uint32_t)(((q - pstart) / cHS) & 1), lim);
   };
   int e_hi = pstart - 1, h_hi = pstart - 1;
   if (prod) {
@@ -399,9 +399,10 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
 
   bool ok = true;
   int pl = pstart;
+  const long long lim = loop_wait_ns(p.wait_ns);   // step-loop waits; the drain keeps kWaitNs
   for (; pl < k1; pl++) {
     bool got = true;
-    if (prod) got = wait_e(pl) && wait_e(pl + 1) && wait_h(pl);
+    if (prod) got = wait_e(pl, lim) && wait_e(pl + 1, lim) && wait_h(pl, lim);
     ok = __syncthreads_and(got);
     if (!ok) break;
     const bool prologue = pl == pstart;
@@ -605,8 +606,8 @@ k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps m
   if (!ok) {
     if (prod) {
       if (p.status) atomicExch(p.status, 1);
-      for (int q = pl; q <= e_hi; q++) wait_e(q);
-      for (int q = pl; q <= h_hi; q++) wait_h(q);
+      for (int q = pl; q <= e_hi; q++) wait_e(q, kWaitNs);
+      for (int q = pl; q <= h_hi; q++) wait_h(q, kWaitNs);
     }
     __syncthreads();
   }

@@ -9,7 +9,11 @@
 
 namespace wk {
 
-constexpr long long kWaitLimit = 1LL << 24;   // mbarrier polls before giving up
+// Bound of one mbarrier wait: kWaitNs of %globaltimer time (100 ms, far
+// above the microseconds a tile load takes), and at most kWaitPolls polls
+// in case the timer does not advance.
+constexpr long long kWaitNs = 100000000LL;
+constexpr long long kWaitPolls = 1LL << 26;
 
 constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
@@ -35,11 +39,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// Bounded wait; false when the limit is reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long it = 0; it < kWaitLimit; it++)
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for the phase of `parity`: true once it completed, false
+// when limit_ns nanoseconds (or kWaitPolls polls) passed first.  A negative
+// limit_ns gives up without polling (the timeout test of the step kernels).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          long long limit_ns = kWaitNs) {
+  if (limit_ns < 0) return false;
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (long long it = 0; it < kWaitPolls; it++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((long long)(globaltimer_ns() - t0) > limit_ns) return false;
+  }
   return false;
+}
+// Bound of the waits of a launch's step loop: wk_fit_desc.wait_ns, 0 = the
+// default.
+__device__ __forceinline__ long long loop_wait_ns(long long wait_ns) {
+  return wait_ns == 0 ? kWaitNs : wait_ns;
 }
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
                                             int z, uint64_t* bar) {

@@ -33,7 +33,7 @@ class RoutinesMixin:
                     field_monitor.update(self.E, self.dt)
                 if callback is not None:
                     callback(self, n * self.dt)
-        torch.cuda.current_stream(self.device).synchronize()
+        self.check_status("wakesolve")
         self._wake_finish(ws, time.time() - t0)
 
     def _wake_setup(self, wakelength, wake=None, compute_plane="both", add_space=None):
@@ -109,6 +109,7 @@ class RoutinesMixin:
                 E1, H1 = self.get_abc()
             if callback is not None:
                 callback(self, n * self.dt)
+        self.check_status("emsolve")
 
     # ABC snapshots (upstream boundaries.py:313-410).  Upstream's CPU path
     # keeps views of the live arrays; these are copies, as on its GPU path.

@@ -250,6 +250,8 @@ class SlabWakeSolve:
         """n_steps steps (optionally with the fused beam parameters)."""
         for n in range(step0, step0 + n_steps):
             self._step(n, beam)
+        for r in self.mine:
+            self.solvers[r].check_status(f"SlabWakeSolve.run (slab {r})")
 
     def fields(self):
         """(E, H) of the owned planes of this process's slabs joined along z,
@@ -317,6 +319,8 @@ class SlabWakeSolve:
         ev1.record()
         for d in devs:
             torch.cuda.synchronize(d)
+        for r in self.mine:
+            self.solvers[r].check_status(f"SlabWakeSolve.wakesolve (slab {r})")
         ms = ev0.elapsed_time(ev1)
         elapsed = time.perf_counter() - t0
         hist = self._join_history(hists)

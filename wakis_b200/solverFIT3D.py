@@ -190,9 +190,7 @@ class SolverFIT3D(RoutinesMixin):
         return torch.cuda.current_stream(self.device).cuda_stream
 
     _KERNELS = {"auto": _native.WK_KERNEL_AUTO, "cell": _native.WK_KERNEL_CELL,
-                "march": _native.WK_KERNEL_MARCH, "fused": _native.WK_KERNEL_FUSED,
-                "twopass": _native.WK_KERNEL_TWOPASS, "slab": _native.WK_KERNEL_SLAB,
-                "tma": _native.WK_KERNEL_TMA}
+                "twopass": _native.WK_KERNEL_TWOPASS, "tma": _native.WK_KERNEL_TMA}
 
     def _sync_desc(self):
         d = self._desc
@@ -351,7 +349,8 @@ class SolverFIT3D(RoutinesMixin):
         device, and the Ez values of the 3x3 test window captured before the
         update (9 x Nz) are copied back into ``ez_out[n]``.  Both host tensors
         should be pinned; all copies and steps are queued on the current
-        stream (call torch.cuda.synchronize() before reading ez_out)."""
+        stream; the call returns after they completed (it reads the status
+        word of the step kernels and raises if one timed out)."""
         n_steps, nz = jz_lines.shape
         ixs = int(np.abs(self.x - xsource).argmin())
         iys = int(np.abs(self.y - ysource).argmin())
@@ -367,14 +366,25 @@ class SolverFIT3D(RoutinesMixin):
             self._advance(1, step0 + n, line=(lbuf, step0 + n, ixs, iys),
                           capture=(cbuf, ixt - 1, iyt - 1, 3, 3, step0 + n))
             ez_out[n].copy_(cbuf.view(9, nz), non_blocking=True)
+        self.check_status("run_with_io")
+
+    def check_status(self, what="step"):
+        """Wait for the solver's stream and raise RuntimeError when a step
+        kernel gave up waiting for a tile load since the last check (its
+        output is then incomplete); the status word is cleared."""
+        _native.read_status(self._status, self._stream(), what)
 
     def one_step(self):
-        """One leap-frog step (upstream _one_step, solverFIT3D.py:482-503)."""
+        """One leap-frog step (upstream _one_step, solverFIT3D.py:482-503).
+        Asynchronous: the status word is read by the calls that wait for
+        the device (run, wakesolve, emsolve, check_status)."""
         self._advance(1)
 
     def run(self, n_steps):
-        """n_steps leap-frog steps in one call."""
+        """n_steps leap-frog steps in one call; waits for the device and
+        raises if a step kernel timed out."""
         self._advance(int(n_steps))
+        self.check_status("run")
 
     # ---------------------------------------------------------- materials
     def _dense_fields(self):
