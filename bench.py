@@ -211,46 +211,76 @@ def _status_ok(solver):
         return False
 
 
+def _ref_sample(args, sp):
+    """Grid of the reference arm: the workload's own grid (or --shape) when
+    the host has the memory for the oracle's sparse operators there (about
+    1.4 kB per cell at the peak of their assembly, measured at 128x128x256),
+    else 128x128x256."""
+    full = tuple(int(v) for v in args.shape.split("x")) if args.shape else tuple(sp["shape"])
+    need = 1.4e3 * float(np.prod(full)) * 1.5
+    try:
+        import psutil
+        avail = float(psutil.virtual_memory().available)
+    except Exception:
+        avail = 0.0
+    if avail >= need:
+        return full, True, avail
+    return (128, 128, 256), False, avail
+
+
 def run_reference(args):
     """CPU oracle on the host cores: Gcell-steps/s of upstream's scipy
-    algorithm on a bounded sample (same geometry, 128x128x256)."""
+    algorithm (same geometry; the workload's own grid when the host memory
+    allows, else a 128x128x256 sample)."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
     from oracle import fit as ofit
     from wakis_b200 import workloads
-    sample = (128, 128, 256)
     sp = workloads.spec(args.workload)
+    sample, same, avail = _ref_sample(args, sp)
+    t_init = time.perf_counter()
     g0 = ofit.Grid(*workloads.BOUNDS, *sample)
     m = workloads.cavity_mask(g0.x, g0.y, g0.z)
     g = ofit.Grid(*workloads.BOUNDS, *sample, solids={"cavity": m}, materials={"cavity": "vacuum"})
     so = ofit.Solver(g, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
                      dtype=np.float32 if args.dtype == "float32" else np.float64,
                      n_pml=sp["n_pml"])
+    t_init = time.perf_counter() - t_init
     cores = os.cpu_count() or 1
     so.set_threads(cores)
     beam = ofit.Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
     for n in range(args.warmup):
         beam.update(so, n * so.dt)
         so.one_step()
+    # K steps, or fewer when they would take more than ~2 minutes
     t0 = time.perf_counter()
+    done = 0
     for n in range(args.warmup, args.warmup + args.steps):
         beam.update(so, n * so.dt)
         so.one_step()
+        done += 1
+        if time.perf_counter() - t0 > 120.0:
+            break
     t = time.perf_counter() - t0
-    value = so.N * args.steps / t / 1e9
+    value = so.N * done / t / 1e9
     line = {"metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * t / done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.dtype == "float32" else "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": args.workload, "cells": int(np.prod(sp["shape"])),
-                       "sample_cells": so.N},
+            "config": {"workload": args.workload,
+                       "cells": int(np.prod([int(v) for v in args.shape.split("x")]
+                                            if args.shape else sp["shape"])),
+                       "sample_cells": so.N, "grid": list(sample), "same_grid": same,
+                       "host_mem_available_gb": round(avail / 1e9, 1),
+                       "init_s": round(t_init, 1)},
             "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores,
                              "kind": "port",
                              "sample": f"oracle (scipy CSR, {cores} threads) on the "
-                                       f"{args.workload} geometry at 128x128x256, "
-                                       f"{args.steps} steps with beam"},
+                                       f"{args.workload} geometry at "
+                                       f"{sample[0]}x{sample[1]}x{sample[2]}, "
+                                       f"{done} steps with beam"},
             "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -583,6 +613,74 @@ def run_slab(args):
         dist.destroy_process_group()
 
 
+def precision_leg(args, dev, fp64_value):
+    """The FP32-compensated state on the same workload and grid in the same
+    run (rank 0, N=1): device-timed rate of K steps (same warm-up, beam and
+    capture as the FP64 line), the roofline of its step kernel at 48 B per
+    cell-step, and the WP / Z errors of a whole FP32c wakesolve against the
+    FP64 one on the precision workload at 112x112x224 with a 0.3 m wake
+    (``workloads.precision_compare``)."""
+    import torch
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    sp = workloads.spec(args.workload)
+    shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else None
+    g, w, s = workloads.build_b200(args.workload, dtype=np.float64, shape=shape,
+                                   precision="fp32c")
+    N = s.N
+    bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
+              ).params(s)
+    ixt = int(np.abs(s.x - w.xtest).argmin())
+    iyt = int(np.abs(s.y - w.ytest).argmin())
+    total = args.warmup + args.steps
+    hist = torch.zeros((9, s.Nz, total + args.steps), dtype=s._cap_dtype, device=dev)
+    cap = (hist, ixt - 1, iyt - 1, 3, 3)
+    s._advance(args.warmup, 0, beam=bp, capture=cap)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s._advance(args.steps, args.warmup, beam=bp, capture=cap)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if not _status_ok(s):
+        return {"error": "a step kernel timed out in the FP32c timed region"}
+    timing = []
+    s._advance(args.steps, total, beam=bp, capture=cap, timing=timing)
+    ms_int = sum(t[0] for t in timing)
+    n_int = sum(t[1] for t in timing)
+    del g, w, s, hist
+    torch.cuda.empty_cache()
+    value = N * args.steps / (ms / 1e3) / 1e9
+    peak, src = _peaks()
+    bpc = BYTES_PER_CELL["fp32c"]
+    achieved = bpc * N * args.steps / (ms_int / 1e3) / 1e9 if ms_int > 0 else None
+    out = {"value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / args.steps,
+           "vs_fp64": value / fp64_value,
+           "dtype": "f32 state + bf16 compensation words, f64-formed coefficients",
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak if achieved else None, "peak_source": src,
+                        "bytes_per_cell_step": bpc,
+                        "kernel": f"k_tma_comp: {n_int} launches, "
+                                  f"{ms_int / max(args.steps, 1):.4f} ms per step",
+                        "traffic": _traffic(args.workload, "fp32c", "tma", N)},
+           "gpu_launches": args.steps}
+    # accuracy of a whole wakesolve, FP32c against FP64 on one grid
+    acc_shape, acc_wl = (112, 112, 224), 0.3
+    r = workloads.precision_compare("precision_448", shape=acc_shape, wakelength=acc_wl)
+    out["accuracy"] = {"workload": f"precision_448 geometry at {acc_shape[0]}x{acc_shape[1]}"
+                                   f"x{acc_shape[2]}, wakelength {acc_wl} m",
+                       "steps": r["fp64"]["steps"],
+                       "relative_errors_vs_fp64": r["errors"],
+                       "bar": 1e-4,
+                       "within_bar": bool(r["errors"]["WP"] <= 1e-4
+                                          and r["errors"]["absZ"] <= 1e-4),
+                       "wakesolve_rate_fp64": r["fp64"]["gcell_steps_per_s"],
+                       "wakesolve_rate_fp32c": r["fp32c"]["gcell_steps_per_s"]}
+    return out
+
+
 def cpu_baseline(args, budget_s=20.0):
     """Single-thread oracle on a bounded sample (rank 0, N=1 only)."""
     from oracle import fit as ofit
@@ -620,6 +718,8 @@ def main():
     ap.add_argument("--workload", default="lossy_256")
     ap.add_argument("--dtype", default="float64", choices=["float64", "float32", "fp32c"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-leg", action="store_true",
+                    help="skip the FP32-compensated leg of the default FP64 run")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "twopass", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
     ap.add_argument("--shape", default=None,
@@ -823,6 +923,10 @@ def main():
             "clocks": clocks,
             "status_word": 0,
         }
+        if ws == 1 and args.dtype == "float64" and not args.no_precision_leg:
+            del g, w, s, hist, cap
+            torch.cuda.empty_cache()
+            line["fp32c"] = precision_leg(args, dev, value)
         if ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args)
         print(json.dumps(line), flush=True)

@@ -300,6 +300,9 @@ int wk_sigma_e(const wk_fit_desc* d, void* J, void* stream);
  * w_src = win_map[w], kz = k + k_off (reversed index for counter-moving),
  * t = key_order[it] (upstream sorts the '#%05d' keys as strings).
  * coef_k = dz[k] (counter-moving: -dz[k]).  All double except hist.
+ * A key_order entry outside [0, hist_nt) adds nothing (the caller passes
+ * nt <= the number of steps the history holds, as upstream reads only the
+ * saved steps).
  */
 int wk_wake_potential(const void* hist, int hist_dtype, long long hist_nt, int Nzh,
                       const int* win_map, int n_win, int carry,

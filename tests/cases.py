@@ -121,3 +121,99 @@ SOURCE_CASES = [
                                xs=slice(4, 9), ys=7, zs=10),
          shape=(16, 16, 24), bc_low=["pec"] * 3, bc_high=["pec"] * 3, Nt=40),
 ]
+
+
+# -- the lossy-wall workload geometry (conductive background, z-PML) ---------
+# The cavity + pipe of the lossy workload (wakis_b200.workloads, lossy_256)
+# at sizes upstream runs in seconds: sigma = 1e4 S/m background (dt clamped
+# to eps_0/sigma), PEC x/y faces, 10-cell PML on both z faces, the Gaussian
+# beam on the axis.  "init" is "random" (seeded fields, every coefficient
+# exercised) or "zero" (beam only; ti is then shortened so that the bunch is
+# at the upstream end of the grid from the first step).
+def _lossy_cases():
+    out = []
+    for shape, dtype, init, steps, seed in (((24, 24, 48), "float64", "random", 12, 100),
+                                            ((24, 24, 48), "float32", "random", 12, 101),
+                                            ((32, 32, 64), "float64", "zero", 40, 102)):
+        ti = None if init == "random" else 2.0 * 0.005 / 299792458.0
+        out.append(dict(shape=shape, dtype=dtype, init=init, steps=steps, seed=seed,
+                        bg=[1.0, 1.0, 1e4], bc_low=["pec", "pec", "pml"],
+                        bc_high=["pec", "pec", "pml"], n_pml=10,
+                        beam=dict(q=1e-9, sigmaz=0.005, beta=1.0, xsource=0.0, ysource=0.0,
+                                  ti=ti)))
+    return out
+
+
+LOSSY_CASES = _lossy_cases()
+
+
+def lossy_edges(case):
+    from wakis_b200 import workloads
+    x0, x1, y0, y1, z0, z1 = workloads.BOUNDS
+    Nx, Ny, Nz = case["shape"]
+    return (np.linspace(x0, x1, Nx + 1), np.linspace(y0, y1, Ny + 1),
+            np.linspace(z0, z1, Nz + 1))
+
+
+def lossy_mask(case):
+    from wakis_b200 import workloads
+    return workloads.cavity_mask(*lossy_edges(case))
+
+
+def case_fields(case, N):
+    """Initial (E, H) of a case with an "init" entry (zero or seeded random)."""
+    dt = np.dtype(case["dtype"]).type
+    if case.get("init") == "zero":
+        return np.zeros(3 * N, dt), np.zeros(3 * N, dt)
+    return initial_fields(case, N)
+
+
+# -- surface impedance (SIBC) on a pillbox wall ------------------------------
+# A C4-style pillbox at 2 mm cells whose wall conductivity is above the
+# resolvable one, so upstream replaces the wall by its surface cells with
+# eps = sigma = 1/Z_s (wakis/solverFIT3D.py:446-466).  Upstream takes the
+# surface cells from VTK's gradient of the solid mask (gridFIT3D.py:519-535);
+# both sides here use wakis_b200.geometry.surface_mask of the same wall mask
+# instead (injected into upstream for the fixtures).
+SIBC_CASES = [
+    dict(kind="step", pillbox=dict(R=0.020, L=0.030, cell=2e-3), sigma=1e4, dtype="float64",
+         steps=10, seed=200, bc_low=["pec", "pec", "abc"], bc_high=["pec", "pec", "abc"],
+         beam=dict(q=1e-9, sigmaz=0.008, beta=0.9, xsource=0.0, ysource=0.0)),
+    dict(kind="wake", pillbox=dict(R=0.020, L=0.030, cell=2e-3), sigma=1e4, dtype="float64",
+         bc_low=["pec", "pec", "abc"], bc_high=["pec", "pec", "abc"], wakelength=0.05,
+         compute_plane="both", wake=dict(q=1e-9, sigmaz=0.008, beta=0.9)),
+]
+
+
+def sibc_geometry(case):
+    """(bounds, shape, wall mask, surface mask) of a SIBC case."""
+    from wakis_b200 import batch, geometry
+    b, shape, wall = batch.pillbox_grid(**case["pillbox"])
+    x = np.linspace(b[0], b[1], shape[0] + 1)
+    y = np.linspace(b[2], b[3], shape[1] + 1)
+    z = np.linspace(b[4], b[5], shape[2] + 1)
+    m = wall(x, y, z)
+    return b, shape, m, geometry.surface_mask(m)
+
+
+# -- emsolve with ABC faces ---------------------------------------------------
+# Upstream's get_abc keeps, on its CPU path, views of the live field arrays
+# (wakis/boundaries.py:313-366 with field.py:223-300), so update_abc copies
+# the current first interior plane onto a low face and leaves a high face as
+# it is; on its GPU path (cupy .get()) the snapshots are copies, and both
+# faces take the values of two steps before.  "abc_copies" selects the GPU
+# semantics (the fixtures emulate them by copying the snapshots).  An axis
+# has ABC on one side only: upstream keeps one snapshot dict per axis, and
+# the second side's dict replaces the first.
+ABC_SOURCE_CASES = [
+    dict(kind="Dipole", kw=dict(field="Ez", nodes=5), shape=(16, 16, 24),
+         bc_low=["pec", "pec", "abc"], bc_high=["pec", "pec", "pec"], Nt=40, abc_copies=False),
+    dict(kind="Dipole", kw=dict(field="Ez", nodes=5), shape=(16, 16, 24),
+         bc_low=["pec", "pec", "abc"], bc_high=["pec", "pec", "pec"], Nt=40, abc_copies=True),
+    dict(kind="Pulse", kw=dict(field="Jz", shape="Gaussian", L=0.004, amplitude=1e3),
+         shape=(16, 16, 24), bc_low=["abc", "pec", "pec"], bc_high=["pec", "abc", "abc"],
+         Nt=50, abc_copies=False),
+    dict(kind="Pulse", kw=dict(field="Jz", shape="Gaussian", L=0.004, amplitude=1e3),
+         shape=(16, 16, 24), bc_low=["abc", "pec", "pec"], bc_high=["pec", "abc", "abc"],
+         Nt=50, abc_copies=True),
+]

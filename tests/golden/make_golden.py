@@ -19,6 +19,14 @@ Outputs (all small, committed):
   ``wakesolve`` + ``WakeSolver.solve`` on small cavities.
 * ``source_cases.npz``  E, H, J after upstream ``emsolve`` driven by each
   hard source (PlaneWave, WavePacket, Dipole, Pulse) on a small vacuum box.
+* ``lossy_cases.npz``  E, H, J after ``one_step`` calls with the beam on the
+  lossy-wall workload geometry (sigma = 1e4 S/m background, z-PML) at small
+  sizes.
+* ``sibc_cases.npz``  a pillbox whose wall takes upstream's surface-impedance
+  branch (the surface mask injected, see ``cases.SIBC_CASES``): fields after
+  a few steps, and a full ``wakesolve`` + ``WakeSolver.solve``.
+* ``abc_cases.npz``  E, H, J after ``emsolve`` with ABC faces, with upstream's
+  CPU snapshot semantics and with copied snapshots (its GPU semantics).
 
 The case definitions live in ``tests/cases.py`` so that the tests rebuild the
 same inputs without the upstream package.
@@ -145,6 +153,101 @@ def source_cases(wakis):
     print("source_cases.npz:", len(cases.SOURCE_CASES), "cases")
 
 
+def lossy_cases(wakis):
+    out = {}
+    for idx, c in enumerate(cases.LOSSY_CASES):
+        x, y, z = cases.lossy_edges(c)
+        g = wakis.GridFIT3D(x=x, y=y, z=z, verbose=0)
+        refshim.inject_solids(g, {"cavity": cases.lossy_mask(c)}, {"cavity": "vacuum"})
+        s = wakis.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                              dtype=np.dtype(c["dtype"]).type, bg=c["bg"], n_pml=c["n_pml"],
+                              use_stl=True, use_sibc=False)
+        E0, H0 = cases.case_fields(c, s.N)
+        s.E.fromarray(E0.copy())
+        s.H.fromarray(H0.copy())
+        beam = wakis.sources.Beam(**c["beam"])
+        for n in range(c["steps"]):
+            beam.update(s, n * s.dt)
+            s.one_step()
+        for f in "EHJ":
+            out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+        out[f"c{idx}_dt"] = np.array(s.dt)
+    np.savez_compressed(os.path.join(HERE, "lossy_cases.npz"), **out)
+    print("lossy_cases.npz:", len(cases.LOSSY_CASES), "cases")
+
+
+def _sibc_grid(wakis, c):
+    """Upstream grid of a SIBC case with the wall solid and its surface mask
+    injected in place of VTK's gradient (GridFIT3D._mark_cells_in_surface)."""
+    b, shape, wall, surf = cases.sibc_geometry(c)
+    g = wakis.GridFIT3D(*b, *shape, verbose=0)
+    refshim.inject_solids(g, {"wall": wall}, {"wall": [1.0, 1.0, c["sigma"]]})
+    g._mark_cells_in_surface = lambda key: g.grid.__setitem__(
+        key, np.asarray(surf, bool).ravel(order="C"))
+    return g
+
+
+def sibc_cases(wakis):
+    out = {}
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            for idx, c in enumerate(cases.SIBC_CASES):
+                g = _sibc_grid(wakis, c)
+                if c["kind"] == "step":
+                    s = wakis.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"],
+                                          verbose=0, dtype=np.dtype(c["dtype"]).type,
+                                          bg="vacuum", use_stl=True, use_sibc=True)
+                    E0, H0 = cases.initial_fields(c, s.N)
+                    s.E.fromarray(E0.copy())
+                    s.H.fromarray(H0.copy())
+                    beam = wakis.sources.Beam(**c["beam"])
+                    for n in range(c["steps"]):
+                        beam.update(s, n * s.dt)
+                        s.one_step()
+                    for f in "EHJ":
+                        out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+                else:
+                    w = wakis.WakeSolver(save=False, verbose=0, **c["wake"])
+                    s = wakis.SolverFIT3D(g, w, bc_low=c["bc_low"], bc_high=c["bc_high"],
+                                          verbose=0, dtype=np.dtype(c["dtype"]).type,
+                                          bg="vacuum", use_stl=True, use_sibc=True)
+                    s.wakesolve(wakelength=c["wakelength"], compute_plane=c["compute_plane"])
+                    for n in ["s", "WP", "Z", "f", "lambdaf", "WP_3d", "WPx", "WPy", "Zx", "Zy"]:
+                        out[f"c{idx}_{n}"] = np.asarray(getattr(w, n))
+                    out[f"c{idx}_Nt"] = np.array(s.Nt)
+                    out[f"c{idx}_Ez"] = s.E.toarray()[2 * s.N:].copy()
+                for f in ("ieps", "sigma"):
+                    out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+                out[f"c{idx}_dt"] = np.array(s.dt)
+        finally:
+            os.chdir(cwd)
+    np.savez_compressed(os.path.join(HERE, "sibc_cases.npz"), **out)
+    print("sibc_cases.npz:", len(cases.SIBC_CASES), "cases")
+
+
+def abc_cases(wakis):
+    out = {}
+    for idx, c in enumerate(cases.ABC_SOURCE_CASES):
+        g = wakis.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)
+        s = wakis.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                              bg="vacuum", use_stl=False, use_sibc=False)
+        assert s.activate_abc
+        if c["abc_copies"]:
+            # upstream's GPU path: every snapshot is a copy (cupy .get())
+            live = s.get_abc
+            s.get_abc = lambda: tuple({a: {k: np.array(v, copy=True) for k, v in d.items()}
+                                       for a, d in snap.items()} for snap in live())
+        src = getattr(wakis.sources, c["kind"])(**c["kw"])
+        s.emsolve(c["Nt"], source=src)
+        for f in "EHJ":
+            out[f"c{idx}_{f}"] = getattr(s, f).toarray().copy()
+        out[f"c{idx}_dt"] = np.array(s.dt)
+    np.savez_compressed(os.path.join(HERE, "abc_cases.npz"), **out)
+    print("abc_cases.npz:", len(cases.ABC_SOURCE_CASES), "cases")
+
+
 if __name__ == "__main__":
     wakis = refshim.install()
     only = sys.argv[1:]
@@ -156,3 +259,9 @@ if __name__ == "__main__":
         wake_cases(wakis)
     if not only or "source" in only:
         source_cases(wakis)
+    if not only or "lossy" in only:
+        lossy_cases(wakis)
+    if not only or "sibc" in only:
+        sibc_cases(wakis)
+    if not only or "abc" in only:
+        abc_cases(wakis)

@@ -64,3 +64,38 @@ def rel_err(a, b):
     den = np.max(np.abs(b)) if b.size else 0.0
     num = np.max(np.abs(a - b)) if b.size else 0.0
     return 0.0 if den == 0 and num == 0 else num / (den if den else 1.0)
+
+
+def oracle_lossy_case(c):
+    from wakis_b200 import workloads
+    g = ofit.Grid(*workloads.BOUNDS, *c["shape"], solids={"cavity": cases.lossy_mask(c)},
+                  materials={"cavity": "vacuum"})
+    return ofit.Solver(g, bc_low=c["bc_low"], bc_high=c["bc_high"],
+                       dtype=np.dtype(c["dtype"]).type, bg=c["bg"], n_pml=c["n_pml"],
+                       use_stl=True, use_sibc=False)
+
+
+def b200_lossy_case(c, precision=None):
+    """The lossy case through the same builder as the benchmark workload
+    (``workloads.build_b200('lossy_256', shape=...)``)."""
+    from wakis_b200 import workloads
+    dtype = np.float64 if precision == "fp32c" else np.dtype(c["dtype"]).type
+    return workloads.build_b200("lossy_256", dtype=dtype, shape=c["shape"], precision=precision)
+
+
+def oracle_sibc_case(c, wake=None):
+    b, shape, wall, surf = cases.sibc_geometry(c)
+    g = ofit.Grid(*b, *shape, solids={"wall": wall}, materials={"wall": [1.0, 1.0, c["sigma"]]})
+    return ofit.Solver(g, bc_low=c["bc_low"], bc_high=c["bc_high"], use_stl=True, use_sibc=True,
+                       bg="vacuum", dtype=np.dtype(c["dtype"]).type, surface_masks={"wall": surf},
+                       wake_fmax=wake.fmax if wake is not None else None)
+
+
+def b200_sibc_case(c, wake=None, precision=None):
+    import wakis_b200 as wb
+    b, shape, wall, surf = cases.sibc_geometry(c)
+    g = wb.GridFIT3D(*b, *shape, verbose=0)
+    g.add_solid("wall", wall, [1.0, 1.0, c["sigma"]])
+    return wb.SolverFIT3D(g, wake, bc_low=c["bc_low"], bc_high=c["bc_high"], use_stl=True,
+                          use_sibc=True, bg="vacuum", dtype=np.dtype(c["dtype"]).type, verbose=0,
+                          precision=precision)

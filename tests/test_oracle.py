@@ -96,3 +96,67 @@ def test_oracle_reproduces_upstream_test001(golden_dir):
         assert np.allclose(fn(w.Z)[::20], fn(gold["Z"]), rtol=tz, atol=tz)
     assert np.cumsum(np.abs(w.Z))[-1] == pytest.approx(float(gold["Z_cumsum"]),
                                                        float(gold["Z_cumsum_rel"]))
+
+
+@pytest.fixture(scope="module")
+def lossy_golden(golden_dir):
+    return np.load(os.path.join(golden_dir, "lossy_cases.npz"))
+
+
+@pytest.fixture(scope="module")
+def sibc_golden(golden_dir):
+    return np.load(os.path.join(golden_dir, "sibc_cases.npz"))
+
+
+@pytest.mark.parametrize("idx", range(len(cases.LOSSY_CASES)))
+def test_oracle_lossy_geometry_matches_upstream(idx, lossy_golden):
+    """The lossy-wall workload geometry (sigma = 1e4 S/m background, dt at
+    the relaxation clamp, 10-cell z-PML, cavity + pipe, beam): the oracle
+    equals upstream value for value."""
+    from helpers import oracle_lossy_case
+    c = cases.LOSSY_CASES[idx]
+    s = oracle_lossy_case(c)
+    assert s.dt == lossy_golden[f"c{idx}_dt"]
+    E0, H0 = cases.case_fields(c, s.N)
+    s.E[:], s.H[:] = E0, H0
+    beam = ofit.Beam(**c["beam"])
+    for n in range(c["steps"]):
+        beam.update(s, n * s.dt)
+        s.one_step()
+    for f in "EHJ":
+        assert np.abs(lossy_golden[f"c{idx}_{f}"]).max() > 0, f
+        assert np.array_equal(getattr(s, f), lossy_golden[f"c{idx}_{f}"]), f
+
+
+def test_oracle_sibc_step_matches_upstream(sibc_golden):
+    """Surface-impedance wall (upstream's SIBC branch with the same surface
+    mask injected): materials, dt and fields after steps value for value."""
+    from helpers import oracle_sibc_case
+    idx = 0
+    c = cases.SIBC_CASES[idx]
+    s = oracle_sibc_case(c)
+    assert s.dt == sibc_golden[f"c{idx}_dt"]
+    assert np.array_equal(s.ieps, sibc_golden[f"c{idx}_ieps"])
+    assert np.array_equal(s.sigma, sibc_golden[f"c{idx}_sigma"])
+    E0, H0 = cases.initial_fields(c, s.N)
+    s.E[:], s.H[:] = E0, H0
+    beam = ofit.Beam(**c["beam"])
+    for n in range(c["steps"]):
+        beam.update(s, n * s.dt)
+        s.one_step()
+    for f in "EHJ":
+        assert np.array_equal(getattr(s, f), sibc_golden[f"c{idx}_{f}"]), f
+
+
+def test_oracle_sibc_wake_matches_upstream(sibc_golden):
+    from helpers import oracle_sibc_case
+    idx = 1
+    c = cases.SIBC_CASES[idx]
+    w = owake.WakeOracle(**c["wake"])
+    s = oracle_sibc_case(c, wake=w)
+    assert s.dt == sibc_golden[f"c{idx}_dt"]
+    Nt = owake.wakesolve(s, w, c["wakelength"], compute_plane=c["compute_plane"])
+    assert Nt == int(sibc_golden[f"c{idx}_Nt"])
+    for n in ["s", "WP", "Z", "f", "lambdaf", "WP_3d", "WPx", "WPy", "Zx", "Zy"]:
+        assert np.array_equal(getattr(w, n), sibc_golden[f"c{idx}_{n}"]), n
+    assert np.array_equal(s.E[2 * s.N:], sibc_golden[f"c{idx}_Ez"])

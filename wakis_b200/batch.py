@@ -173,28 +173,40 @@ def pillbox_params(n=64, seed=0):
             for q in range(n)]
 
 
-def build_pillbox(R, L, beta, sigma, cell=1e-3, pipe=0.008, sigmaz=0.008, precision=None,
-                  dtype=np.float64, device=None):
-    """(grid, wake, solver) of one pillbox: a vacuum cylinder of radius R and
-    length L centred at the origin with a vacuum beam pipe of radius 8 mm
-    along z, inside a conducting wall (solid of conductivity sigma, surface
-    impedance above the resolvable conductivity as upstream does); 1 mm
-    cells, the transverse size rounded up to a multiple of 4 cells, PEC on
-    x/y and ABC on z; the pipe runs max(45 mm, L) past each cavity end."""
-    from .gridFIT3D import GridFIT3D
-    from .solverFIT3D import SolverFIT3D
-    from .wakeSolver import WakeSolver
+def pillbox_grid(R, L, cell=1e-3, pipe=0.008):
+    """Bounds (x0, x1, y0, y1, z0, z1), cell counts (Nx, Ny, Nz) and a
+    function of the grid edges (x, y, z) giving the wall mask of a pillbox:
+    a vacuum cylinder of radius R and length L centred at the origin with a
+    vacuum beam pipe along z, inside a conducting wall; the transverse size
+    is rounded up to a multiple of 4 cells and the pipe runs max(45 mm, L)
+    past each cavity end.  A cell is vacuum when any of its corners is
+    inside the vacuum region."""
     nxy = int(np.ceil(2 * (R + 0.005) / cell / 4.0)) * 4
     half = nxy * cell / 2
     zl = L / 2 + max(0.045, L)
     nz = int(round(2 * zl / cell))
-    g = GridFIT3D(-half, half, -half, half, -zl, zl, nxy, nxy, nz, verbose=0)
     vac = geometry.CylinderZ(R, zmin=-L / 2, zmax=L / 2) | geometry.CylinderZ(pipe)
     wall = geometry.Box(-2 * half, 2 * half, -2 * half, 2 * half, -2 * zl, 2 * zl) - vac
-    mask = geometry.cell_mask(wall, g.x, g.y, g.z)
-    # a cell is vacuum when any corner is inside the vacuum region
-    mask &= ~geometry.cell_mask(vac, g.x, g.y, g.z)
-    g.add_solid("wall", mask, [1.0, 1.0, sigma])
+
+    def mask(x, y, z):
+        m = geometry.cell_mask(wall, x, y, z)
+        m &= ~geometry.cell_mask(vac, x, y, z)
+        return m
+
+    return (-half, half, -half, half, -zl, zl), (nxy, nxy, nz), mask
+
+
+def build_pillbox(R, L, beta, sigma, cell=1e-3, pipe=0.008, sigmaz=0.008, precision=None,
+                  dtype=np.float64, device=None):
+    """(grid, wake, solver) of one pillbox (``pillbox_grid``): wall of
+    conductivity sigma (surface impedance above the resolvable conductivity,
+    as upstream does), 1 mm cells, PEC on x/y and ABC on z."""
+    from .gridFIT3D import GridFIT3D
+    from .solverFIT3D import SolverFIT3D
+    from .wakeSolver import WakeSolver
+    bounds, shape, wall_mask = pillbox_grid(R, L, cell=cell, pipe=pipe)
+    g = GridFIT3D(*bounds, *shape, verbose=0)
+    g.add_solid("wall", wall_mask(g.x, g.y, g.z), [1.0, 1.0, sigma])
     w = WakeSolver(q=1e-9, sigmaz=sigmaz, beta=beta, xsource=0.0, ysource=0.0, xtest=0.0,
                    ytest=0.0, save=False, verbose=0)
     s = SolverFIT3D(g, w, bc_low=["pec", "pec", "abc"], bc_high=["pec", "pec", "abc"],

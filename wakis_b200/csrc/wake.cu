@@ -52,6 +52,7 @@ __global__ void k_wake_potential(const H* __restrict__ hist, long long hist_nt, 
         if (it < 0) it += nt;          // negative index wraps as in numpy
         if (it < 0) continue;
         long long t = key_order[it];
+        if (t < 0 || t >= hist_nt) continue;   // no such history column
         double e = (double)hw[(long long)kz * hist_nt + t];
         acc = __dadd_rn(acc, __dmul_rn(e, coef));
       }

@@ -111,36 +111,62 @@ class RoutinesMixin:
                 callback(self, n * self.dt)
         self.check_status("emsolve")
 
-    # ABC snapshots (upstream boundaries.py:313-410).  Upstream's CPU path
-    # keeps views of the live arrays; these are copies, as on its GPU path.
+    # ABC snapshots (upstream boundaries.py:313-410).  One dict per axis, as
+    # upstream keeps them: with ABC on both sides of an axis the high side's
+    # dict replaces the low side's, and update_abc then raises KeyError as
+    # upstream does.  With views (upstream's CPU path, use_gpu=False) an
+    # entry reads its plane when update_abc uses it, so a low face takes the
+    # current first interior plane and a high face keeps its own values;
+    # with copies (upstream's GPU path) both take the values of the call.
     def get_abc(self):
         E_abc, H_abc = {}, {}
-        sl = {0: lambda p: (p, slice(None), slice(None)), 1: lambda p: (slice(None), p, slice(None)),
-              2: lambda p: (slice(None), slice(None), p)}
+        snap = (lambda f, idx: _LivePlane(f, idx)) if self._abc_views else _plane_copy
         for a in range(3):
             if self.bc_low[a].lower() == "abc":
                 E_abc[a], H_abc[a] = {}, {}
                 for d in "xyz":
-                    E_abc[a][d + "lo"] = self.E[(*sl[a](1), d)]
-                    H_abc[a][d + "lo"] = self.H[(*sl[a](1), d)]
+                    E_abc[a][d + "lo"] = snap(self.E, (*_plane(a, 1), d))
+                    H_abc[a][d + "lo"] = snap(self.H, (*_plane(a, 1), d))
         for a in range(3):
             if self.bc_high[a].lower() == "abc":
                 E_abc[a], H_abc[a] = {}, {}
                 for d in "xyz":
-                    E_abc[a][d + "hi"] = self.E[(*sl[a](-1), d)]
-                    H_abc[a][d + "hi"] = self.H[(*sl[a](-1), d)]
+                    E_abc[a][d + "hi"] = snap(self.E, (*_plane(a, -1), d))
+                    H_abc[a][d + "hi"] = snap(self.H, (*_plane(a, -1), d))
         return E_abc, H_abc
 
     def update_abc(self, E_abc, H_abc):
-        sl = {0: lambda p: (p, slice(None), slice(None)), 1: lambda p: (slice(None), p, slice(None)),
-              2: lambda p: (slice(None), slice(None), p)}
+        val = lambda v: v.read() if isinstance(v, _LivePlane) else v
         for a in range(3):
             if self.bc_low[a].lower() == "abc":
                 for d in "xyz":
-                    self.E[(*sl[a](0), d)] = E_abc[a][d + "lo"]
-                    self.H[(*sl[a](0), d)] = H_abc[a][d + "lo"]
+                    self.E[(*_plane(a, 0), d)] = val(E_abc[a][d + "lo"])
+                    self.H[(*_plane(a, 0), d)] = val(H_abc[a][d + "lo"])
         for a in range(3):
             if self.bc_high[a].lower() == "abc":
                 for d in "xyz":
-                    self.E[(*sl[a](-1), d)] = E_abc[a][d + "hi"]
-                    self.H[(*sl[a](-1), d)] = H_abc[a][d + "hi"]
+                    self.E[(*_plane(a, -1), d)] = val(E_abc[a][d + "hi"])
+                    self.H[(*_plane(a, -1), d)] = val(H_abc[a][d + "hi"])
+
+
+def _plane(axis, p):
+    """Index tuple (without the component) of plane p normal to `axis`."""
+    idx = [slice(None)] * 3
+    idx[axis] = p
+    return tuple(idx)
+
+
+def _plane_copy(field, idx):
+    """Device copy of one component plane, idx = (i, j, k, component)."""
+    return field._comp(idx[3])[idx[0], idx[1], idx[2]].clone()
+
+
+class _LivePlane:
+    """A plane of a field read when it is used (upstream's CPU snapshots are
+    numpy views of the live field arrays)."""
+
+    def __init__(self, field, idx):
+        self.field, self.idx = field, idx
+
+    def read(self):
+        return _plane_copy(self.field, self.idx)

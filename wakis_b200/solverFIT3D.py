@@ -49,7 +49,7 @@ class SolverFIT3D(RoutinesMixin):
     def __init__(self, grid, wake=None, cfln=0.5, dt=None,
                  bc_low=("Periodic", "Periodic", "Periodic"),
                  bc_high=("Periodic", "Periodic", "Periodic"),
-                 use_stl=False, use_conductors=False, use_gpu=True, use_mpi=False,
+                 use_stl=False, use_conductors=False, use_gpu=False, use_mpi=False,
                  use_sibc=True, fmax=1e9, dtype=np.float64, n_pml=10, bg=(1.0, 1.0),
                  verbose=1, device=None, backend="b200", precision=None, coefficients=None):
         """``precision="fp32c"`` keeps E and H as FP32 values plus bf16
@@ -59,7 +59,13 @@ class SolverFIT3D(RoutinesMixin):
 
         ``coefficients``: a compact coefficient set already built for this
         grid (``coefficients.build``, or a z-slab of one, ``slab.py``); the
-        boundary, material and time-step arguments are then not re-applied."""
+        boundary, material and time-step arguments are then not re-applied.
+
+        The state always lives on the device.  ``use_gpu`` only selects which
+        of upstream's two behaviours ``emsolve`` reproduces where they
+        differ: the ABC snapshots of ``get_abc`` are views of the live fields
+        on upstream's CPU path (``use_gpu=False``, upstream's default) and
+        copies on its GPU path (``use_gpu=True``)."""
         if backend != "b200":
             raise ValueError(f"backend {backend!r}: this package only provides 'b200'")
         if use_mpi:
@@ -75,6 +81,7 @@ class SolverFIT3D(RoutinesMixin):
         self.nstep = 0
         self.use_stl, self.use_gpu, self.use_mpi = use_stl, True, False
         self.use_sibc = use_sibc
+        self._abc_views = not use_gpu
         self.fmax = fmax
         self.grid = grid
         self.background = bg

@@ -65,6 +65,8 @@ class WakeSolver:
     # ------------------------------------------------------------ history
     def set_history(self, hist, n_steps, one_d=False):
         """Attach the device Ez history [window][k][step] of n_steps steps."""
+        if int(n_steps) > hist.shape[-1]:
+            raise ValueError(f"history of {hist.shape[-1]} steps, n_steps={n_steps}")
         self._hist = hist
         self._hist_steps = int(n_steps)
         self._hist_1d = bool(one_d)
