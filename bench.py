@@ -722,6 +722,9 @@ def main():
                     help="skip the FP32-compensated leg of the default FP64 run")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "twopass", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
+    ap.add_argument("--steps-per-launch", type=int, default=0, choices=[0, 1],
+                    help="0: two steps per launch (temporal blocking) where it applies; "
+                         "1: one step per launch")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
     ap.add_argument("--accuracy", action="store_true",
@@ -789,6 +792,7 @@ def main():
     split = args.kernel == "split"
     s.kernel = "auto" if split else args.kernel
     s.tile = tuple(int(v) for v in args.tile.split("x"))
+    s.steps_per_launch = args.steps_per_launch
     bp = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")}
               ).params(s)
     ixt = int(np.abs(s.x - w.xtest).argmin())
@@ -837,12 +841,16 @@ def main():
     # + 2 shell launches, two-pass 2 interior + 2 shell launches; the other
     # schedules launch a fixed set
     fixed = {"split": 4, "cell": 1}
-    n_per = n_int // max(args.steps, 1)
-    # the TMA schedule needs no shell launch when every face is PEC-masked
+    # the TMA schedule needs no shell launch when every face is PEC-masked;
+    # there the default runs two steps per launch (k_tma2) where it applies,
+    # so fewer interior launches than steps
     pec_faces = all(b.lower() in ("pec", "electric", "pml") for b in s.bc_low + s.bc_high)
+    two_step = pec_faces and 0 < n_int < args.steps
+    n_per = 1 if two_step else n_int // max(args.steps, 1)
     tma_per_step = 1 if pec_faces else 3
     per_step = fixed.get(args.kernel, {1: tma_per_step, 2: 4}.get(n_per, 2 * n_per))
-    launches = args.steps * per_step  # step kernels launched in the timed region
+    # step kernels launched in the timed region
+    launches = n_int if two_step else args.steps * per_step
     # cells the TMA / interior kernel updates: the whole grid when every face
     # is PEC-masked, all of x and y when the x/y faces are, else the interior
     # without the two-cell shell
@@ -854,7 +862,7 @@ def main():
         interior = s.Nx * s.Ny * (s.Nz - 4)
     else:
         interior = (s.Nx - 4) * (s.Ny - 4) * (s.Nz - 4)
-    schedule = {1: "tma", 2: "twopass"}.get(n_int // max(args.steps, 1), args.kernel)
+    schedule = "tma2" if two_step else {1: "tma", 2: "twopass"}.get(n_per, args.kernel)
 
     # end to end through the public API: per-step H2D line current, D2H window
     prof = Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource", "ysource")})
@@ -910,7 +918,8 @@ def main():
                        "l2": "state %.0f MB > L2, no flush" % (
                            4 * 3 * N * s._E[0].element_size() / 1e6),
                        "step": "fused beam + Ez 3x3 capture + H and E half-steps",
-                       "kernel": args.kernel, "schedule": schedule, "tile": args.tile},
+                       "kernel": args.kernel, "schedule": schedule, "tile": args.tile,
+                       "steps_per_launch": 2 if two_step else 1},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": src,
                          "bytes_per_cell_step": bpc, "kernel": kernel_note,

@@ -143,6 +143,12 @@ typedef struct wk_fit_desc {
    * loads it issued and returns (a test of the timeout path, which leaves
    * the output of the step incomplete).                                   */
   long long wait_ns;
+  /* Steps per launch of the TMA schedule: 0 (the default) = two steps per
+   * launch (temporal blocking, k_tma2) where that kernel applies (every face
+   * PEC-masked, faces_clean, J = 0 without conductivity or sigma*E with it,
+   * no step_dev) and n_steps >= 4, else one; 1 = always one.  The result
+   * and its buffer parity do not depend on it.                            */
+  int steps_per_launch;
 } wk_fit_desc;
 
 #define WK_KERNEL_AUTO 0   /* WK_KERNEL_TMA when its conditions hold, else
@@ -320,6 +326,50 @@ int wk_wake_potential(const void* hist, int hist_dtype, long long hist_nt, int N
  */
 int wk_trans_wake(const double* WP3d, int ns, double ds, double dxsum, double dysum,
                   double* WPx, double* WPy, void* stream);
+
+/*
+ * Streaming form of wk_wake_potential, for runs whose whole Ez history does
+ * not fit in memory: the history arrives in chunks of steps, and each chunk
+ * is added into an accumulator as it completes.
+ *
+ * wk_wake_accumulate: the steps step0 .. step0+n_steps-1 of the Ez window
+ * history are in ring[(w_src*Nzh + kz)*ring_nt + (step - step0)] (the
+ * capture layout of wk_fit_desc with cap_step0 = step0, n_steps <=
+ * ring_nt).  Step m sits at position p = pos[m] of upstream's sorted key
+ * list ('#%05d' keys sorted as strings; pos = NULL: p = m, exact below 10^5
+ * steps); it adds Ez(w, k, m) * coef_k into acc[w][n] (double, n_win x ns,
+ * zeroed by the caller before the first chunk) for every s sample n with
+ * it(n, k) == p < nt, it and coef_k as in wk_wake_potential.
+ * wk_wake_finalize: WP3d[w][n] = ((carry ? WP3d[w-1][n] : 0) + acc[w][n]) /
+ * qnorm, windows in order.
+ * The sums run in another order than upstream's (by step, and the carried
+ * value added after instead of before), so WP3d agrees with
+ * wk_wake_potential to rounding, not value for value.  No counterpart in
+ * the reference (it keeps the whole history in an HDF5 file).
+ */
+int wk_wake_accumulate(const void* ring, int ring_dtype, long long ring_nt, int Nzh,
+                       long long step0, int n_steps, const int* win_map, int n_win,
+                       const double* z, const double* dz, int nz, int k_off, const double* s,
+                       int ns, const long long* pos, long long nt, double v, double zmin,
+                       double zmax, double t0, double ti, double dt, int counter_moving,
+                       double* acc, void* stream);
+int wk_wake_finalize(const double* acc, int n_win, int ns, int carry, double qnorm,
+                     double* WP3d, void* stream);
+
+/*
+ * wk_trans_wake for long s axes: the same Panofsky-Wenzel quotient
+ * (wakis/wakeSolver.py:556-612) with the prefix integrals formed by
+ * segmented scans in double-double arithmetic (~106-bit running sums,
+ * rounded once), O(ns) instead of the O(ns^2) per-sample pairwise sums;
+ * the integrals differ from numpy's pairwise ones only by the rounding of
+ * the latter.  `scratch` is caller-owned device memory of at least
+ * wk_trans_wake_scan_scratch_bytes(ns) bytes, 16-byte aligned (the segment
+ * sums).  No counterpart in the reference.
+ */
+long long wk_trans_wake_scan_scratch_bytes(int ns);
+int wk_trans_wake_scan(const double* WP3d, int ns, double ds, double dxsum, double dysum,
+                       double* WPx, double* WPy, void* scratch, long long scratch_bytes,
+                       void* stream);
 
 /*
  * Zero-padded DFT bins X[m] = sum_{n<len} x[n] * exp(-2*pi*i*m*n/N) for

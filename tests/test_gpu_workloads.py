@@ -295,3 +295,102 @@ def test_abc_on_both_sides_of_an_axis_raises_like_upstream():
                        verbose=0, bg="vacuum", use_stl=False, use_sibc=False)
     with pytest.raises(KeyError):
         s.emsolve(2, source=wb.sources.Dipole(field="Ez", nodes=5))
+
+
+# ------------------------------------------------------- temporal blocking
+@pytest.mark.parametrize("shape,dtype,tile", [((64, 64, 128), np.float64, 0),
+                                              ((64, 64, 128), np.float64, 3),
+                                              ((72, 40, 52), np.float64, 7),
+                                              ((72, 40, 52), np.float64, 1),
+                                              ((64, 64, 128), np.float32, 0),
+                                              ((136, 24, 33), np.float32, 5)])
+def test_two_steps_per_launch_equal_one(shape, dtype, tile):
+    """k_tma2 (two steps per launch, overlapped tiles) against k_tma (one
+    step per launch) on the lossy geometry: 42 steps with the fused beam and
+    the Ez capture give the same fields and history value for value (the
+    first step runs alone, then ten pairs of two-step launches and one
+    single step)."""
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    sp = workloads.spec("lossy_256")
+    out = []
+    for spl in (0, 1):
+        _, _, s = workloads.build_b200("lossy_256", shape=shape, dtype=dtype)
+        s.steps_per_launch = spl
+        s.tile = (0, tile)
+        ixt = int(np.abs(s.x).argmin())
+        iyt = int(np.abs(s.y).argmin())
+        hist = torch.zeros((9, s.Nz, 42), dtype=s._cap_dtype, device="cuda")
+        timing = []
+        s._advance(42, 0, beam=Beam(**_short_beam(sp)).params(s),
+                   capture=(hist, ixt - 1, iyt - 1, 3, 3), timing=timing)
+        s.check_status()
+        out.append((s.E.numpy(), s.H.numpy(), s.J.numpy(), hist.cpu().numpy(),
+                    sum(t[1] for t in timing)))
+    a, b = out
+    assert a[4] == 1 + 20 + 1 and b[4] == 42      # launches: the pairs ran as k_tma2
+    assert np.abs(b[0]).max() > 0
+    for x, y in zip(a[:4], b[:4]):
+        assert np.array_equal(x, y)
+
+
+def test_two_steps_per_launch_non_conductive():
+    """J = 0 (vacuum in a PEC box, every face PEC) with the fused beam: the
+    two-step kernel equals the one-step kernel (40 steps)."""
+    import wakis_b200 as wb
+    from wakis_b200.sources import Beam
+    c = cases.WAKE_CASES[0]
+    out = []
+    for spl in (0, 1):
+        g = wb.GridFIT3D(*c["bounds"], *c["shape"], verbose=0)
+        g.add_solid("cav", cases.wake_mask(c, g.x, g.y, g.z), c["material"])
+        s = wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], use_stl=True,
+                           bg=c["bg"], verbose=0)
+        assert not s.use_conductivity
+        s.steps_per_launch = spl
+        s._advance(40, 0, beam=Beam(q=1e-9, sigmaz=0.004, beta=1.0, ti=0.0).params(s))
+        s.check_status()
+        out.append((s.E.numpy(), s.H.numpy()))
+    assert np.abs(out[1][0]).max() > 0
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_two_steps_per_launch_matches_oracle():
+    """The default path (now two steps per launch) on the lossy geometry at
+    64x64x128 from seeded random fields with clean faces: the face entries
+    of the random E are zeroed first, then the faces are marked clean; 40
+    steps against the oracle within 1e-12."""
+    from wakis_b200 import workloads
+    from wakis_b200.sources import Beam
+    sp = workloads.spec("lossy_256")
+    so, c = _oracle_lossy((64, 64, 128))
+    _, _, s = workloads.build_b200("lossy_256", shape=(64, 64, 128))
+    E0, H0 = cases.initial_fields(c, so.N)
+    # tangential E on every face set to +0 (the state a wakesolve keeps)
+    Nx, Ny, Nz = so.shape
+    for d in range(3):
+        v = E0[d * so.N:(d + 1) * so.N].reshape(Nz, Ny, Nx)
+        if d != 0:
+            v[:, :, 0] = 0.0
+            v[:, :, -1] = 0.0
+        if d != 1:
+            v[:, 0, :] = 0.0
+            v[:, -1, :] = 0.0
+        if d != 2:
+            v[0] = 0.0
+            v[-1] = 0.0
+    so.E[:], so.H[:] = E0, H0
+    s.E.fromarray(E0)
+    s.H.fromarray(H0)
+    s._faces_clean = True
+    bkw = _short_beam(sp)
+    timing = []
+    s._advance(40, 0, beam=Beam(**bkw).params(s), timing=timing)
+    s.check_status()
+    assert sum(t[1] for t in timing) < 40
+    beam = ofit.Beam(**bkw)
+    for m in range(40):
+        beam.update(so, m * so.dt)
+        so.one_step()
+    for f in "EHJ":
+        assert rel_err(getattr(s, f).numpy(), getattr(so, f)) <= FIELD_TOL, f

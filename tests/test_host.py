@@ -175,3 +175,19 @@ def test_adjoint_operators_equal_oracle_matrices(idx):
     scale = np.max(np.abs(Bo)) or 1.0
     tol = 1e-6 if c["dtype"] == "float32" else 1e-14
     assert np.max(np.abs(B - Bo)) <= tol * scale
+
+
+def test_key_order_matches_string_sort():
+    """Upstream reads the Ez history in the order of its '#%05d' keys sorted
+    as strings (wakeSolver.py:488-491); the vectorised order and its inverse
+    (the position of each step) match Python's sort, past 10^5 and 10^6."""
+    from wakis_b200.wakeSolver import WakeSolver
+    for n in (0, 7, 99999, 100000, 100001, 234567, 1000011):
+        ref = [int(k[1:]) for k in sorted("#" + str(i).zfill(5) for i in range(n))]
+        order = WakeSolver._key_order(n)
+        assert order.tolist() == ref
+        pos = WakeSolver._key_positions(n)
+        if n <= 100000:
+            assert pos is None
+        else:
+            assert np.array_equal(order[pos], np.arange(n))

@@ -44,6 +44,7 @@ class FitDesc(ctypes.Structure):
         ("step_dev", _vp),
         ("faces_clean", _i),
         ("wait_ns", _ll),
+        ("steps_per_launch", _i),
     ]
 
 
@@ -69,6 +70,11 @@ _SIGS = {
     "wk_trans_wake": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp]),
     "wk_dft_bins": (_i, [_vp, _i, _ll, _ll, _i, _vp, _vp]),
     "wk_read_status": (_i, [_vp, _i, _vp]),
+    "wk_wake_accumulate": (_i, [_vp, _i, _ll, _i, _ll, _i, _vp, _i, _vp, _vp, _i, _i, _vp, _i,
+                                _vp, _ll, _d, _d, _d, _d, _d, _d, _i, _vp, _vp]),
+    "wk_wake_finalize": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
+    "wk_trans_wake_scan_scratch_bytes": (_ll, [_i]),
+    "wk_trans_wake_scan": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp, _ll, _vp]),
 }
 
 EXPORTED = tuple(_SIGS)

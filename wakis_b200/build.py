@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwakis_b200.so")
-SOURCES = ["abi.cu", "fit_step.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma_comp.cu",
+SOURCES = ["abi.cu", "fit_step.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma2.cu", "fit_tma_comp.cu",
            "wake.cu", "adjoint.cu", "monitor.cu"]
 HEADERS = ["abi_internal.h", "fit_common.cuh", "fit_kernels.cuh", "fit_comp.cuh", "tma_util.cuh"]
 

@@ -53,6 +53,7 @@ struct FitParams {
   const long long* step_dev;   // optional device step counter
   int faces_clean;             // tangential E on PEC faces is +0 (wk_fit_desc)
   long long wait_ns;           // bound of the TMA step-loop waits (wk_fit_desc)
+  int steps_per_launch;        // wk_fit_desc.steps_per_launch
   unsigned nx_mul;   // fast division by Nx: q = umulhi(n, nx_mul) >> nx_shift
   int nx_shift;
 };

@@ -122,6 +122,7 @@ inline FitParams<T> make_params(const wk_fit_desc* d, int par) {
   p.step_dev = d->step_dev;
   p.faces_clean = d->faces_clean;
   p.wait_ns = d->wait_ns;
+  p.steps_per_launch = d->steps_per_launch;
   return p;
 }
 
@@ -233,5 +234,12 @@ template <typename T>
 bool tma_supported(const FitParams<T>& p);
 template <typename T>
 cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC);
+
+// Two steps per launch (fit_tma2.cu): k_tma2 covers grids whose faces are
+// all PEC-masked and clean, with J = 0 or sigma*E.
+template <typename T>
+bool tma2_supported(const FitParams<T>& p);
+template <typename T>
+cudaError_t launch_tma2(const FitParams<T>& p, long long step, cudaStream_t st, int KC);
 
 }  // namespace wk

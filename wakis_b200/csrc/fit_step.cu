@@ -105,7 +105,19 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
     use_tma = ok;
   }
   if (use_tma) {
-    for (int s = 0; s < n_steps; s++) {
+    int s = 0;
+    // two steps per launch where k_tma2 applies; an even number of such
+    // launches keeps the result in E[par ^ (n_steps & 1)]
+    if (d->steps_per_launch != 1 && !d->step_dev && n_steps >= 4 &&
+        tma2_supported<T>(make_params<T>(d, par))) {
+      const int pairs = (n_steps / 4) * 2;
+      for (int q = 0; q < pairs; q++, s += 2) {
+        cudaError_t e = launch_tma2<T>(make_params<T>(d, par), step0 + s, st, d->tile_planes);
+        if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
+        par ^= 1;
+      }
+    }
+    for (; s < n_steps; s++) {
       FitParams<T> p = make_params<T>(d, par);
       cudaError_t e = launch_tma<T>(p, step0 + s, st, d->tile_planes);
       if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));

@@ -18,13 +18,42 @@ from .sources import Beam
 
 
 class RoutinesMixin:
+    # the whole Ez history is kept on the device up to this size (bytes);
+    # longer runs integrate it chunk by chunk (history="stream")
+    HISTORY_MAX_BYTES = 4 << 30
+    STREAM_CHUNK = 256
+
     def wakesolve(self, wakelength, wake=None, callback=None, compute_plane="both",
                   plot=False, save_J=False, add_space=None, use_field_monitor=False,
-                  field_monitor=None, **kwargs):
-        ws = self._wake_setup(wakelength, wake, compute_plane, add_space)
+                  field_monitor=None, history="auto", **kwargs):
+        """``history``: "full" keeps the whole Ez window history on the
+        device and integrates it afterwards as upstream does (value for
+        value); "stream" adds each chunk of steps into the wake-potential
+        sums as it completes (memory O(samples) instead of O(steps), equal
+        to the full form to rounding); "auto" streams when the full history
+        would exceed HISTORY_MAX_BYTES."""
+        ws = self._wake_setup(wakelength, wake, compute_plane, add_space, history=history)
         bp, cap, Nt = ws["beam_params"], ws["capture"], ws["Nt"]
         t0 = time.time()
-        if callback is None and not (use_field_monitor and field_monitor is not None):
+        if ws["stream"]:
+            self._wake_axes(ws)
+            w = self.wake
+            w.stream_begin(Nt, 1 if ws["longitudinal"] else 9, ws["longitudinal"], self.device)
+            ring, rest = cap[0], cap[1:]
+            R = ring.shape[-1]
+            for n0 in range(0, Nt, R):
+                c = min(R, Nt - n0)
+                if callback is None and not (use_field_monitor and field_monitor is not None):
+                    self._advance(c, n0, beam=bp, capture=(ring,) + rest + (n0,))
+                else:
+                    for n in range(n0, n0 + c):
+                        self._advance(1, n, beam=bp, capture=(ring,) + rest + (n0,))
+                        if use_field_monitor and field_monitor is not None:
+                            field_monitor.update(self.E, self.dt)
+                        if callback is not None:
+                            callback(self, n * self.dt)
+                w.stream_add(ring, n0, c)
+        elif callback is None and not (use_field_monitor and field_monitor is not None):
             self._advance(Nt, 0, beam=bp, capture=cap)
         else:
             for n in range(Nt):
@@ -36,7 +65,8 @@ class RoutinesMixin:
         self.check_status("wakesolve")
         self._wake_finish(ws, time.time() - t0)
 
-    def _wake_setup(self, wakelength, wake=None, compute_plane="both", add_space=None):
+    def _wake_setup(self, wakelength, wake=None, compute_plane="both", add_space=None,
+                    history="full"):
         """Everything wakesolve prepares before stepping (upstream
         routines.py:322-375): test indices, Nt from the wakelength, the beam
         parameters and the device Ez history with its capture window."""
@@ -67,20 +97,32 @@ class RoutinesMixin:
         Nt = int(tmax / self.dt)
         self.tmax, self.Nt = tmax, Nt
         beam = Beam(q=w.q, sigmaz=w.sigmaz, beta=w.beta, xsource=w.xsource, ysource=w.ysource)
-        hist = torch.zeros((ni * nj, self.Nz, max(Nt, 1)), dtype=self._cap_dtype,
-                           device=self.device)
+        esize = torch.tensor([], dtype=self._cap_dtype).element_size()
+        full_bytes = ni * nj * self.Nz * max(Nt, 1) * esize
+        if history not in ("auto", "full", "stream"):
+            raise ValueError(f"history {history!r}: 'auto', 'full' or 'stream'")
+        stream = history == "stream" or (history == "auto" and
+                                         full_bytes > self.HISTORY_MAX_BYTES)
+        cols = min(self.STREAM_CHUNK, max(Nt, 1)) if stream else max(Nt, 1)
+        hist = torch.zeros((ni * nj, self.Nz, cols), dtype=self._cap_dtype, device=self.device)
         return {"beam": beam, "beam_params": beam.params(self), "hist": hist,
                 "capture": (hist, i0, j0, ni, nj), "Nt": Nt, "longitudinal": longitudinal,
-                "xx": xx, "yy": yy, "compute_plane": compute_plane}
+                "xx": xx, "yy": yy, "compute_plane": compute_plane, "stream": stream}
 
-    def _wake_finish(self, ws, elapsed=0.0):
-        """Integrate the captured Ez history (upstream routines.py:462-482)."""
+    def _wake_axes(self, ws):
+        """The WakeSolver's axes of this run (upstream routines.py:462-476)."""
         w, z = self.wake, self.z
-        self.beam = ws["beam"]
         w.xf, w.yf, w.zf = self.x[ws["xx"]], self.y[ws["yy"]], z[slice(0, self.Nz)]
         w.dx, w.dy, w.dz = self.grid.dx, self.grid.dy, self.grid.dz
         w.t = np.arange(0, ws["Nt"] * self.dt, self.dt)
-        w.set_history(ws["hist"], n_steps=ws["Nt"], one_d=ws["longitudinal"])
+
+    def _wake_finish(self, ws, elapsed=0.0):
+        """Integrate the captured Ez history (upstream routines.py:462-482)."""
+        w = self.wake
+        self.beam = ws["beam"]
+        self._wake_axes(ws)
+        if not ws.get("stream"):
+            w.set_history(ws["hist"], n_steps=ws["Nt"], one_d=ws["longitudinal"])
         w.solve(compute_plane=ws["compute_plane"])
         self.logger.wakeSolver = w.logger.wakeSolver
         self.logger.wakeSolver["wakelength"] = w.wakelength

@@ -192,6 +192,9 @@ class SolverFIT3D(RoutinesMixin):
         self._desc = d
         self.kernel = "auto"
         self.tile = (0, 0)
+        # 0: two steps per launch where the temporal-blocking kernel applies
+        # (wk_fit_desc.steps_per_launch), 1: one step per launch
+        self.steps_per_launch = 0
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
@@ -203,6 +206,7 @@ class SolverFIT3D(RoutinesMixin):
         d = self._desc
         d.kernel = self._KERNELS[self.kernel]
         d.tile_rows, d.tile_planes = int(self.tile[0]), int(self.tile[1])
+        d.steps_per_launch = int(self.steps_per_launch)
         d.par = self._par
         d.dt = float(self.dt)
         d.dt_is_f32 = int(isinstance(self.dt, np.float32))
@@ -348,31 +352,43 @@ class SolverFIT3D(RoutinesMixin):
             self._j_line = (ixs, iys, vals)
 
     def run_with_io(self, jz_lines, ez_out, step0=0, xtest=0.0, ytest=0.0, xsource=0.0,
-                    ysource=0.0):
-        """Advance len(jz_lines) steps exchanging data with host memory every
-        step, the data movement of upstream's GPU wakesolve loop
-        (wakis/routines.py:435-445): before step n the Jz line current of
-        the beam line (Nz values, ``jz_lines[n]``) is copied from host to
-        device, and the Ez values of the 3x3 test window captured before the
-        update (9 x Nz) are copied back into ``ez_out[n]``.  Both host tensors
-        should be pinned; all copies and steps are queued on the current
-        stream; the call returns after they completed (it reads the status
-        word of the step kernels and raises if one timed out)."""
+                    ysource=0.0, chunk=4):
+        """Advance len(jz_lines) steps exchanging data with host memory for
+        every step, the data movement of upstream's GPU wakesolve loop
+        (wakis/routines.py:435-445): the Jz line current of the beam line of
+        step n (Nz values, ``jz_lines[n]``) is copied from host to device
+        before step n, and the Ez values of the 3x3 test window captured
+        before the update of step n (9 x Nz) are copied back into
+        ``ez_out[n]``.  The copies go in chunks of ``chunk`` steps (lines of
+        the chunk up, the chunk's steps, its windows down), so that the step
+        kernels can run two steps per launch.  Both host tensors should be
+        pinned; all copies and steps are queued on the current stream; the
+        call returns after they completed (it reads the status word of the
+        step kernels and raises if one timed out)."""
         n_steps, nz = jz_lines.shape
+        chunk = max(1, int(chunk))
         ixs = int(np.abs(self.x - xsource).argmin())
         iys = int(np.abs(self.y - ysource).argmin())
         ixt = int(np.abs(self.x - xtest).argmin())
         iyt = int(np.abs(self.y - ytest).argmin())
-        if getattr(self, "_io_bufs", None) is None or self._io_bufs[0].shape[0] != nz:
+        bufs = getattr(self, "_io_bufs", None)
+        if bufs is None or bufs[0].shape != (chunk, nz):
             td = self._cap_dtype
-            self._io_bufs = (torch.empty(nz, dtype=td, device=self.device),
-                             torch.empty((9, nz, 1), dtype=td, device=self.device))
-        lbuf, cbuf = self._io_bufs
-        for n in range(n_steps):
-            lbuf.copy_(jz_lines[n], non_blocking=True)
-            self._advance(1, step0 + n, line=(lbuf, step0 + n, ixs, iys),
+            bufs = (torch.empty((chunk, nz), dtype=td, device=self.device),
+                    {c: torch.empty((9, nz, c), dtype=td, device=self.device)
+                     for c in range(1, chunk + 1)})
+            self._io_bufs = bufs
+        lbuf, cbufs = bufs
+        n = 0
+        while n < n_steps:
+            c = min(chunk, n_steps - n)
+            cbuf = cbufs[c]
+            lb = lbuf[:c]
+            lb.copy_(jz_lines[n:n + c], non_blocking=True)
+            self._advance(c, step0 + n, line=(lb, step0 + n, ixs, iys),
                           capture=(cbuf, ixt - 1, iyt - 1, 3, 3, step0 + n))
-            ez_out[n].copy_(cbuf.view(9, nz), non_blocking=True)
+            ez_out[n:n + c].copy_(cbuf.permute(2, 0, 1), non_blocking=True)
+            n += c
         self.check_status("run_with_io")
 
     def check_status(self, what="step"):

@@ -56,6 +56,7 @@ class WakeSolver:
         if self.save:
             os.makedirs(self.folder, exist_ok=True)
         self._hist = None
+        self._stream = None
         self.logger.wakeSolver.update(dict(ti=self.ti, q=q, sigmaz=sigmaz, beta=beta,
                                            xsource=xsource, ysource=ysource, xtest=xtest,
                                            ytest=ytest, chargedist=chargedist,
@@ -70,12 +71,85 @@ class WakeSolver:
         self._hist = hist
         self._hist_steps = int(n_steps)
         self._hist_1d = bool(one_d)
+        self._stream = None
 
-    def _key_order(self, n):
+    @staticmethod
+    def _key_order(n):
         """Step index of each history column in upstream's read order: the
-        '#%05d' keys sorted as strings (wakeSolver.py:488-491)."""
-        keys = sorted("#" + str(i).zfill(5) for i in range(n))
-        return np.array([int(k[1:]) for k in keys], dtype=np.int64)
+        '#%05d' keys sorted as strings (wakeSolver.py:488-491).  The keys are
+        the decimal digits of the step, zero-padded to 5: as strings they
+        sort by the digits read as a fraction (value * 10^(D - length), D the
+        longest length), a key before the longer keys it is a prefix of."""
+        m = np.arange(n, dtype=np.int64)
+        length = np.maximum(5, np.floor(np.log10(np.maximum(m, 1))).astype(np.int64) + 1)
+        # guard the float log10 at powers of ten
+        length = np.where(m >= 10 ** np.minimum(length, 18), length + 1, length)
+        length = np.where((length > 5) & (m < 10 ** np.maximum(length - 1, 0)), length - 1,
+                          length)
+        D = int(length.max()) if n else 5
+        scaled = m * (10 ** (D - length))
+        return np.lexsort((length, scaled)).astype(np.int64)
+
+    @classmethod
+    def _key_positions(cls, n):
+        """Position of each step's key in upstream's sorted key list (the
+        inverse of _key_order); None when every key keeps its place
+        (n <= 10^5)."""
+        if n <= 100000:
+            return None
+        order = cls._key_order(n)
+        pos = np.empty(n, dtype=np.int64)
+        pos[order] = np.arange(n, dtype=np.int64)
+        return pos
+
+    # ------------------------------------------------- streamed history
+    def stream_begin(self, n_steps, n_win, one_d, device):
+        """Start a streamed integration of n_steps steps (the wake-potential
+        sums are added chunk by chunk with ``stream_add`` while the solver
+        steps, instead of keeping the whole [window][k][step] history).
+        Needs the axes (t, xf, yf, zf, dz) and the wakelength set."""
+        if one_d and self.skip_cells != 0:
+            raise ValueError("could not broadcast input array: skip_cells with a 1-D history")
+        nt, dt, zmin, zmax, z, s = self._axis()
+        nt = min(nt, int(n_steps))
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=device)
+        pos = self._key_positions(int(n_steps))
+        st = {"n_win": n_win, "one_d": bool(one_d), "nt": nt, "dt": dt, "zmin": zmin,
+              "zmax": zmax, "z": f64(z), "dz": f64(self.dz), "s": f64(s), "ns": len(s),
+              "nz": len(z), "win": torch.arange(n_win, dtype=torch.int32, device=device),
+              "pos": None if pos is None else torch.as_tensor(pos, device=device),
+              "acc": torch.zeros((n_win, len(s)), dtype=torch.float64, device=device)}
+        self._stream = st
+        self._hist = None
+        self._hist_1d = bool(one_d)
+        self.s = s
+        return st
+
+    def stream_add(self, ring, step0, n_steps):
+        """Add the steps step0 .. step0+n_steps-1 held in ring columns
+        0 .. n_steps-1 ([window][k][column], the capture layout)."""
+        st = self._stream
+        lib = _native.lib()
+        hdt = _native.WK_F64 if ring.dtype == torch.float64 else _native.WK_F32
+        stream = torch.cuda.current_stream(ring.device).cuda_stream
+        rc = lib.wk_wake_accumulate(
+            ring.data_ptr(), hdt, ring.shape[-1], ring.shape[1], int(step0), int(n_steps),
+            st["win"].data_ptr(), st["n_win"], st["z"].data_ptr(), st["dz"].data_ptr(), st["nz"],
+            int(self.skip_cells), st["s"].data_ptr(), st["ns"],
+            None if st["pos"] is None else st["pos"].data_ptr(), int(st["nt"]), float(self.v),
+            float(st["zmin"]), float(st["zmax"]), float(self.t[0]), float(self.ti),
+            float(st["dt"]), int(self.counter_moving), st["acc"].data_ptr(), stream)
+        _native.check(rc, "wk_wake_accumulate")
+
+    def _stream_wp(self, carry):
+        st = self._stream
+        lib = _native.lib()
+        WP3d = torch.empty_like(st["acc"])
+        stream = torch.cuda.current_stream(WP3d.device).cuda_stream
+        rc = lib.wk_wake_finalize(st["acc"].data_ptr(), st["n_win"], st["ns"], int(carry),
+                                  float(self.q * 1e12), WP3d.data_ptr(), stream)
+        _native.check(rc, "wk_wake_finalize")
+        return WP3d
 
     def _axis(self):
         nt = len(self.t)
@@ -92,6 +166,10 @@ class WakeSolver:
         return nt, dt, zmin, zmax, z, s
 
     def _wp(self, n_win, carry):
+        if getattr(self, "_stream", None) is not None:
+            if self._stream["n_win"] != n_win:
+                raise ValueError("the streamed history holds another window count")
+            return self._stream_wp(carry)
         if self._hist is None:
             raise RuntimeError("no Ez history: run SolverFIT3D.wakesolve first")
         lib = _native.lib()
@@ -150,6 +228,10 @@ class WakeSolver:
         self._WP_dev = WP[0]
         self.WP = WP[0].cpu().numpy()
 
+    # s axes longer than this take the O(ns) double-double scan instead of
+    # the per-sample pairwise sums of upstream's np.sum (O(ns^2))
+    TRANS_PAIRWISE_MAX = 65536
+
     def calc_trans_WP(self, **kwargs):
         lib = _native.lib()
         ds = self.s[2] - self.s[1]
@@ -158,10 +240,20 @@ class WakeSolver:
         dev = self._WP3d_dev.device
         WPx = torch.empty(ns, dtype=torch.float64, device=dev)
         WPy = torch.empty(ns, dtype=torch.float64, device=dev)
-        rc = lib.wk_trans_wake(self._WP3d_dev.data_ptr(), ns, float(ds), float(dxf[0] + dxf[1]),
-                               float(dyf[0] + dyf[1]), WPx.data_ptr(), WPy.data_ptr(),
-                               torch.cuda.current_stream(dev).cuda_stream)
-        _native.check(rc, "wk_trans_wake")
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        if ns > self.TRANS_PAIRWISE_MAX or kwargs.get("scan", False):
+            nb = int(lib.wk_trans_wake_scan_scratch_bytes(ns))
+            scratch = torch.empty(max(nb, 16), dtype=torch.uint8, device=dev)
+            rc = lib.wk_trans_wake_scan(self._WP3d_dev.data_ptr(), ns, float(ds),
+                                        float(dxf[0] + dxf[1]), float(dyf[0] + dyf[1]),
+                                        WPx.data_ptr(), WPy.data_ptr(), scratch.data_ptr(),
+                                        scratch.numel(), stream)
+            _native.check(rc, "wk_trans_wake_scan")
+        else:
+            rc = lib.wk_trans_wake(self._WP3d_dev.data_ptr(), ns, float(ds),
+                                   float(dxf[0] + dxf[1]), float(dyf[0] + dyf[1]),
+                                   WPx.data_ptr(), WPy.data_ptr(), stream)
+            _native.check(rc, "wk_trans_wake")
         self._WPx_dev, self._WPy_dev = WPx, WPy
         self.WPx, self.WPy = WPx.cpu().numpy(), WPy.cpu().numpy()
 
