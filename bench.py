@@ -15,12 +15,12 @@ value  = cells x steps / device time of the K timed steps (CUDA events,
 e2e    = the same through SolverFIT3D.run_with_io: every step copies the
          beam-line current host->device and the captured Ez window
          device->host (pinned buffers), wall clock around the K steps.
-Multi-GPU (torchrun): every rank runs an independent replica of the
-workload (weak scaling, no data-path collective); NCCL only carries the
-barrier and the max of the timings.  --decomp slab instead steps a chain of
-N workload blocks along z, one per rank, exchanging ghost planes with the
-neighbouring ranks every step (wakis_b200/slab.py); --slabs K splits the
-workload into K z-slabs on one GPU.
+Multi-GPU (torchrun): a chain of N workload blocks along z, one per rank
+(weak scaling), exchanging --slab-depth ghost planes with the neighbouring
+ranks every --slab-depth steps through NCCL point-to-point messages
+(wakis_b200/slab.py); --decomp replicas instead runs independent replicas
+(no data-path collective).  --slabs K splits the workload into K z-slabs on
+one GPU.
 
 --impl reference times the CPU oracle (a restatement of upstream's scipy
 solver) on the host cores with all threads, on a bounded sample of the
@@ -488,7 +488,7 @@ def run_slab(args):
     x, y, z = workloads.stacked_edges(args.workload, n_blocks, shape)
     Nx, Ny, Nz = len(x) - 1, len(y) - 1, len(z) - 1
     N = Nx * Ny * Nz
-    lay = slab.layout(Nz, n)
+    lay = slab.layout(Nz, n, args.slab_depth)
     solvers = {r: workloads.build_stacked(args.workload, n_blocks, shape=shape,
                                           planes=(lay[r].lo, lay[r].hi), dtype=dtype,
                                           precision=precision, device=dev)[2] for r in mine}
@@ -510,11 +510,16 @@ def run_slab(args):
     caps = {r: (torch.zeros((9, solvers[r].Nz, total), dtype=solvers[r]._cap_dtype, device=dev),
                 ixt - 1, iyt - 1, 3, 3) for r in mine}
 
+    G = lay[0].depth
+
     def steps(n0, k):
-        for m in range(n0, n0 + k):
+        m = n0
+        while m < n0 + k:
+            c = min(G, n0 + k - m)
             for r in mine:
-                solvers[r]._advance(1, m, beam=bp, capture=caps[r])
+                solvers[r]._advance(c, m, beam=bp, capture=caps[r])
             ex(lay, solvers)
+            m += c
 
     def barrier():
         if ws > 1:
@@ -565,9 +570,10 @@ def run_slab(args):
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for m in range(args.steps):
+    for m in range(0, args.steps, G):
+        c = min(G, args.steps - m)
         for r in mine:
-            solvers[r].run_with_io(jz[r][m:m + 1], ez[r][m:m + 1], step0=step0 + m)
+            solvers[r].run_with_io(jz[r][m:m + c], ez[r][m:m + c], step0=step0 + m)
         ex(lay, solvers)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
@@ -592,6 +598,7 @@ def run_slab(args):
                        "parallelism": f"zslab{ws}" if ws > 1 else f"zslab{n}-on-1gpu",
                        "slabs": [[s.k0, s.k1] for s in lay],
                        "exchange": "NCCL point-to-point" if ws > 1 else "device copies",
+                       "ghost_depth": G,
                        "l2": "state above L2, no flush",
                        "step": "fused beam + Ez 3x3 capture + H and E half-steps + ghost "
                                "exchange"},
@@ -744,10 +751,13 @@ def main():
     ap.add_argument("--slabs", type=int, default=0,
                     help="z-slab decomposition on one GPU: the workload split into this many "
                          "z-slabs in one process (ghost planes copied every step)")
-    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
-                    help="with torchrun (N > 1): independent replicas (default) or one block "
-                         "of a chain of N workload blocks per rank with the z-slab ghost "
-                         "exchange over NCCL")
+    ap.add_argument("--decomp", default="slab", choices=["replicas", "slab"],
+                    help="with torchrun (N > 1): one block of a chain of N workload blocks per "
+                         "rank with the z-slab ghost exchange over NCCL (default), or "
+                         "independent replicas")
+    ap.add_argument("--slab-depth", type=int, default=4,
+                    help="z-slab ghost planes per side = steps between exchanges (4: the "
+                         "slabs run two steps per launch)")
     ap.add_argument("--batch-compare", action="store_true",
                     help="also run the batch in FP64 and report per-instance WP/|Z| errors")
     args = ap.parse_args()

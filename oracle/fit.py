@@ -206,6 +206,7 @@ class Solver:
             if self.dt > self.tau.min():
                 self.dt = self.tau.min()
 
+        self._metrics = (L, iA, tL, itA)
         self._operators(L, iA, tL, itA)
 
     # -- boundaries (boundaries.py:14-188) ----------------------------------
@@ -335,6 +336,13 @@ class Solver:
         self.A = iDa * iDmu * self.C * Ds
         self.B = iDeps * itDa * self.C.transpose() * tDs
         self._dtA = None
+
+    def update_tensors(self):
+        """Re-form the operators after edits of ieps / imu / sigma
+        (solverFIT3D.py:356-414, tensor='all'); dt is not re-evaluated and
+        the first-step ghost zeroing is skipped, as upstream."""
+        self._operators(*self._metrics)
+        self.step_0 = False
 
     # -- time stepping ------------------------------------------------------
     def zero_ghosts(self):

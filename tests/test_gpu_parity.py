@@ -709,3 +709,73 @@ def test_full_size_step_is_linear():
         s._advance(8, 0)
     assert torch.equal(b.E.array, 2.0 * a.E.array)
     assert torch.equal(b.H.array, 2.0 * a.H.array)
+
+
+def test_adjoint_gradient_matches_oracle_finite_differences():
+    """The FP64 adjoint gradient against central differences of the oracle
+    (the CPU restatement of upstream's solver, a fresh solver per
+    evaluation): cavity_40 with a 16^3 design region of per-cell eps_r in
+    [1, 10] and sigma in [0, 5] S/m (below the relaxation clamp, so every
+    evaluation keeps the CFL time step), 800 steps; loss and its
+    post-processing as ImpedanceDesign.loss_from_history.  Two random
+    directions, Richardson-extrapolated, within 1e-5."""
+    import os as _os
+
+    from wakis_b200 import workloads
+    from wakis_b200.adjoint import ImpedanceDesign
+    from scipy.constants import epsilon_0 as EPS0
+    _, _, s = workloads.build_b200("cavity_40")
+    m = np.zeros((s.Nx, s.Ny, s.Nz), bool)
+    m[12:28, 12:28, 32:48] = True
+    p = ImpedanceDesign(s, m, f_band=(0.5e9, 3e9), n_steps=800, segment=30)
+    rng = np.random.default_rng(11)
+    nd = int(m.sum())
+    er = rng.uniform(1.0, 10.0, nd)
+    sg = rng.uniform(0.0, 5.0, nd)
+    p.set_params(er, sg)
+    L = p.forward()
+    ge, gs = p.backward()
+    sp = workloads.spec("cavity_40")
+    cells = np.flatnonzero(m.ravel(order="F"))
+    g0 = ofit.Grid(*workloads.BOUNDS, *sp["shape"])
+    cav = workloads.cavity_mask(g0.x, g0.y, g0.z)
+
+    def oracle_loss(e_r, sig):
+        g = ofit.Grid(*workloads.BOUNDS, *sp["shape"], solids={"cavity": cav, "design": m},
+                      materials={"cavity": "vacuum", "design": [1.0, 1.0, 1.0]})
+        wo = owake.WakeOracle(**sp["wake"])
+        so = ofit.Solver(g, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True,
+                         bg=sp["bg"], dtype=np.float64, wake_fmax=wo.fmax)
+        assert so.dt == s.dt
+        so.set_threads(_os.cpu_count() or 1)
+        N = so.N
+        for d in range(3):
+            so.ieps[d * N + cells] = 1.0 / (e_r * EPS0)
+            so.sigma[d * N + cells] = sig
+        so.update_tensors()
+        so.zero_ghosts()
+        beam = ofit.Beam(**{k: sp["wake"][k] for k in ("q", "sigmaz", "beta", "xsource",
+                                                         "ysource")})
+        ixt = int(np.abs(so.x - sp["wake"]["xtest"]).argmin())
+        iyt = int(np.abs(so.y - sp["wake"]["ytest"]).argmin())
+        hist = np.zeros((so.Nz, p.n_steps))
+        ez = lambda: ofit.comp_view(so.E, 2, so.shape)
+        for n in range(p.n_steps):
+            beam.update(so, n * so.dt)
+            hist[:, n] = ez()[ixt, iyt, :]
+            so.one_step()
+        return float(p.loss_from_history(torch.as_tensor(hist, device="cuda")).item())
+
+    assert abs(oracle_loss(er, sg) - L) <= 1e-10 * abs(L)
+    for t in range(2):
+        ve = rng.standard_normal(nd)
+        vs = rng.standard_normal(nd)
+
+        def central(h):
+            return (oracle_loss(er + h * ve, sg + h * vs)
+                    - oracle_loss(er - h * ve, sg - h * vs)) / (2.0 * h)
+
+        fd = (4.0 * central(5e-4) - central(1e-3)) / 3.0
+        ad = ge @ ve + gs @ vs
+        print("adjoint vs oracle FD", t, abs(ad - fd) / abs(fd))
+        assert abs(ad - fd) <= 1e-5 * abs(fd), (t, ad, fd)

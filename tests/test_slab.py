@@ -103,11 +103,18 @@ def test_partition_and_layout():
                                                        (14, 20, 12, 20)]
     with pytest.raises(ValueError):
         slab.partition(3, 4)
+    lay = slab.layout(20, 3, depth=4)
+    assert [(s.k0, s.k1, s.lo, s.hi, s.depth) for s in lay] == [
+        (0, 7, 0, 12, 4), (7, 14, 2, 19, 4), (14, 20, 9, 20, 4)]
+    with pytest.raises(ValueError):
+        slab.layout(20, 3, depth=7)
 
 
-@pytest.mark.parametrize("n", [2, 3])
+@pytest.mark.parametrize("n,depth", [(2, 1), (3, 1), (2, 2), (2, 4), (3, 3)])
 @pytest.mark.parametrize("idx", VALID)
-def test_emulated_slabs_equal_single_domain(idx, n):
+def test_emulated_slabs_equal_single_domain(idx, n, depth):
+    """Slabs with `depth` ghost planes per side, exchanging every `depth`
+    steps: after 4 steps the owned planes equal the single domain."""
     c = cases.STEP_CASES[idx]
     k = _coef(c)
     shape = k.shape
@@ -116,8 +123,8 @@ def test_emulated_slabs_equal_single_domain(idx, n):
     E0, H0 = cases.initial_fields(c, N)
     E0, H0 = E0.astype(k.dtype), H0.astype(k.dtype)
     sigma = coefficients.dense_materials(k)[2].astype(k.dtype)
-    Eg, Hg = _single_domain(k, E0, H0, sigma, 3)
-    lay = slab.layout(Nz, n)
+    Eg, Hg = _single_domain(k, E0, H0, sigma, 4)
+    lay = slab.layout(Nz, n, depth)
     solvers = {}
     for s in lay:
         ks = slab.slice_coefficients(k, s.lo, s.hi)
@@ -125,10 +132,14 @@ def test_emulated_slabs_equal_single_domain(idx, n):
                                     _local(H0, shape, s.lo, s.hi),
                                     _local(sigma, shape, s.lo, s.hi))
     ex = slab.LocalExchange()
-    for _ in range(3):
-        for s in lay:
-            solvers[s.index].step()
+    done = 0
+    while done < 4:
+        blk = min(depth, 4 - done)
+        for _ in range(blk):
+            for s in lay:
+                solvers[s.index].step()
         ex(lay, solvers)
+        done += blk
     Eg3 = Eg.reshape(3, Nz, Nx * Ny)
     Hg3 = Hg.reshape(3, Nz, Nx * Ny)
     for s in lay:
@@ -157,7 +168,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, ws, port, idx, out):
+def _rank_main(rank, ws, port, idx, out, depth=1):
     import datetime
 
     import torch.distributed as dist
@@ -173,14 +184,18 @@ def _rank_main(rank, ws, port, idx, out):
         E0, H0 = cases.initial_fields(c, Nx * Ny * Nz)
         E0, H0 = E0.astype(k.dtype), H0.astype(k.dtype)
         sigma = coefficients.dense_materials(k)[2].astype(k.dtype)
-        lay = slab.layout(Nz, ws)
+        lay = slab.layout(Nz, ws, depth)
         s = lay[rank]
         so = _EmuSlab(slab.slice_coefficients(k, s.lo, s.hi), _local(E0, shape, s.lo, s.hi),
                       _local(H0, shape, s.lo, s.hi), _local(sigma, shape, s.lo, s.hi))
         ex = slab.DistExchange()
-        for _ in range(3):
-            so.step()
+        done = 0
+        while done < 4:
+            blk = min(depth, 4 - done)
+            for _ in range(blk):
+                so.step()
             ex(lay, {rank: so})
+            done += blk
         E, H = _owned(so, s, shape)
         out.put((rank, E.copy(), H.copy()))
         dist.barrier()
@@ -188,12 +203,14 @@ def _rank_main(rank, ws, port, idx, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("idx", VALID[:3])
-def test_two_gloo_ranks_equal_single_domain(idx):
+@pytest.mark.parametrize("idx,depth", [(VALID[0], 1), (VALID[1], 1), (VALID[2], 1),
+                                       (VALID[2], 2), (VALID[4], 4)])
+def test_two_gloo_ranks_equal_single_domain(idx, depth):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, idx, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, idx, q, depth))
+             for r in range(2)]
     for p in procs:
         p.start()
     got = {}
@@ -208,8 +225,8 @@ def test_two_gloo_ranks_equal_single_domain(idx):
     Nx, Ny, Nz = k.shape
     E0, H0 = cases.initial_fields(c, Nx * Ny * Nz)
     sigma = coefficients.dense_materials(k)[2].astype(k.dtype)
-    Eg, Hg = _single_domain(k, E0.astype(k.dtype), H0.astype(k.dtype), sigma, 3)
-    lay = slab.layout(Nz, 2)
+    Eg, Hg = _single_domain(k, E0.astype(k.dtype), H0.astype(k.dtype), sigma, 4)
+    lay = slab.layout(Nz, 2, depth)
     for s in lay:
         E, H = got[s.index]
         assert np.array_equal(E, Eg.reshape(3, Nz, -1)[:, s.k0:s.k1])
@@ -227,8 +244,8 @@ def _cavity_args():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [2, 3])
-def test_slab_wakesolve_equals_single_domain(n):
+@pytest.mark.parametrize("n,depth", [(2, 1), (3, 1), (2, 4)])
+def test_slab_wakesolve_equals_single_domain(n, depth):
     """cavity_40 (PEC x/y, ABC z, beam and 3x3 Ez capture, 1896 steps) split
     into n z-slabs on one GPU: fields, WP and Z value for value equal to the
     single-domain wakesolve."""
@@ -238,7 +255,7 @@ def test_slab_wakesolve_equals_single_domain(n):
     s1 = wb.SolverFIT3D(g, w1, verbose=0, **kw)
     s1.wakesolve(wakelength=sp["wakelength"])
     w2 = wb.WakeSolver(save=False, verbose=0, **sp["wake"])
-    sw = slab.SlabWakeSolve(g, w2, n_slabs=n, **kw)
+    sw = slab.SlabWakeSolve(g, w2, n_slabs=n, depth=depth, **kw)
     sw.wakesolve(wakelength=sp["wakelength"])
     assert sw.Nt == s1.Nt
     for so in sw.solvers.values():
@@ -270,17 +287,20 @@ def test_slab_wakesolve_fp32c_close_to_single_domain():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,shape,n", [("cavity_40", (24, 24, 40), 2),
-                                          ("lossy_256", (32, 32, 48), 3)])
-def test_stacked_chain_built_per_slab_equals_single_domain(name, shape, n):
+@pytest.mark.parametrize("name,shape,n,depth", [("cavity_40", (24, 24, 40), 2, 1),
+                                                ("lossy_256", (32, 32, 48), 3, 1),
+                                                ("lossy_256", (32, 32, 48), 3, 4)])
+def test_stacked_chain_built_per_slab_equals_single_domain(name, shape, n, depth):
     """The weak-scaling workload of the slab decomposition: a chain of n
     workload blocks along z.  Each slab built on its own (the chain's edges
     for its planes, masks evaluated locally, internal ends without mask or
     PML), stepped with the fused beam and the ghost exchange, equals the
-    single-domain chain value for value after 300 steps."""
+    single-domain chain value for value after 300 steps (with 4 ghost planes
+    per side the lossy slabs run their steps two per launch between
+    exchanges every 4 steps)."""
     from wakis_b200 import workloads
     _, w, s1 = workloads.build_stacked(name, n, shape=shape)
-    lay = slab.layout(s1.Nz, n)
+    lay = slab.layout(s1.Nz, n, depth)
     solvers = {sl.index: workloads.build_stacked(name, n, shape=shape,
                                                  planes=(sl.lo, sl.hi))[2] for sl in lay}
     for so in solvers.values():
@@ -291,9 +311,10 @@ def test_stacked_chain_built_per_slab_equals_single_domain(name, shape, n):
     steps = 300
     s1._advance(steps, 0, beam=bp)
     ex = slab.LocalExchange()
-    for k in range(steps):
+    for k in range(0, steps, depth):
+        c = min(depth, steps - k)
         for so in solvers.values():
-            so._advance(1, k, beam=bp)
+            so._advance(c, k, beam=bp)
         ex(lay, solvers)
     nxy = s1.Nx * s1.Ny
     Eg = s1.E.numpy().reshape(3, s1.Nz, nxy)

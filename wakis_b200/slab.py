@@ -9,9 +9,14 @@ plane of H to the +z neighbour and of E to the -z neighbour
 step on its own planes plus ghost planes, and ONE exchange per step
 refreshes the ghosts:
 
-* a slab owning the planes [k0, k1) holds [lo, hi) = [max(k0-2, 0),
-  min(k1+2, Nz)); planes k0-1 and k1 are ghosts carrying the neighbours'
-  values, planes k0-2 and k1+1 are padding whose values are never used;
+* a slab owning the planes [k0, k1) holds [lo, hi) = [max(k0-G-1, 0),
+  min(k1+G+1, Nz)) for an exchange every G steps (the ghost depth, 1 by
+  default); planes k0-G .. k0-1 and k1 .. k1+G-1 are ghosts carrying the
+  neighbours' values, planes k0-G-1 and k1+G are padding whose values are
+  never used.  A step spreads what a plane depends on by one plane each
+  way, so G ghost planes carry the owned planes through G steps, and the
+  slab runs G steps per call (two steps per launch where the
+  temporal-blocking kernel applies, at G = 4);
 * the step forms H of ghost plane k0-1 from E(k0-1) and E(k0), both
   current, so E(k0) reads the right new H(k0-1) without a mid-step
   exchange; H(k1-1) reads E(k1) from the upper ghost;
@@ -23,9 +28,9 @@ refreshes the ghosts:
   faces are PEC-like runs the single-launch full-domain TMA kernel; the
   summation order of the H rows stays the global one.
 
-After each step the ghost planes receive the neighbours' new E and H (and,
-with precision="fp32c", their compensation words), so the fields equal the
-single-domain run value for value.  The material ids and the z-dependent
+After every G steps the ghost planes receive the neighbours' new E and H
+(and, with precision="fp32c", their compensation words), so the fields
+equal the single-domain run value for value.  The material ids and the z-dependent
 metric tables are slices of the global compact coefficient set, built once
 on the host; the time step is the global one.
 
@@ -60,23 +65,32 @@ def partition(Nz, n):
 
 @dataclass(frozen=True)
 class Slab:
-    """Slab r: owned planes [k0, k1), held planes [lo, hi) of Nz."""
+    """Slab r: owned planes [k0, k1), held planes [lo, hi) of Nz, ghost
+    depth (planes exchanged, steps between exchanges) `depth`."""
     index: int
     k0: int
     k1: int
     lo: int
     hi: int
+    depth: int = 1
 
     @property
     def n_local(self):
         return self.hi - self.lo
 
 
-def layout(Nz, n):
+def layout(Nz, n, depth=1):
     """The slabs of an n-way split of Nz planes (ghost and padding planes
-    included in [lo, hi))."""
-    return [Slab(r, k0, k1, max(k0 - 2, 0), min(k1 + 2, Nz))
-            for r, (k0, k1) in enumerate(partition(Nz, n))]
+    included in [lo, hi)) for an exchange every `depth` steps; every slab
+    owns at least `depth` planes."""
+    depth = int(depth)
+    if depth < 1:
+        raise ValueError(f"ghost depth {depth}")
+    parts = partition(Nz, n)
+    if n > 1 and min(k1 - k0 for k0, k1 in parts) < depth:
+        raise ValueError(f"slabs of {Nz} planes / {n} own fewer than {depth} planes")
+    return [Slab(r, k0, k1, max(k0 - depth - 1, 0), min(k1 + depth + 1, Nz), depth)
+            for r, (k0, k1) in enumerate(parts)]
 
 
 def slice_coefficients(c, lo, hi):
@@ -134,21 +148,28 @@ class LocalExchange:
 
     def __call__(self, slabs, solvers):
         for a, b in zip(slabs[:-1], slabs[1:]):
+            G = a.depth
             pa, pb = _planes(solvers[a.index]), _planes(solvers[b.index])
             for fa, fb in zip(pa, pb):
-                # last owned plane of a -> lower ghost of b; first owned plane
-                # of b -> upper ghost of a
-                fb[:, a.k1 - 1 - b.lo].copy_(fa[:, a.k1 - 1 - a.lo], non_blocking=True)
-                fa[:, b.k0 - a.lo].copy_(fb[:, b.k0 - b.lo], non_blocking=True)
+                # last G owned planes of a -> lower ghosts of b; first G owned
+                # planes of b -> upper ghosts of a
+                fb[:, a.k1 - G - b.lo:a.k1 - b.lo].copy_(fa[:, a.k1 - G - a.lo:a.k1 - a.lo],
+                                                         non_blocking=True)
+                fa[:, b.k0 - a.lo:b.k0 + G - a.lo].copy_(fb[:, b.k0 - b.lo:b.k0 + G - b.lo],
+                                                         non_blocking=True)
 
 
 class DistExchange:
     """Ghost-plane exchange with the neighbouring ranks through
     torch.distributed point-to-point messages (NCCL over NVLink between GPUs,
-    gloo on CPU): rank r holds slab r, sends its first owned plane down and
-    its last owned plane up, and receives its two ghost planes.  The sends
-    and receives of a step go out as one batch (``batch_isend_irecv``), so
-    the order in which neighbours post them cannot deadlock."""
+    gloo on CPU): rank r holds slab r, sends its first G owned planes down
+    and its last G owned planes up, and receives its ghost planes.  Each
+    message is one field component over G consecutive planes, a contiguous
+    range of the state buffer itself: nothing is packed, copied or
+    allocated per exchange (the message lists of the two ping-pong buffers
+    are built once).  The sends and receives of an exchange go out as one
+    batch (``batch_isend_irecv``), so the order in which neighbours post
+    them cannot deadlock."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
@@ -156,30 +177,37 @@ class DistExchange:
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
+        self._ops = {}
 
     def _global(self, r):
         return self.dist.get_global_rank(self.group, r) if self.group is not None else r
 
+    def _op_list(self, s, solver):
+        key = (id(solver), solver._par, s.depth)
+        ops = self._ops.get(key)
+        if ops is None:
+            dist, G = self.dist, s.depth
+            ops = []
+            for f in _planes(solver):
+                for d in range(f.shape[0]):
+                    for nb, send0, recv0 in ((s.index - 1, s.k0, s.k0 - G),
+                                             (s.index + 1, s.k1 - G, s.k1)):
+                        if nb < 0 or nb >= self.world:
+                            continue
+                        peer = self._global(nb)
+                        snd = f[d, send0 - s.lo:send0 - s.lo + G]
+                        rcv = f[d, recv0 - s.lo:recv0 - s.lo + G]
+                        ops.append(dist.P2POp(dist.isend, snd, peer, self.group))
+                        ops.append(dist.P2POp(dist.irecv, rcv, peer, self.group))
+            self._ops[key] = ops
+        return ops
+
     def __call__(self, slabs, solvers):
         if self.world == 1:
             return
-        dist = self.dist
         s = slabs[self.rank]
-        ops, unpack = [], []
-        for f in _planes(solvers[self.rank]):
-            for nb, k_send, k_recv in ((s.index - 1, s.k0, s.k0 - 1), (s.index + 1, s.k1 - 1, s.k1)):
-                if nb < 0 or nb >= self.world:
-                    continue
-                snd = f[:, k_send - s.lo].contiguous()
-                rcv = torch.empty_like(snd)
-                peer = self._global(nb)
-                ops.append(dist.P2POp(dist.isend, snd, peer, self.group))
-                ops.append(dist.P2POp(dist.irecv, rcv, peer, self.group))
-                unpack.append((f, k_recv - s.lo, rcv, snd))
-        for req in dist.batch_isend_irecv(ops):
+        for req in self.dist.batch_isend_irecv(self._op_list(s, solvers[self.rank])):
             req.wait()
-        for f, k, rcv, _ in unpack:
-            f[:, k].copy_(rcv)
 
 
 class SlabWakeSolve:
@@ -191,13 +219,16 @@ class SlabWakeSolve:
     device) and the ghost planes are copied device to device; without it and
     with torch.distributed initialised, rank r of ``group`` steps slab r on
     its current CUDA device and the ghosts travel as point-to-point messages.
+    ``depth``: ghost planes per side = steps between exchanges (4: the slabs
+    run their steps in pairs per launch where the temporal-blocking kernel
+    applies).
     """
 
     def __init__(self, grid, wake=None, n_slabs=None, group=None, cfln=0.5, dt=None,
                  bc_low=("Periodic", "Periodic", "Periodic"),
                  bc_high=("Periodic", "Periodic", "Periodic"), use_stl=False, use_sibc=True,
                  fmax=None, dtype=np.float64, n_pml=10, bg=(1.0, 1.0), precision=None,
-                 devices=None, verbose=0):
+                 devices=None, verbose=0, depth=1):
         from .solverFIT3D import SolverFIT3D
         self.grid, self.wake = grid, wake
         self.Nx, self.Ny, self.Nz = grid.Nx, grid.Ny, grid.Nz
@@ -213,7 +244,8 @@ class SlabWakeSolve:
             self.exchange = LocalExchange()
             n = int(n_slabs)
             mine = list(range(n))
-        self.slabs = layout(self.Nz, n)
+        self.slabs = layout(self.Nz, n, depth)
+        self.depth = int(depth)
         self.mine = mine
         if fmax is None:
             fmax = wake.fmax if wake is not None else 1e9
@@ -240,16 +272,24 @@ class SlabWakeSolve:
         self.z = grid.z[:-1] + grid.dz / 2
 
     # ----------------------------------------------------------- stepping
-    def _step(self, n, beam=None, captures=None):
+    def _block(self, n0, count, beam=None, captures=None):
+        """Steps n0 .. n0+count-1 (count <= depth) of every slab, then the
+        exchange."""
         for r in self.mine:
             cap = captures[r] if captures is not None else None
-            self.solvers[r]._advance(1, n, beam=beam, capture=cap)
+            self.solvers[r]._advance(count, n0, beam=beam, capture=cap)
         self.exchange(self.slabs, self.solvers)
+
+    def _steps(self, n0, n_steps, beam=None, captures=None):
+        n = n0
+        while n < n0 + n_steps:
+            c = min(self.depth, n0 + n_steps - n)
+            self._block(n, c, beam, captures)
+            n += c
 
     def run(self, n_steps, step0=0, beam=None):
         """n_steps steps (optionally with the fused beam parameters)."""
-        for n in range(step0, step0 + n_steps):
-            self._step(n, beam)
+        self._steps(step0, n_steps, beam)
         for r in self.mine:
             self.solvers[r].check_status(f"SlabWakeSolve.run (slab {r})")
 
@@ -314,8 +354,7 @@ class SlabWakeSolve:
         ev1 = torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
         ev0.record()
-        for n in range(Nt):
-            self._step(n, bp, caps)
+        self._steps(0, Nt, bp, caps)
         ev1.record()
         for d in devs:
             torch.cuda.synchronize(d)
