@@ -729,9 +729,9 @@ def main():
                     help="skip the FP32-compensated leg of the default FP64 run")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "twopass", "cell", "split"])
     ap.add_argument("--tile", default="0x0", help="rows x planes per block (0 = auto)")
-    ap.add_argument("--steps-per-launch", type=int, default=0, choices=[0, 1],
-                    help="0: two steps per launch (temporal blocking) where it applies; "
-                         "1: one step per launch")
+    ap.add_argument("--steps-per-launch", type=int, default=0, choices=[0, 1, 2],
+                    help="2: two steps per launch (temporal blocking) where it applies; "
+                         "1: one step per launch; 0: the library's default (one)")
     ap.add_argument("--shape", default=None,
                     help="override the grid, e.g. 128x128x256 (profiling runs)")
     ap.add_argument("--accuracy", action="store_true",
@@ -756,8 +756,8 @@ def main():
                          "rank with the z-slab ghost exchange over NCCL (default), or "
                          "independent replicas")
     ap.add_argument("--slab-depth", type=int, default=4,
-                    help="z-slab ghost planes per side = steps between exchanges (4: the "
-                         "slabs run two steps per launch)")
+                    help="z-slab ghost planes per side = steps between exchanges (fewer, "
+                         "larger messages as it grows)")
     ap.add_argument("--batch-compare", action="store_true",
                     help="also run the batch in FP64 and report per-instance WP/|Z| errors")
     args = ap.parse_args()
@@ -852,7 +852,7 @@ def main():
     # schedules launch a fixed set
     fixed = {"split": 4, "cell": 1}
     # the TMA schedule needs no shell launch when every face is PEC-masked;
-    # there the default runs two steps per launch (k_tma2) where it applies,
+    # with --steps-per-launch 2 it runs pairs of steps as one launch (k_tma2),
     # so fewer interior launches than steps
     pec_faces = all(b.lower() in ("pec", "electric", "pml") for b in s.bc_low + s.bc_high)
     two_step = pec_faces and 0 < n_int < args.steps

@@ -143,11 +143,14 @@ typedef struct wk_fit_desc {
    * loads it issued and returns (a test of the timeout path, which leaves
    * the output of the step incomplete).                                   */
   long long wait_ns;
-  /* Steps per launch of the TMA schedule: 0 (the default) = two steps per
-   * launch (temporal blocking, k_tma2) where that kernel applies (every face
+  /* Steps per launch of the TMA schedule: 2 = two steps per launch
+   * (temporal blocking, k_tma2) where that kernel applies (every face
    * PEC-masked, faces_clean, J = 0 without conductivity or sigma*E with it,
-   * no step_dev) and n_steps >= 4, else one; 1 = always one.  The result
-   * and its buffer parity do not depend on it.                            */
+   * no step_dev) and n_steps >= 4, else one; 1 = always one; 0 (the
+   * default) = the faster on B200 for the state type: one step per launch
+   * for FP64 and FP32 (k_tma2 halves the DRAM bytes but issues more
+   * instructions per cell at a lower occupancy).  The result and its buffer
+   * parity do not depend on it.                                            */
   int steps_per_launch;
 } wk_fit_desc;
 

@@ -45,7 +45,7 @@ def _valid(idx):
 VALID = [i for i in range(len(cases.STEP_CASES)) if _valid(i)]
 
 
-SCHEDULES = {"auto": ("auto", (0, 0)), "tma": ("tma", (0, 0)), "tma1": ("tma", (0, 1)),
+SCHEDULES = {"auto": ("auto", (0, 0)),
              "twopass": ("twopass", (0, 0)), "twopass2": ("twopass", (0, 2)),
              "twopass4": ("twopass", (0, 4)), "cell": ("cell", (0, 0)), "split": None}
 

@@ -263,7 +263,9 @@ def test_sibc_pillbox_in_batched_run_matches_upstream(golden_dir):
     b.run()
     # the batch sets each wakelength from the step count (same Nt, another
     # s axis end): integrate the same history on the case's wakelength
+    # (the bunch profile is formed again on that axis)
     w.wakelength = c["wakelength"]
+    w.lambdas = None
     w.solve("both")
     _sibc_wake_check(w, s, g)
 
@@ -314,7 +316,7 @@ def test_two_steps_per_launch_equal_one(shape, dtype, tile):
     from wakis_b200.sources import Beam
     sp = workloads.spec("lossy_256")
     out = []
-    for spl in (0, 1):
+    for spl in (2, 1):
         _, _, s = workloads.build_b200("lossy_256", shape=shape, dtype=dtype)
         s.steps_per_launch = spl
         s.tile = (0, tile)
@@ -341,7 +343,7 @@ def test_two_steps_per_launch_non_conductive():
     from wakis_b200.sources import Beam
     c = cases.WAKE_CASES[0]
     out = []
-    for spl in (0, 1):
+    for spl in (2, 1):
         g = wb.GridFIT3D(*c["bounds"], *c["shape"], verbose=0)
         g.add_solid("cav", cases.wake_mask(c, g.x, g.y, g.z), c["material"])
         s = wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], use_stl=True,
@@ -356,7 +358,7 @@ def test_two_steps_per_launch_non_conductive():
 
 
 def test_two_steps_per_launch_matches_oracle():
-    """The default path (now two steps per launch) on the lossy geometry at
+    """Two steps per launch (steps_per_launch = 2) on the lossy geometry at
     64x64x128 from seeded random fields with clean faces: the face entries
     of the random E are zeroed first, then the faces are marked clean; 40
     steps against the oracle within 1e-12."""
@@ -383,6 +385,7 @@ def test_two_steps_per_launch_matches_oracle():
     s.E.fromarray(E0)
     s.H.fromarray(H0)
     s._faces_clean = True
+    s.steps_per_launch = 2
     bkw = _short_beam(sp)
     timing = []
     s._advance(40, 0, beam=Beam(**bkw).params(s), timing=timing)

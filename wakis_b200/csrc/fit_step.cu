@@ -108,7 +108,7 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
     int s = 0;
     // two steps per launch where k_tma2 applies; an even number of such
     // launches keeps the result in E[par ^ (n_steps & 1)]
-    if (d->steps_per_launch != 1 && !d->step_dev && n_steps >= 4 &&
+    if (d->steps_per_launch == 2 && !d->step_dev && n_steps >= 4 &&
         tma2_supported<T>(make_params<T>(d, par))) {
       const int pairs = (n_steps / 4) * 2;
       for (int q = 0; q < pairs; q++, s += 2) {

@@ -15,8 +15,9 @@ refreshes the ghosts:
   neighbours' values, planes k0-G-1 and k1+G are padding whose values are
   never used.  A step spreads what a plane depends on by one plane each
   way, so G ghost planes carry the owned planes through G steps, and the
-  slab runs G steps per call (two steps per launch where the
-  temporal-blocking kernel applies, at G = 4);
+  slab runs G steps per call (G >= 4 lets the solver's steps_per_launch = 2
+  run them in pairs per launch of the temporal-blocking kernel); larger G
+  means fewer, larger messages and G + 1 extra planes computed per side;
 * the step forms H of ghost plane k0-1 from E(k0-1) and E(k0), both
   current, so E(k0) reads the right new H(k0-1) without a mid-step
   exchange; H(k1-1) reads E(k1) from the upper ghost;
@@ -219,9 +220,7 @@ class SlabWakeSolve:
     device) and the ghost planes are copied device to device; without it and
     with torch.distributed initialised, rank r of ``group`` steps slab r on
     its current CUDA device and the ghosts travel as point-to-point messages.
-    ``depth``: ghost planes per side = steps between exchanges (4: the slabs
-    run their steps in pairs per launch where the temporal-blocking kernel
-    applies).
+    ``depth``: ghost planes per side = steps between exchanges.
     """
 
     def __init__(self, grid, wake=None, n_slabs=None, group=None, cfln=0.5, dt=None,

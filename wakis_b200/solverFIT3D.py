@@ -192,8 +192,9 @@ class SolverFIT3D(RoutinesMixin):
         self._desc = d
         self.kernel = "auto"
         self.tile = (0, 0)
-        # 0: two steps per launch where the temporal-blocking kernel applies
-        # (wk_fit_desc.steps_per_launch), 1: one step per launch
+        # wk_fit_desc.steps_per_launch: 2 runs pairs of steps as one launch of
+        # the temporal-blocking kernel where it applies, 1 one step per
+        # launch, 0 the faster on B200 (one step per launch)
         self.steps_per_launch = 0
 
     def _stream(self):
@@ -376,9 +377,10 @@ class SolverFIT3D(RoutinesMixin):
             td = self._cap_dtype
             bufs = (torch.empty((chunk, nz), dtype=td, device=self.device),
                     {c: torch.empty((9, nz, c), dtype=td, device=self.device)
-                     for c in range(1, chunk + 1)})
+                     for c in range(1, chunk + 1)},
+                    torch.empty((chunk, 9, nz), dtype=td, device=self.device))
             self._io_bufs = bufs
-        lbuf, cbufs = bufs
+        lbuf, cbufs, stage = bufs
         n = 0
         while n < n_steps:
             c = min(chunk, n_steps - n)
@@ -387,7 +389,13 @@ class SolverFIT3D(RoutinesMixin):
             lb.copy_(jz_lines[n:n + c], non_blocking=True)
             self._advance(c, step0 + n, line=(lb, step0 + n, ixs, iys),
                           capture=(cbuf, ixt - 1, iyt - 1, 3, 3, step0 + n))
-            ez_out[n:n + c].copy_(cbuf.permute(2, 0, 1), non_blocking=True)
+            if c == 1:
+                ez_out[n].copy_(cbuf.view(9, nz), non_blocking=True)
+            else:
+                # step-major on the device first, so the copy down is one
+                # contiguous block
+                stage[:c].copy_(cbuf.permute(2, 0, 1))
+                ez_out[n:n + c].copy_(stage[:c], non_blocking=True)
             n += c
         self.check_status("run_with_io")
 
