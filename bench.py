@@ -368,13 +368,17 @@ def run_batch(args):
 def run_adjoint(args):
     """Differentiation form (rank 0 only).  The cavity_40 geometry on
     128x128x256 cells (PEC walls) with a central 64^3 design region of
-    per-cell eps_r ~ U[1, 10] and sigma ~ U[0, 10] S/m (seed 1); loss =
-    int_{0.5}^{3 GHz} |Z_par|^2 df; forward + adjoint in FP64, FP32,
-    FP32-compensated forward with an FP64 adjoint and FP32-compensated
-    forward with an FP32 adjoint, with sqrt(N)-step checkpoints; 16 random
-    directions checked against central
-    differences of FP64 forward runs (Richardson-extrapolated from steps
-    1e-3 and 5e-4 along the direction)."""
+    per-cell eps_r ~ U[1, 10] and sigma ~ U[0, --adjoint-sigma-max] S/m (seed
+    1; 1e3 as the configuration states); loss = int_{0.5}^{3 GHz} |Z_par|^2
+    df; forward + adjoint in FP64, FP32, FP32-compensated forward (TMA
+    kernel, float update factors) with an FP64 or FP32 adjoint, and the
+    FP32-compensated forward of the two-pass kernels (update factors formed
+    in FP64 per cell), with sqrt(N)-step checkpoints; 16 random directions
+    checked against central differences of FP64 forward runs
+    (Richardson-extrapolated from steps 1e-3 and 5e-4 along the direction).
+    The time step is upstream's for the seeded parameters: the CFL step,
+    clamped to the smallest relaxation time eps_0 eps_r / sigma of the design
+    cells (solverFIT3D.py:301-310), fixed for every evaluation."""
     ws, rank, local = _dist()
     if rank != 0:
         return
@@ -383,12 +387,14 @@ def run_adjoint(args):
     from wakis_b200 import workloads
     from wakis_b200.adjoint import ImpedanceDesign
     shape = tuple(int(v) for v in args.shape.split("x")) if args.shape else (128, 128, 256)
-    nsteps = args.adjoint_steps
     rng = np.random.default_rng(1)
+    smax = float(args.adjoint_sigma_max)
+    dt_fixed = [None]
 
-    def problem(dtype, precision=None, adjoint_dtype=None):
+    def problem(dtype, precision=None, adjoint_dtype=None, kernel="auto"):
         _, _, s = workloads.build_b200("cavity_40", dtype=dtype, shape=shape,
-                                       precision=precision)
+                                       precision=precision, dt=dt_fixed[0])
+        s.kernel = kernel
         m = np.zeros(shape, bool)
         c = [n // 2 for n in shape]
         h = [min(32, n // 4) for n in shape]
@@ -397,15 +403,39 @@ def run_adjoint(args):
                 int(m.sum()))
 
     runs = {}
-    forms = (("f64", np.float64, None, None), ("f32", np.float32, None, None),
-             ("fp32c", np.float64, "fp32c", None), ("fp32c_adj32", np.float64, "fp32c", np.float32))
-    for name, dt_, prec, adt in forms:
+    forms = (("f64", np.float64, None, None, "auto"), ("f32", np.float32, None, None, "auto"),
+             ("fp32c", np.float64, "fp32c", None, "auto"),
+             ("fp32c_adj32", np.float64, "fp32c", np.float32, "auto"),
+             ("fp32c_f64coef", np.float64, "fp32c", None, "twopass"))
+    # the seeded parameters and upstream's time step for them
+    _, _, s_cfl = workloads.build_b200("cavity_40", shape=shape)
+    dt_cfl = float(s_cfl.dt)
+    del s_cfl
+    m0 = np.zeros(shape, bool)
+    c0 = [n // 2 for n in shape]
+    h0 = [min(32, n // 4) for n in shape]
+    m0[c0[0] - h0[0]:c0[0] + h0[0], c0[1] - h0[1]:c0[1] + h0[1], c0[2] - h0[2]:c0[2] + h0[2]] = True
+    nd0 = int(m0.sum())
+    er = rng.uniform(1.0, 10.0, nd0)
+    sg = rng.uniform(0.0, smax, nd0)
+    pos = sg > 0
+    tau = (er[pos] * 8.8541878128e-12) / sg[pos]
+    dt_fixed[0] = min(dt_cfl, float(tau.min())) if pos.any() else dt_cfl
+    # steps: as given, else 4000 (the configuration) or, when the clamp
+    # shortens dt so much that 4000 steps do not carry the bunch through the
+    # domain, the steps for 2000 wake samples behind it
+    nsteps = args.adjoint_steps
+    if nsteps <= 0:
+        sp = workloads.spec("cavity_40")
+        v = 299792458.0 * sp["wake"]["beta"]
+        span = workloads.BOUNDS[5] - workloads.BOUNDS[4]
+        ti_v = 8.548921333333334 * sp["wake"]["sigmaz"]
+        need = int(np.ceil((span + ti_v + 2000 * v * dt_fixed[0]) / (v * dt_fixed[0])))
+        nsteps = max(4000, need) if dt_fixed[0] < dt_cfl else 4000
+    for name, dt_, prec, adt, kern in forms:
         t0 = time.perf_counter()
-        prob, nd = problem(dt_, prec, adt)
+        prob, nd = problem(dt_, prec, adt, kern)
         t_setup = time.perf_counter() - t0
-        if name == "f64":
-            er = rng.uniform(1.0, 10.0, nd)
-            sg = rng.uniform(0.0, 10.0, nd)
         prob.set_params(er, sg)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -443,7 +473,10 @@ def run_adjoint(args):
             errs[name].append(abs(ad - fd) / abs(fd) if fd else abs(ad))
     line = {"metric": "adjoint gradient vs central differences (relative)", "grid": list(shape),
             "design_cells": nd, "steps": nsteps, "data": "synthetic",
-            "sigma_range": [0.0, 10.0], "eps_r_range": [1.0, 10.0],
+            "sigma_range": [0.0, smax], "eps_r_range": [1.0, 10.0],
+            "dt": dt_fixed[0], "dt_cfl": dt_cfl,
+            "dt_policy": "CFL step clamped to the smallest eps_0 eps_r / sigma of the seeded "
+                         "design cells (upstream's clamp), fixed for every evaluation",
             "fd": "FP64 forward runs, Richardson-extrapolated central differences"}
     for name, r in runs.items():
         line[name] = {"loss": r["L"], "grad_rel_err_max": max(errs[name]),
@@ -747,7 +780,11 @@ def main():
                          "FP64 / FP32 / FP32-compensated forward + adjoint (4000 steps), "
                          "gradient checked on 16 random "
                          "directions against central differences of FP64 forward runs")
-    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--adjoint-steps", type=int, default=0,
+                    help="steps of the differentiation form (0: 4000, or enough for the wake "
+                         "when the relaxation clamp shortens dt)")
+    ap.add_argument("--adjoint-sigma-max", type=float, default=1e3,
+                    help="design-cell sigma ~ U[0, this] S/m (1e3: the configuration)")
     ap.add_argument("--slabs", type=int, default=0,
                     help="z-slab decomposition on one GPU: the workload split into this many "
                          "z-slabs in one process (ghost planes copied every step)")

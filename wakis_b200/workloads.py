@@ -57,8 +57,9 @@ def cavity_mask(x, y, z):
     return geometry.cell_mask(cavity_shape(), x, y, z)
 
 
-def build_b200(name, dtype=np.float64, shape=None, precision=None):
-    """(grid, wake, solver) of a workload on the device."""
+def build_b200(name, dtype=np.float64, shape=None, precision=None, dt=None):
+    """(grid, wake, solver) of a workload on the device (``dt``: a given time
+    step instead of the CFL one, as SolverFIT3D's argument)."""
     from .gridFIT3D import GridFIT3D
     from .solverFIT3D import SolverFIT3D
     from .wakeSolver import WakeSolver
@@ -72,7 +73,7 @@ def build_b200(name, dtype=np.float64, shape=None, precision=None):
                                                  g.x, g.y, g.z), ins["material"])
     w = WakeSolver(save=False, verbose=0, **sp["wake"])
     s = SolverFIT3D(g, w, bc_low=sp["bc_low"], bc_high=sp["bc_high"], use_stl=True, bg=sp["bg"],
-                    dtype=dtype, n_pml=sp["n_pml"], verbose=0, precision=precision)
+                    dtype=dtype, n_pml=sp["n_pml"], verbose=0, precision=precision, dt=dt)
     return g, w, s
 
 
