@@ -375,6 +375,26 @@ int wk_trans_wake_scan(const double* WP3d, int ns, double ds, double dxsum, doub
                        void* stream);
 
 /*
+ * wk_trans_wake_scan without caller scratch, for callers that cannot hand
+ * this library device memory of its own: a host program whose device
+ * memory is all reserved up front by another allocator (a framework's
+ * caching pool, a fixed per-process budget) or a plugin loaded into such a
+ * program, where a cudaMalloc here would fail or break the owner's
+ * accounting.  This entry point allocates nothing: its segment sums live in
+ * a 256 KiB array built into the library, which every GPU that loads the
+ * library holds until the process exits.  The caller still passes WP3d,
+ * WPx and WPy.  ns above 4096 * 65536 samples is rejected (WK_E_RANGE).
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array and it keeps the
+ * last call's segment sums (each call writes every sum it reads before
+ * reading it): calls that overlap on one GPU, on different streams, race on
+ * it (each GPU has its own copy).  No counterpart in the reference.
+ */
+int wk_trans_wake_scan_noalloc(const double* WP3d, int ns, double ds, double dxsum,
+                               double dysum, double* WPx, double* WPy, void* stream);
+
+/*
  * Zero-padded DFT bins X[m] = sum_{n<len} x[n] * exp(-2*pi*i*m*n/N) for
  * m = 0..nbins-1 (the bins 0 <= f < fmax of np.fft.fft(x, n=N) kept by
  * calc_long_Z / calc_trans_Z, wakis/wakeSolver.py:679-766), for `nsig`

@@ -75,6 +75,7 @@ _SIGS = {
     "wk_wake_finalize": (_i, [_vp, _i, _i, _i, _d, _vp, _vp]),
     "wk_trans_wake_scan_scratch_bytes": (_ll, [_i]),
     "wk_trans_wake_scan": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp, _ll, _vp]),
+    "wk_trans_wake_scan_noalloc": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -11,6 +11,8 @@
 //                    (calc_long_Z / calc_trans_Z, 679-766) as a direct DFT.
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/wakis_b200.h"
 #include "abi_internal.h"
 
@@ -467,4 +469,54 @@ extern "C" int wk_trans_wake_scan(const double* WP3d, int ns, double ds, double 
                    scratch_bytes, need);
   return trans_scan_launch(WP3d, ns, ds, dxsum, dysum, WPx, WPy, (DD*)scratch, 1 << 20,
                            (cudaStream_t)stream, "wk_trans_wake_scan");
+}
+
+// ------------------------------------------------- without allocation ----
+// wk_trans_wake_scan_noalloc keeps its segment sums in this file-scope
+// device array instead of caller memory.  Every GPU that loads the library
+// holds it (kNoAllocSegments x 4 double-double sums = 256 KiB) until the
+// process exits; all calls share it.
+constexpr int kNoAllocSegments = 4096;
+constexpr long long kNoAllocMaxSamples = (long long)kNoAllocSegments * 65536;
+static __device__ __align__(256) DD g_trans_scratch[kNoAllocSegments * 4];
+
+// Device address of g_trans_scratch, looked up once per device (in host
+// code the symbol names a host-side stand-in, not device memory).
+static constexpr int kMaxDevices = 64;
+static DD* g_trans_scratch_dev[kMaxDevices];
+static cudaError_t g_trans_scratch_err[kMaxDevices];
+static std::once_flag g_trans_scratch_once[kMaxDevices];
+
+extern "C" int wk_trans_wake_scan_noalloc(const double* WP3d, int ns, double ds, double dxsum,
+                                          double dysum, double* WPx, double* WPy,
+                                          void* stream) {
+  if (!WP3d || !WPx || !WPy)
+    return wk_fail(WK_E_NULL, "wk_trans_wake_scan_noalloc: NULL pointer");
+  if (ns < 0) return wk_fail(WK_E_RANGE, "wk_trans_wake_scan_noalloc: ns %d", ns);
+  if ((long long)ns > kNoAllocMaxSamples)
+    return wk_fail(WK_E_RANGE,
+                   "wk_trans_wake_scan_noalloc: %d samples is above this entry point's "
+                   "maximum of %lld (its built-in scratch holds %d segment sums of at most "
+                   "65536 samples each); use wk_trans_wake_scan with caller scratch",
+                   ns, kNoAllocMaxSamples, kNoAllocSegments);
+  if (ns == 0) return WK_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return wk_fail(-(int)e, "wk_trans_wake_scan_noalloc: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return wk_fail(WK_E_RANGE, "wk_trans_wake_scan_noalloc: device %d", dev);
+  std::call_once(g_trans_scratch_once[dev], [dev] {
+    void* ptr = nullptr;
+    g_trans_scratch_err[dev] = cudaGetSymbolAddress(&ptr, g_trans_scratch);
+    g_trans_scratch_dev[dev] = static_cast<DD*>(ptr);
+  });
+  if (g_trans_scratch_err[dev] != cudaSuccess || !g_trans_scratch_dev[dev])
+    return wk_fail(-(int)(g_trans_scratch_err[dev] != cudaSuccess ? g_trans_scratch_err[dev]
+                                                                  : cudaErrorInvalidSymbol),
+                   "wk_trans_wake_scan_noalloc: device address of the scratch array: %s",
+                   cudaGetErrorString(g_trans_scratch_err[dev]));
+  return trans_scan_launch(WP3d, ns, ds, dxsum, dysum, WPx, WPy, g_trans_scratch_dev[dev],
+                           kNoAllocSegments, (cudaStream_t)stream,
+                           "wk_trans_wake_scan_noalloc");
 }
