@@ -323,19 +323,23 @@ def run_batch(args):
 
     def run(precision, dtype):
         t0 = time.perf_counter()
-        built = [batch.build_pillbox(**q, precision=precision, dtype=dtype) for q in params]
+        built = [batch.build_pillbox(**q, precision=precision, dtype=dtype,
+                                     multiple=args.batch_multiple) for q in params]
         t_build = time.perf_counter() - t0
-        b = batch.BatchedWakeSolve([x[2] for x in built], args.batch_steps)
+        b = batch.BatchedWakeSolve([x[2] for x in built], args.batch_steps,
+                                   launch=args.batch_launch if precision else "graph",
+                                   form=args.batch_form)
         t1 = time.perf_counter()
         tm = b.run()
         t_run = time.perf_counter() - t1
         res = [(np.array(x[1].WP), np.array(x[1].Z)) for x in built]
         shapes = [(x[2].Nx, x[2].Ny, x[2].Nz) for x in built]
+        tuned = dict(b.tuned)
         del built, b
         torch.cuda.empty_cache()
-        return tm, res, shapes, t_build, t_run
+        return tm, res, shapes, t_build, t_run, tuned
 
-    tm, res, shapes, t_build, t_run = run(prec, dt)
+    tm, res, shapes, t_build, t_run, tuned = run(prec, dt)
     cells = tm["cells"]
     line = {"metric": METRIC, "value": tm["gcell_steps_per_s"], "unit": "Gcell-steps/s",
             "n_gpus": 1, "steps": args.batch_steps, "warmup": 0,
@@ -345,13 +349,18 @@ def run_batch(args):
             "data": "synthetic",
             "config": {"workload": f"batch_{args.batch}_pillboxes_seed0", "instances": args.batch,
                        "cells_total": cells, "grids_min": min(shapes), "grids_max": max(shapes),
-                       "graph": "2 steps of every instance per replay, 8 streams"},
+                       "transverse_multiple": args.batch_multiple,
+                       "launch": tm["launch"],
+                       "graph": ("device work list over all instances (wk_batch_run), a chunk "
+                                 "of steps captured once and replayed" if tm["launch"] == "batched"
+                                 else "2 steps of every instance per replay, 8 streams"),
+                       "tuned": tuned},
             "e2e": {"value": cells * args.batch_steps / t_run / 1e9, "unit": "Gcell-steps/s",
                     "note": "wall clock of the batched run incl. the wake integration",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "build_s": t_build}
     if args.batch_compare and prec == "fp32c":
-        tm64, res64, _, _, _ = run(None, np.float64)
+        tm64, res64, _, _, _, _ = run(None, np.float64)
 
         def rel(a, b):
             den = np.max(np.abs(b))
@@ -370,10 +379,11 @@ def run_adjoint(args):
     128x128x256 cells (PEC walls) with a central 64^3 design region of
     per-cell eps_r ~ U[1, 10] and sigma ~ U[0, --adjoint-sigma-max] S/m (seed
     1; 1e3 as the configuration states); loss = int_{0.5}^{3 GHz} |Z_par|^2
-    df; forward + adjoint in FP64, FP32, FP32-compensated forward (TMA
-    kernel, float update factors) with an FP64 or FP32 adjoint, and the
-    FP32-compensated forward of the two-pass kernels (update factors formed
-    in FP64 per cell), with sqrt(N)-step checkpoints; 16 random directions
+    df; forward + adjoint in FP64, FP32, and the FP32-compensated forward
+    (per-cell materials: the two-pass kernels) with the float stencil or the
+    compensated stencil (comp_stencil: neighbour values v + c, increments
+    formed with error-free float transformations), each with an FP64 or
+    FP32 adjoint, with sqrt(N)-step checkpoints; 16 random directions
     checked against central differences of FP64 forward runs
     (Richardson-extrapolated from steps 1e-3 and 5e-4 along the direction).
     The time step is upstream's for the seeded parameters: the CFL step,
@@ -391,10 +401,10 @@ def run_adjoint(args):
     smax = float(args.adjoint_sigma_max)
     dt_fixed = [None]
 
-    def problem(dtype, precision=None, adjoint_dtype=None, kernel="auto"):
+    def problem(dtype, precision=None, adjoint_dtype=None, comp_stencil=False):
         _, _, s = workloads.build_b200("cavity_40", dtype=dtype, shape=shape,
                                        precision=precision, dt=dt_fixed[0])
-        s.kernel = kernel
+        s.comp_stencil = comp_stencil
         m = np.zeros(shape, bool)
         c = [n // 2 for n in shape]
         h = [min(32, n // 4) for n in shape]
@@ -403,10 +413,11 @@ def run_adjoint(args):
                 int(m.sum()))
 
     runs = {}
-    forms = (("f64", np.float64, None, None, "auto"), ("f32", np.float32, None, None, "auto"),
-             ("fp32c", np.float64, "fp32c", None, "auto"),
-             ("fp32c_adj32", np.float64, "fp32c", np.float32, "auto"),
-             ("fp32c_f64coef", np.float64, "fp32c", None, "twopass"))
+    forms = (("f64", np.float64, None, None, False), ("f32", np.float32, None, None, False),
+             ("fp32c", np.float64, "fp32c", None, False),
+             ("fp32c_adj32", np.float64, "fp32c", np.float32, False),
+             ("fp32c_cs", np.float64, "fp32c", None, True),
+             ("fp32c_cs_adj32", np.float64, "fp32c", np.float32, True))
     # the seeded parameters and upstream's time step for them
     _, _, s_cfl = workloads.build_b200("cavity_40", shape=shape)
     dt_cfl = float(s_cfl.dt)
@@ -432,9 +443,9 @@ def run_adjoint(args):
         ti_v = 8.548921333333334 * sp["wake"]["sigmaz"]
         need = int(np.ceil((span + ti_v + 2000 * v * dt_fixed[0]) / (v * dt_fixed[0])))
         nsteps = max(4000, need) if dt_fixed[0] < dt_cfl else 4000
-    for name, dt_, prec, adt, kern in forms:
+    for name, dt_, prec, adt, cst in forms:
         t0 = time.perf_counter()
-        prob, nd = problem(dt_, prec, adt, kern)
+        prob, nd = problem(dt_, prec, adt, cst)
         t_setup = time.perf_counter() - t0
         prob.set_params(er, sg)
         torch.cuda.synchronize()
@@ -775,6 +786,13 @@ def main():
                     help="batched form: this many random pillbox cavities (seed 0) in "
                          "one captured CUDA graph, FP32c, --batch-steps steps each")
     ap.add_argument("--batch-steps", type=int, default=4000)
+    ap.add_argument("--batch-launch", default="auto", choices=["auto", "batched", "graph"],
+                    help="batched form: the device work list over all instances "
+                         "(wk_batch_run), or a graph of per-instance launches")
+    ap.add_argument("--batch-form", default="auto", choices=["auto", "persistent", "phases"],
+                    help="batched launch form (auto: chosen by the autotuner)")
+    ap.add_argument("--batch-multiple", type=int, default=8,
+                    help="batched form: transverse cell counts rounded up to this multiple")
     ap.add_argument("--adjoint", action="store_true",
                     help="differentiation form: 128x128x256 cavity with a 64^3 design region, "
                          "FP64 / FP32 / FP32-compensated forward + adjoint (4000 steps), "

@@ -152,6 +152,16 @@ typedef struct wk_fit_desc {
    * instructions per cell at a lower occupancy).  The result and its buffer
    * parity do not depend on it.                                            */
   int steps_per_launch;
+  /* WK_F32C only.  0 (the default): the rows read the float parts v of the
+   * neighbouring state and sum in float; the compensated add then keeps
+   * the state to ~32 bits, but each increment carries the rounding of a
+   * float row sum.  1: compensated stencil: the rows read the full pairs
+   * v + c, the update factors are split into two floats and the increment
+   * is formed with error-free float transformations (~44 bits), so that
+   * long runs whose increments are large against the state (conductive
+   * cells near the relaxation limit) follow the FP64 trajectory closely;
+   * runs the two-pass kernels (WK_KERNEL_TMA is refused).                  */
+  int comp_stencil;
 } wk_fit_desc;
 
 #define WK_KERNEL_AUTO 0   /* WK_KERNEL_TMA when its conditions hold, else
@@ -180,6 +190,68 @@ typedef struct wk_fit_desc {
  * counterpart in the reference.
  */
 int wk_counter_add(long long* ctr, long long inc, void* stream);
+
+/*
+ * Batched FP32-compensated stepping: many independent grids (each with its
+ * own shape, dt, materials, beam and Ez capture) advanced by ONE persistent
+ * cooperative launch per call.  Upstream runs one SolverFIT3D.wakesolve per
+ * geometry (wakis/routines.py:231-482, each step SolverFIT3D._one_step,
+ * wakis/solverFIT3D.py:482-503); the result of every instance equals that of
+ * wk_fit_step on its own descriptor.
+ *
+ * Every instance is WK_F32C, has its four x/y faces PEC-masked (face mode 1:
+ * all six faces; mode 2: the z faces are not, e.g. ABC, and the four
+ * z-boundary planes take the general rows), id_bytes 1 or 2, J mode
+ * WK_J_ZERO or WK_J_SIGMA_E, Nx % 4 == 0, at most 64 materials and
+ * step_dev == NULL; all instances share the face mode, id width and J mode.
+ * tile_planes of a descriptor sets the planes per work item (0 = 24).
+ *
+ * wk_batch_workspace_bytes: device bytes the plan needs (-1 on an argument
+ *   error, see wk_last_error).
+ * wk_batch_prepare: checks the descriptors (an array of n_inst structs),
+ *   encodes every instance's TMA descriptors for both buffer parities, forms
+ *   the work lists and copies all of it into `workspace` (caller-owned
+ *   device memory, 128-byte aligned, at least wk_batch_workspace_bytes),
+ *   then waits for `stream`.  The live parity of instance q at step t is
+ *   descs[q].par ^ ((t - t_ref) & 1).  Not for stream capture.
+ * wk_batch_run: advances every instance by n_steps steps, step indices
+ *   t = step0 + s (+ *step_dev when step_dev is not NULL, read on the device
+ *   when a launch starts, so captured launches can be replayed), on
+ *   `stream` (capturable).  plan->form WK_BATCH_PERSISTENT: one cooperative
+ *   launch whose blocks walk the work lists of every step, meeting at a
+ *   grid barrier after each phase; each barrier wait is bounded by
+ *   barrier_ns nanoseconds (<= 0: 2 s).  WK_BATCH_PHASES: up to four
+ *   launches per step (barrier_ns unused).  A wait or a tile load that runs
+ *   out sets the status word of the instance concerned (instance 0 for a
+ *   barrier) and the launch ends (wk_read_status).
+ * No counterpart in the reference.
+ */
+#define WK_BATCH_PERSISTENT 0   /* one cooperative launch per wk_batch_run  */
+#define WK_BATCH_PHASES 1       /* per step, one launch per list of items:
+                                   tiles (TMA-loaded compensation words),
+                                   tiles (per-thread loads), H rows of the
+                                   boundary planes, then their E rows       */
+typedef struct wk_batch_plan {
+  void* workspace;
+  long long workspace_bytes;
+  int n_inst;
+  int n_items[2];          /* work items of the two phases of a step         */
+  int grid;                /* persistent blocks (SMs x blocks per SM)        */
+  int smem;                /* dynamic shared memory per block                */
+  int variant;             /* kernel instantiation                           */
+  int device;
+  long long offsets[4];    /* instances, TMA descriptors, items (two phases) */
+  int n_parts[3];          /* phase-A items: TMA-word tiles, other tiles,
+                              boundary-plane H rows                          */
+  int form;                /* WK_BATCH_PERSISTENT (set by wk_batch_prepare)
+                              or WK_BATCH_PHASES; the caller may change it  */
+} wk_batch_plan;
+
+long long wk_batch_workspace_bytes(const wk_fit_desc* descs, int n_inst);
+int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long t_ref, void* workspace,
+                     long long workspace_bytes, wk_batch_plan* plan, void* stream);
+int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long step0,
+                 const long long* step_dev, long long barrier_ns, void* stream);
 
 /*
  * Adjoint (reverse-mode) FIT step, used for gradients of a wake/impedance

@@ -60,16 +60,18 @@ def test_wake_args_rejected(lib):
     assert lib.wk_dft_bins(None, 1, 1, 1, 1, None, None) == 1
 
 
-def test_descriptor_layout_matches_header(tmp_path):
-    """ctypes FitDesc offsets equal the C struct's (gcc offsetof)."""
+@pytest.mark.parametrize("cname,ctype", [("wk_fit_desc", _native.FitDesc),
+                                          ("wk_batch_plan", _native.BatchPlan)])
+def test_descriptor_layout_matches_header(tmp_path, cname, ctype):
+    """ctypes struct offsets equal the C struct's (gcc offsetof)."""
     import shutil
     import subprocess
     if shutil.which("gcc") is None:
         pytest.skip("gcc not available")
-    fields = [f[0] for f in _native.FitDesc._fields_]
+    fields = [f[0] for f in ctype._fields_]
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "wakis_b200.h"',
-           'int main(void){', 'printf("size %zu\\n", sizeof(wk_fit_desc));']
-    src += [f'printf("{f} %zu\\n", offsetof(wk_fit_desc, {f}));' for f in fields]
+           'int main(void){', f'printf("size %zu\\n", sizeof({cname}));']
+    src += [f'printf("{f} %zu\\n", offsetof({cname}, {f}));' for f in fields]
     src += ["return 0;}"]
     c = tmp_path / "layout.c"
     c.write_text("\n".join(src))
@@ -78,6 +80,23 @@ def test_descriptor_layout_matches_header(tmp_path):
                    check=True)
     out = dict(line.split() for line in
                subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
-    assert int(out["size"]) == ctypes.sizeof(_native.FitDesc)
+    assert int(out["size"]) == ctypes.sizeof(ctype)
     for f in fields:
-        assert int(out[f]) == getattr(_native.FitDesc, f).offset, f
+        assert int(out[f]) == getattr(ctype, f).offset, f
+
+
+def test_batch_args_rejected(lib):
+    """The batched entry points check their arguments on the host."""
+    assert lib.wk_batch_workspace_bytes(None, 1) == -1
+    assert b"descs" in lib.wk_last_error()
+    d = (_native.FitDesc * 1)()
+    assert lib.wk_batch_workspace_bytes(d, 0) == -1
+    d[0].Nx, d[0].Ny, d[0].Nz = 1, 4, 4
+    assert lib.wk_batch_workspace_bytes(d, 1) == -1
+    plan = _native.BatchPlan()
+    assert lib.wk_batch_prepare(d, 1, 0, None, 0, ctypes.byref(plan), None) == 1
+    assert lib.wk_batch_run(None, 1, 0, None, 0, None) == 1
+    # a plan that wk_batch_prepare did not fill
+    plan.workspace = 128
+    plan.variant = -1
+    assert lib.wk_batch_run(ctypes.byref(plan), 1, 0, None, 0, None) == 6

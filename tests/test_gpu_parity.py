@@ -374,6 +374,37 @@ def test_fp32c_tma_fields_close_to_oracle(bcs, shape):
     assert rel_err(_decoded(s, "H"), o.H) <= 1e-5
 
 
+@pytest.mark.parametrize("idx", [2, 5])
+def test_fp32c_compensated_stencil_tracks_fp64(idx):
+    """The compensated stencil (comp_stencil: every neighbour value read as
+    v + c, increments formed with error-free float transformations) keeps
+    the FP32c state on the FP64 oracle's trajectory: from random
+    float-exact fields on a 16x12x20 grid, E and H after 8 steps
+    (conductive materials, PML faces) within 1e-8 relative and at least
+    twice as close as with the float stencil.  (Over the thousands of steps
+    of a wake or adjoint run the gap grows: the float stencil's increments
+    carry a float rounding every step; see the adjoint gradient test.)"""
+    c = dict(cases.STEP_CASES[idx])
+    c.update(shape=(16, 12, 20), dtype="float64", steps=8, n_pml=3)
+    o = oracle_step_case(c)
+    # float-exact initial fields: writing the state sets v = float(value), c = 0
+    E0, H0 = (f.astype(np.float32).astype(np.float64) for f in cases.initial_fields(c, o.N))
+    o.E[:], o.H[:] = E0, H0
+    for _ in range(c["steps"]):
+        o.one_step()
+    err = {}
+    for cst in (False, True):
+        s = b200_step_case(c, precision="fp32c")
+        s.kernel = "twopass"
+        s.comp_stencil = cst
+        s.E.fromarray(E0)
+        s.H.fromarray(H0)
+        s._advance(c["steps"], 0)
+        err[cst] = max(rel_err(_decoded(s, "E"), o.E), rel_err(_decoded(s, "H"), o.H))
+    assert err[True] <= 1e-8, err
+    assert err[True] * 2 <= err[False], err
+
+
 def _small_pillboxes(precision=None):
     from wakis_b200 import batch
     ps = [dict(R=0.020, L=0.030, beta=0.9, sigma=1e4), dict(R=0.026, L=0.036, beta=0.6, sigma=3e5),
@@ -414,12 +445,14 @@ def test_batched_fp32c_close_to_fp64():
 
 
 def _design_problem(dtype, n_steps=800, adjoint_dtype=None, precision=None,
-                    operators="stencil"):
+                    operators="stencil", comp_stencil=False):
     """cavity_40 geometry with an 8x8x8-cell design region at the centre,
-    PEC walls (dt not clamped), FP32, FP64 or FP32-compensated."""
+    PEC walls (dt not clamped), FP32, FP64 or FP32-compensated (with the
+    float or the compensated stencil)."""
     from wakis_b200 import workloads
     from wakis_b200.adjoint import ImpedanceDesign
     _, _, s = workloads.build_b200("cavity_40", dtype=dtype, precision=precision)
+    s.comp_stencil = comp_stencil
     m = np.zeros((s.Nx, s.Ny, s.Nz), bool)
     m[16:24, 16:24, 36:44] = True
     return ImpedanceDesign(s, m, f_band=(0.5e9, 3e9), n_steps=n_steps, segment=30,
@@ -486,11 +519,11 @@ def test_adjoint_operators_match_step_kernels():
     assert rel_err(s.E.numpy(), E1) <= 1e-13
 
 
-@pytest.mark.parametrize("dtype,prec,adt,tol", [
-    (np.float64, None, None, 1e-5), (np.float64, "fp32c", None, 1e-5),
-    (np.float64, "fp32c", np.float32, 1e-5),
-    (np.float32, None, None, 5e-2), (np.float32, None, np.float64, 5e-2)])
-def test_adjoint_gradient_matches_central_differences(dtype, prec, adt, tol):
+@pytest.mark.parametrize("dtype,prec,adt,tol,cst", [
+    (np.float64, None, None, 1e-5, False), (np.float64, "fp32c", None, 1e-5, False),
+    (np.float64, "fp32c", np.float32, 1e-5, False), (np.float64, "fp32c", None, 1e-5, True),
+    (np.float32, None, None, 5e-2, False), (np.float32, None, np.float64, 5e-2, False)])
+def test_adjoint_gradient_matches_central_differences(dtype, prec, adt, tol, cst):
     """dL/d(eps_r, sigma) of L = int_{0.5}^{3 GHz} |Z|^2 df from the adjoint
     against central finite differences of FP64 forward runs along 4 random
     directions of the 1024 parameters: within 1e-5 with the FP64 adjoint
@@ -502,7 +535,7 @@ def test_adjoint_gradient_matches_central_differences(dtype, prec, adt, tol):
     nd = 512
     er = rng.uniform(1.0, 10.0, nd)
     sg = rng.uniform(0.0, 10.0, nd)
-    p = _design_problem(dtype, adjoint_dtype=adt, precision=prec)
+    p = _design_problem(dtype, adjoint_dtype=adt, precision=prec, comp_stencil=cst)
     p.set_params(er, sg)
     L = p.forward()
     ge, gs = p.backward()

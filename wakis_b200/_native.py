@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libwakis_b200.so")
 WK_F64, WK_F32, WK_F32C = 0, 1, 2
 WK_J_ZERO, WK_J_SIGMA_E, WK_J_ARRAY = 0, 1, 2
 WK_KERNEL_AUTO, WK_KERNEL_CELL, WK_KERNEL_TWOPASS, WK_KERNEL_TMA = 0, 1, 4, 6
+WK_BATCH_PERSISTENT, WK_BATCH_PHASES = 0, 1
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -45,6 +46,17 @@ class FitDesc(ctypes.Structure):
         ("faces_clean", _i),
         ("wait_ns", _ll),
         ("steps_per_launch", _i),
+        ("comp_stencil", _i),
+    ]
+
+
+class BatchPlan(ctypes.Structure):
+    """Mirror of ``wk_batch_plan`` in include/wakis_b200.h."""
+
+    _fields_ = [
+        ("workspace", _vp), ("workspace_bytes", _ll), ("n_inst", _i), ("n_items", _i * 2),
+        ("grid", _i), ("smem", _i), ("variant", _i), ("device", _i), ("offsets", _ll * 4),
+        ("n_parts", _i * 3), ("form", _i),
     ]
 
 
@@ -58,6 +70,9 @@ _SIGS = {
                                ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i)]),
     "wk_sigma_e": (_i, [ctypes.POINTER(FitDesc), _vp, _vp]),
     "wk_counter_add": (_i, [_vp, _ll, _vp]),
+    "wk_batch_workspace_bytes": (_ll, [_vp, _i]),
+    "wk_batch_prepare": (_i, [_vp, _i, _ll, _vp, _ll, ctypes.POINTER(BatchPlan), _vp]),
+    "wk_batch_run": (_i, [ctypes.POINTER(BatchPlan), _i, _ll, _vp, _ll, _vp]),
     "wk_field_monitor": (_i, [_vp, _i, _ll, _vp, _i, _vp, _vp]),
     "wk_adj_h": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, ctypes.c_double, _vp, _vp, _vp]),
     "wk_adj_e": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp]),

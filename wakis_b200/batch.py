@@ -3,13 +3,22 @@ own dt, beta and materials) stepped together on one GPU.
 
 Upstream runs one ``SolverFIT3D.wakesolve`` per geometry (wakis/routines.py:
 231-482); here every instance keeps its own solver, beam and Ez history, and
-the stepping of all of them is one CUDA graph: two steps of every instance,
-spread over a few streams, then an increment of a device step counter that
-the kernels read (``wk_fit_desc.step_dev``).  The graph is captured once and
-replayed Nt/2 times, so the host issues one launch per two steps of the whole
-batch instead of ~3 launches per step per instance.  Before the run a small
-autotuner times the candidate chunk lengths (planes per block of the TMA
-kernels, ``SolverFIT3D.tile``) on each distinct grid and keeps the fastest.
+the stepping of all of them is shared:
+
+* ``launch="batched"`` (FP32-compensated instances, ``wk_batch_run``): one
+  device work list of (instance, tile, z-chunk) items and boundary-plane
+  items over all instances, run either as ONE persistent cooperative launch
+  per chunk of steps (its blocks walk the lists of every step and meet at a
+  bounded grid barrier after each phase) or as one launch per list and step
+  (form "phases").  The step index comes from a device counter, so the
+  chunk is captured once in a CUDA graph and replayed.  An autotuner times
+  both forms and the candidate planes per work item (the z depth of the
+  tiles, ``SolverFIT3D.tile``) on the whole batch and keeps the fastest.
+* ``launch="graph"``: one CUDA graph of two steps of every instance (one
+  launch per instance and step, spread over a few streams) plus an increment
+  of the device step counter (``wk_fit_desc.step_dev``), replayed Nt/2 times;
+  the autotuner picks the planes per block of each distinct grid.
+
 Afterwards each ``WakeSolver`` integrates its own history as wakesolve does.
 """
 
@@ -23,6 +32,8 @@ from . import _native
 from . import geometry
 
 KC_CANDIDATES = (0, 4, 8, 16, 32)
+# planes per work item tried by the autotuner of the batched launches
+BATCH_KC_CANDIDATES = (16, 32, 48, 64, 96)
 
 
 def autotune(solver, candidates=KC_CANDIDATES, steps=4):
@@ -50,19 +61,126 @@ def autotune(solver, candidates=KC_CANDIDATES, steps=4):
     return solver.tile[1], tried
 
 
+FORMS = {"persistent": _native.WK_BATCH_PERSISTENT, "phases": _native.WK_BATCH_PHASES}
+
+
+class BatchPlan:
+    """A prepared batched run over a list of FP32-compensated solvers
+    (``wk_batch_prepare``): the workspace (device memory owned here), the
+    plan and the descriptors it was built from.  ``descs`` holds one
+    ``FitDesc`` per solver (beam, capture and J mode filled in); the live
+    buffers of step ``t_ref`` are each descriptor's ``par``.  ``form``:
+    "persistent" or "phases" (``wk_batch_plan.form``)."""
+
+    def __init__(self, solvers, descs, t_ref, form="persistent"):
+        lib = _native.lib()
+        self.solvers = list(solvers)
+        n = len(self.solvers)
+        arr = (_native.FitDesc * n)()
+        for q, d in enumerate(descs):
+            ctypes.memmove(ctypes.byref(arr[q]), ctypes.byref(d), ctypes.sizeof(d))
+        self.descs = arr
+        nbytes = lib.wk_batch_workspace_bytes(arr, n)
+        if nbytes < 0:
+            raise ValueError("wk_batch_workspace_bytes: " +
+                             lib.wk_last_error().decode(errors="replace"))
+        dev = self.solvers[0].device
+        self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+        self.plan = _native.BatchPlan()
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _native.check(lib.wk_batch_prepare(arr, n, int(t_ref), self.workspace.data_ptr(),
+                                           int(nbytes), ctypes.byref(self.plan), stream),
+                      "wk_batch_prepare")
+        self.plan.form = FORMS[form]
+
+    def run(self, n_steps, step0=0, step_dev=None, barrier_ns=0, stream=None):
+        """Enqueue n_steps steps (step indices step0 + s, plus *step_dev
+        when given) on `stream`: one persistent launch, or the launches of
+        every list and step."""
+        lib = _native.lib()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.solvers[0].device).cuda_stream
+        _native.check(lib.wk_batch_run(ctypes.byref(self.plan), int(n_steps), int(step0),
+                                       step_dev, int(barrier_ns), stream), "wk_batch_run")
+
+
+def batched_ok(solvers):
+    """True when the batched launches can take these solvers: all
+    FP32-compensated, on one device, with x/y faces PEC-masked and the same
+    face mode, id width and J mode (checked again by wk_batch_prepare)."""
+    if not solvers:
+        return False
+    s0 = solvers[0]
+    for s in solvers:
+        if s.precision != "fp32c" or s.device != s0.device or s.Nx % 4:
+            return False
+        if s._desc.id_bytes > 2 or s.use_conductivity != s0.use_conductivity:
+            return False
+        pec = list(s._desc.pec_face)
+        if s._desc.has_pmc or not s._desc.has_pec or any(pec[:4]):
+            return False
+        if (pec[4] == 0 and pec[5] == 0) != (list(s0._desc.pec_face)[4:] == [0, 0]):
+            return False
+    return True
+
+
+def autotune_batch(solvers, candidates=BATCH_KC_CANDIDATES, forms=tuple(FORMS), steps=4):
+    """Pick the launch form and the planes per work item of the batched run
+    by timing `steps` source-free steps of the whole batch per candidate
+    with CUDA events; every solver's ``tile`` is set to the winner.  The
+    fields start at zero and stay zero (no source); they are reset
+    afterwards.  Returns ((form, planes), {(form, planes): ms})."""
+    dev = solvers[0].device
+    tried = {}
+    for kc in candidates:
+        for s in solvers:
+            s.tile = (0, kc)
+            s._first_step()
+        descs = [_native.FitDesc.from_buffer_copy(s._step_desc()) for s in solvers]
+        for form in forms:
+            plan = BatchPlan(solvers, descs, t_ref=0, form=form)
+            plan.run(1, 0)                                   # warm
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            plan.run(steps, 1)
+            ev1.record()
+            torch.cuda.synchronize(dev)
+            tried[(form, kc)] = ev0.elapsed_time(ev1)
+    best = min(tried, key=tried.get)
+    for s in solvers:
+        s.tile = (0, best[1])
+        s.reset_fields()
+        s.nstep = 0
+        s.step_0 = True
+        s.check_status("autotune_batch")
+    return best, tried
+
+
 class BatchedWakeSolve:
     """Run ``wakesolve`` for a list of solvers (each built with its own
-    WakeSolver) in one captured CUDA graph per pair of steps.
+    WakeSolver), sharing the stepping of all of them.
 
     n_steps: steps per instance (every instance gets the same count; the
     wakelength of each is set so that upstream's Nt formula gives n_steps).
-    streams: number of CUDA streams the instances are spread over inside the
-    graph.  tune: run the chunk-length autotuner first.
+    launch: "batched" (the device work list over all instances,
+    wk_batch_run, for FP32-compensated instances), "graph" (replayed graph of
+    per-instance launches) or "auto" (batched when ``batched_ok``).  form:
+    the batched launch form, "persistent", "phases" or "auto" (chosen by the
+    autotuner; "persistent" without tuning).  streams: number of CUDA
+    streams the instances are spread over inside the graph (launch="graph").
+    chunk: steps per captured chunk of the batched launch.  tune: run the
+    autotuner first.
     """
 
-    def __init__(self, solvers, n_steps, compute_plane="both", streams=8, tune=True):
+    def __init__(self, solvers, n_steps, compute_plane="both", streams=8, tune=True,
+                 launch="auto", chunk=500, form="auto"):
         if n_steps < 2:
             raise ValueError("n_steps must be >= 2")
+        if launch not in ("auto", "batched", "graph"):
+            raise ValueError(f"launch {launch!r}")
+        if form not in ("auto",) + tuple(FORMS):
+            raise ValueError(f"form {form!r}")
         self.solvers = list(solvers)
         self.n_steps = int(n_steps)
         self.compute_plane = compute_plane
@@ -70,6 +188,14 @@ class BatchedWakeSolve:
         self.tune = tune
         self.tuned = {}
         self.timing = {}
+        if launch == "auto":
+            launch = "batched" if batched_ok(self.solvers) else "graph"
+        elif launch == "batched" and not batched_ok(self.solvers):
+            raise ValueError("launch='batched' needs FP32-compensated instances with "
+                             "PEC-masked x/y faces, sharing face mode, id width and J mode")
+        self.launch = launch
+        self.form = form
+        self.chunk = max(1, int(chunk))
 
     @staticmethod
     def wakelength_for(solver, n_steps):
@@ -78,18 +204,7 @@ class BatchedWakeSolve:
         z = solver.z
         return (n_steps + 0.5) * float(solver.dt) * w.v - w.ti * w.v - (z.max() - z.min())
 
-    def run(self):
-        dev = self.solvers[0].device
-        lib = _native.lib()
-        if self.tune:
-            shapes = {}
-            for s in self.solvers:
-                key = (s.Nx, s.Ny, s.Nz, s.precision)
-                if key not in shapes:
-                    shapes[key] = autotune(s)
-                else:
-                    s.tile = (0, shapes[key][0])
-            self.tuned = {str(k): v[0] for k, v in shapes.items()}
+    def _setup(self):
         states = []
         for s in self.solvers:
             wl = self.wakelength_for(s, self.n_steps)
@@ -100,6 +215,85 @@ class BatchedWakeSolve:
                 raise ValueError(f"{self.n_steps} steps do not reach past the domain "
                                  f"(wakelength {wl:.4g} m): no wake samples")
             states.append(ws)
+        return states
+
+    def run(self):
+        dev = self.solvers[0].device
+        if self.launch == "batched":
+            form = self.form
+            if self.tune:
+                forms = tuple(FORMS) if form == "auto" else (form,)
+                best, tried = autotune_batch(self.solvers, forms=forms)
+                form = best[0]
+                self.tuned = {"form": best[0], "planes_per_item": best[1],
+                              "tried_ms": {f"{k[0]}/{k[1]}": v for k, v in tried.items()}}
+            elif form == "auto":
+                form = "persistent"
+            self.tuned["form"] = form
+            states = self._setup()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            for s, ws in zip(self.solvers, states):
+                s._advance(1, 0, beam=ws["beam_params"], capture=ws["capture"])
+            descs = [_native.FitDesc.from_buffer_copy(
+                s._step_desc(ws["beam_params"], ws["capture"])) for s, ws in zip(self.solvers,
+                                                                                 states)]
+            plan = BatchPlan(self.solvers, descs, t_ref=1, form=form)
+            rest = self.n_steps - 1
+            chunk = min(self.chunk, rest)
+            reps, tail = divmod(rest, chunk)
+            counter = torch.ones(1, dtype=torch.int64, device=dev)
+            main = torch.cuda.Stream(dev)
+            main.wait_stream(torch.cuda.current_stream(dev))
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=main):
+                plan.run(chunk, 0, step_dev=counter.data_ptr(), stream=main.cuda_stream)
+                _native.check(_native.lib().wk_counter_add(
+                    ctypes.c_void_p(counter.data_ptr()), chunk, ctypes.c_void_p(main.cuda_stream)),
+                    "wk_counter_add")
+            torch.cuda.current_stream(dev).wait_stream(main)
+            for _ in range(reps):
+                graph.replay()
+            torch.cuda.current_stream(dev).wait_stream(main)
+            if tail:
+                plan.run(tail, 1 + reps * chunk)
+            ev1.record()
+            torch.cuda.synchronize(dev)
+            ms = ev0.elapsed_time(ev1)
+            wall = time.perf_counter() - t0
+            del graph
+            for s in self.solvers:
+                s._par ^= rest & 1
+                s.nstep += rest
+            self.tuned["launches"] = reps + (1 if tail else 0)
+            self.tuned["steps_per_launch"] = chunk
+        else:
+            ms, wall, states = self._run_graph(dev)
+        for q, s in enumerate(self.solvers):
+            s.check_status(f"BatchedWakeSolve.run (instance {q})")
+        cells = sum(s.N for s in self.solvers)
+        self.timing = {"ms": ms, "wall_s": wall, "cells": cells, "steps": self.n_steps,
+                       "launch": self.launch,
+                       "gcell_steps_per_s": cells * self.n_steps / (ms / 1e3) / 1e9}
+        for s, ws in zip(self.solvers, states):
+            s._wake_finish(ws, wall)
+        return self.timing
+
+    def _run_graph(self, dev):
+        lib = _native.lib()
+        if self.tune:
+            shapes = {}
+            for s in self.solvers:
+                key = (s.Nx, s.Ny, s.Nz, s.precision)
+                if key not in shapes:
+                    shapes[key] = autotune(s)
+                else:
+                    s.tile = (0, shapes[key][0])
+            self.tuned = {str(k): v[0] for k, v in shapes.items()}
+        states = self._setup()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         ev0 = torch.cuda.Event(enable_timing=True)
@@ -150,14 +344,7 @@ class BatchedWakeSolve:
         ms = ev0.elapsed_time(ev1)
         wall = time.perf_counter() - t0
         del graph
-        for q, s in enumerate(self.solvers):
-            s.check_status(f"BatchedWakeSolve.run (instance {q})")
-        cells = sum(s.N for s in self.solvers)
-        self.timing = {"ms": ms, "wall_s": wall, "cells": cells, "steps": self.n_steps,
-                       "gcell_steps_per_s": cells * self.n_steps / (ms / 1e3) / 1e9}
-        for s, ws in zip(self.solvers, states):
-            s._wake_finish(ws, wall)
-        return self.timing
+        return ms, wall, states
 
 
 # ----------------------------------------------------------- pillboxes ----
@@ -173,15 +360,16 @@ def pillbox_params(n=64, seed=0):
             for q in range(n)]
 
 
-def pillbox_grid(R, L, cell=1e-3, pipe=0.008):
+def pillbox_grid(R, L, cell=1e-3, pipe=0.008, multiple=4):
     """Bounds (x0, x1, y0, y1, z0, z1), cell counts (Nx, Ny, Nz) and a
     function of the grid edges (x, y, z) giving the wall mask of a pillbox:
     a vacuum cylinder of radius R and length L centred at the origin with a
     vacuum beam pipe along z, inside a conducting wall; the transverse size
-    is rounded up to a multiple of 4 cells and the pipe runs max(45 mm, L)
+    is rounded up to a multiple of `multiple` cells (8 lets the compensation
+    words of every row arrive by TMA) and the pipe runs max(45 mm, L)
     past each cavity end.  A cell is vacuum when any of its corners is
     inside the vacuum region."""
-    nxy = int(np.ceil(2 * (R + 0.005) / cell / 4.0)) * 4
+    nxy = int(np.ceil(2 * (R + 0.005) / cell / multiple)) * multiple
     half = nxy * cell / 2
     zl = L / 2 + max(0.045, L)
     nz = int(round(2 * zl / cell))
@@ -197,14 +385,14 @@ def pillbox_grid(R, L, cell=1e-3, pipe=0.008):
 
 
 def build_pillbox(R, L, beta, sigma, cell=1e-3, pipe=0.008, sigmaz=0.008, precision=None,
-                  dtype=np.float64, device=None):
+                  dtype=np.float64, device=None, multiple=4):
     """(grid, wake, solver) of one pillbox (``pillbox_grid``): wall of
     conductivity sigma (surface impedance above the resolvable conductivity,
     as upstream does), 1 mm cells, PEC on x/y and ABC on z."""
     from .gridFIT3D import GridFIT3D
     from .solverFIT3D import SolverFIT3D
     from .wakeSolver import WakeSolver
-    bounds, shape, wall_mask = pillbox_grid(R, L, cell=cell, pipe=pipe)
+    bounds, shape, wall_mask = pillbox_grid(R, L, cell=cell, pipe=pipe, multiple=multiple)
     g = GridFIT3D(*bounds, *shape, verbose=0)
     g.add_solid("wall", wall_mask(g.x, g.y, g.z), [1.0, 1.0, sigma])
     w = WakeSolver(q=1e-9, sigmaz=sigmaz, beta=beta, xsource=0.0, ysource=0.0, xtest=0.0,

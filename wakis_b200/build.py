@@ -14,8 +14,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwakis_b200.so")
 SOURCES = ["abi.cu", "fit_step.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma2.cu", "fit_tma_comp.cu",
-           "wake.cu", "adjoint.cu", "monitor.cu"]
-HEADERS = ["abi_internal.h", "fit_common.cuh", "fit_kernels.cuh", "fit_comp.cuh", "tma_util.cuh"]
+           "fit_batch.cu", "wake.cu", "adjoint.cu", "monitor.cu"]
+HEADERS = ["abi_internal.h", "fit_common.cuh", "fit_kernels.cuh", "fit_comp.cuh", "fit_tma_comp.cuh",
+           "tma_util.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -105,45 +105,113 @@ k_e_comp(FitParams<double> p, CompState st, long long step) {
   }
 }
 
-// Shell of the compensated step (block-uniform decode, ShellGrid): the state
-// is decoded to FP64, lean rows where they apply, general rows elsewhere,
-// and the FP64 result is split back into (float, bf16).
-__global__ void __launch_bounds__(kShellBlock) k_h_comp_shell(FitParams<double> p, CompState st,
-                                                               ShellGrid g) {
-  Cell c;
-  if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
-  const int Nx = p.Nx;
-  const long long N = p.N, NxNy = p.NxNy;
-  const long long n = c.i + (long long)c.j * Nx + (long long)c.k * NxNy;
-  auto E = [&](int e, long long m) -> double {
-    return comp_value(st.E_in[e * N + m], st.Ec_in[e * N + m]);
+// Interior rows with the compensated stencil (comp_stencil = 1): every E
+// (H) value a row reads is the pair v + c of the state, the update factors
+// are split into two floats, and the increment is formed with the pair
+// operations of fit_comp.cuh before the compensated add; the J = sigma E term
+// uses the pair of E_old as well.
+__global__ void __launch_bounds__(kCompX * kCompY)
+k_h_comp_cs(FitParams<double> p, CompState st) {
+  const int i = 2 + blockIdx.x * kCompX + threadIdx.x;
+  const int j = 2 + blockIdx.y * kCompY + threadIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const long long N = p.N;
+  const int sy = p.Nx, sz = (int)p.NxNy;
+  const long long n = i + (long long)j * sy + (long long)k * sz;
+  // E pair of component d at n + off
+  auto ev = [&](int d, long long off) { return st.E_in[d * N + n + off]; };
+  auto ec = [&](int d, long long off) { return comp_dec(st.Ec_in[d * N + n + off]); };
+  auto diff = [&](int d, long long oa, long long ob) {
+    return pair_diff(ev(d, oa), ec(d, oa), ev(d, ob), ec(d, ob));
   };
-  const int id = load_id(p.mat_id, p.id_bytes, n);
-  double h[3];
-#pragma unroll
-  for (int d = 0; d < 3; d++) h[d] = comp_value(st.H_in[d * N + n], st.Hc_in[d * N + n]);
-  if (lean_h<double>(c.i, c.j, c.k, Nx, p.Ny, p.Nz)) {
-    const double* m0 = p.mat + 9 * id;
-    const double R0 = p.iAx[c.j + (long long)c.k * p.Ny] * m0[3];
-    const double R1 = p.iAy[c.i + (long long)c.k * Nx] * m0[4];
-    const double R2 = p.iAz[c.i + (long long)c.j * Nx] * m0[5];
-    h_lean(p.dt, p.h_desc != 0, R0, R1, R2, p.Lx[c.i], p.Ly[c.j], p.Lz[c.k], E(0, n), E(1, n),
-           E(2, n), E(1, n + 1), E(2, n + 1), E(0, n + Nx), E(2, n + Nx), E(0, n + NxNy),
-           E(1, n + NxNy), h[0], h[1], h[2]);
-  } else {
-    const long long off[4] = {0, 1, (long long)Nx, NxNy};
-    auto ev = [&](int e, int kind) -> double { return E(e, n + off[kind]); };
-#pragma unroll
-    for (int d = 0; d < 3; d++) h[d] = h_row_acc(p, h[d], d, c, n, id, ev);
-  }
+  const double* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+  const double dt = p.dt;
+  const double Lx = p.Lx[i], Ly = p.Ly[j], Lz = p.Lz[k];
+  const double R0 = p.iAx[j + k * p.Ny] * m0[3];
+  const double R1 = p.iAy[i + k * sy] * m0[4];
+  const double R2 = p.iAz[i + j * sy] * m0[5];
+  FPair S[3];
+  // S_x = a (Ey(n) - Ey(n+NxNy)) + b (Ez(n+Nx) - Ez(n)), a = dt iAx imu Ly, b = .. Lz
+  S[0] = pair_add(pair_mul(pair_of(dt * (R0 * Ly)), diff(1, 0, sz)),
+                  pair_mul(pair_of(dt * (R0 * Lz)), diff(2, sy, 0)));
+  // S_y = a (Ex(n+NxNy) - Ex(n)) + b (Ez(n) - Ez(n+1))
+  S[1] = pair_add(pair_mul(pair_of(dt * (R1 * Lx)), diff(0, sz, 0)),
+                  pair_mul(pair_of(dt * (R1 * Lz)), diff(2, 0, 1)));
+  // S_z = a (Ex(n) - Ex(n+Nx)) + b (Ey(n+1) - Ey(n))
+  S[2] = pair_add(pair_mul(pair_of(dt * (R2 * Lx)), diff(0, 0, sy)),
+                  pair_mul(pair_of(dt * (R2 * Ly)), diff(1, 1, 0)));
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     float t;
     comp_t q;
-    comp_split(h[d], t, q);
+    comp_add_pair(st.H_in[d * N + n], st.Hc_in[d * N + n], FPair{-S[d].hi, -S[d].lo}, t, q);
     st.H_out[d * N + n] = t;
     st.Hc_out[d * N + n] = q;
   }
+}
+
+__global__ void __launch_bounds__(kCompX * kCompY)
+k_e_comp_cs(FitParams<double> p, CompState st, long long step) {
+  step = step_index(p, step);
+  const int i = 2 + blockIdx.x * kCompX + threadIdx.x;
+  const int j = 2 + blockIdx.y * kCompY + threadIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > p.Nx - 3 || j > p.Ny - 3) return;
+  const long long N = p.N;
+  const int sy = p.Nx, sz = (int)p.NxNy;
+  const long long n = i + (long long)j * sy + (long long)k * sz;
+  // new-H pair of component d at n - off
+  auto hv = [&](int d, long long off) { return st.H_out[d * N + n - off]; };
+  auto hc = [&](int d, long long off) { return comp_dec(st.Hc_out[d * N + n - off]); };
+  auto diff = [&](int d, long long oa, long long ob) {
+    return pair_diff(hv(d, oa), hc(d, oa), hv(d, ob), hc(d, ob));
+  };
+  const float e[3] = {st.E_in[n], st.E_in[N + n], st.E_in[2 * N + n]};
+  const comp_t eq[3] = {st.Ec_in[n], st.Ec_in[N + n], st.Ec_in[2 * N + n]};
+  const double* m0 = p.mat + 9 * load_id(p.mat_id, p.id_bytes, n);
+  const double dt = p.dt;
+  const double tLx = p.tLx[i], tLy = p.tLy[j], tLz = p.tLz[k];
+  const double R0 = m0[0] * p.itAx[j + k * p.Ny];
+  const double R1 = m0[1] * p.itAy[i + k * sy];
+  const double R2 = m0[2] * p.itAz[i + j * sy];
+  FPair cu[3];
+  // curl_x = c1 (Hy(n-NxNy) - Hy(n)) + c2 (Hz(n) - Hz(n-Nx)), c1 = dt ieps itAx tLy, c2 = .. tLz
+  cu[0] = pair_add(pair_mul(pair_of(dt * (R0 * tLy)), diff(1, sz, 0)),
+                   pair_mul(pair_of(dt * (R0 * tLz)), diff(2, 0, sy)));
+  // curl_y = c1 (Hx(n) - Hx(n-NxNy)) + c2 (Hz(n-1) - Hz(n))
+  cu[1] = pair_add(pair_mul(pair_of(dt * (R1 * tLx)), diff(0, 0, sz)),
+                   pair_mul(pair_of(dt * (R1 * tLz)), diff(2, 1, 0)));
+  // curl_z = c1 (Hx(n-Nx) - Hx(n)) + c2 (Hy(n) - Hy(n-1))
+  cu[2] = pair_add(pair_mul(pair_of(dt * (R2 * tLx)), diff(0, sy, 0)),
+                   pair_mul(pair_of(dt * (R2 * tLy)), diff(1, 0, 1)));
+  Cell c;
+  c.i = i; c.j = j; c.k = k;
+  if (p.cap_on) capture(p, c, n, step, comp_value(e[2], eq[2]));
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    FPair jt{0.f, 0.f};   // dt ieps J of the row
+    if (d == 2 && i == p.ixs && j == p.iys && (p.line_on || p.beam_on)) {
+      const double jv = j_in(p, d, c, n, step, 0.0, 0.0);
+      jt = pair_of(dt * m0[d] * jv);
+    } else if (p.j_mode == WK_J_SIGMA_E) {
+      jt = pair_mul(pair_of(dt * m0[d] * m0[6 + d]), FPair{e[d], comp_dec(eq[d])});
+    }
+    float t;
+    comp_t q;
+    comp_add_pair(e[d], eq[d], pair_sub(cu[d], jt), t, q);
+    st.E_out[d * N + n] = t;
+    st.Ec_out[d * N + n] = q;
+  }
+}
+
+// Shell of the compensated step (block-uniform decode, ShellGrid): one
+// cell per thread (comp_shell_h / comp_shell_e, fit_comp.cuh).
+__global__ void __launch_bounds__(kShellBlock) k_h_comp_shell(FitParams<double> p, CompState st,
+                                                               ShellGrid g) {
+  Cell c;
+  if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
+  comp_shell_h(p, st, c);
 }
 
 __global__ void __launch_bounds__(kShellBlock) k_e_comp_shell(FitParams<double> p, CompState st,
@@ -151,39 +219,7 @@ __global__ void __launch_bounds__(kShellBlock) k_e_comp_shell(FitParams<double> 
   step = step_index(p, step);
   Cell c;
   if (!shell_cell_of(g, blockIdx.x, threadIdx.x, p.Nx, p.Ny, p.Nz, c)) return;
-  const int Nx = p.Nx;
-  const long long N = p.N, NxNy = p.NxNy;
-  const long long n = c.i + (long long)c.j * Nx + (long long)c.k * NxNy;
-  auto Hn = [&](int e, long long m) -> double { return (double)st.H_out[e * N + m]; };
-  const int id = load_id(p.mat_id, p.id_bytes, n);
-  const double ez_old = comp_value(st.E_in[2 * N + n], st.Ec_in[2 * N + n]);
-  if (p.cap_on) capture(p, c, n, step, ez_old);
-  double curl[3];
-  const bool lean = lean_e<double>(c.i, c.j, c.k, Nx, p.Ny, p.Nz);
-  if (lean) {
-    const double* m0 = p.mat + 9 * id;
-    const double R0 = m0[0] * p.itAx[c.j + (long long)c.k * p.Ny];
-    const double R1 = m0[1] * p.itAy[c.i + (long long)c.k * Nx];
-    const double R2 = m0[2] * p.itAz[c.i + (long long)c.j * Nx];
-    e_lean(R0, R1, R2, p.tLx[c.i], p.tLy[c.j], p.tLz[c.k], Hn(0, n), Hn(1, n), Hn(2, n),
-           Hn(1, n - 1), Hn(2, n - 1), Hn(0, n - Nx), Hn(2, n - Nx), Hn(0, n - NxNy),
-           Hn(1, n - NxNy), curl[0], curl[1], curl[2]);
-  }
-  const long long off[4] = {0, 1, (long long)Nx, NxNy};
-  auto hv = [&](int e, int kind) -> double { return Hn(e, n - off[kind]); };
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const double ieps = p.mat[9 * id + d], sigma = p.mat[9 * id + 6 + d];
-    const double eold = d == 2 ? ez_old : comp_value(st.E_in[d * N + n], st.Ec_in[d * N + n]);
-    const double jv = j_in(p, d, c, n, step, eold, sigma);
-    const double cu = lean ? curl[d] : e_curl_acc(p, d, c, n, ieps, hv);
-    const double enew = eold + p.dt * (cu - ieps * jv);
-    float t;
-    comp_t q;
-    comp_split(enew, t, q);
-    st.E_out[d * N + n] = t;
-    st.Ec_out[d * N + n] = q;
-  }
+  comp_shell_e(p, st, c, step);
 }
 
 __global__ void k_comp_zero_ghosts(FitParams<double> p, float* E, float* H, comp_t* Ec,
@@ -230,7 +266,10 @@ int wk_comp_step(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_
   const ShellGrid sg = shell_grid(d->Nx, d->Ny, d->Nz);
   const unsigned sb = (unsigned)(sg.nbA + sg.nbB + sg.nbC);
   bool tma = false;
-  if (d->kernel == WK_KERNEL_AUTO || d->kernel == WK_KERNEL_TMA) {
+  const bool cstencil = d->comp_stencil != 0;
+  if (cstencil && d->kernel == WK_KERNEL_TMA)
+    return wk_fail(WK_E_MODE, "wk_fit_step: the compensated stencil runs the two-pass kernels");
+  if (!cstencil && (d->kernel == WK_KERNEL_AUTO || d->kernel == WK_KERNEL_TMA)) {
     tma = tma_comp_supported(d, make_params<double>(d, par));
     if (!tma && d->kernel == WK_KERNEL_TMA)
       return wk_fail(WK_E_SHAPE, "wk_fit_step: compensated TMA kernel needs Nx %% 4 == 0, "
@@ -255,11 +294,13 @@ int wk_comp_step(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_
       }
     } else {
       timer_begin(st);
-      k_h_comp<<<grid, blk, 0, st>>>(p, cs);
+      if (cstencil) k_h_comp_cs<<<grid, blk, 0, st>>>(p, cs);
+      else k_h_comp<<<grid, blk, 0, st>>>(p, cs);
       timer_end(st);
       k_h_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, sg);
       timer_begin(st);
-      k_e_comp<<<grid, blk, 0, st>>>(p, cs, step0 + s);
+      if (cstencil) k_e_comp_cs<<<grid, blk, 0, st>>>(p, cs, step0 + s);
+      else k_e_comp<<<grid, blk, 0, st>>>(p, cs, step0 + s);
       timer_end(st);
       k_e_comp_shell<<<sb, kShellBlock, 0, st>>>(p, cs, step0 + s, sg);
     }

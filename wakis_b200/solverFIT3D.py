@@ -196,6 +196,10 @@ class SolverFIT3D(RoutinesMixin):
         # the temporal-blocking kernel where it applies, 1 one step per
         # launch, 0 the faster on B200 (one step per launch)
         self.steps_per_launch = 0
+        # precision='fp32c' only: True forms every increment from the full
+        # (float + compensation) neighbour values with error-free float
+        # transformations (wk_fit_desc.comp_stencil; two-pass kernels)
+        self.comp_stencil = False
 
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
@@ -208,6 +212,7 @@ class SolverFIT3D(RoutinesMixin):
         d.kernel = self._KERNELS[self.kernel]
         d.tile_rows, d.tile_planes = int(self.tile[0]), int(self.tile[1])
         d.steps_per_launch = int(self.steps_per_launch)
+        d.comp_stencil = int(bool(self.comp_stencil) and self.precision == "fp32c")
         d.par = self._par
         d.dt = float(self.dt)
         d.dt_is_f32 = int(isinstance(self.dt, np.float32))
