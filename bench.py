@@ -465,6 +465,8 @@ def run_adjoint(args):
             torch.cuda.empty_cache()
         else:
             p64 = prob
+            p64.ckpt = {}      # only its forward runs are needed from here on
+            torch.cuda.empty_cache()
     errs = {name: [] for name in runs}
 
     def central(v_e, v_s, h):

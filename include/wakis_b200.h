@@ -218,12 +218,12 @@ int wk_counter_add(long long* ctr, long long inc, void* stream);
  *   t = step0 + s (+ *step_dev when step_dev is not NULL, read on the device
  *   when a launch starts, so captured launches can be replayed), on
  *   `stream` (capturable).  plan->form WK_BATCH_PERSISTENT: one cooperative
- *   launch whose blocks walk the work lists of every step, meeting at a
- *   grid barrier after each phase; each barrier wait is bounded by
- *   barrier_ns nanoseconds (<= 0: 2 s).  WK_BATCH_PHASES: up to four
- *   launches per step (barrier_ns unused).  A wait or a tile load that runs
- *   out sets the status word of the instance concerned (instance 0 for a
- *   barrier) and the launch ends (wk_read_status).
+ *   launch whose blocks claim the items of every step in order; an item
+ *   waits only for its own instance's earlier work (per-instance completion
+ *   counters, no grid-wide barrier), each wait bounded by wait_ns
+ *   nanoseconds (<= 0: 2 s).  WK_BATCH_PHASES: up to four launches per step
+ *   (wait_ns unused).  A wait or a tile load that runs out sets the status
+ *   word of the instance concerned and the launch ends (wk_read_status).
  * No counterpart in the reference.
  */
 #define WK_BATCH_PERSISTENT 0   /* one cooperative launch per wk_batch_run  */
@@ -251,7 +251,7 @@ long long wk_batch_workspace_bytes(const wk_fit_desc* descs, int n_inst);
 int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long t_ref, void* workspace,
                      long long workspace_bytes, wk_batch_plan* plan, void* stream);
 int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long step0,
-                 const long long* step_dev, long long barrier_ns, void* stream);
+                 const long long* step_dev, long long wait_ns, void* stream);
 
 /*
  * Adjoint (reverse-mode) FIT step, used for gradients of a wake/impedance

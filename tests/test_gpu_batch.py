@@ -2,8 +2,8 @@
 wk_batch_run, wakis_b200.batch with launch="batched"), as one persistent
 cooperative launch or as one launch per list and step: every instance equals
 its own wakesolve value for value, and the bounded waits of the persistent
-launch (tile loads, grid barriers) end it with the status word set instead of
-hanging.
+launch (tile loads, waits for an instance's earlier work) end it with the
+status word set instead of hanging.
 
 Upstream runs one wakesolve per geometry (wakis/routines.py:231-482); the
 batched launches must reproduce each of them exactly: their tiles run the
@@ -142,13 +142,19 @@ def test_persistent_tile_wait_timeout_sets_status():
     assert all(int(s._status.item()) == 0 for _, _, s in inst)
 
 
-def test_persistent_barrier_timeout_sets_status():
-    """Grid-barrier waits bounded by 1 ns give up (the blocks that are not
-    the last to arrive): instance 0's status word is set and the launch
-    ends."""
+def test_persistent_dependency_wait_timeout_sets_status():
+    """Dependency waits bounded by 1 ns give up (items of step 1 claimed
+    before their instance's step 0 is done): the status word of an instance
+    is set, every block leaves, and the context steps correctly afterwards."""
     inst = _pillboxes()
     plan = _plan(inst)
-    plan.run(4, 0, barrier_ns=1)
+    plan.run(4, 0, wait_ns=1)
     torch.cuda.synchronize()
-    assert int(inst[0][2]._status.item()) == 1
-    inst[0][2]._status.zero_()
+    assert sum(int(s._status.item()) for _, _, s in inst) >= 1
+    for _, _, s in inst:
+        s._status.zero_()
+        s.reset_fields()
+    ok = _plan(inst)
+    ok.run(2, 0)
+    torch.cuda.synchronize()
+    assert all(int(s._status.item()) == 0 for _, _, s in inst)

@@ -93,7 +93,7 @@ class BatchPlan:
                       "wk_batch_prepare")
         self.plan.form = FORMS[form]
 
-    def run(self, n_steps, step0=0, step_dev=None, barrier_ns=0, stream=None):
+    def run(self, n_steps, step0=0, step_dev=None, wait_ns=0, stream=None):
         """Enqueue n_steps steps (step indices step0 + s, plus *step_dev
         when given) on `stream`: one persistent launch, or the launches of
         every list and step."""
@@ -101,7 +101,7 @@ class BatchPlan:
         if stream is None:
             stream = torch.cuda.current_stream(self.solvers[0].device).cuda_stream
         _native.check(lib.wk_batch_run(ctypes.byref(self.plan), int(n_steps), int(step0),
-                                       step_dev, int(barrier_ns), stream), "wk_batch_run")
+                                       step_dev, int(wait_ns), stream), "wk_batch_run")
 
 
 def batched_ok(solvers):

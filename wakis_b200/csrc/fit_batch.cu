@@ -1,27 +1,40 @@
 // Batched FP32-compensated step: many independent grids (uneven shapes, each
-// with its own dt, beam, materials and Ez capture) advanced together by ONE
-// persistent launch (sm_100a).
+// with its own dt, beam, materials and Ez capture) advanced together over
+// one device work list (sm_100a).
 //
 // Upstream runs one SolverFIT3D.wakesolve per geometry (wakis/routines.py:
 // 231-482); a batch of small grids launched one by one leaves most of the
-// GPU idle in each launch's tail.  Here a cooperative launch of
-// (SMs x blocks per SM) blocks walks a device work list for every step:
+// GPU idle in each launch's tail.  Here the work of a step is a list of
+// items over all instances:
 //
 //   phase A  the TMA tiles of every instance (comp_tile, the block work of
 //            the one-grid kernel, fit_tma_comp.cuh) and, for instances whose
-//            z faces are not PEC-masked, the H half of the four z-boundary
+//            z faces are not PEC-masked, the H rows of the four z-boundary
 //            planes (comp_shell_h);
-//   phase B  (only with such instances) the E half of those planes, which
-//            reads the new H of the tiles next to them (comp_shell_e).
+//   phase B  (only with such instances) the E rows of those planes, which
+//            read the new H of the tiles next to them (comp_shell_e).
 //
-// Blocks claim items with an atomic ticket per phase and meet at a grid
-// barrier after each phase; every barrier wait, like every mbarrier wait of
-// the tiles, is bounded by a %globaltimer deadline, after which the block
-// records the failure in the status word and the launch ends.  Each item
-// copies its instance's parameters into shared memory; the TMA descriptors
-// of every instance and buffer parity live in the caller's workspace.  The
-// parity of the live buffers of step t is par_ref ^ ((t - t_ref) & 1), so
-// one captured launch can be replayed with a device step counter.
+// Two launch forms run the lists:
+//
+// * persistent (WK_BATCH_PERSISTENT): ONE cooperative launch of (SMs x
+//   blocks per SM) blocks for a chunk of steps.  Blocks claim items in order
+//   (step, phase, item) from one atomic ticket.  Instances do not depend on
+//   each other, so there is no grid-wide barrier: before an item of instance
+//   q the block waits until q's own earlier work is done (phase-A items of
+//   q's previous steps, and for a phase-B item those of this step), counted
+//   by per-instance completion counters.  Every item a block waits for was
+//   claimed before its own, by a block that is resident (cooperative
+//   launch), so the waits always end; each is also bounded by a
+//   %globaltimer deadline, after which the block records the failure in the
+//   status word and all blocks leave.
+// * phases (WK_BATCH_PHASES): per step, one launch per list (tiles whose
+//   compensation words come by TMA, the other tiles, boundary-plane H rows,
+//   boundary-plane E rows); the stream orders them.
+//
+// Each item reads its instance's parameters from the workspace; the TMA
+// descriptors of every instance and buffer parity live there too.  The
+// parity of the live buffers of step t is par_ref ^ ((t - t_ref) & 1), so a
+// captured chunk can be replayed with a device step counter.
 #include <cstring>
 #include <vector>
 
@@ -33,15 +46,14 @@ namespace wk {
 
 namespace {
 
-constexpr long long kBarrierNs = 2000000000LL;   // 2 s of %globaltimer per barrier wait
-constexpr long long kBarrierPolls = 1LL << 28;
+constexpr long long kDepNs = 2000000000LL;   // 2 s of %globaltimer per dependency wait
+constexpr long long kDepPolls = 1LL << 28;
 
+// Zeroed at the start of every run (with the completion counters after it).
 struct BatchSync {
-  unsigned arrive;
-  unsigned gen;
-  unsigned ticket[2];
-  int abort;
-  int pad[3];
+  unsigned ticket;          // next item (step, phase, index) to claim
+  int abort;                // a block gave up: every block leaves
+  int pad[2];
 };
 
 struct BatchInst {
@@ -50,6 +62,8 @@ struct BatchInst {
   long long t_ref;          // the step index whose step reads parity par_ref
   int par_ref;
   int ct;                   // compensation words by TMA (Nx % 8 == 0)
+  unsigned nA, nB;          // items of this instance in phase A, phase B
+  int pad;
 };
 static_assert(sizeof(FitParams<double>) % 8 == 0, "parameters are copied as 8-byte words");
 static_assert(sizeof(CompState) % 8 == 0, "state pointers are copied as 8-byte words");
@@ -62,6 +76,7 @@ struct BatchItem {
 
 struct BatchArgs {
   BatchSync* sync;
+  unsigned* done;           // [inst][phase] completed items of the run
   const BatchInst* insts;
   const CompMaps* maps;     // [inst][parity]
   const BatchItem* items[2];
@@ -69,7 +84,7 @@ struct BatchArgs {
   int n_steps;
   long long step0;
   const long long* step_dev;
-  long long barrier_ns;
+  long long wait_ns;        // bound of each dependency wait
 };
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -78,37 +93,20 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   return v;
 }
 
-// Grid-wide barrier of the persistent launch (the launch is cooperative, so
-// every block is resident).  The last block to arrive resets the arrival
-// count and the ticket of the phase that ended, then releases the others.
-// Returns false for every thread of a block whose wait ran out.
-__device__ bool grid_barrier(BatchSync* s, int phase, long long limit_ns) {
-  // this thread's global writes become visible to the TMA loads (async
-  // proxy) that other blocks issue after the barrier
-  asm volatile("fence.proxy.async.global;" ::: "memory");
-  __syncthreads();
-  int ok = 1;
-  if (threadIdx.x == 0) {
-    const unsigned g = ld_acquire_u32(&s->gen);
-    __threadfence();
-    if (atomicAdd(&s->arrive, 1u) == gridDim.x - 1) {
-      atomicExch(&s->arrive, 0u);
-      atomicExch(&s->ticket[phase], 0u);
-      __threadfence();
-      atomicAdd(&s->gen, 1u);
-    } else {
-      const unsigned long long t0 = globaltimer_ns();
-      for (long long it = 0; ld_acquire_u32(&s->gen) == g; it++) {
-        if (it > kBarrierPolls || (long long)(globaltimer_ns() - t0) > limit_ns) {
-          ok = 0;
-          break;
-        }
-        __nanosleep(128);
-      }
-    }
-    __threadfence();
+// Wait (thread 0) until instance counters reach the given counts, the
+// launch is aborted, or limit_ns passes; true when the counts were reached.
+__device__ bool wait_done(const unsigned* done, unsigned needA, unsigned needB,
+                          const int* abort, long long limit_ns) {
+  if (ld_acquire_u32(reinterpret_cast<const unsigned*>(abort))) return false;
+  if (ld_acquire_u32(done) >= needA && ld_acquire_u32(done + 1) >= needB) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (long long it = 0; it < kDepPolls; it++) {
+    __nanosleep(64);
+    if (ld_acquire_u32(done) >= needA && ld_acquire_u32(done + 1) >= needB) return true;
+    if (ld_acquire_u32(reinterpret_cast<const unsigned*>(abort))) return false;
+    if ((long long)(globaltimer_ns() - t0) > limit_ns) return false;
   }
-  return __syncthreads_and(ok) != 0;
+  return false;
 }
 
 // The instance parameters of the current item (copied from the workspace
@@ -144,50 +142,63 @@ __device__ __noinline__ void batch_shell(int kind, int plane, long long t) {
 
 template <typename IdT, bool SIG, int MODE>
 __global__ void __launch_bounds__(cThreads, 2) k_batch_comp(const __grid_constant__ BatchArgs a) {
-  __shared__ int s_it;
-  constexpr int kPhases = MODE == 2 ? 2 : 1;
+  __shared__ unsigned s_it;
   const int tid = threadIdx.x;
   const long long base = a.step0 + (a.step_dev ? *a.step_dev : 0);
-  for (int s = 0; s < a.n_steps; s++) {
+  const unsigned per_step = (unsigned)(a.n_items[0] + a.n_items[1]);
+  const unsigned total = per_step * (unsigned)a.n_steps;
+  for (;;) {
+    __syncthreads();   // the previous item is done with s_it, g_sp and g_scs
+    if (tid == 0) s_it = atomicAdd(&a.sync->ticket, 1u);
+    __syncthreads();
+    const unsigned it = s_it;
+    if (it >= total) break;
+    const unsigned s = it / per_step, r = it - s * per_step;
+    const int ph = r < (unsigned)a.n_items[0] ? 0 : 1;
+    const BatchItem w = ph ? a.items[1][r - a.n_items[0]] : a.items[0][r];
+    const BatchInst& I = a.insts[w.inst];
+    // phase A of step s needs all of the instance's work of step s-1; phase
+    // B of step s needs its phase-A items of step s
+    int ok = 1;
+    if (tid == 0)
+      ok = wait_done(a.done + 2 * w.inst, (s + (unsigned)ph) * I.nA, s * I.nB, &a.sync->abort,
+                     a.wait_ns);
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) {
+        if (!ld_acquire_u32(reinterpret_cast<const unsigned*>(&a.sync->abort)) && I.p.status)
+          atomicExch(I.p.status, 1);
+        atomicExch(&a.sync->abort, 1);
+      }
+      return;
+    }
     const long long t = base + s;
-    for (int ph = 0; ph < kPhases; ph++) {
-      const BatchItem* items = a.items[ph];
-      const int n = a.n_items[ph];
-      for (;;) {
-        __syncthreads();   // the previous item is done with s_it, sp and scs
-        if (tid == 0) s_it = (int)atomicAdd(&a.sync->ticket[ph], 1u);
-        __syncthreads();
-        const int it = s_it;
-        if (it >= n) break;
-        const BatchItem w = items[it];
-        const BatchInst& I = a.insts[w.inst];
-        const int par = (I.par_ref + (int)((t - I.t_ref) & 1)) & 1;
-        {
-          const uint64_t* src = reinterpret_cast<const uint64_t*>(&I.p);
-          uint64_t* dst = reinterpret_cast<uint64_t*>(&g_sp);
-          for (int q = tid; q < (int)(sizeof(FitParams<double>) / 8); q += cThreads)
-            dst[q] = src[q];
-          if (tid < (int)(sizeof(CompState) / 8))
-            reinterpret_cast<uint64_t*>(&g_scs)[tid] =
-                reinterpret_cast<const uint64_t*>(&I.cs[par])[tid];
-        }
-        __syncthreads();
-        bool ok = true;
-        const CompMaps* maps = &a.maps[2 * w.inst + par];
-        if (w.kind != 0) batch_shell(w.kind, w.a, t);
-        else if (I.ct) ok = batch_tile<IdT, SIG, MODE, true>(maps, t, w.a, w.b);
-        else ok = batch_tile<IdT, SIG, MODE, false>(maps, t, w.a, w.b);
-        if (!ok) {
-          if (tid == 0) atomicExch(&a.sync->abort, 1);
-          break;
-        }
-      }
-      if (!grid_barrier(a.sync, ph, a.barrier_ns)) {
-        if (tid == 0 && a.insts[0].p.status) atomicExch(a.insts[0].p.status, 1);
-        return;
-      }
-      // every block reads the flag after the same barrier: all leave together
-      if (ld_acquire_u32(reinterpret_cast<const unsigned*>(&a.sync->abort))) return;
+    const int par = (I.par_ref + (int)((t - I.t_ref) & 1)) & 1;
+    {
+      const uint64_t* src = reinterpret_cast<const uint64_t*>(&I.p);
+      uint64_t* dst = reinterpret_cast<uint64_t*>(&g_sp);
+      for (int q = tid; q < (int)(sizeof(FitParams<double>) / 8); q += cThreads)
+        dst[q] = src[q];
+      if (tid < (int)(sizeof(CompState) / 8))
+        reinterpret_cast<uint64_t*>(&g_scs)[tid] =
+            reinterpret_cast<const uint64_t*>(&I.cs[par])[tid];
+    }
+    __syncthreads();
+    bool good = true;
+    const CompMaps* maps = &a.maps[2 * w.inst + par];
+    if (w.kind != 0) batch_shell(w.kind, w.a, t);
+    else if (I.ct) good = batch_tile<IdT, SIG, MODE, true>(maps, t, w.a, w.b);
+    else good = batch_tile<IdT, SIG, MODE, false>(maps, t, w.a, w.b);
+    if (!good) {
+      if (tid == 0) atomicExch(&a.sync->abort, 1);
+      return;
+    }
+    // publish: this thread's global writes become visible to the TMA loads
+    // (async proxy) and plain loads of the blocks that wait for the count
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(a.done + 2 * w.inst + ph, 1u);
     }
   }
 }
@@ -259,10 +270,12 @@ constexpr size_t align_up(size_t b, size_t a) { return (b + a - 1) / a * a; }
 struct Layout {
   size_t sync, insts, maps, items_a, items_b, total;
 };
+// [sync, counters][instances][maps][items A][items B]; the first region
+// (everything before `insts`) is zeroed by every run
 Layout batch_layout(int n_inst, size_t na, size_t nb) {
   Layout L;
   L.sync = 0;
-  L.insts = align_up(sizeof(BatchSync), 128);
+  L.insts = align_up(sizeof(BatchSync) + 2 * sizeof(unsigned) * (size_t)n_inst, 128);
   L.maps = align_up(L.insts + n_inst * sizeof(BatchInst), 128);
   L.items_a = align_up(L.maps + 2 * (size_t)n_inst * sizeof(CompMaps), 128);
   L.items_b = align_up(L.items_a + na * sizeof(BatchItem), 128);
@@ -337,6 +350,8 @@ int batch_build(const wk_fit_desc* descs, int n_inst, long long t_ref, const cha
     const int gz = (planes + KC - 1) / KC;
     if (gx > 32767 || gy > 32767 || gz > 32767)
       return wk_fail(WK_E_SHAPE, "%s: instance %d: too many tiles", where, q);
+    insts->back().nA = (unsigned)(gx * gy * gz + (mode == 2 ? 4 : 0));
+    insts->back().nB = mode == 2 ? 4u : 0u;
     std::vector<BatchItem>* tl = I.ct ? ia : &tiles_plain;
     for (int bz = 0; bz < gz; bz++)
       for (int by = 0; by < gy; by++)
@@ -466,7 +481,7 @@ extern "C" int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long 
 }
 
 extern "C" int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long step0,
-                            const long long* step_dev, long long barrier_ns, void* stream) {
+                            const long long* step_dev, long long wait_ns, void* stream) {
   const char* where = "wk_batch_run";
   if (!plan || !plan->workspace) return wk_fail(WK_E_NULL, "%s: plan or workspace is NULL", where);
   if (plan->variant < 0 || plan->variant >= kBatchVariants || plan->grid < 1)
@@ -492,7 +507,8 @@ extern "C" int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long st
   a.n_steps = n_steps;
   a.step0 = step0;
   a.step_dev = step_dev;
-  a.barrier_ns = barrier_ns > 0 ? barrier_ns : kBarrierNs;
+  a.done = reinterpret_cast<unsigned*>(ws + sizeof(BatchSync));
+  a.wait_ns = wait_ns > 0 ? wait_ns : kDepNs;
   cudaStream_t st = (cudaStream_t)stream;
   if (plan->form == WK_BATCH_PHASES) {
     const BatchItem* lists[4] = {a.items[0], a.items[0] + plan->n_parts[0],
@@ -514,9 +530,13 @@ extern "C" int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long st
   }
   if (plan->form != WK_BATCH_PERSISTENT)
     return wk_fail(WK_E_MODE, "%s: form %d", where, plan->form);
-  // counters and flags start at zero on every run (a run that gave up
-  // leaves them set)
-  e = cudaMemsetAsync(ws, 0, sizeof(BatchSync), st);
+  const long long per_step_items = (long long)plan->n_items[0] + plan->n_items[1];
+  if ((long long)per_step_items * n_steps >= (1LL << 32))
+    return wk_fail(WK_E_RANGE, "%s: %d steps of %lld items exceed the ticket range", where,
+                   n_steps, per_step_items);
+  // the ticket, the abort flag and the completion counters start at zero
+  // on every run (a run that gave up leaves them set)
+  e = cudaMemsetAsync(ws, 0, (size_t)plan->offsets[0], st);
   if (e != cudaSuccess) return wk_fail(-(int)e, "%s: %s", where, cudaGetErrorString(e));
   cudaLaunchConfig_t cfg;
   memset(&cfg, 0, sizeof(cfg));
