@@ -217,3 +217,29 @@ ABC_SOURCE_CASES = [
          shape=(16, 16, 24), bc_low=["abc", "pec", "pec"], bc_high=["pec", "abc", "abc"],
          Nt=50, abc_copies=True),
 ]
+
+
+# -- Field storage and indexing ----------------------------------------------
+# A small random field and the index patterns, assignments and arithmetic of
+# upstream wakis/field.py (to_matrix, get_abs, __getitem__/__setitem__ with
+# (i, j, k, comp) tuples, lexicographic ints and slices, __mul__/__add__ with
+# scalars, flat arrays, (Nx, Ny, Nz) matrices and fields, compute_ijk).
+FIELD_CASE = dict(shape=(5, 4, 6), seed=300)
+
+
+def field_inputs():
+    """(flat field array, second flat field, (Nx, Ny, Nz) matrix, flat 3N array)."""
+    Nx, Ny, Nz = FIELD_CASE["shape"]
+    N = Nx * Ny * Nz
+    rng = np.random.default_rng(FIELD_CASE["seed"])
+    return (rng.standard_normal(3 * N), rng.standard_normal(3 * N),
+            rng.standard_normal((Nx, Ny, Nz)), rng.standard_normal(3 * N))
+
+
+# (name, key) of the reads compared, and the writes applied in order
+FIELD_READS = [("g_point", (2, 1, 3, "y")), ("g_block", (slice(1, 4), 2, slice(None), "z")),
+               ("g_abs", (slice(None), 1, 2, "Abs")), ("g_x0", (0, slice(None), 5, 0)),
+               ("g_int", 17), ("g_slice", slice(5, 40, 3))]
+FIELD_WRITES = [((slice(1, 3), slice(None), 2, "x"), 7.5), ((0, 0, 0, "z"), -1.0), (10, 3.0),
+                (slice(20, 25), "arange5"), ((slice(None), slice(None), 4, "y"), "plane_y4")]
+FIELD_IJK = [0, 7, 33, 119]

@@ -4,7 +4,7 @@ package (pure Python, loaded through ``refshim``).
 Run on a machine that has the upstream source tree, naming its root in
 ``WAKIS_UPSTREAM``:
 
-    WAKIS_UPSTREAM=<upstream tree> python tests/golden/make_golden.py [step|wake|source|test001]
+    WAKIS_UPSTREAM=<upstream tree> python tests/golden/make_golden.py [step|wake|source|test001|...]
 
 Outputs (all small, committed):
 
@@ -27,6 +27,8 @@ Outputs (all small, committed):
   a few steps, and a full ``wakesolve`` + ``WakeSolver.solve``.
 * ``abc_cases.npz``  E, H, J after ``emsolve`` with ABC faces, with upstream's
   CPU snapshot semantics and with copied snapshots (its GPU semantics).
+* ``field_cases.npz``  upstream ``Field`` storage, indexing, assignment and
+  arithmetic on a small random field (``cases.FIELD_*``).
 
 The case definitions live in ``tests/cases.py`` so that the tests rebuild the
 same inputs without the upstream package.
@@ -248,6 +250,40 @@ def abc_cases(wakis):
     print("abc_cases.npz:", len(cases.ABC_SOURCE_CASES), "cases")
 
 
+def field_cases(wakis):
+    F = wakis.field.Field
+    Nx, Ny, Nz = cases.FIELD_CASE["shape"]
+    a, b, m, flat = cases.field_inputs()
+    f = F(Nx, Ny, Nz)
+    f.fromarray(a.copy())
+    g = F(Nx, Ny, Nz)
+    g.fromarray(b.copy())
+    out = {}
+    for d in "xyz":
+        out[f"mat_{d}"] = np.array(f.to_matrix(d))
+    out["abs"] = np.array(f.get_abs())
+    out["abs_flat"] = np.array(f.get_abs(as_matrix=False))
+    for name, key in cases.FIELD_READS:
+        out[name] = np.array(f[key])
+    h = f.copy()
+    for key, val in cases.FIELD_WRITES:
+        if val == "arange5":
+            val = np.arange(5.0)
+        elif val == "plane_y4":
+            val = m[:, :, 4]
+        h[key] = val
+    out["after_writes"] = np.array(h.toarray())
+    out["mul_scalar"] = (f * 2.5).toarray()
+    out["mul_matrix"] = (f * m).toarray()
+    out["mul_flat"] = (f * flat).toarray()
+    out["add_field"] = (f + g).toarray()
+    out["add_matrix"] = (f + m).toarray()
+    out["add_flat"] = (f + flat).toarray()
+    out["ijk"] = np.array([f.compute_ijk(n) for n in cases.FIELD_IJK])
+    np.savez_compressed(os.path.join(HERE, "field_cases.npz"), **out)
+    print("field_cases.npz:", len(out), "arrays")
+
+
 if __name__ == "__main__":
     wakis = refshim.install()
     only = sys.argv[1:]
@@ -265,3 +301,5 @@ if __name__ == "__main__":
         sibc_cases(wakis)
     if not only or "abc" in only:
         abc_cases(wakis)
+    if not only or "field" in only:
+        field_cases(wakis)

@@ -100,18 +100,55 @@ class Field:
     def field_x(self):
         return self.array[0:self.N]
 
+    @field_x.setter
+    def field_x(self, value):
+        self._set_block(0, value)
+
     @property
     def field_y(self):
         return self.array[self.N:2 * self.N]
+
+    @field_y.setter
+    def field_y(self, value):
+        self._set_block(1, value)
 
     @property
     def field_z(self):
         return self.array[2 * self.N:3 * self.N]
 
-    def get_abs(self):
-        """|F| as an (Nx, Ny, Nz) host array."""
-        x, y, z = (self._comp(k) for k in "xyz")
-        return torch.sqrt(x * x + y * y + z * z).cpu().numpy()
+    @field_z.setter
+    def field_z(self, value):
+        self._set_block(2, value)
+
+    def _set_block(self, d, value):
+        """Component d from an (Nx, Ny, Nz) matrix or a flat N array
+        (upstream field_x/field_y/field_z setters, wakis/field.py:95-120)."""
+        if np.ndim(value) > 1:
+            self.from_matrix(value, d)
+        else:
+            self._before_write()
+            self.array[d * self.N:(d + 1) * self.N] = self._as_tensor(value).reshape(-1)
+
+    def get_abs(self, as_matrix=True):
+        """|F| as an (Nx, Ny, Nz) host array, or flat (N,) with
+        as_matrix=False (upstream get_abs, wakis/field.py:536-574)."""
+        if as_matrix:
+            x, y, z = (self._comp(k).detach().cpu().numpy() for k in "xyz")
+        else:
+            x, y, z = (v.detach().cpu().numpy() for v in (self.field_x, self.field_y,
+                                                          self.field_z))
+        # on the host with numpy's correctly rounded square root, as upstream
+        return np.sqrt(x ** 2 + y ** 2 + z ** 2)
+
+    def compute_ijk(self, n):
+        """(i, j, k) of the lexicographic index n (upstream compute_ijk,
+        wakis/field.py:511-534)."""
+        if n > self.N:
+            raise IndexError("Lexico-graphic index cannot be higher than product of dimensions")
+        k = n // (self.Nx * self.Ny)
+        i = (n - k * self.Nx * self.Ny) % self.Nx
+        j = (n - k * self.Nx * self.Ny) // self.Nx
+        return i, j, k
 
     # -------------------------------------------------------------- indexing
     def __getitem__(self, key):
