@@ -299,6 +299,25 @@ int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* lamH, const void* 
                  const void* decay, void* lamE_out, void* stream);
 
 /*
+ * Hard-source write of step `step` (+ *step_dev when not NULL) into
+ * component `component` of a field (3N entries; dtype WK_F64, WK_F32 or
+ * WK_F32C, the last with its bf16 compensation words `comp`) over the box
+ * [i0,i1) x [j0,j1) x [k0,k1):
+ *   F[c, i, j, k] = (A[t] * prof[(i-i0) + (j-j0)*ni + (k-k0)*ni*nj]) * B[t]
+ * (FP64 products in that order, rounded once to the field's type; prof NULL:
+ * no profile factor, B NULL: no second factor).  A and B hold n_steps FP64
+ * values; a step outside [0, n_steps) writes nothing (and is rejected on the
+ * host when step_dev is NULL).  Replaces the assignment of
+ * PlaneWave / WavePacket / Dipole / Pulse .update(solver, t)
+ * (wakis/sources.py:142-762) that emsolve makes before each step
+ * (wakis/routines.py:207), with the per-step factors tabulated once.
+ */
+int wk_source_write(void* field, int dtype, void* comp, int Nx, int Ny, int Nz, int component,
+                    int i0, int i1, int j0, int j1, int k0, int k1, const double* prof,
+                    const double* A, const double* B, long long n_steps,
+                    const long long* step_dev, long long step, void* stream);
+
+/*
  * Frequency-domain monitor update: for f < nf and d < 3,
  * acc[f][d][n] += E_d[n] * phases[f] (complex double, interleaved re/im,
  * acc laid out [nf][3][N] in the flat field order).  Replaces the loop of

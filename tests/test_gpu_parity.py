@@ -578,6 +578,42 @@ def test_emsolve_sources_match_upstream(idx, golden_dir):
         assert rel_err(got, want) <= 1e-12, (f, rel_err(got, want))
 
 
+@pytest.mark.parametrize("idx", range(len(cases.SOURCE_CASES)))
+def test_emsolve_device_sources_equal_update(idx):
+    """emsolve with the source values tabulated once and written on the
+    device before each step (wk_source_write) equals emsolve through the
+    source's update() value for value (E, H, J)."""
+    import wakis_b200 as wb
+    c = cases.SOURCE_CASES[idx]
+    out = {}
+    for dev in (True, False):
+        g = wb.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)
+        s = wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                           bg="vacuum", use_stl=False, use_sibc=False)
+        src = getattr(wb.sources, c["kind"])(**c["kw"])
+        s.emsolve(c["Nt"], source=src, device_sources=dev)
+        out[dev] = [getattr(s, f).numpy() for f in "EHJ"]
+    for a, b in zip(out[True], out[False]):
+        assert np.array_equal(a, b)
+
+
+def test_emsolve_device_sources_fp32c():
+    """The device-written sources with the compensated state: the written
+    cells carry the source value to ~32 bits (float + compensation word),
+    and the run stays within 1e-6 of the FP64 one."""
+    import wakis_b200 as wb
+    c = cases.SOURCE_CASES[1]
+    res = {}
+    for prec in (None, "fp32c"):
+        g = wb.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)
+        s = wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                           bg="vacuum", use_stl=False, use_sibc=False, precision=prec)
+        s.emsolve(c["Nt"], source=getattr(wb.sources, c["kind"])(**c["kw"]))
+        res[prec] = (_decoded(s, "E"), _decoded(s, "H")) if prec else (s.E.numpy(), s.H.numpy())
+    for a, b in zip(res["fp32c"], res[None]):
+        assert rel_err(a, b) <= 1e-6
+
+
 def _const_field(Nx, Ny, Nz, values):
     from wakis_b200.field import Field
     f = Field(Nx, Ny, Nz, dtype=float, device="cuda")

@@ -70,6 +70,8 @@ _SIGS = {
                                ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_i)]),
     "wk_sigma_e": (_i, [ctypes.POINTER(FitDesc), _vp, _vp]),
     "wk_counter_add": (_i, [_vp, _ll, _vp]),
+    "wk_source_write": (_i, [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp,
+                             _ll, _vp, _ll, _vp]),
     "wk_batch_workspace_bytes": (_ll, [_vp, _i]),
     "wk_batch_prepare": (_i, [_vp, _i, _ll, _vp, _ll, ctypes.POINTER(BatchPlan), _vp]),
     "wk_batch_run": (_i, [ctypes.POINTER(BatchPlan), _i, _ll, _vp, _ll, _vp]),

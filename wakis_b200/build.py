@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libwakis_b200.so")
 SOURCES = ["abi.cu", "fit_step.cu", "fit_fused.cu", "fit_comp.cu", "fit_tma.cu", "fit_tma2.cu", "fit_tma_comp.cu",
-           "fit_batch.cu", "wake.cu", "adjoint.cu", "monitor.cu"]
+           "fit_batch.cu", "wake.cu", "adjoint.cu", "monitor.cu", "sources.cu"]
 HEADERS = ["abi_internal.h", "fit_common.cuh", "fit_kernels.cuh", "fit_comp.cuh", "fit_tma_comp.cuh",
            "tma_util.cuh"]
 

@@ -134,15 +134,27 @@ class RoutinesMixin:
         """Nt steps with an optional host source ``source.update(self, t)``
         and callback (upstream routines.py:17-229, without HDF5 saving or
         plotting).  ABC boundaries are updated after every step from the
-        n-2 snapshot as upstream does."""
+        n-2 snapshot as upstream does.  A source that tabulates its values
+        (``device_terms``: PlaneWave, WavePacket, Dipole, Pulse) is written
+        on the device before every step (``wk_source_write``) instead of
+        through ``update``; ``device_sources=False`` keeps ``update``."""
         self.Nt = Nt
         if source is not None:
             self.source = source
+        terms = None
+        if source is not None and kwargs.get("device_sources", True) and \
+                hasattr(source, "device_terms"):
+            terms = source.device_terms(self, Nt)
+            if terms is not None:
+                terms = [self._upload_source_term(t) for t in terms]
         if self.activate_abc:
             E2, H2 = self.get_abc()
             E1, H1 = self.get_abc()
         for n in range(Nt):
-            if source is not None:
+            if terms is not None:
+                for t in terms:
+                    self._write_source_term(t, n, Nt)
+            elif source is not None:
                 source.update(self, n * self.dt)
             self.one_step()
             if self.activate_abc:
@@ -152,6 +164,46 @@ class RoutinesMixin:
             if callback is not None:
                 callback(self, n * self.dt)
         self.check_status("emsolve")
+
+    def _upload_source_term(self, term):
+        """The tables of a source term on the device (FP64)."""
+        dev = self.device
+        up = dict(term)
+        for k in ("A", "B", "prof"):
+            v = term[k]
+            if v is not None:
+                v = np.asarray(v, np.float64)
+                if k == "prof":
+                    v = v.ravel(order="F")      # i fastest, as the kernel reads it
+                up[k] = torch.as_tensor(np.ascontiguousarray(v), device=dev)
+        return up
+
+    def _write_source_term(self, term, n, n_steps):
+        """Write step n of a source term into the live field (E, H: the live
+        ping-pong buffer and, with fp32c, its compensation words; J: the
+        stored current, materialised first)."""
+        from . import _native
+        fld = term["field"]
+        comp = None
+        if fld == "J":
+            self._materialize_J()
+            buf = self._J
+            dtype = _native.WK_F64 if self._J.dtype == torch.float64 else _native.WK_F32
+        else:
+            self._field_written(self.E if fld == "E" else self.H, reset_comp=False)
+            bufs = self._E if fld == "E" else self._H
+            buf = bufs[self._par]
+            if self.precision == "fp32c":
+                comp = (self._Ec if fld == "E" else self._Hc)[self._par]
+                dtype = _native.WK_F32C
+            else:
+                dtype = _native.WK_F64 if buf.dtype == torch.float64 else _native.WK_F32
+        ptr = lambda t: None if t is None else t.data_ptr()
+        i0, i1, j0, j1, k0, k1 = term["box"]
+        _native.check(self._lib.wk_source_write(
+            buf.data_ptr(), dtype, ptr(comp), self.Nx, self.Ny, self.Nz, term["component"],
+            i0, i1, j0, j1, k0, k1, ptr(term["prof"]), ptr(term["A"]), ptr(term["B"]),
+            n_steps, None, n, self._stream()), "wk_source_write")
 
     # ABC snapshots (upstream boundaries.py:313-410).  One dict per axis, as
     # upstream keeps them: with ABC on both sides of an axis the high side's

@@ -221,10 +221,11 @@ class SolverFIT3D(RoutinesMixin):
         return d
 
     # -------------------------------------------------------------- J state
-    def _field_written(self, fld):
+    def _field_written(self, fld, reset_comp=True):
         """E is about to change between steps: upstream's stored J = sigma*E
         must keep the old E, so materialise it first.  With precision
-        'fp32c' the compensation words of a written field are reset."""
+        'fp32c' the compensation words of a written field are reset (unless
+        the writer sets them itself: reset_comp=False)."""
         if fld is self.E:
             self._faces_clean = False
         if fld is self.E and self._j_state == _J_SIGMA_E:
@@ -232,7 +233,7 @@ class SolverFIT3D(RoutinesMixin):
                 raise RuntimeError("precision='fp32c': E cannot be written between "
                                    "conductive steps (J = sigma*E is kept implicit)")
             self._materialize_J()
-        if self.precision == "fp32c":
+        if self.precision == "fp32c" and reset_comp:
             bufs = self._Ec if fld is self.E else (self._Hc if fld is self.H else None)
             if bufs is not None:
                 bufs[self._par].zero_()

@@ -6,9 +6,14 @@ values into ``solver.E``, ``solver.H`` or ``solver.J`` (device fields).
 ``Beam`` (sources.py:76-110) is also computed by the step kernel itself
 inside ``wakesolve`` (``beam_params``), so no per-step host work or transfer
 is needed there.  ``PlaneWave``, ``WavePacket``, ``Dipole`` and ``Pulse``
-(sources.py:142-762) are hard sources on a slice or a point; their values
-are formed on the host with the same expressions as upstream and written
-with one device copy per field and step.
+(sources.py:142-762) are hard sources on a box (a plane or a point) of one
+field component.  ``update`` forms their values on the host with upstream's
+expressions and writes them with one device copy per field and step.
+``device_terms`` tabulates the same values for all steps of an ``emsolve``
+run at once, as (A(t) * P) * B(t) with the per-step factors A, B evaluated
+by the same per-step expressions (same numpy types) and P the profile as
+upstream's assignment places it; ``emsolve`` then writes them on the device
+(``wk_source_write``) with no per-step host work.
 """
 
 import numpy as np
@@ -95,19 +100,31 @@ class PlaneWave:
         self.kz = self.w / c_light
         self.tmax = np.inf if self.nodes is None else self.nodes / self.f
 
-    def update(self, solver, t):
+    def _first(self, solver):
         if self.is_first_update:
             self.xs = slice(0, solver.Nx) if self.xs is None else self.xs
             self.ys = slice(0, solver.Ny) if self.ys is None else self.ys
             self.is_first_update = False
+
+    def _values(self, t):
         if t <= self.tmax:
             wave = np.cos(self.w * t + self.phase)
-            solver.H[self.xs, self.ys, self.zs, "y"] = -self.amplitude * wave
-            solver.E[self.xs, self.ys, self.zs, "x"] = (self.amplitude * wave
-                                                        / (self.kz / (mu_0 * self.vp)))
-        else:
-            solver.H[self.xs, self.ys, self.zs, "y"] = 0.0
-            solver.E[self.xs, self.ys, self.zs, "x"] = 0.0
+            return -self.amplitude * wave, self.amplitude * wave / (self.kz / (mu_0 * self.vp))
+        return 0.0, 0.0
+
+    def update(self, solver, t):
+        self._first(solver)
+        h, e = self._values(t)
+        solver.H[self.xs, self.ys, self.zs, "y"] = h
+        solver.E[self.xs, self.ys, self.zs, "x"] = e
+
+    def device_terms(self, solver, n_steps):
+        """Hy and Ex of steps 0..n_steps-1 (t = n*dt) as device terms."""
+        self._first(solver)
+        hv, ev = zip(*(self._values(n * solver.dt) for n in range(n_steps))) if n_steps else ((), ())
+        terms = [_term(solver, "H", "y", self.xs, self.ys, self.zs, hv),
+                 _term(solver, "E", "x", self.xs, self.ys, self.zs, ev)]
+        return None if None in terms else terms
 
 
 class WavePacket:
@@ -130,7 +147,7 @@ class WavePacket:
             self.tinj = 6 * self.sigmaz
         self.is_first_update = True
 
-    def update(self, solver, t):
+    def _first(self, solver):
         if self.is_first_update:
             self.xs = slice(0, solver.Nx) if self.xs is None else self.xs
             self.ys = slice(0, solver.Ny) if self.ys is None else self.ys
@@ -141,15 +158,68 @@ class WavePacket:
             if self.tinj is None:
                 self.tinj = 6 * self.sigmaz
             self.is_first_update = False
+
+    def _gxy(self, solver):
+        X, Y = np.meshgrid(solver.x[self.xs], solver.y[self.ys])
+        return np.exp(-(X ** 2 + Y ** 2) / (2 * self.sigmaxy ** 2))
+
+    def _factors(self, solver, t):
+        """(-amp wave, amp mu0 c wave, gt) at time t: the value written is
+        (factor * gxy) * gt, in upstream's order."""
         s0 = solver.z.min() - self.tinj
         s = solver.z.min() - self.beta * c_light * t
-        X, Y = np.meshgrid(solver.x[self.xs], solver.y[self.ys])
-        gxy = np.exp(-(X ** 2 + Y ** 2) / (2 * self.sigmaxy ** 2))
         gt = np.exp(-((s - s0) ** 2) / (2 * self.sigmaz ** 2))
         wave = np.cos(self.w * t + self.phase)
-        solver.H[self.xs, self.ys, self.zs, "y"] = -self.amplitude * wave * gxy * gt
-        solver.E[self.xs, self.ys, self.zs, "x"] = (self.amplitude * mu_0 * c_light * wave
-                                                    * gxy * gt)
+        return -self.amplitude * wave, self.amplitude * mu_0 * c_light * wave, gt
+
+    def update(self, solver, t):
+        self._first(solver)
+        gxy = self._gxy(solver)
+        ah, ae, gt = self._factors(solver, t)
+        solver.H[self.xs, self.ys, self.zs, "y"] = ah * gxy * gt
+        solver.E[self.xs, self.ys, self.zs, "x"] = ae * gxy * gt
+
+    def device_terms(self, solver, n_steps):
+        """Hy and Ex of steps 0..n_steps-1 (t = n*dt) as device terms."""
+        self._first(solver)
+        gxy = self._gxy(solver)
+        f = [self._factors(solver, n * solver.dt) for n in range(n_steps)]
+        ah, ae, gt = (zip(*f) if f else ((), (), ()))
+        terms = [_term(solver, "H", "y", self.xs, self.ys, self.zs, ah, gt, gxy),
+                 _term(solver, "E", "x", self.xs, self.ys, self.zs, ae, gt, gxy)]
+        return None if None in terms else terms
+
+
+def _span(idx, n):
+    """[a, b) of an int or a unit-step slice over n entries; None otherwise."""
+    if isinstance(idx, (int, np.integer)):
+        i = int(idx) + (n if idx < 0 else 0)
+        return (i, i + 1) if 0 <= i < n else None
+    if isinstance(idx, slice) and idx.step in (None, 1):
+        a, b, _ = idx.indices(n)
+        return (a, max(a, b))
+    return None
+
+
+_COMPONENTS = {"x": 0, "y": 1, "z": 2, 0: 0, 1: 1, 2: 2}
+
+
+def _term(solver, field, component, xs, ys, zs, A, B=None, values=None):
+    """One device term: field name, component, box, profile P (as upstream's
+    assignment of `values` places it in the box, None for a scalar), A, B."""
+    comp = _COMPONENTS.get(component)
+    box = (_span(xs, solver.Nx), _span(ys, solver.Ny), _span(zs, solver.Nz))
+    if comp is None or field not in ("E", "H", "J") or None in box:
+        return None
+    prof = None
+    if values is not None:
+        img = np.zeros((solver.Nx, solver.Ny, solver.Nz))
+        img[xs, ys, zs] = values
+        (i0, i1), (j0, j1), (k0, k1) = box
+        prof = img[i0:i1, j0:j1, k0:k1]
+    return dict(field=field, component=comp, box=tuple(v for ab in box for v in ab),
+                prof=prof, A=np.asarray(A, np.float64),
+                B=None if B is None else np.asarray(B, np.float64))
 
 
 def _field_of(solver, name):
@@ -177,7 +247,7 @@ class Dipole:
             self.field, self.component = field[0], field[1]
         self.is_first_update = True
 
-    def update(self, solver, t):
+    def _first(self, solver):
         if self.is_first_update:
             self.xs = int(solver.Nx / 2) if self.xs is None else self.xs
             self.ys = int(solver.Ny / 2) if self.ys is None else self.ys
@@ -186,12 +256,27 @@ class Dipole:
                 self.f = self.nodes / ((solver.z.max() - solver.z.min()) / c_light)
             self.w = 2 * np.pi * self.f
             self.is_first_update = False
+
+    def _value(self, t):
+        return self.amplitude * np.sin(self.w * t + self.phase)
+
+    def update(self, solver, t):
+        self._first(solver)
         fld = _field_of(solver, self.field)
         if fld is None:
             print(f'Field "{self.field}" not valid, should be "E", "H" or "J"]')
             return
-        fld[self.xs, self.ys, self.zs, self.component] = (self.amplitude
-                                                          * np.sin(self.w * t + self.phase))
+        fld[self.xs, self.ys, self.zs, self.component] = self._value(t)
+
+    def device_terms(self, solver, n_steps):
+        """The source component of steps 0..n_steps-1 (t = n*dt) as a device
+        term (None when the field or the box is not one the device writes)."""
+        self._first(solver)
+        if _field_of(solver, self.field) is None:
+            return None
+        t = _term(solver, self.field, self.component, self.xs, self.ys, self.zs,
+                  [self._value(n * solver.dt) for n in range(n_steps)])
+        return None if t is None else [t]
 
 
 class Pulse:
@@ -232,7 +317,7 @@ class Pulse:
         t = t * c_light - self.delay
         return 1.0 if (t < self.L and t > 0.0) else 0.0
 
-    def update(self, solver, t):
+    def _first(self, solver):
         if self.is_first_update:
             self.xs = int(solver.Nx / 2) if self.xs is None else self.xs
             self.ys = int(solver.Ny / 2) if self.ys is None else self.ys
@@ -240,8 +325,22 @@ class Pulse:
             if self.L is None:
                 self.L = 50 * solver.dt
             self.is_first_update = False
+
+    def update(self, solver, t):
+        self._first(solver)
         fld = _field_of(solver, self.field)
         if fld is None:
             print(f'Field "{self.field}" not valid, should be "E", "H" or "J"]')
             return
         fld[self.xs, self.ys, self.zs, self.component] = self.amplitude * self.tprofile(t)
+
+    def device_terms(self, solver, n_steps):
+        """The source component of steps 0..n_steps-1 (t = n*dt) as a device
+        term (None without a time profile, or for a field or box the device
+        does not write)."""
+        self._first(solver)
+        if _field_of(solver, self.field) is None or not hasattr(self, "tprofile"):
+            return None
+        t = _term(solver, self.field, self.component, self.xs, self.ys, self.zs,
+                  [self.amplitude * self.tprofile(n * solver.dt) for n in range(n_steps)])
+        return None if t is None else [t]
