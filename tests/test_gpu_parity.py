@@ -581,20 +581,25 @@ def test_emsolve_sources_match_upstream(idx, golden_dir):
 @pytest.mark.parametrize("idx", range(len(cases.SOURCE_CASES)))
 def test_emsolve_device_sources_equal_update(idx):
     """emsolve with the source values tabulated once and written on the
-    device before each step (wk_source_write) equals emsolve through the
-    source's update() value for value (E, H, J)."""
+    device before each step (wk_source_write; step by step, and replayed
+    from a captured CUDA graph with a device step counter) equals emsolve
+    through the source's update() value for value (E, H, J), with a vacuum
+    and with a conductive background."""
     import wakis_b200 as wb
     c = cases.SOURCE_CASES[idx]
-    out = {}
-    for dev in (True, False):
-        g = wb.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)
-        s = wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
-                           bg="vacuum", use_stl=False, use_sibc=False)
-        src = getattr(wb.sources, c["kind"])(**c["kw"])
-        s.emsolve(c["Nt"], source=src, device_sources=dev)
-        out[dev] = [getattr(s, f).numpy() for f in "EHJ"]
-    for a, b in zip(out[True], out[False]):
-        assert np.array_equal(a, b)
+    for bg in ("vacuum", [1.0, 1.0, 5.0]):
+        out = {}
+        for mode in ("graph", "eager", "update"):
+            g = wb.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)
+            s = wb.SolverFIT3D(g, bc_low=c["bc_low"], bc_high=c["bc_high"], verbose=0,
+                               bg=bg, use_stl=False, use_sibc=False)
+            src = getattr(wb.sources, c["kind"])(**c["kw"])
+            s.emsolve(c["Nt"], source=src, device_sources=mode != "update",
+                      graph=mode == "graph")
+            out[mode] = [getattr(s, f).numpy() for f in "EHJ"]
+        for mode in ("graph", "eager"):
+            for a, b in zip(out[mode], out["update"]):
+                assert np.array_equal(a, b), (bg, mode)
 
 
 def test_emsolve_device_sources_fp32c():

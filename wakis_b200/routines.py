@@ -9,6 +9,7 @@ there.  Only a user callback or field monitor makes the loop return to the
 host between steps, as upstream calls them every step.
 """
 
+import ctypes
 import time
 
 import numpy as np
@@ -147,6 +148,11 @@ class RoutinesMixin:
             terms = source.device_terms(self, Nt)
             if terms is not None:
                 terms = [self._upload_source_term(t) for t in terms]
+        if (terms is not None and not self.activate_abc and callback is None and
+                kwargs.get("graph", True) and Nt > 2 * self._GRAPH_STEPS):
+            self._emsolve_graph(terms, Nt)
+            self.check_status("emsolve")
+            return
         if self.activate_abc:
             E2, H2 = self.get_abc()
             E1, H1 = self.get_abc()
@@ -165,6 +171,58 @@ class RoutinesMixin:
                 callback(self, n * self.dt)
         self.check_status("emsolve")
 
+    # steps per replay of the captured emsolve chunk (even: the ping-pong
+    # parity at the start of every replay is the one it was captured with)
+    _GRAPH_STEPS = 16
+
+    def _emsolve_graph(self, terms, Nt):
+        """emsolve with device sources, no ABC and no callback: the first two
+        steps eagerly (ghost zeroing; the stored-J state settles once a
+        source has written after a step), then chunks of _GRAPH_STEPS steps
+        (source writes + step) captured once in a CUDA graph and replayed,
+        the source tables indexed by a device step counter; the remaining
+        steps eagerly."""
+        from . import _native
+        lib = self._lib
+        for n in range(2):
+            for t in terms:
+                self._write_source_term(t, n, Nt)
+            self.one_step()
+        K = self._GRAPH_STEPS
+        reps = (Nt - 2) // K
+        dev = self.device
+        counter = torch.full((1,), 2, dtype=torch.int64, device=dev)
+        par0 = self._par
+        base = self._step_desc()
+        descs = []
+        for q in range(K):
+            d = _native.FitDesc.from_buffer_copy(base)
+            d.par = par0 ^ (q & 1)
+            descs.append(d)
+        main = torch.cuda.Stream(dev)
+        main.wait_stream(torch.cuda.current_stream(dev))
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=main):
+            st = ctypes.c_void_p(main.cuda_stream)
+            for q in range(K):
+                self._par = par0 ^ (q & 1)
+                for t in terms:
+                    self._write_source_term(t, q, Nt, step_dev=counter, stream=st)
+                _native.check(lib.wk_fit_step(descs[q], 1, 0, st), "wk_fit_step")
+            _native.check(lib.wk_counter_add(ctypes.c_void_p(counter.data_ptr()), K, st),
+                          "wk_counter_add")
+        self._par = par0
+        torch.cuda.current_stream(dev).wait_stream(main)
+        for _ in range(reps):
+            graph.replay()
+        torch.cuda.current_stream(dev).wait_stream(main)
+        del graph
+        self.nstep += reps * K
+        for n in range(2 + reps * K, Nt):
+            for t in terms:
+                self._write_source_term(t, n, Nt)
+            self.one_step()
+
     def _upload_source_term(self, term):
         """The tables of a source term on the device (FP64)."""
         dev = self.device
@@ -178,10 +236,10 @@ class RoutinesMixin:
                 up[k] = torch.as_tensor(np.ascontiguousarray(v), device=dev)
         return up
 
-    def _write_source_term(self, term, n, n_steps):
-        """Write step n of a source term into the live field (E, H: the live
-        ping-pong buffer and, with fp32c, its compensation words; J: the
-        stored current, materialised first)."""
+    def _write_source_term(self, term, n, n_steps, step_dev=None, stream=None):
+        """Write step n (+ *step_dev) of a source term into the live field
+        (E, H: the live ping-pong buffer and, with fp32c, its compensation
+        words; J: the stored current, materialised first)."""
         from . import _native
         fld = term["field"]
         comp = None
@@ -203,7 +261,8 @@ class RoutinesMixin:
         _native.check(self._lib.wk_source_write(
             buf.data_ptr(), dtype, ptr(comp), self.Nx, self.Ny, self.Nz, term["component"],
             i0, i1, j0, j1, k0, k1, ptr(term["prof"]), ptr(term["A"]), ptr(term["B"]),
-            n_steps, None, n, self._stream()), "wk_source_write")
+            n_steps, ptr(step_dev), n, self._stream() if stream is None else stream),
+            "wk_source_write")
 
     # ABC snapshots (upstream boundaries.py:313-410).  One dict per axis, as
     # upstream keeps them: with ABC on both sides of an axis the high side's
