@@ -603,11 +603,12 @@ def test_emsolve_device_sources_equal_update(idx):
 
 
 def test_emsolve_device_sources_fp32c():
-    """The device-written sources with the compensated state: the written
-    cells carry the source value to ~32 bits (float + compensation word),
-    and the run stays within 1e-6 of the FP64 one."""
+    """The device-written sources with the compensated state (a point
+    source on E in a PEC box): the written cells carry the source value to
+    ~32 bits (float + compensation word), and the run stays within 1e-6 of
+    the FP64 one."""
     import wakis_b200 as wb
-    c = cases.SOURCE_CASES[1]
+    c = cases.SOURCE_CASES[2]
     res = {}
     for prec in (None, "fp32c"):
         g = wb.GridFIT3D(*cases.SOURCE_BOUNDS, *c["shape"], verbose=0)

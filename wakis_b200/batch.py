@@ -8,9 +8,9 @@ the stepping of all of them is shared:
 * ``launch="batched"`` (FP32-compensated instances, ``wk_batch_run``): one
   device work list of (instance, tile, z-chunk) items and boundary-plane
   items over all instances, run either as ONE persistent cooperative launch
-  per chunk of steps (its blocks walk the lists of every step and meet at a
-  bounded grid barrier after each phase) or as one launch per list and step
-  (form "phases").  The step index comes from a device counter, so the
+  per chunk of steps (its blocks claim the items of every step in order and
+  an item waits, bounded, only for its own instance's earlier work) or as
+  one launch per list and step (form "phases").  The step index comes from a device counter, so the
   chunk is captured once in a CUDA graph and replayed.  An autotuner times
   both forms and the candidate planes per work item (the z depth of the
   tiles, ``SolverFIT3D.tile``) on the whole batch and keeps the fastest.

@@ -188,6 +188,13 @@ class RoutinesMixin:
             for t in terms:
                 self._write_source_term(t, n, Nt)
             self.one_step()
+        if self.use_conductivity and any(t["field"] in ("E", "J") for t in terms):
+            # a write to E or J between conductive steps keeps upstream's
+            # stored J = sigma*E of the step before (the eager loop
+            # materialises it before each write): with the J array
+            # materialised once, every captured step reads it and writes
+            # sigma*E_new back for the next one
+            self._materialize_J()
         K = self._GRAPH_STEPS
         reps = (Nt - 2) // K
         dev = self.device
