@@ -557,13 +557,13 @@ def run_slab(args):
                 ixt - 1, iyt - 1, 3, 3) for r in mine}
 
     G = lay[0].depth
+    streams = slab.side_streams(solvers, mine)
 
     def steps(n0, k):
         m = n0
         while m < n0 + k:
             c = min(G, n0 + k - m)
-            for r in mine:
-                solvers[r]._advance(c, m, beam=bp, capture=caps[r])
+            slab.advance(solvers, mine, c, m, bp, caps, streams)
             ex(lay, solvers)
             m += c
 
@@ -613,16 +613,38 @@ def run_slab(args):
           for r in mine}
     ez = {r: torch.empty((args.steps, 9, solvers[r].Nz), dtype=solvers[r]._cap_dtype
                          ).pin_memory() for r in mine}
+    main = torch.cuda.current_stream(dev)
+    # warm-up of the I/O path (its device staging buffers are allocated on
+    # the first call, on the stream of the call), one exchange block
+    nw = min(G, args.steps)
+    for r in mine:
+        if streams:
+            streams[r].wait_stream(main)
+        with torch.cuda.stream(streams[r] if streams else main):
+            solvers[r].run_with_io(jz[r][:nw].clone().pin_memory(),
+                                   torch.empty_like(ez[r][:nw]).pin_memory(), step0=step0)
+        if streams:
+            main.wait_stream(streams[r])
+    ex(lay, solvers)
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for m in range(0, args.steps, G):
         c = min(G, args.steps - m)
         for r in mine:
-            solvers[r].run_with_io(jz[r][m:m + c], ez[r][m:m + c], step0=step0 + m)
+            if streams:
+                streams[r].wait_stream(main)
+            with torch.cuda.stream(streams[r] if streams else main):
+                solvers[r].run_with_io(jz[r][m:m + c], ez[r][m:m + c], step0=step0 + m,
+                                       wait=False)
+        if streams:
+            for r in mine:
+                main.wait_stream(streams[r])
         ex(lay, solvers)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
+    for r in mine:
+        solvers[r].check_status("bench (slabs, end to end)")
     clocks = region_clocks or clk.stop()
     if region_clocks is not None:
         clk.stop()
@@ -645,6 +667,7 @@ def run_slab(args):
                        "slabs": [[s.k0, s.k1] for s in lay],
                        "exchange": "NCCL point-to-point" if ws > 1 else "device copies",
                        "ghost_depth": G,
+                       "slab_streams": "one per slab" if streams else "current stream",
                        "l2": "state above L2, no flush",
                        "step": "fused beam + Ez 3x3 capture + H and E half-steps + ghost "
                                "exchange"},

@@ -110,6 +110,22 @@ def test_partition_and_layout():
         slab.layout(20, 3, depth=7)
 
 
+def test_side_streams_only_for_several_cuda_slabs():
+    """Slabs get their own streams only when one process holds two or more
+    of them on CUDA devices; otherwise advance() runs them in turn on the
+    current stream (no stream is created on a host without a GPU)."""
+    from types import SimpleNamespace
+    cpu = {r: SimpleNamespace(device=torch.device("cpu")) for r in range(3)}
+    assert slab.side_streams(cpu, [0, 1, 2]) is None
+    one = {0: SimpleNamespace(device=torch.device("cuda", 0))}
+    assert slab.side_streams(one, [0]) is None
+    calls = []
+    fake = {r: SimpleNamespace(_advance=lambda c, n0, beam=None, capture=None, r=r:
+                               calls.append((r, c, n0, capture))) for r in range(2)}
+    slab.advance(fake, [0, 1], 4, 8, captures={0: "c0", 1: "c1"})
+    assert calls == [(0, 4, 8, "c0"), (1, 4, 8, "c1")]
+
+
 @pytest.mark.parametrize("n,depth", [(2, 1), (3, 1), (2, 2), (2, 4), (3, 3)])
 @pytest.mark.parametrize("idx", VALID)
 def test_emulated_slabs_equal_single_domain(idx, n, depth):

@@ -144,6 +144,39 @@ def _planes(solver):
     return [b.view(3, solver.Nz, nxy) for b in bufs]
 
 
+def side_streams(solvers, mine):
+    """One stream per slab of `mine` when this process holds more than one
+    slab on a CUDA device (else None): ``advance`` then runs the slabs of
+    one device concurrently, so that one slab's step kernel fills the last
+    wave of another's."""
+    devs = [solvers[r].device for r in mine]
+    if len(mine) < 2 or any(getattr(d, "type", None) != "cuda" for d in devs):
+        return None
+    return {r: torch.cuda.Stream(device=solvers[r].device) for r in mine}
+
+
+def advance(solvers, mine, count, n0, beam=None, captures=None, streams=None):
+    """`count` steps from step n0 of the slabs `mine` (fused beam parameters
+    and Ez capture per slab optional).  With `streams` (``side_streams``)
+    each slab's launches go to its own stream, ordered after the work on
+    the device's current stream and joined back into it before the return,
+    so what follows on the current stream (the exchange) sees every slab's
+    steps."""
+    if streams is None:
+        for r in mine:
+            solvers[r]._advance(count, n0, beam=beam,
+                                capture=captures[r] if captures is not None else None)
+        return
+    for r in mine:
+        s = streams[r]
+        s.wait_stream(torch.cuda.current_stream(solvers[r].device))
+        with torch.cuda.stream(s):
+            solvers[r]._advance(count, n0, beam=beam,
+                                capture=captures[r] if captures is not None else None)
+    for r in mine:
+        torch.cuda.current_stream(solvers[r].device).wait_stream(streams[r])
+
+
 class LocalExchange:
     """Ghost-plane exchange between slabs held by this process (any devices)."""
 
@@ -266,6 +299,7 @@ class SlabWakeSolve:
                 dtype=dtype, verbose=0, precision=precision, device=devices[r],
                 coefficients=slice_coefficients(c, s.lo, s.hi), fmax=fmax)
         self.precision = precision
+        self.streams = side_streams(self.solvers, mine)
         self.x = grid.x[:-1] + grid.dx / 2
         self.y = grid.y[:-1] + grid.dy / 2
         self.z = grid.z[:-1] + grid.dz / 2
@@ -274,9 +308,7 @@ class SlabWakeSolve:
     def _block(self, n0, count, beam=None, captures=None):
         """Steps n0 .. n0+count-1 (count <= depth) of every slab, then the
         exchange."""
-        for r in self.mine:
-            cap = captures[r] if captures is not None else None
-            self.solvers[r]._advance(count, n0, beam=beam, capture=cap)
+        advance(self.solvers, self.mine, count, n0, beam, captures, self.streams)
         self.exchange(self.slabs, self.solvers)
 
     def _steps(self, n0, n_steps, beam=None, captures=None):

@@ -359,7 +359,7 @@ class SolverFIT3D(RoutinesMixin):
             self._j_line = (ixs, iys, vals)
 
     def run_with_io(self, jz_lines, ez_out, step0=0, xtest=0.0, ytest=0.0, xsource=0.0,
-                    ysource=0.0, chunk=4):
+                    ysource=0.0, chunk=4, wait=True):
         """Advance len(jz_lines) steps exchanging data with host memory for
         every step, the data movement of upstream's GPU wakesolve loop
         (wakis/routines.py:435-445): the Jz line current of the beam line of
@@ -371,7 +371,9 @@ class SolverFIT3D(RoutinesMixin):
         kernels can run two steps per launch.  Both host tensors should be
         pinned; all copies and steps are queued on the current stream; the
         call returns after they completed (it reads the status word of the
-        step kernels and raises if one timed out)."""
+        step kernels and raises if one timed out).  With ``wait=False`` it
+        returns once they are queued: the caller then waits for the stream
+        before it reads ``ez_out`` and calls ``check_status``."""
         n_steps, nz = jz_lines.shape
         chunk = max(1, int(chunk))
         ixs = int(np.abs(self.x - xsource).argmin())
@@ -403,7 +405,8 @@ class SolverFIT3D(RoutinesMixin):
                 stage[:c].copy_(cbuf.permute(2, 0, 1))
                 ez_out[n:n + c].copy_(stage[:c], non_blocking=True)
             n += c
-        self.check_status("run_with_io")
+        if wait:
+            self.check_status("run_with_io")
 
     def check_status(self, what="step"):
         """Wait for the solver's stream and raise RuntimeError when a step
