@@ -292,11 +292,27 @@ int wk_adj_grad(int dtype, const long long* cells, long long ncell, long long N,
  *   wk_adj_h_fit: lH_out = lH_in + dt * B0^T (ieps .* lE)
  *   wk_adj_e_fit: lE_out = decay .* lE_in - A^T lH      (decay may be NULL: 1)
  * lH_in may equal lH_out and lE_in may equal lE_out.  Fewer than 2^31 cells.
+ * fu / fw (3N entries of dtype) are the cell factors of wk_adj_factors:
+ * with them the products of each cell are formed once per z-marching tile;
+ * with NULL, or with d->kernel == WK_KERNEL_CELL, one thread per cell forms
+ * the products of its neighbours from the tables itself (the cross-check:
+ * the same values).
  */
-int wk_adj_h_fit(const wk_fit_desc* d, int dtype, const void* lamE, const void* lamH_in,
-                 void* lamH_out, void* stream);
-int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* lamH, const void* lamE_in,
-                 const void* decay, void* lamE_out, void* stream);
+int wk_adj_h_fit(const wk_fit_desc* d, int dtype, const void* fu, const void* lamE,
+                 const void* lamH_in, void* lamH_out, void* stream);
+int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* fw, const void* lamH,
+                 const void* lamE_in, const void* decay, void* lamE_out, void* stream);
+
+/*
+ * The cell factors of the two transposes, in the adjoint type dtype:
+ *   fu[c N + n] = itA_c(n) pec_c(n) ieps_c(n)          (B0^T ieps)
+ *   fw[c N + n] = dt iA_c(n) imu_c(n) pmc_c(n)          (A^T)
+ * each product rounded as the stencils of wk_adj_h_fit / wk_adj_e_fit form
+ * it.  They depend only on the descriptor's coefficient tables, so a
+ * backward pass forms them once.  Either pointer may be NULL, not both.
+ * No counterpart in the reference.
+ */
+int wk_adj_factors(const wk_fit_desc* d, int dtype, void* fu, void* fw, void* stream);
 
 /*
  * Hard-source write of step `step` (+ *step_dev when not NULL) into

@@ -497,6 +497,53 @@ def test_adjoint_stencil_transposes_equal_csr(dtype, adt):
         assert np.max(np.abs(a - b)) <= tol * np.max(np.abs(b))
 
 
+@pytest.mark.parametrize("adt", [np.float64, np.float32])
+@pytest.mark.parametrize("shape", [(7, 5, 9), (37, 13, 11), (64, 16, 10), (33, 9, 17)])
+@pytest.mark.parametrize("idx", VALID[::5])
+def test_adjoint_tiled_transposes_equal_per_cell(idx, shape, adt):
+    """The z-marching tiled transposes (the default of wk_adj_h_fit /
+    wk_adj_e_fit), with the cell factors from the tables or from
+    wk_adj_factors, equal the one-thread-per-cell kernels value for value,
+    in place, with and without the decay factor, on grids whose edges cut
+    the 32x8 tiles (the flat-offset neighbours past a row or plane end) and
+    on every face mix of the step cases."""
+    import ctypes
+    from wakis_b200 import _native
+    c = dict(cases.STEP_CASES[idx], shape=shape)
+    s = b200_step_case(c)
+    base = _native.FitDesc.from_buffer_copy(s._sync_desc())
+    N = s.N
+    rng = np.random.default_rng(idx + sum(shape))
+    tdt = torch.float64 if adt == np.float64 else torch.float32
+    wk = _native.WK_F64 if adt == np.float64 else _native.WK_F32
+    mk = lambda lo, hi: torch.tensor(rng.uniform(lo, hi, 3 * N), dtype=tdt, device="cuda")
+    lamE, lamH, decay = mk(-1, 1), mk(-1, 1), mk(0.5, 1)
+    lib = _native.lib()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    fu, fw = torch.empty_like(lamE), torch.empty_like(lamE)
+    _native.check(lib.wk_adj_factors(base, wk, ptr(fu), ptr(fw), st), "wk_adj_factors")
+    out = {}
+    for kern, fac in ((_native.WK_KERNEL_CELL, False), (_native.WK_KERNEL_AUTO, False),
+                      (_native.WK_KERNEL_AUTO, True)):
+        d = _native.FitDesc.from_buffer_copy(base)
+        d.kernel = kern
+        pu, pw = (ptr(fu), ptr(fw)) if fac else (None, None)
+        h, e, e2 = lamH.clone(), lamE.clone(), lamE.clone()
+        _native.check(lib.wk_adj_h_fit(d, wk, pu, ptr(lamE), ptr(h), ptr(h), st),
+                      "wk_adj_h_fit")
+        _native.check(lib.wk_adj_e_fit(d, wk, pw, ptr(h), ptr(e), ptr(decay), ptr(e), st),
+                      "wk_adj_e_fit")
+        _native.check(lib.wk_adj_e_fit(d, wk, pw, ptr(lamH), ptr(e2), None, ptr(e2), st),
+                      "wk_adj_e_fit")
+        out[(kern, fac)] = [t.cpu().numpy() for t in (h, e, e2)]
+    ref = out[(_native.WK_KERNEL_CELL, False)]
+    for key in ((_native.WK_KERNEL_AUTO, False), (_native.WK_KERNEL_AUTO, True)):
+        for a, b in zip(out[key], ref):
+            assert np.array_equal(a, b), key
+            assert np.any(a != 0)
+
+
 def test_adjoint_operators_match_step_kernels():
     """A and B0 assembled on the host reproduce the step kernels: from
     random (E, H) one FP64 step equals H - A E, E + dt ieps (B0 H')."""

@@ -80,8 +80,9 @@ _SIGS = {
     "wk_adj_e": (_i, [_i, _vp, _vp, _vp, _ll, _vp, _vp, _vp, _vp, _vp]),
     "wk_adj_grad": (_i, [_i, _vp, _ll, _ll, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_double,
                          _vp, _vp, _vp]),
-    "wk_adj_h_fit": (_i, [ctypes.POINTER(FitDesc), _i, _vp, _vp, _vp, _vp]),
-    "wk_adj_e_fit": (_i, [ctypes.POINTER(FitDesc), _i, _vp, _vp, _vp, _vp, _vp]),
+    "wk_adj_h_fit": (_i, [ctypes.POINTER(FitDesc), _i, _vp, _vp, _vp, _vp, _vp]),
+    "wk_adj_e_fit": (_i, [ctypes.POINTER(FitDesc), _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "wk_adj_factors": (_i, [ctypes.POINTER(FitDesc), _i, _vp, _vp, _vp]),
     "wk_wake_potential": (_i, [_vp, _i, _ll, _i, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _i,
                                _vp, _ll, _d, _d, _d, _d, _d, _d, _d, _i, _vp, _vp]),
     "wk_trans_wake": (_i, [_vp, _i, _d, _d, _d, _vp, _vp, _vp]),

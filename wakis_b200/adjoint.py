@@ -18,8 +18,10 @@ time step (the relaxation-time clamp of the constructor is not re-evaluated).
   index wrap as the wake kernel), so torch autograd gives dL/dEz(k, n).
 * Backward: segment by segment from the end, the forward states of the
   segment are recomputed from its checkpoint, then the adjoint steps
-  (``wk_adj_h_fit``, ``wk_adj_e_fit``: A^T and B0^T applied as stencils over
-  the compact coefficient tables the step kernels read; ``operators="csr"``
+  (``wk_adj_h_fit``, ``wk_adj_e_fit``: A^T and B0^T applied as z-marching
+  tiled stencils, with the cell factors formed once per backward pass from
+  the compact coefficient tables the step kernels read
+  (``wk_adj_factors``); ``operators="csr"``
   uses ``wk_adj_h`` / ``wk_adj_e`` with CSR matrices assembled on the host
   instead) run backwards with dL/dEz injected at the test line, and
   ``wk_adj_grad``
@@ -405,11 +407,12 @@ class ImpedanceDesign:
                 ptr(gS), ctypes.c_void_p(st)), "wk_adj_grad")
             if self.operators == "stencil":
                 d = B["coef_desc"]
-                _native.check(lib.wk_adj_h_fit(d, self.wk, ptr(lE), ptr(lH), ptr(lH),
-                                               ctypes.c_void_p(st)), "wk_adj_h_fit")
+                _native.check(lib.wk_adj_h_fit(d, self.wk, ptr(B["fu"]), ptr(lE), ptr(lH),
+                                               ptr(lH), ctypes.c_void_p(st)), "wk_adj_h_fit")
                 _native.check(lib.wk_adj_e_fit(
-                    d, self.wk, ptr(lH), ptr(lE), ptr(B["decay"]) if use_sig else None,
-                    ptr(lE), ctypes.c_void_p(st)), "wk_adj_e_fit")
+                    d, self.wk, ptr(B["fw"]), ptr(lH), ptr(lE),
+                    ptr(B["decay"]) if use_sig else None, ptr(lE), ctypes.c_void_p(st)),
+                    "wk_adj_e_fit")
             else:
                 _native.check(lib.wk_adj_h(
                     self.wk, ptr(self.B0T.rowptr), ptr(self.B0T.col), ptr(self.B0T.val),
@@ -468,6 +471,14 @@ class ImpedanceDesign:
             "ones": torch.ones(3 * N, dtype=self.tdtype, device=dev),
         }
         B["coef_desc"] = _native.FitDesc.from_buffer_copy(s._sync_desc())
+        if self.operators == "stencil":
+            # the cell factors of the two transposes, formed once
+            B["fu"] = torch.empty(3 * N, dtype=self.tdtype, device=dev)
+            B["fw"] = torch.empty(3 * N, dtype=self.tdtype, device=dev)
+            _native.check(self.lib.wk_adj_factors(
+                B["coef_desc"], self.wk, ctypes.c_void_p(B["fu"].data_ptr()),
+                ctypes.c_void_p(B["fw"].data_ptr()),
+                ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)), "wk_adj_factors")
 
         def stage(a, m):
             if B["bJ"] is not None:

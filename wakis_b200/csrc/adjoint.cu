@@ -88,25 +88,52 @@ k_adj_grad(const long long* __restrict__ cells, long long ncell, long long N,
 //       u_d(n) = itA_d(n) pec_d(n) ieps_d(n) lamE[d, n]            (n < N)
 //   lamE'[e, m] = decay[e, m] lamE[e, m] - L_e(m) pec_e(m) sum sg w_d(m - off),
 //       w_d(n) = dt iA_d(n) imu_d(n) pmc_d(n) lamH'[d, n]          (n >= 0)
-// with the signs and offsets of the curl (x: +1, y: +Nx, z: +Nx*Ny).
+// with the signs and offsets of the curl (x: +1, y: +Nx, z: +Nx*Ny).  The
+// products are rounded one by one (no fused multiply-add), so that every
+// form of these sums gives the same values.
+// the cell factor of u_d (itA_d pec_d ieps_d) and of w_d (dt iA_d imu_d pmc_d)
 template <typename T, typename L>
-__device__ __forceinline__ L adj_u(const FitParams<T>& p, const L* lamE, int d, Cell c,
-                                   long long n) {
+__device__ __forceinline__ L adj_fu(const FitParams<T>& p, int d, Cell c, long long n) {
   const int id = load_id(p.mat_id, p.id_bytes, n);
   T f = d == 0 ? p.itAx[c.j + (long long)c.k * p.Ny]
                : (d == 1 ? p.itAy[c.i + (long long)c.k * p.Nx] : p.itAz[c.i + (long long)c.j * p.Nx]);
   if (p.has_pec && !face_val(p.pec_face, d, c.i, c.j, c.k, p.Nx, p.Ny, p.Nz)) f = T(0);
-  return (L)f * (L)p.mat[9 * id + d] * lamE[d * p.N + n];
+  return mul((L)f, (L)p.mat[9 * id + d]);
+}
+
+template <typename T, typename L>
+__device__ __forceinline__ L adj_fw(const FitParams<T>& p, int d, Cell c, long long n) {
+  const int id = load_id(p.mat_id, p.id_bytes, n);
+  T f = d == 0 ? p.iAx[c.j + (long long)c.k * p.Ny]
+               : (d == 1 ? p.iAy[c.i + (long long)c.k * p.Nx] : p.iAz[c.i + (long long)c.j * p.Nx]);
+  if (p.has_pmc && !face_val(p.pmc_face, d, c.i, c.j, c.k, p.Nx, p.Ny, p.Nz)) f = T(0);
+  return mul(mul((L)p.dt, (L)f), (L)p.mat[9 * id + 3 + d]);
+}
+
+template <typename T, typename L>
+__device__ __forceinline__ L adj_u(const FitParams<T>& p, const L* lamE, int d, Cell c,
+                                   long long n) {
+  return mul(adj_fu<T, L>(p, d, c, n), lamE[d * p.N + n]);
 }
 
 template <typename T, typename L>
 __device__ __forceinline__ L adj_w(const FitParams<T>& p, const L* lamH, int d, Cell c,
                                    long long n) {
-  const int id = load_id(p.mat_id, p.id_bytes, n);
-  T f = d == 0 ? p.iAx[c.j + (long long)c.k * p.Ny]
-               : (d == 1 ? p.iAy[c.i + (long long)c.k * p.Nx] : p.iAz[c.i + (long long)c.j * p.Nx]);
-  if (p.has_pmc && !face_val(p.pmc_face, d, c.i, c.j, c.k, p.Nx, p.Ny, p.Nz)) f = T(0);
-  return (L)p.dt * (L)f * (L)p.mat[9 * id + 3 + d] * lamH[d * p.N + n];
+  return mul(adj_fw<T, L>(p, d, c, n), lamH[d * p.N + n]);
+}
+
+// fu[d N + n] and fw[d N + n] of every cell (either may be NULL)
+template <typename T, typename L>
+__global__ void __launch_bounds__(kAdjThreads)
+k_adj_factors(FitParams<T> p, L* fu, L* fw) {
+  const long long m = blockIdx.x * (long long)kAdjThreads + threadIdx.x;
+  if (m >= p.N) return;
+  const Cell c = cell_of(m, p.Nx, p.Ny);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (fu) fu[d * p.N + m] = adj_fu<T, L>(p, d, c, m);
+    if (fw) fw[d * p.N + m] = adj_fw<T, L>(p, d, c, m);
+  }
 }
 
 template <typename T, typename L>
@@ -132,7 +159,7 @@ k_adj_h_fit(FitParams<T> p, const L* __restrict__ lamE, const L* lamH_in, L* lam
   const L dt = (L)p.dt;
 #pragma unroll
   for (int e = 0; e < 3; e++)
-    lamH_out[e * N + m] = lamH_in[e * N + m] + dt * (L)coltL(p, e, c.i, c.j, c.k) * acc[e];
+    lamH_out[e * N + m] = add(lamH_in[e * N + m], mul(mul(dt, (L)coltL(p, e, c.i, c.j, c.k)), acc[e]));
 }
 
 template <typename T, typename L>
@@ -159,7 +186,162 @@ k_adj_e_fit(FitParams<T> p, const L* __restrict__ lamH, const L* lamE_in,
 #pragma unroll
   for (int e = 0; e < 3; e++) {
     const L dec = decay ? decay[e * N + m] : L(1);
-    lamE_out[e * N + m] = dec * lamE_in[e * N + m] - (L)colL(p, e, c.i, c.j, c.k) * acc[e];
+    lamE_out[e * N + m] = sub(mul(dec, lamE_in[e * N + m]), mul((L)colL(p, e, c.i, c.j, c.k), acc[e]));
+  }
+}
+
+// Tiled transposes (wk_adj_h_fit / wk_adj_e_fit with the cell factors of
+// wk_adj_factors): block (bx, by, bz) owns the cells i in [i0, i0+32),
+// j in [j0, j0+8) of the planes [k0, k0+KC) and marches in z, one thread per
+// cell.  The products u = fu lamE (H transpose, DIR > 0) or w = fw lamH (E
+// transpose, DIR < 0) of a plane are formed once, for the tile plus the
+// one-cell halo the stencil reaches (+x/+y for u, -x/-y for w), into a
+// 3-slot ring of shared-memory planes; every output then reads its
+// neighbours' products there (u of planes k and k+1, w of planes k and k-1)
+// with the same expressions, in the same order, as the one-thread-per-cell
+// kernels above, which stay as the cross-check (wk_fit_desc.kernel =
+// WK_KERNEL_CELL, or no factors).  The factor and adjoint values of the
+// thread's own entry are loaded one plane ahead into registers, so that the
+// loads of the next plane are in flight while this one is formed and
+// written.  A halo entry one past the grid's last column or row holds the
+// product of the cell that the flat-offset operators reach there (the next
+// row or plane), as plus_x / plus_y / minus_x / minus_y give it.
+constexpr int kAX = 32, kAY = 8, kATh = kAX * kAY;
+constexpr int kAW = kAX + 1;                       // entry row width
+constexpr int kAEnt = kAW * (kAY + 1);             // entries per plane and component
+constexpr int kAHalo = kAX + kAY;                  // halo entries per plane
+
+// Source cell of the entry (i, j) of plane q: the cell itself inside the
+// grid; one past the last column / row (DIR > 0) or before the first
+// (DIR < 0) the flat-offset neighbour of the grid's edge cell; false where
+// no cell (the flat index leaves [0, N)) or the entry is not read.
+template <int DIR>
+__device__ __forceinline__ bool adj_src(int i, int j, int q, int Nx, int Ny, int Nz, Cell& c) {
+  if (q < 0 || q >= Nz + (DIR > 0 ? 1 : 0)) return false;
+  if (i >= 0 && i < Nx && j >= 0 && j < Ny) {
+    c.i = i; c.j = j; c.k = q;
+    return q < Nz;
+  }
+  Cell e;
+  if (DIR > 0) {
+    if (i == Nx && j >= 0 && j < Ny) { e.i = Nx - 1; e.j = j; e.k = q; c = plus_x(e, Nx, Ny); }
+    else if (j == Ny && i >= 0 && i < Nx) { e.i = i; e.j = Ny - 1; e.k = q; c = plus_y(e, Ny); }
+    else return false;
+    return c.k < Nz;
+  }
+  if (i == -1 && j >= 0 && j < Ny) { e.i = 0; e.j = j; e.k = q; c = minus_x(e, Nx, Ny); }
+  else if (j == -1 && i >= 0 && i < Nx) { e.i = i; e.j = 0; e.k = q; c = minus_y(e, Ny); }
+  else return false;
+  return c.k >= 0 && c.k < Nz;
+}
+
+// factor and adjoint value of the three components of one entry (0 where
+// adj_src gives no cell)
+template <typename L>
+struct AdjRaw {
+  L f[3], v[3];
+};
+
+template <int DIR, typename L>
+__device__ __forceinline__ void adj_raw(const L* fac, const L* lam, int i, int j, int q, int Nx,
+                                        int Ny, int Nz, long long N, AdjRaw<L>& r) {
+  Cell c;
+  const bool v = adj_src<DIR>(i, j, q, Nx, Ny, Nz, c);
+  const long long n = v ? c.i + (long long)c.j * Nx + (long long)c.k * Nx * (long long)Ny : 0;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    r.f[d] = v ? fac[d * N + n] : L(0);
+    r.v[d] = v ? lam[d * N + n] : L(0);
+  }
+}
+
+template <typename L>
+__device__ __forceinline__ void adj_put(const AdjRaw<L>& r, L* slot, int e) {
+#pragma unroll
+  for (int d = 0; d < 3; d++) slot[d * kAEnt + e] = mul(r.f[d], r.v[d]);
+}
+
+// DIR > 0: xout = xin + dt tL pmc (sum of u), lam = lamE (wk_adj_h_fit);
+// DIR < 0: xout = decay xin - L pec (sum of w), lam = lamH (wk_adj_e_fit).
+template <typename T, typename L, int DIR>
+__global__ void __launch_bounds__(kATh, 3)
+k_adj_tile(FitParams<T> p, const L* __restrict__ fac, const L* __restrict__ lam, const L* xin,
+           const L* __restrict__ decay, L* xout, int KC) {
+  __shared__ L S[3][3 * kAEnt];                    // [slot][comp][entry]
+  constexpr int o = DIR > 0 ? 0 : 1;               // entry of tile cell (0, 0)
+  const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
+  const long long N = p.N;
+  const int i0 = blockIdx.x * kAX, j0 = blockIdx.y * kAY;
+  const int k0 = blockIdx.z * KC, k1 = min(k0 + KC, Nz);
+  const int tid = threadIdx.x, a = tid & (kAX - 1), b = tid / kAX;
+  const int i = i0 + a, j = j0 + b;
+  const bool own = i < Nx && j < Ny;
+  const int e0 = (b + o) * kAW + a + o;
+  // the halo entry of threads tid < kAHalo: kAY of the x halo column, then
+  // kAX of the y halo row
+  const bool halo = tid < kAHalo;
+  const int ha = tid < kAY ? (DIR > 0 ? kAX : -1) : tid - kAY;
+  const int hb = tid < kAY ? tid : (DIR > 0 ? kAY : -1);
+  const int he = (hb + o) * kAW + ha + o;
+  // plane q written at iteration it: p0 + 1 + it (u(k+1) or w(k)); slot 0
+  // holds plane p0 (u(k0) or w(k0-1))
+  const int p0 = DIR > 0 ? k0 : k0 - 1;
+  AdjRaw<L> r1, r2;
+  adj_raw<DIR>(fac, lam, i, j, p0, Nx, Ny, Nz, N, r2);
+  adj_put(r2, S[0], e0);
+  if (halo) {
+    AdjRaw<L> h;
+    adj_raw<DIR>(fac, lam, i0 + ha, j0 + hb, p0, Nx, Ny, Nz, N, h);
+    adj_put(h, S[0], he);
+  }
+  adj_raw<DIR>(fac, lam, i, j, p0 + 1, Nx, Ny, Nz, N, r1);
+  int sa = 0;                                      // slot of plane p0 + it
+  for (int k = k0; k < k1; k++) {
+    const int sb = sa == 2 ? 0 : sa + 1;           // slot of plane p0 + it + 1
+    const int q = p0 + 1 + (k - k0);
+    if (k + 1 < k1) adj_raw<DIR>(fac, lam, i, j, q + 1, Nx, Ny, Nz, N, r2);
+    const long long m = i + (long long)j * Nx + (long long)k * p.NxNy;
+    L xi[3], dc[3];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      xi[e] = own ? xin[e * N + m] : L(0);
+      dc[e] = (DIR < 0 && own && decay) ? decay[e * N + m] : L(1);
+    }
+    adj_put(r1, S[sb], e0);
+    if (halo) {
+      AdjRaw<L> h;
+      adj_raw<DIR>(fac, lam, i0 + ha, j0 + hb, q, Nx, Ny, Nz, N, h);
+      adj_put(h, S[sb], he);
+    }
+    __syncthreads();
+    if (own) {
+      if (DIR > 0) {
+        const L* uc = S[sa];                       // u(k)
+        const L* un = S[sb];                       // u(k+1)
+        const L u0 = uc[e0], u1 = uc[kAEnt + e0], u2 = uc[2 * kAEnt + e0];
+        const L u0y = uc[e0 + kAW], u2y = uc[2 * kAEnt + e0 + kAW];
+        const L u1x = uc[kAEnt + e0 + 1], u2x = uc[2 * kAEnt + e0 + 1];
+        const L u0z = un[e0], u1z = un[kAEnt + e0];
+        const L acc[3] = {u1 - u1z + u2y - u2, u0z - u0 - u2x + u2, u0 - u0y + u1x - u1};
+        const L dt = (L)p.dt;
+#pragma unroll
+        for (int e = 0; e < 3; e++)
+          xout[e * N + m] = add(xi[e], mul(mul(dt, (L)coltL(p, e, i, j, k)), acc[e]));
+      } else {
+        const L* wc = S[sb];                       // w(k)
+        const L* wp = S[sa];                       // w(k-1)
+        const L w0 = wc[e0], w1 = wc[kAEnt + e0], w2 = wc[2 * kAEnt + e0];
+        const L w0y = wc[e0 - kAW], w2y = wc[2 * kAEnt + e0 - kAW];
+        const L w1x = wc[kAEnt + e0 - 1], w2x = wc[2 * kAEnt + e0 - 1];
+        const L w0z = wp[e0], w1z = wp[kAEnt + e0];
+        const L acc[3] = {w1z - w1 + w2 - w2y, w0 - w0z - w2 + w2x, w0y - w0 + w1 - w1x};
+#pragma unroll
+        for (int e = 0; e < 3; e++)
+          xout[e * N + m] = sub(mul(dc[e], xi[e]), mul((L)colL(p, e, i, j, k), acc[e]));
+      }
+    }
+    r1 = r2;
+    sa = sb;
   }
 }
 
@@ -239,31 +421,55 @@ extern "C" int wk_adj_grad(int dtype, const long long* cells, long long ncell, l
 // Matrix-free reverse step from the solver descriptor (coefficient tables of
 // wk_fit_desc; the state buffers of the descriptor are not touched).
 namespace {
-template <typename L>
-int adj_fit_launch(const wk_fit_desc* d, int which, const void* a, const void* b,
-                   const void* decay, void* out, cudaStream_t st) {
+// Planes per block of the tiled transposes: enough blocks for about two
+// waves of 148 SMs x 3 resident blocks, and at least 8 planes so that the
+// plane formed before the march stays a small share.
+dim3 adj_tile_grid(const wk_fit_desc* d, int* KC) {
+  const int gx = (d->Nx + kAX - 1) / kAX, gy = (d->Ny + kAY - 1) / kAY;
+  const long long tiles = (long long)gx * gy;
+  const long long want = (2LL * 148 * 3 + tiles - 1) / tiles;
+  int kc = (int)((d->Nz + want - 1) / want);
+  if (kc < 8) kc = 8;
+  if (kc > d->Nz) kc = d->Nz;
+  *KC = kc;
+  return dim3(gx, gy, (d->Nz + kc - 1) / kc);
+}
+
+template <typename T, typename L>
+void adj_fit_run(const wk_fit_desc* d, const FitParams<T>& p, int which, const void* fac,
+                 const void* a, const void* b, const void* decay, void* out, cudaStream_t st) {
   const long long N = (long long)d->Nx * d->Ny * d->Nz;
-  const bool coef64 = d->dtype == WK_F64 || d->dtype == WK_F32C;
-  if (coef64) {
-    FitParams<double> p = make_params<double>(d, d->par);
+  if (d->kernel == WK_KERNEL_CELL || !fac) {
     if (which == 0)
-      k_adj_h_fit<double, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b, (L*)out);
+      k_adj_h_fit<T, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b, (L*)out);
     else
-      k_adj_e_fit<double, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b,
-                                                                  (const L*)decay, (L*)out);
-  } else {
-    FitParams<float> p = make_params<float>(d, d->par);
-    if (which == 0)
-      k_adj_h_fit<float, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b, (L*)out);
-    else
-      k_adj_e_fit<float, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b,
-                                                                 (const L*)decay, (L*)out);
+      k_adj_e_fit<T, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b,
+                                                             (const L*)decay, (L*)out);
+    return;
   }
+  int KC;
+  const dim3 grid = adj_tile_grid(d, &KC);
+  if (which == 0)
+    k_adj_tile<T, L, 1><<<grid, kATh, 0, st>>>(p, (const L*)fac, (const L*)a, (const L*)b,
+                                               nullptr, (L*)out, KC);
+  else
+    k_adj_tile<T, L, -1><<<grid, kATh, 0, st>>>(p, (const L*)fac, (const L*)a, (const L*)b,
+                                                (const L*)decay, (L*)out, KC);
+}
+
+template <typename L>
+int adj_fit_launch(const wk_fit_desc* d, int which, const void* fac, const void* a,
+                   const void* b, const void* decay, void* out, cudaStream_t st) {
+  const bool coef64 = d->dtype == WK_F64 || d->dtype == WK_F32C;
+  if (coef64)
+    adj_fit_run<double, L>(d, make_params<double>(d, d->par), which, fac, a, b, decay, out, st);
+  else
+    adj_fit_run<float, L>(d, make_params<float>(d, d->par), which, fac, a, b, decay, out, st);
   return WK_OK;
 }
 
-int adj_fit(const wk_fit_desc* d, int dtype, int which, const void* a, const void* b,
-            const void* decay, void* out, void* stream, const char* where) {
+int adj_fit(const wk_fit_desc* d, int dtype, int which, const void* fac, const void* a,
+            const void* b, const void* decay, void* out, void* stream, const char* where) {
   int rc = wk_validate_fit(d, where);
   if (rc) return rc;
   if (dtype != WK_F64 && dtype != WK_F32) return wk_fail(WK_E_DTYPE, "%s: dtype", where);
@@ -271,19 +477,45 @@ int adj_fit(const wk_fit_desc* d, int dtype, int which, const void* a, const voi
   if ((long long)d->Nx * d->Ny * d->Nz >= (1LL << 31))
     return wk_fail(WK_E_SHAPE, "%s: more than 2^31 cells", where);
   cudaStream_t st = (cudaStream_t)stream;
-  if (dtype == WK_F64) adj_fit_launch<double>(d, which, a, b, decay, out, st);
-  else adj_fit_launch<float>(d, which, a, b, decay, out, st);
+  if (dtype == WK_F64) adj_fit_launch<double>(d, which, fac, a, b, decay, out, st);
+  else adj_fit_launch<float>(d, which, fac, a, b, decay, out, st);
   return wk_check_launch(where);
+}
+
+template <typename L>
+void adj_factors_launch(const wk_fit_desc* d, void* fu, void* fw, cudaStream_t st) {
+  const long long N = (long long)d->Nx * d->Ny * d->Nz;
+  if (d->dtype == WK_F64 || d->dtype == WK_F32C)
+    k_adj_factors<double, L><<<blocks(N), kAdjThreads, 0, st>>>(make_params<double>(d, d->par),
+                                                                (L*)fu, (L*)fw);
+  else
+    k_adj_factors<float, L><<<blocks(N), kAdjThreads, 0, st>>>(make_params<float>(d, d->par),
+                                                               (L*)fu, (L*)fw);
 }
 }  // namespace
 
-extern "C" int wk_adj_h_fit(const wk_fit_desc* d, int dtype, const void* lamE,
-                            const void* lamH_in, void* lamH_out, void* stream) {
-  return adj_fit(d, dtype, 0, lamE, lamH_in, nullptr, lamH_out, stream, "wk_adj_h_fit");
+extern "C" int wk_adj_factors(const wk_fit_desc* d, int dtype, void* fu, void* fw,
+                              void* stream) {
+  const char* where = "wk_adj_factors";
+  int rc = wk_validate_fit(d, where);
+  if (rc) return rc;
+  if (dtype != WK_F64 && dtype != WK_F32) return wk_fail(WK_E_DTYPE, "%s: dtype", where);
+  if (!fu && !fw) return wk_fail(WK_E_NULL, "%s: fu and fw are NULL", where);
+  if ((long long)d->Nx * d->Ny * d->Nz >= (1LL << 31))
+    return wk_fail(WK_E_SHAPE, "%s: more than 2^31 cells", where);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == WK_F64) adj_factors_launch<double>(d, fu, fw, st);
+  else adj_factors_launch<float>(d, fu, fw, st);
+  return wk_check_launch(where);
 }
 
-extern "C" int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* lamH,
+extern "C" int wk_adj_h_fit(const wk_fit_desc* d, int dtype, const void* fu, const void* lamE,
+                            const void* lamH_in, void* lamH_out, void* stream) {
+  return adj_fit(d, dtype, 0, fu, lamE, lamH_in, nullptr, lamH_out, stream, "wk_adj_h_fit");
+}
+
+extern "C" int wk_adj_e_fit(const wk_fit_desc* d, int dtype, const void* fw, const void* lamH,
                             const void* lamE_in, const void* decay, void* lamE_out,
                             void* stream) {
-  return adj_fit(d, dtype, 1, lamH, lamE_in, decay, lamE_out, stream, "wk_adj_e_fit");
+  return adj_fit(d, dtype, 1, fw, lamH, lamE_in, decay, lamE_out, stream, "wk_adj_e_fit");
 }
