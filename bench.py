@@ -23,8 +23,9 @@ ranks every --slab-depth steps through NCCL point-to-point messages
 one GPU.
 
 --impl reference times the CPU oracle (a restatement of upstream's scipy
-solver) on the host cores with all threads, on a bounded sample of the
-workload (same geometry at 128x128x256), rank 0 only.
+solver) on the host cores with all threads, rank 0 only: the workload's own
+grid when the host has the memory for its sparse operators, else the same
+geometry at 128x128x256; at most about 2 minutes of timed steps.
 """
 
 import argparse
@@ -443,6 +444,13 @@ def run_adjoint(args):
         ti_v = 8.548921333333334 * sp["wake"]["sigmaz"]
         need = int(np.ceil((span + ti_v + 2000 * v * dt_fixed[0]) / (v * dt_fixed[0])))
         nsteps = max(4000, need) if dt_fixed[0] < dt_cfl else 4000
+    if args.adjoint_forms:
+        keep = args.adjoint_forms.split(",")
+        unknown = sorted(set(keep) - {f[0] for f in forms})
+        if unknown or "f64" not in keep:
+            raise SystemExit(f"--adjoint-forms: unknown {unknown} (f64 is required: its forward "
+                             f"runs give the finite differences)")
+        forms = tuple(f for f in forms if f[0] in keep)
     for name, dt_, prec, adt, cst in forms:
         t0 = time.perf_counter()
         prob, nd = problem(dt_, prec, adt, cst)
@@ -476,7 +484,7 @@ def run_adjoint(args):
         lm = p64.forward(keep=False)
         return (lp - lm) / (2.0 * h)
 
-    for _ in range(16):
+    for _ in range(args.adjoint_directions):
         ve = rng.standard_normal(nd)
         vs = rng.standard_normal(nd)
         # Richardson extrapolation of central differences at h and h/2: O(h^4)
@@ -826,6 +834,11 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=0,
                     help="steps of the differentiation form (0: 4000, or enough for the wake "
                          "when the relaxation clamp shortens dt)")
+    ap.add_argument("--adjoint-forms", default="",
+                    help="comma-separated subset of the adjoint forms (f64, f32, fp32c, "
+                         "fp32c_adj32, fp32c_cs, fp32c_cs_adj32; default all)")
+    ap.add_argument("--adjoint-directions", type=int, default=16,
+                    help="random directions checked against central differences")
     ap.add_argument("--adjoint-sigma-max", type=float, default=1e3,
                     help="design-cell sigma ~ U[0, this] S/m (1e3: the configuration)")
     ap.add_argument("--slabs", type=int, default=0,
