@@ -329,7 +329,7 @@ def run_batch(args):
         t_build = time.perf_counter() - t0
         b = batch.BatchedWakeSolve([x[2] for x in built], args.batch_steps,
                                    launch=args.batch_launch if precision else "graph",
-                                   form=args.batch_form)
+                                   form=args.batch_form, tiles=args.batch_tiles)
         t1 = time.perf_counter()
         tm = b.run()
         t_run = time.perf_counter() - t1
@@ -824,6 +824,9 @@ def main():
                          "(wk_batch_run), or a graph of per-instance launches")
     ap.add_argument("--batch-form", default="auto", choices=["auto", "persistent", "phases"],
                     help="batched launch form (auto: chosen by the autotuner)")
+    ap.add_argument("--batch-tiles", default="auto", choices=["auto", "64x8", "fill", "32x16"],
+                    help="tile shapes of the batched launch (auto: chosen by the autotuner; "
+                         "fill: per instance, the shape with fewer idle lanes)")
     ap.add_argument("--batch-multiple", type=int, default=8,
                     help="batched form: transverse cell counts rounded up to this multiple")
     ap.add_argument("--adjoint", action="store_true",

@@ -113,8 +113,9 @@ typedef struct wk_fit_desc {
   int* status;             /* device status word (0 = ok), may be NULL       */
   /* Kernel choice for wk_fit_step (WK_KERNEL_* below).
    * tile_planes (0 = automatic) sets the planes per block of the TMA kernel
-   * and the planes per thread of the two-pass kernels; tile_rows is not
-   * read.                                                                  */
+   * and the planes per thread of the two-pass kernels.  tile_rows sets the
+   * tile shape of the WK_F32C TMA kernel and of the batched launches: 8
+   * for 64x8 tiles, 16 or 0 (the default) for 32x16 tiles.                 */
   int kernel;
   int tile_rows, tile_planes;
   /* WK_F32C only: per-component compensation words of E and H (bf16 bit
@@ -204,7 +205,9 @@ int wk_counter_add(long long* ctr, long long inc, void* stream);
  * z-boundary planes take the general rows), id_bytes 1 or 2, J mode
  * WK_J_ZERO or WK_J_SIGMA_E, Nx % 4 == 0, at most 64 materials and
  * step_dev == NULL; all instances share the face mode, id width and J mode.
- * tile_planes of a descriptor sets the planes per work item (0 = 24).
+ * tile_planes of a descriptor sets the planes per work item (0 = 24) and
+ * tile_rows its tile shape: 8 for 64x8 tiles, 16 (or 0) for 32x16 tiles
+ * (fewer idle lanes where Nx lies just above a multiple of 64).
  *
  * wk_batch_workspace_bytes: device bytes the plan needs (-1 on an argument
  *   error, see wk_last_error).
@@ -221,16 +224,17 @@ int wk_counter_add(long long* ctr, long long inc, void* stream);
  *   launch whose blocks claim the items of every step in order; an item
  *   waits only for its own instance's earlier work (per-instance completion
  *   counters, no grid-wide barrier), each wait bounded by wait_ns
- *   nanoseconds (<= 0: 2 s).  WK_BATCH_PHASES: up to four launches per step
+ *   nanoseconds (<= 0: 2 s).  WK_BATCH_PHASES: up to six launches per step
  *   (wait_ns unused).  A wait or a tile load that runs out sets the status
  *   word of the instance concerned and the launch ends (wk_read_status).
  * No counterpart in the reference.
  */
 #define WK_BATCH_PERSISTENT 0   /* one cooperative launch per wk_batch_run  */
 #define WK_BATCH_PHASES 1       /* per step, one launch per list of items:
-                                   tiles (TMA-loaded compensation words),
-                                   tiles (per-thread loads), H rows of the
-                                   boundary planes, then their E rows       */
+                                   64x8 and 32x16 tiles with TMA-loaded
+                                   compensation words, the same with
+                                   per-thread loads, H rows of the boundary
+                                   planes, then their E rows                */
 typedef struct wk_batch_plan {
   void* workspace;
   long long workspace_bytes;
@@ -241,8 +245,9 @@ typedef struct wk_batch_plan {
   int variant;             /* kernel instantiation                           */
   int device;
   long long offsets[4];    /* instances, TMA descriptors, items (two phases) */
-  int n_parts[3];          /* phase-A items: TMA-word tiles, other tiles,
-                              boundary-plane H rows                          */
+  int n_parts[5];          /* phase-A items: TMA-word 64x8 tiles, TMA-word
+                              32x16 tiles, other 64x8 tiles, other 32x16
+                              tiles, boundary-plane H rows                   */
   int form;                /* WK_BATCH_PERSISTENT (set by wk_batch_prepare)
                               or WK_BATCH_PHASES; the caller may change it  */
 } wk_batch_plan;

@@ -87,17 +87,36 @@ def test_batch_equals_individual_wakesolve(form):
 
 
 @pytest.mark.parametrize("form", ["persistent", "phases"])
-def test_batch_all_faces_masked(form):
+def test_batch_32x16_tiles_equal_individual_wakesolve(form):
+    """The pillboxes on 32x16 tiles (28- and 32-cell planes: tiles cut by
+    the grid edge in x and in y, compensation words by TMA and by
+    per-thread loads), autotuned planes per item."""
+    from wakis_b200 import batch
+    inst = _pillboxes()
+    b = batch.BatchedWakeSolve([x[2] for x in inst], 601, launch="batched", chunk=97, form=form,
+                               tiles="32x16")
+    b.run()
+    assert b.tuned["tile_policy"] == "32x16" and b.tuned["tiles_32x16"] == 3
+    _same(inst, _solo(_pillboxes(), 601))
+
+
+@pytest.mark.parametrize("tiles", ["64x8", "fill", "32x16"])
+@pytest.mark.parametrize("form", ["persistent", "phases"])
+def test_batch_all_faces_masked(form, tiles):
     """Conductive walls with z-PML on two grid shapes (one phase per step,
     one instance with TMA-loaded compensation words and one without) in one
-    chunk with fixed planes per item."""
+    chunk with fixed planes per item; with tiles="fill" one instance runs
+    on 32x16 tiles and the other on 64x8 tiles in the same launch."""
     from wakis_b200 import batch
     shapes = [(32, 32, 64), (36, 24, 56)]
     inst = _lossy(shapes)
     for _, _, s in inst:
         s.tile = (0, 16)
-    batch.BatchedWakeSolve([x[2] for x in inst], 500, launch="batched", tune=False,
-                           chunk=1000, form=form).run()
+    b = batch.BatchedWakeSolve([x[2] for x in inst], 500, launch="batched", tune=False,
+                               chunk=1000, form=form, tiles=tiles)
+    b.run()
+    rows = [s.tile[0] for _, _, s in inst]
+    assert rows == {"64x8": [8, 8], "fill": [16, 8], "32x16": [16, 16]}[tiles]
     _same(inst, _solo(_lossy(shapes), 500))
 
 

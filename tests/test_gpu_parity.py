@@ -348,6 +348,38 @@ def test_fp32c_tma_close_to_twopass(tile):
     assert rel_err(ha.cpu().numpy(), hb.cpu().numpy()) <= 2e-6
 
 
+@pytest.mark.parametrize("shape", [(40, 40, 80), (36, 20, 30), (72, 44, 24)])
+@pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
+                                 (["pec", "pec", "abc"], ["pec", "pec", "abc"]),
+                                 (["periodic", "pec", "pml"], ["periodic", "pec", "pml"])])
+def test_fp32c_tma_32x16_tiles_equal_64x8(bcs, shape):
+    """The compensated TMA kernel on 32x16 tiles (wk_fit_desc.tile_rows =
+    16, the default) gives the 64x8 tiles' (tile_rows = 8) fields,
+    compensation words and Ez capture value for value: every cell runs the
+    same rows, only the split of the grid into blocks differs (all three
+    face modes; grids cut by both tile shapes; row pitch with and without
+    TMA-loaded compensation words)."""
+    from wakis_b200.sources import Beam
+    c = dict(cases.STEP_CASES[2])
+    c.update(shape=shape, dtype="float64", bc_low=bcs[0], bc_high=bcs[1], n_pml=3)
+    runs = []
+    for rows in (8, 16):
+        s = b200_step_case(c, precision="fp32c")
+        s.kernel, s.tile = "tma", (rows, 0)
+        E0, H0 = cases.initial_fields(c, s.N)
+        s.E.fromarray(E0)
+        s.H.fromarray(H0)
+        bp = Beam(q=1e-9, sigmaz=0.005, beta=1.0).params(s)
+        h = torch.zeros((9, s.Nz, 40), dtype=torch.float64, device="cuda")
+        s._advance(40, 0, beam=bp, capture=(h, s.Nx // 2 - 1, s.Ny // 2 - 1, 3, 3))
+        assert int(s._status.item()) == 0
+        bits = lambda t: t.view(torch.int16) if t.dtype == torch.bfloat16 else t
+        runs.append([bits(t).cpu().numpy() for t in (s._E[s._par], s._H[s._par],
+                                                      s._Ec[s._par], s._Hc[s._par], h)])
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("shape", [(16, 12, 20), (20, 12, 20)])
 @pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
                                  (["periodic", "pec", "pml"], ["periodic", "pec", "pml"])])

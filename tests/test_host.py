@@ -191,3 +191,20 @@ def test_key_order_matches_string_sort():
             assert pos is None
         else:
             assert np.array_equal(order[pos], np.arange(n))
+
+
+def test_batch_tile_policy():
+    """The batched launches' tile-shape policy: the share of tile lanes that
+    hold a cell, and the shape "fill" picks (32x16 only where it leaves
+    fewer lanes idle than 64x8)."""
+    from types import SimpleNamespace
+    from wakis_b200 import batch
+    assert batch.tile_fill(64, 8, 64) == 1.0
+    assert batch.tile_fill(72, 72, 64) == pytest.approx(72 * 72 / (128 * 72))
+    assert batch.tile_fill(72, 72, 32) == pytest.approx(72 * 72 / (96 * 80))
+    rows = lambda nx, ny, pol: batch.tile_rows_for(SimpleNamespace(Nx=nx, Ny=ny), pol)
+    assert rows(72, 72, "fill") == 16 and rows(128, 128, "fill") == 8
+    assert rows(36, 24, "fill") == 8 and rows(32, 32, "fill") == 16
+    assert rows(72, 72, "64x8") == 8 and rows(128, 128, "32x16") == 16
+    with pytest.raises(ValueError):
+        rows(64, 64, "16x32")

@@ -56,7 +56,7 @@ class BatchPlan(ctypes.Structure):
     _fields_ = [
         ("workspace", _vp), ("workspace_bytes", _ll), ("n_inst", _i), ("n_items", _i * 2),
         ("grid", _i), ("smem", _i), ("variant", _i), ("device", _i), ("offsets", _ll * 4),
-        ("n_parts", _i * 3), ("form", _i),
+        ("n_parts", _i * 5), ("form", _i),
     ]
 
 

@@ -10,9 +10,11 @@ the stepping of all of them is shared:
   items over all instances, run either as ONE persistent cooperative launch
   per chunk of steps (its blocks claim the items of every step in order and
   an item waits, bounded, only for its own instance's earlier work) or as
-  one launch per list and step (form "phases").  The step index comes from a device counter, so the
-  chunk is captured once in a CUDA graph and replayed.  An autotuner times
-  both forms and the candidate planes per work item (the z depth of the
+  one launch per list and step (form "phases").  The step index comes from
+  a device counter, so the chunk is captured once in a CUDA graph and
+  replayed.  An autotuner times both forms, the tile-shape policies (64x8
+  or 32x16 tiles for every instance, or per instance the shape with fewer
+  idle lanes) and the candidate planes per work item (the z depth of the
   tiles, ``SolverFIT3D.tile``) on the whole batch and keeps the fastest.
 * ``launch="graph"``: one CUDA graph of two steps of every instance (one
   launch per instance and step, spread over a few streams) plus an increment
@@ -34,6 +36,29 @@ from . import geometry
 KC_CANDIDATES = (0, 4, 8, 16, 32)
 # planes per work item tried by the autotuner of the batched launches
 BATCH_KC_CANDIDATES = (16, 32, 48, 64, 96)
+# tile-shape policies of the batched launches: every instance on 64x8 or
+# 32x16 tiles, or each on the shape whose tiles leave fewer lanes idle
+TILE_POLICIES = ("64x8", "fill", "32x16")
+
+
+def tile_fill(nx, ny, width):
+    """Share of the tile lanes that hold a cell when an nx x ny plane is
+    covered by width x (512 / width) tiles."""
+    h = 512 // width
+    return (nx * ny) / (-(-nx // width) * width * (-(-ny // h) * h))
+
+
+def tile_rows_for(solver, policy):
+    """wk_fit_desc.tile_rows of a batched instance under a tile policy:
+    8 (64x8 tiles) or 16 (32x16 tiles)."""
+    if policy == "64x8":
+        return 8
+    if policy == "32x16":
+        return 16
+    if policy == "fill":
+        return 16 if tile_fill(solver.Nx, solver.Ny, 32) > tile_fill(solver.Nx, solver.Ny, 64) \
+            else 8
+    raise ValueError(f"tile policy {policy!r}")
 
 
 def autotune(solver, candidates=KC_CANDIDATES, steps=4):
@@ -124,32 +149,40 @@ def batched_ok(solvers):
     return True
 
 
-def autotune_batch(solvers, candidates=BATCH_KC_CANDIDATES, forms=tuple(FORMS), steps=4):
-    """Pick the launch form and the planes per work item of the batched run
-    by timing `steps` source-free steps of the whole batch per candidate
-    with CUDA events; every solver's ``tile`` is set to the winner.  The
-    fields start at zero and stay zero (no source); they are reset
-    afterwards.  Returns ((form, planes), {(form, planes): ms})."""
+def autotune_batch(solvers, candidates=BATCH_KC_CANDIDATES, forms=tuple(FORMS), steps=4,
+                   policies=TILE_POLICIES):
+    """Pick the launch form, the tile-shape policy and the planes per work
+    item of the batched run by timing `steps` source-free steps of the
+    whole batch per candidate with CUDA events; every solver's ``tile`` is
+    set to the winner ((8 or 16 tile rows, planes)).  The fields start at
+    zero and stay zero (no source); they are reset afterwards.  Returns
+    ((form, planes, policy), {(form, planes, policy): ms})."""
     dev = solvers[0].device
     tried = {}
-    for kc in candidates:
-        for s in solvers:
-            s.tile = (0, kc)
-            s._first_step()
-        descs = [_native.FitDesc.from_buffer_copy(s._step_desc()) for s in solvers]
-        for form in forms:
-            plan = BatchPlan(solvers, descs, t_ref=0, form=form)
-            plan.run(1, 0)                                   # warm
-            ev0 = torch.cuda.Event(enable_timing=True)
-            ev1 = torch.cuda.Event(enable_timing=True)
-            ev0.record()
-            plan.run(steps, 1)
-            ev1.record()
-            torch.cuda.synchronize(dev)
-            tried[(form, kc)] = ev0.elapsed_time(ev1)
+    shapes_seen = set()
+    for policy in policies:
+        rows = tuple(tile_rows_for(s, policy) for s in solvers)
+        if rows in shapes_seen:          # the same shapes as a policy timed before
+            continue
+        shapes_seen.add(rows)
+        for kc in candidates:
+            for s, r in zip(solvers, rows):
+                s.tile = (r, kc)
+                s._first_step()
+            descs = [_native.FitDesc.from_buffer_copy(s._step_desc()) for s in solvers]
+            for form in forms:
+                plan = BatchPlan(solvers, descs, t_ref=0, form=form)
+                plan.run(1, 0)                                   # warm
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record()
+                plan.run(steps, 1)
+                ev1.record()
+                torch.cuda.synchronize(dev)
+                tried[(form, kc, policy)] = ev0.elapsed_time(ev1)
     best = min(tried, key=tried.get)
     for s in solvers:
-        s.tile = (0, best[1])
+        s.tile = (tile_rows_for(s, best[2]), best[1])
         s.reset_fields()
         s.nstep = 0
         s.step_0 = True
@@ -167,20 +200,26 @@ class BatchedWakeSolve:
     wk_batch_run, for FP32-compensated instances), "graph" (replayed graph of
     per-instance launches) or "auto" (batched when ``batched_ok``).  form:
     the batched launch form, "persistent", "phases" or "auto" (chosen by the
-    autotuner; "persistent" without tuning).  streams: number of CUDA
-    streams the instances are spread over inside the graph (launch="graph").
+    autotuner; "persistent" without tuning).  tiles: the tile shapes of the
+    batched launch, "64x8", "32x16", "fill" (per instance, the shape with
+    fewer idle lanes) or "auto" (chosen by the autotuner; "fill" without
+    tuning).  streams: number of CUDA streams the instances are spread over
+    inside the graph (launch="graph").
     chunk: steps per captured chunk of the batched launch.  tune: run the
     autotuner first.
     """
 
     def __init__(self, solvers, n_steps, compute_plane="both", streams=8, tune=True,
-                 launch="auto", chunk=500, form="auto"):
+                 launch="auto", chunk=500, form="auto", tiles="auto"):
         if n_steps < 2:
             raise ValueError("n_steps must be >= 2")
         if launch not in ("auto", "batched", "graph"):
             raise ValueError(f"launch {launch!r}")
         if form not in ("auto",) + tuple(FORMS):
             raise ValueError(f"form {form!r}")
+        if tiles not in ("auto",) + TILE_POLICIES:
+            raise ValueError(f"tiles {tiles!r}")
+        self.tiles = tiles
         self.solvers = list(solvers)
         self.n_steps = int(n_steps)
         self.compute_plane = compute_plane
@@ -223,11 +262,20 @@ class BatchedWakeSolve:
             form = self.form
             if self.tune:
                 forms = tuple(FORMS) if form == "auto" else (form,)
-                best, tried = autotune_batch(self.solvers, forms=forms)
+                best, tried = autotune_batch(self.solvers, forms=forms,
+                                             policies=TILE_POLICIES if self.tiles == "auto"
+                                             else (self.tiles,))
                 form = best[0]
                 self.tuned = {"form": best[0], "planes_per_item": best[1],
-                              "tried_ms": {f"{k[0]}/{k[1]}": v for k, v in tried.items()}}
-            elif form == "auto":
+                              "tile_policy": best[2],
+                              "tiles_32x16": sum(1 for s in self.solvers if s.tile[0] == 16),
+                              "tried_ms": {f"{k[0]}/{k[1]}/{k[2]}": v
+                                           for k, v in tried.items()}}
+            else:
+                for s in self.solvers:
+                    s.tile = (tile_rows_for(s, "fill" if self.tiles == "auto" else self.tiles),
+                              s.tile[1])
+            if form == "auto":
                 form = "persistent"
             self.tuned["form"] = form
             states = self._setup()

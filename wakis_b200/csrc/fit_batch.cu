@@ -27,9 +27,14 @@
 //   launch), so the waits always end; each is also bounded by a
 //   %globaltimer deadline, after which the block records the failure in the
 //   status word and all blocks leave.
-// * phases (WK_BATCH_PHASES): per step, one launch per list (tiles whose
-//   compensation words come by TMA, the other tiles, boundary-plane H rows,
-//   boundary-plane E rows); the stream orders them.
+// * phases (WK_BATCH_PHASES): per step, one launch per list (64x8 and 32x16
+//   tiles whose compensation words come by TMA, the same with per-thread
+//   loads, boundary-plane H rows, boundary-plane E rows); the stream orders
+//   them.
+//
+// Each instance has its own tile shape (wk_fit_desc.tile_rows: 32x16 or
+// 64x8 tiles), so that grids whose x extent lies just above a multiple of
+// 64 do not leave most lanes of their last tile column idle.
 //
 // Each item reads its instance's parameters from the workspace; the TMA
 // descriptors of every instance and buffer parity live there too.  The
@@ -63,7 +68,7 @@ struct BatchInst {
   int par_ref;
   int ct;                   // compensation words by TMA (Nx % 8 == 0)
   unsigned nA, nB;          // items of this instance in phase A, phase B
-  int pad;
+  int tw;                   // tile width: 64 (64x8 tiles) or 32 (32x16)
 };
 static_assert(sizeof(FitParams<double>) % 8 == 0, "parameters are copied as 8-byte words");
 static_assert(sizeof(CompState) % 8 == 0, "state pointers are copied as 8-byte words");
@@ -118,12 +123,14 @@ __shared__ CompState g_scs;
 // The work of one item, each in a function of its own (not inlined), so that
 // the tile march keeps the register allocation of the one-grid kernel
 // instead of sharing it with the step and phase loops around it.
-// CT: the instance's compensation words come by TMA (Nx % 8 == 0).
-template <typename IdT, bool SIG, int MODE, bool CT>
+// CT: the instance's compensation words come by TMA (Nx % 8 == 0); TW:
+// its tile width.
+template <typename IdT, bool SIG, int MODE, bool CT, int TW>
 __device__ __noinline__ bool batch_tile(const CompMaps* maps, long long t, int a, int b) {
   extern __shared__ __align__(128) unsigned char sm_raw[];
-  return comp_tile<IdT, SIG, MODE, CT ? 1 : 0, true>(g_sp, g_scs, *maps, t, b >> 16, a & 0xffff,
-                                                     a >> 16, b & 0xffff, CT, sm_raw);
+  return comp_tile<IdT, SIG, MODE, CT ? 1 : 0, true, TW>(g_sp, g_scs, *maps, t, b >> 16,
+                                                         a & 0xffff, a >> 16, b & 0xffff, CT,
+                                                         sm_raw);
 }
 // one whole z-boundary plane per item: warps take rows, lanes columns
 __device__ __noinline__ void batch_shell(int kind, int plane, long long t) {
@@ -186,8 +193,12 @@ __global__ void __launch_bounds__(cThreads, 2) k_batch_comp(const __grid_constan
     bool good = true;
     const CompMaps* maps = &a.maps[2 * w.inst + par];
     if (w.kind != 0) batch_shell(w.kind, w.a, t);
-    else if (I.ct) good = batch_tile<IdT, SIG, MODE, true>(maps, t, w.a, w.b);
-    else good = batch_tile<IdT, SIG, MODE, false>(maps, t, w.a, w.b);
+    else if (I.ct)
+      good = I.tw == 32 ? batch_tile<IdT, SIG, MODE, true, 32>(maps, t, w.a, w.b)
+                        : batch_tile<IdT, SIG, MODE, true, 64>(maps, t, w.a, w.b);
+    else
+      good = I.tw == 32 ? batch_tile<IdT, SIG, MODE, false, 32>(maps, t, w.a, w.b)
+                        : batch_tile<IdT, SIG, MODE, false, 64>(maps, t, w.a, w.b);
     if (!good) {
       if (tid == 0) atomicExch(&a.sync->abort, 1);
       return;
@@ -209,7 +220,7 @@ __global__ void __launch_bounds__(cThreads, 2) k_batch_comp(const __grid_constan
 // parameters are read where they lie (read-only for the launch), and each
 // kernel holds one kind of work, so the tile march keeps the registers of
 // the one-grid kernel.
-template <typename IdT, bool SIG, int MODE, bool CT>
+template <typename IdT, bool SIG, int MODE, bool CT, int TW>
 __global__ void __launch_bounds__(cThreads, 2)
 k_batch_tiles(const __grid_constant__ BatchArgs a, const BatchInst* __restrict__ insts,
               const BatchItem* __restrict__ list, int s) {
@@ -218,9 +229,9 @@ k_batch_tiles(const __grid_constant__ BatchArgs a, const BatchInst* __restrict__
   const BatchItem w = list[blockIdx.x];
   const BatchInst& I = insts[w.inst];
   const int par = (I.par_ref + (int)((t - I.t_ref) & 1)) & 1;
-  comp_tile<IdT, SIG, MODE, CT ? 1 : 0, false>(I.p, I.cs[par], a.maps[2 * w.inst + par], t,
-                                               w.b >> 16, w.a & 0xffff, w.a >> 16, w.b & 0xffff,
-                                               CT, sm_raw);
+  comp_tile<IdT, SIG, MODE, CT ? 1 : 0, false, TW>(I.p, I.cs[par], a.maps[2 * w.inst + par],
+                                                   t, w.b >> 16, w.a & 0xffff, w.a >> 16,
+                                                   w.b & 0xffff, CT, sm_raw);
 }
 
 __global__ void __launch_bounds__(cThreads)
@@ -253,14 +264,22 @@ const BatchKern kBatchKerns[kBatchVariants] = {
     k_batch_comp<uint8_t, false, 2>,  k_batch_comp<uint8_t, true, 2>,
     k_batch_comp<uint16_t, false, 2>, k_batch_comp<uint16_t, true, 2>};
 using TileKern = void (*)(const BatchArgs, const BatchInst*, const BatchItem*, int);
-#define WK_BATCH_TILES(CT)                                                                      \
-  {k_batch_tiles<uint8_t, false, 1, CT>,  k_batch_tiles<uint8_t, true, 1, CT>,                  \
-   k_batch_tiles<uint16_t, false, 1, CT>, k_batch_tiles<uint16_t, true, 1, CT>,                 \
-   k_batch_tiles<uint8_t, false, 2, CT>,  k_batch_tiles<uint8_t, true, 2, CT>,                  \
-   k_batch_tiles<uint16_t, false, 2, CT>, k_batch_tiles<uint16_t, true, 2, CT>}
-const TileKern kTileKerns[2][kBatchVariants] = {WK_BATCH_TILES(false), WK_BATCH_TILES(true)};
+#define WK_BATCH_TILES(CT, TW)                                                                  \
+  {k_batch_tiles<uint8_t, false, 1, CT, TW>,  k_batch_tiles<uint8_t, true, 1, CT, TW>,          \
+   k_batch_tiles<uint16_t, false, 1, CT, TW>, k_batch_tiles<uint16_t, true, 1, CT, TW>,         \
+   k_batch_tiles<uint8_t, false, 2, CT, TW>,  k_batch_tiles<uint8_t, true, 2, CT, TW>,          \
+   k_batch_tiles<uint16_t, false, 2, CT, TW>, k_batch_tiles<uint16_t, true, 2, CT, TW>}
+// [list]: TMA-word 64x8 tiles, TMA-word 32x16, other 64x8, other 32x16
+const TileKern kTileKerns[4][kBatchVariants] = {WK_BATCH_TILES(true, 64), WK_BATCH_TILES(true, 32),
+                                                WK_BATCH_TILES(false, 64),
+                                                WK_BATCH_TILES(false, 32)};
 #undef WK_BATCH_TILES
-bool g_tile_attr[2][kBatchVariants][64];
+constexpr int kTileLists = 4;
+// dynamic shared memory of the batched kernels: the larger tile layout
+constexpr int kBatchSmem = CLayout<true, true, 64>::bytes > CLayout<true, true, 32>::bytes
+                               ? CLayout<true, true, 64>::bytes
+                               : CLayout<true, true, 32>::bytes;
+bool g_tile_attr[kTileLists][kBatchVariants][64];
 int g_batch_per_sm[kBatchVariants][64];
 int g_batch_sms[kBatchVariants][64];
 bool g_batch_attr[kBatchVariants][64];
@@ -289,15 +308,16 @@ constexpr int kBatchDefaultKC = 24;
 // Checks every descriptor, forms the work lists and the variant; fills
 // `insts` (parameters and state only; maps are encoded by the caller).
 // Phase A lists the tiles of the instances whose compensation words come by
-// TMA, then the other tiles, then the H rows of the boundary planes
-// (parts[0..2] items each); phase B the E rows of the boundary planes.
+// TMA (64x8, then 32x16), then the other tiles (64x8, then 32x16), then the
+// H rows of the boundary planes (parts[0..4] items each); phase B the E rows
+// of the boundary planes.
 int batch_build(const wk_fit_desc* descs, int n_inst, long long t_ref, const char* where,
                 std::vector<BatchInst>* insts, std::vector<BatchItem>* ia,
                 std::vector<BatchItem>* ib, int* variant, int* parts) {
   if (!descs) return wk_fail(WK_E_NULL, "%s: descs is NULL", where);
   if (n_inst < 1 || n_inst > (1 << 20)) return wk_fail(WK_E_RANGE, "%s: n_inst %d", where, n_inst);
   int var = -1;
-  std::vector<BatchItem> tiles_plain, shells_a;
+  std::vector<BatchItem> tiles[kTileLists], shells_a;
   for (int q = 0; q < n_inst; q++) {
     const wk_fit_desc* d = &descs[q];
     int rc = wk_validate_fit(d, where);
@@ -324,6 +344,10 @@ int batch_build(const wk_fit_desc* descs, int n_inst, long long t_ref, const cha
                      q);
     if (d->id_bytes > 2)
       return wk_fail(WK_E_DTYPE, "%s: instance %d: id_bytes must be 1 or 2", where, q);
+    if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16)
+      return wk_fail(WK_E_RANGE, "%s: instance %d: tile_rows %d (0, 8 or 16)", where, q,
+                     d->tile_rows);
+    const int tw = d->tile_rows == 8 ? 64 : 32;
     const int v = (mode - 1) * 4 + (d->id_bytes - 1) * 2 + (d->j_mode == WK_J_SIGMA_E ? 1 : 0);
     if (var >= 0 && v != var)
       return wk_fail(WK_E_MODE, "%s: instance %d differs from instance 0 in face mode, id width "
@@ -336,6 +360,7 @@ int batch_build(const wk_fit_desc* descs, int n_inst, long long t_ref, const cha
     I.cs[1] = comp_state(d, 1);
     I.t_ref = t_ref;
     I.par_ref = d->par;
+    I.tw = tw;
     I.ct = (p.Nx % 8 == 0 && ((uintptr_t)d->Hc[0] % 16) == 0 && ((uintptr_t)d->Hc[1] % 16) == 0 &&
             ((uintptr_t)d->Ec[0] % 16) == 0 && ((uintptr_t)d->Ec[1] % 16) == 0)
                ? 1
@@ -346,13 +371,14 @@ int batch_build(const wk_fit_desc* descs, int n_inst, long long t_ref, const cha
     const int planes = mode == 1 ? d->Nz : d->Nz - 4;
     if (KC > planes) KC = planes;
     if (KC > 32767) KC = 32767;
-    const int gx = (d->Nx + cTX - 1) / cTX, gy = (d->Ny + cTY - 1) / cTY;
+    const int tx = tw, ty = 512 / tw;
+    const int gx = (d->Nx + tx - 1) / tx, gy = (d->Ny + ty - 1) / ty;
     const int gz = (planes + KC - 1) / KC;
     if (gx > 32767 || gy > 32767 || gz > 32767)
       return wk_fail(WK_E_SHAPE, "%s: instance %d: too many tiles", where, q);
     insts->back().nA = (unsigned)(gx * gy * gz + (mode == 2 ? 4 : 0));
     insts->back().nB = mode == 2 ? 4u : 0u;
-    std::vector<BatchItem>* tl = I.ct ? ia : &tiles_plain;
+    std::vector<BatchItem>* tl = &tiles[(I.ct ? 0 : 2) + (tw == 32 ? 1 : 0)];
     for (int bz = 0; bz < gz; bz++)
       for (int by = 0; by < gy; by++)
         for (int bx = 0; bx < gx; bx++)
@@ -364,10 +390,11 @@ int batch_build(const wk_fit_desc* descs, int n_inst, long long t_ref, const cha
       }
     }
   }
-  parts[0] = (int)ia->size();
-  parts[1] = (int)tiles_plain.size();
-  parts[2] = (int)shells_a.size();
-  ia->insert(ia->end(), tiles_plain.begin(), tiles_plain.end());
+  for (int l = 0; l < kTileLists; l++) {
+    parts[l] = (int)tiles[l].size();
+    ia->insert(ia->end(), tiles[l].begin(), tiles[l].end());
+  }
+  parts[kTileLists] = (int)shells_a.size();
   // the small shell items last, where they fill the tail of the phase
   ia->insert(ia->end(), shells_a.begin(), shells_a.end());
   *variant = var;
@@ -383,7 +410,7 @@ using namespace wk;
 extern "C" long long wk_batch_workspace_bytes(const wk_fit_desc* descs, int n_inst) {
   std::vector<BatchInst> insts;
   std::vector<BatchItem> ia, ib;
-  int var = 0, parts[3];
+  int var = 0, parts[kTileLists + 1];
   if (batch_build(descs, n_inst, 0, "wk_batch_workspace_bytes", &insts, &ia, &ib, &var, parts))
     return -1;
   return (long long)batch_layout(n_inst, ia.size(), ib.size()).total;
@@ -398,7 +425,7 @@ extern "C" int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long 
     return wk_fail(WK_E_ALIGN, "%s: workspace must be 128-byte aligned", where);
   std::vector<BatchInst> insts;
   std::vector<BatchItem> ia, ib;
-  int var = 0, parts[3];
+  int var = 0, parts[kTileLists + 1];
   int rc = batch_build(descs, n_inst, t_ref, where, &insts, &ia, &ib, &var, parts);
   if (rc) return rc;
   if (ia.size() > (size_t)INT32_MAX || ib.size() > (size_t)INT32_MAX)
@@ -413,19 +440,23 @@ extern "C" int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long 
   CompMaps* maps = reinterpret_cast<CompMaps*>(img.data() + L.maps);
   for (int q = 0; q < n_inst; q++) {
     const wk_fit_desc* d = &descs[q];
+    const bool w32 = insts[q].tw == 32;
+    const int ebx = w32 ? CGeom<true, 32>::ebx : CGeom<true, 64>::ebx;
+    const int hbx = w32 ? CGeom<true, 32>::hbx : CGeom<true, 64>::hbx;
+    const int cbx = w32 ? CGeom<true, 32>::cbx : CGeom<true, 64>::cbx;
+    const int by = w32 ? CShape<32>::BY : CShape<64>::BY;
+    const int hby = w32 ? CShape<32>::HBY : CShape<64>::HBY;
     for (int par = 0; par < 2; par++) {
       const CompState cs = comp_state(d, par);
       CompMaps& m = maps[2 * q + par];
       for (int c = 0; c < 3; c++) {
         const long long N = insts[q].p.N;
-        if (!encode_3d(&m.e[c], cs.E_in + c * N, 4, d->Nx, d->Ny, d->Nz, CGeom<true>::ebx, cBY) ||
-            !encode_3d(&m.h[c], cs.H_in + c * N, 4, d->Nx, d->Ny, d->Nz, cBX, cHBY))
+        if (!encode_3d(&m.e[c], cs.E_in + c * N, 4, d->Nx, d->Ny, d->Nz, ebx, by) ||
+            !encode_3d(&m.h[c], cs.H_in + c * N, 4, d->Nx, d->Ny, d->Nz, hbx, hby))
           return wk_fail(WK_E_SHAPE, "%s: instance %d: tensor map encoding failed", where, q);
         if (insts[q].ct &&
-            (!encode_3d(&m.c[c], cs.Hc_in + c * N, 2, d->Nx, d->Ny, d->Nz, CGeom<true>::cbx,
-                        cHBY) ||
-             !encode_3d(&m.c[3 + c], cs.Ec_in + c * N, 2, d->Nx, d->Ny, d->Nz, CGeom<true>::cbx,
-                        cHBY)))
+            (!encode_3d(&m.c[c], cs.Hc_in + c * N, 2, d->Nx, d->Ny, d->Nz, cbx, hby) ||
+             !encode_3d(&m.c[3 + c], cs.Ec_in + c * N, 2, d->Nx, d->Ny, d->Nz, cbx, hby)))
           return wk_fail(WK_E_SHAPE, "%s: instance %d: tensor map encoding failed", where, q);
       }
     }
@@ -436,7 +467,7 @@ extern "C" int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long 
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return wk_fail(-(int)e, "%s: %s", where, cudaGetErrorString(e));
   if (dev < 0 || dev >= 64) return wk_fail(WK_E_RANGE, "%s: device %d", where, dev);
-  const int smem = CLayout<true, true>::bytes;
+  const int smem = kBatchSmem;
   const BatchKern kern = kBatchKerns[var];
   if (!g_batch_attr[var][dev]) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -450,12 +481,12 @@ extern "C" int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long 
       return wk_fail(WK_E_SHAPE, "%s: the batched kernel does not fit on an SM", where);
     g_batch_attr[var][dev] = true;
   }
-  for (int ct = 0; ct < 2; ct++) {
-    if (g_tile_attr[ct][var][dev]) continue;
-    e = cudaFuncSetAttribute(kTileKerns[ct][var], cudaFuncAttributeMaxDynamicSharedMemorySize,
+  for (int l = 0; l < kTileLists; l++) {
+    if (g_tile_attr[l][var][dev]) continue;
+    e = cudaFuncSetAttribute(kTileKerns[l][var], cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem);
     if (e != cudaSuccess) return wk_fail(-(int)e, "%s: %s", where, cudaGetErrorString(e));
-    g_tile_attr[ct][var][dev] = true;
+    g_tile_attr[l][var][dev] = true;
   }
   cudaStream_t st = (cudaStream_t)stream;
   e = cudaMemcpyAsync(workspace, img.data(), L.total, cudaMemcpyHostToDevice, st);
@@ -475,7 +506,7 @@ extern "C" int wk_batch_prepare(const wk_fit_desc* descs, int n_inst, long long 
   plan->offsets[1] = (long long)L.maps;
   plan->offsets[2] = (long long)L.items_a;
   plan->offsets[3] = (long long)L.items_b;
-  for (int q = 0; q < 3; q++) plan->n_parts[q] = parts[q];
+  for (int q = 0; q <= kTileLists; q++) plan->n_parts[q] = parts[q];
   plan->form = WK_BATCH_PERSISTENT;
   return WK_OK;
 }
@@ -511,16 +542,24 @@ extern "C" int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long st
   a.wait_ns = wait_ns > 0 ? wait_ns : kDepNs;
   cudaStream_t st = (cudaStream_t)stream;
   if (plan->form == WK_BATCH_PHASES) {
-    const BatchItem* lists[4] = {a.items[0], a.items[0] + plan->n_parts[0],
-                                 a.items[0] + plan->n_parts[0] + plan->n_parts[1], a.items[1]};
-    const int counts[4] = {plan->n_parts[0], plan->n_parts[1], plan->n_parts[2], plan->n_items[1]};
+    // the tile lists and the boundary-plane H rows of phase A, then phase B
+    const BatchItem* lists[kTileLists + 2];
+    int counts[kTileLists + 2];
+    const BatchItem* at = a.items[0];
+    for (int l = 0; l <= kTileLists; l++) {
+      lists[l] = at;
+      counts[l] = plan->n_parts[l];
+      at += counts[l];
+    }
+    lists[kTileLists + 1] = a.items[1];
+    counts[kTileLists + 1] = plan->n_items[1];
     timer_begin(st);
     for (int s = 0; s < n_steps; s++) {
-      for (int l = 0; l < 4; l++) {
+      for (int l = 0; l < kTileLists + 2; l++) {
         if (counts[l] == 0) continue;
-        if (l < 2)
-          kTileKerns[l == 0 ? 1 : 0][plan->variant]<<<counts[l], cThreads, plan->smem, st>>>(
-              a, a.insts, lists[l], s);
+        if (l < kTileLists)
+          kTileKerns[l][plan->variant]<<<counts[l], cThreads, plan->smem, st>>>(a, a.insts,
+                                                                              lists[l], s);
         else
           k_batch_shells<<<counts[l], cThreads, 0, st>>>(a, a.insts, lists[l], s);
       }

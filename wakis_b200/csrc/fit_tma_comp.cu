@@ -9,16 +9,17 @@ namespace wk {
 
 namespace {
 
-template <typename IdT, bool SIG, int MODE, bool CT>
+template <typename IdT, bool SIG, int MODE, bool CT, int TW>
 __global__ void __launch_bounds__(cThreads, 2)
 k_tma_comp(FitParams<double> p, CompState cs, const __grid_constant__ CompMaps maps,
            long long step, int KC) {
   extern __shared__ __align__(128) unsigned char sm_raw[];
-  comp_tile<IdT, SIG, MODE, CT ? 1 : 0, false>(p, cs, maps, step, KC, blockIdx.x, blockIdx.y,
-                                               blockIdx.z, CT, sm_raw);
+  comp_tile<IdT, SIG, MODE, CT ? 1 : 0, false, TW>(p, cs, maps, step, KC, blockIdx.x,
+                                                   blockIdx.y, blockIdx.z, CT, sm_raw);
 }
 
-constexpr int kCompKernels = 36;
+// id width x J mode x face mode x compensation words by TMA x tile width
+constexpr int kCompKernels = 72;
 int g_comp_sms[kCompKernels][64], g_comp_per_sm[kCompKernels][64];
 bool g_comp_attr[kCompKernels][64];
 
@@ -44,23 +45,46 @@ bool tma_comp_supported(const wk_fit_desc* d, const FitParams<double>& p) {
   return tma_encode_fn() != nullptr;
 }
 
+// Box and layout figures of one tile width
+struct CompDims {
+  int tx, ty, ebx, hbx, cbx, by, hby, smem;
+};
+template <int TW>
+CompDims comp_dims(bool full, bool ct) {
+  using S = CShape<TW>;
+  CompDims c;
+  c.tx = S::TX;
+  c.ty = S::TY;
+  c.ebx = full ? CGeom<true, TW>::ebx : CGeom<false, TW>::ebx;
+  c.hbx = full ? CGeom<true, TW>::hbx : CGeom<false, TW>::hbx;
+  c.cbx = full ? CGeom<true, TW>::cbx : CGeom<false, TW>::cbx;
+  c.by = S::BY;
+  c.hby = S::HBY;
+  c.smem = full ? (ct ? CLayout<true, true, TW>::bytes : CLayout<true, false, TW>::bytes)
+                : (ct ? CLayout<false, true, TW>::bytes : CLayout<false, false, TW>::bytes);
+  return c;
+}
+
 cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, int par,
                             long long step, cudaStream_t st, int KC) {
   const int mode = tma_comp_mode(p);
   const bool full = mode != 0;
   CompState cs = comp_state(d, par);
   CompMaps maps;
-  const int ebx = full ? CGeom<true>::ebx : CGeom<false>::ebx;
-  const int cbx = full ? CGeom<true>::cbx : CGeom<false>::cbx;
   // compensation words by TMA: 16-byte row pitch and component bases
   const bool ct = p.Nx % 8 == 0 && ((uintptr_t)cs.Hc_in % 16) == 0 &&
                   ((uintptr_t)cs.Ec_in % 16) == 0;
+  // tile shape: 64x8 with tile_rows == 8, else 32x16 (the faster on B200:
+  // less halo work per tile, the same rows for every cell)
+  const bool w32 = d->tile_rows != 8;
+  const CompDims cd = w32 ? comp_dims<32>(full, ct) : comp_dims<64>(full, ct);
   for (int c = 0; c < 3; c++) {
-    if (!encode_3d(&maps.e[c], cs.E_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, ebx, cBY) ||
-        !encode_3d(&maps.h[c], cs.H_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, cBX, cHBY))
+    if (!encode_3d(&maps.e[c], cs.E_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, cd.ebx, cd.by) ||
+        !encode_3d(&maps.h[c], cs.H_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, cd.hbx, cd.hby))
       return cudaErrorInvalidValue;
-    if (ct && (!encode_3d(&maps.c[c], cs.Hc_in + c * p.N, 2, p.Nx, p.Ny, p.Nz, cbx, cHBY) ||
-               !encode_3d(&maps.c[3 + c], cs.Ec_in + c * p.N, 2, p.Nx, p.Ny, p.Nz, cbx, cHBY)))
+    if (ct &&
+        (!encode_3d(&maps.c[c], cs.Hc_in + c * p.N, 2, p.Nx, p.Ny, p.Nz, cd.cbx, cd.hby) ||
+         !encode_3d(&maps.c[3 + c], cs.Ec_in + c * p.N, 2, p.Nx, p.Ny, p.Nz, cd.cbx, cd.hby)))
       return cudaErrorInvalidValue;
   }
   int dev = 0;
@@ -69,23 +93,23 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   const int ib = p.id_bytes == 1 ? 0 : (p.id_bytes == 2 ? 1 : 2);
   const bool sig = p.j_mode == WK_J_SIGMA_E;
-  const int slot = (ct ? 18 : 0) + mode * 6 + ib * 2 + (sig ? 1 : 0);
+  const int slot = (w32 ? 36 : 0) + (ct ? 18 : 0) + mode * 6 + ib * 2 + (sig ? 1 : 0);
   using K = void (*)(FitParams<double>, CompState, const CompMaps, long long, int);
-#define WK_COMP_KERNS(CT)                                                          \
-  k_tma_comp<uint8_t, false, 0, CT>, k_tma_comp<uint8_t, true, 0, CT>,             \
-      k_tma_comp<uint16_t, false, 0, CT>, k_tma_comp<uint16_t, true, 0, CT>,       \
-      k_tma_comp<uint32_t, false, 0, CT>, k_tma_comp<uint32_t, true, 0, CT>,       \
-      k_tma_comp<uint8_t, false, 1, CT>, k_tma_comp<uint8_t, true, 1, CT>,         \
-      k_tma_comp<uint16_t, false, 1, CT>, k_tma_comp<uint16_t, true, 1, CT>,       \
-      k_tma_comp<uint32_t, false, 1, CT>, k_tma_comp<uint32_t, true, 1, CT>,       \
-      k_tma_comp<uint8_t, false, 2, CT>, k_tma_comp<uint8_t, true, 2, CT>,         \
-      k_tma_comp<uint16_t, false, 2, CT>, k_tma_comp<uint16_t, true, 2, CT>,       \
-      k_tma_comp<uint32_t, false, 2, CT>, k_tma_comp<uint32_t, true, 2, CT>
-  const K kerns[kCompKernels] = {WK_COMP_KERNS(false), WK_COMP_KERNS(true)};
+#define WK_COMP_KERNS(CT, TW)                                                              \
+  k_tma_comp<uint8_t, false, 0, CT, TW>, k_tma_comp<uint8_t, true, 0, CT, TW>,             \
+      k_tma_comp<uint16_t, false, 0, CT, TW>, k_tma_comp<uint16_t, true, 0, CT, TW>,       \
+      k_tma_comp<uint32_t, false, 0, CT, TW>, k_tma_comp<uint32_t, true, 0, CT, TW>,       \
+      k_tma_comp<uint8_t, false, 1, CT, TW>, k_tma_comp<uint8_t, true, 1, CT, TW>,         \
+      k_tma_comp<uint16_t, false, 1, CT, TW>, k_tma_comp<uint16_t, true, 1, CT, TW>,       \
+      k_tma_comp<uint32_t, false, 1, CT, TW>, k_tma_comp<uint32_t, true, 1, CT, TW>,       \
+      k_tma_comp<uint8_t, false, 2, CT, TW>, k_tma_comp<uint8_t, true, 2, CT, TW>,         \
+      k_tma_comp<uint16_t, false, 2, CT, TW>, k_tma_comp<uint16_t, true, 2, CT, TW>,       \
+      k_tma_comp<uint32_t, false, 2, CT, TW>, k_tma_comp<uint32_t, true, 2, CT, TW>
+  const K kerns[kCompKernels] = {WK_COMP_KERNS(false, 64), WK_COMP_KERNS(true, 64),
+                                 WK_COMP_KERNS(false, 32), WK_COMP_KERNS(true, 32)};
 #undef WK_COMP_KERNS
   const K kern = kerns[slot];
-  const int smem = full ? (ct ? CLayout<true, true>::bytes : CLayout<true, false>::bytes)
-                        : (ct ? CLayout<false, true>::bytes : CLayout<false, false>::bytes);
+  const int smem = cd.smem;
   if (!g_comp_attr[slot][dev]) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -99,7 +123,7 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   }
   const int span_x = full ? p.Nx : p.Nx - 4, span_y = full ? p.Ny : p.Ny - 4;
   const int planes = mode == 1 ? p.Nz : p.Nz - 4;
-  const int gx = (span_x + cTX - 1) / cTX, gy = (span_y + cTY - 1) / cTY;
+  const int gx = (span_x + cd.tx - 1) / cd.tx, gy = (span_y + cd.ty - 1) / cd.ty;
   if (KC <= 0)
     KC = tma_auto_kc((long long)gx * gy, planes,
                      (long long)g_comp_sms[slot][dev] * g_comp_per_sm[slot][dev]);

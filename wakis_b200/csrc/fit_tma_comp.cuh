@@ -10,17 +10,18 @@
 //
 // The face modes are those of the FP64 kernel (k_tma): the interior with
 // shell launches, all of x and y, or the whole grid.  Block (bx, by, bz) owns
-// the tile i in [i0, i0+64), j in [j0, j0+8) of planes [k0, k0+KC) and
-// marches in z.  An idle lane of warp 9 issues cp.async.bulk.tensor loads (no
+// the tile i in [i0, i0+TW), j in [j0, j0+512/TW) of planes [k0, k0+KC)
+// (TW = 64, or 32 for batched instances: CShape) and marches in z.  An idle
+// lane of warp 9 issues cp.async.bulk.tensor loads (no
 // multicast) of E (three planes in a ring), H (two planes) and, with
 // Nx % 8 == 0, the bf16 compensation words of plane k with H(k), into shared
 // memory, each slot completing on its own mbarrier; the loads of E(k+2) and
 // H(k+1) go out at the start of plane k.
 //
 // Threads work on pairs of cells (i, i+1) with packed f32x2 arithmetic:
-// warps 0-7 own the 256 pairs of the tile (row = warp, pair = lane) in both
-// half-steps, warp 8 the 32 pairs of the halo row j0-1, and 9 lanes of warp
-// 9 the halo column i0-1 (single cells).  The halo H is recomputed with the
+// warps 0-7 own the 256 pairs of the tile (64x8: row = warp, pair = lane)
+// in both half-steps, warp 8 the pairs of the halo row j0-1, and lanes of
+// warp 9 the halo column i0-1 (single cells).  The halo H is recomputed with the
 // same compensated update as its owner's, so it is the value the owner
 // stores.  The new Hx, Hy of a tile pair stay in registers as H(k-1) of the
 // next plane.  The material ids and the FP64 inputs of the per-plane factor
@@ -40,21 +41,40 @@
 
 namespace wk {
 
-constexpr int cTX = 64, cTY = 8;
-constexpr int cBX = 68, cBY = 10;         // E box (floats): x from i0-2, y from j0-1
-constexpr int cHBY = 9;                   // H box rows (68 wide)
 constexpr int cES = 3, cHS = 2;
 static_assert(cES == 3 && cHS == 2, "the step loop counts the ring slots for 3 E and 2 H slots");
 constexpr int cThreads = 320;
-constexpr int cEW = 66;                   // Hs row: index eb*66 + ea + 1
-constexpr int cExt = cEW * (cTY + 1);     // 594
 constexpr int cMat = 64;                  // materials (16 floats each) in smem
 constexpr int cMatW = 16;
-// per-plane factor rows (floats): H x-row (per ext row j), H y-row (per ext
-// column i, stored at ea+1 so that pairs are 8-byte aligned), E x-row (per
-// tile row), E y-row (per tile column); dt folded in
-constexpr int R_HXA = 0, R_HXB = 10, R_HYA = 20, R_HYB = 86, R_EXA = 152, R_EXB = 160,
-              R_EYA = 168, R_EYB = 232, cRow = 296;
+
+// Tile shape: TW columns x 512/TW rows.  Warps 0-7 hold the 256 pairs of
+// cells of the tile (TW/2 pairs a row, 64/TW rows a warp), warp 8 the TW/2
+// pairs of the halo row, warp 9 the 512/TW + 1 cells of the halo column.
+// 64x8 is the one-grid kernel's; 32x16 fills the lanes of grids whose x
+// extent lies just above a multiple of 64 better (batched instances).
+template <int TW>
+struct CShape {
+  static_assert(TW == 64 || TW == 32, "tile widths 64 and 32");
+  static constexpr int TX = TW, TY = 512 / TW;
+  static constexpr int PL = TX / 2;           // pairs (lanes) per tile row
+  static constexpr int BX = TX + 4;           // E box (interior) and H box width
+  static constexpr int BY = TY + 2;           // E box rows, from j0-1
+  static constexpr int HBY = TY + 1;          // H and compensation box rows
+  static constexpr int EW = TX + 2;           // Hs row: index eb*EW + ea + 1
+  static constexpr int Ext = EW * (TY + 1);
+  // per-plane factor rows (floats): H x-row (per ext row j, TY+1 entries
+  // padded to an even count), H y-row (per ext column i, stored at ea+1 so
+  // that pairs are 8-byte aligned), E x-row (per tile row), E y-row (per
+  // tile column); dt folded in
+  static constexpr int HX = (TY + 2) / 2 * 2;
+  static constexpr int R_HXA = 0, R_HXB = HX, R_HYA = 2 * HX, R_HYB = R_HYA + TX + 2,
+                       R_EXA = R_HYB + TX + 2, R_EXB = R_EXA + TY, R_EYA = R_EXB + TY,
+                       R_EYB = R_EYA + TX, Row = R_EYB + TX;
+  static_assert(Row <= cThreads, "one factor-row entry per thread");
+};
+// the one-grid kernel's shape
+constexpr int cTX = CShape<64>::TX, cTY = CShape<64>::TY;
+constexpr int cBX = CShape<64>::BX, cBY = CShape<64>::BY, cHBY = CShape<64>::HBY;
 
 struct CompMaps {
   CUtensorMap e[3];
@@ -62,34 +82,37 @@ struct CompMaps {
   CUtensorMap c[6];        // compensation words (CT): Hc x/y/z, then Ec x/y/z
 };
 
-// FULL (every face PEC-masked): tiles from i0 = 64 bx cover the whole grid
-// and both boxes start at i0-4 (16-byte aligned): E 72 wide, H 68 wide.
-// The compensation-word boxes (CT) are 9 rows from j0-1 and start at an x
-// that is a multiple of 8 (16 bytes of bf16 words): i0-8, 80 wide (FULL),
-// or i0-2, 72 wide.
-template <bool FULL>
+// FULL (every face PEC-masked): tiles from i0 = TW bx cover the whole grid
+// and both boxes start at i0-4 (16-byte aligned): E TW+8 wide, H TW+4 wide.
+// The compensation-word boxes (CT) are TY+1 rows from j0-1 and start at an
+// x that is a multiple of 8 (16 bytes of bf16 words): i0-8, TW+16 wide
+// (FULL), or i0-2, TW+8 wide.
+template <bool FULL, int TW = 64>
 struct CGeom {
-  static constexpr int ebx = FULL ? cTX + 8 : cBX;   // E box width
-  static constexpr int hbx = cBX;                    // H box width (68)
-  static constexpr int xo = FULL ? 3 : 1;            // box x of ext column 0
-  static constexpr int xs_off = FULL ? 4 : 2;        // box start = i0 - xs_off
-  static constexpr int cbx = FULL ? cTX + 16 : cTX + 8;   // compensation box width
-  static constexpr int cxs_off = FULL ? 8 : 2;            // its start = i0 - cxs_off
-  static constexpr int cxo = cxs_off - 1;                 // its x of ext column 0
+  using S = CShape<TW>;
+  static constexpr int ebx = FULL ? S::TX + 8 : S::BX;     // E box width
+  static constexpr int hbx = S::BX;                        // H box width
+  static constexpr int xo = FULL ? 3 : 1;                  // box x of ext column 0
+  static constexpr int xs_off = FULL ? 4 : 2;              // box start = i0 - xs_off
+  static constexpr int cbx = FULL ? S::TX + 16 : S::TX + 8;   // compensation box width
+  static constexpr int cxs_off = FULL ? 8 : 2;                // its start = i0 - cxs_off
+  static constexpr int cxo = cxs_off - 1;                     // its x of ext column 0
 };
 
-template <bool FULL, bool CT>
+template <bool FULL, bool CT, int TW = 64>
 struct CLayout {
-  static constexpr int eslot = round128(CGeom<FULL>::ebx * cBY * 4);
-  static constexpr int hslot = round128(CGeom<FULL>::hbx * cHBY * 4);
-  static constexpr int cslot = CT ? round128(CGeom<FULL>::cbx * cHBY * 2) : 0;
+  using S = CShape<TW>;
+  using G = CGeom<FULL, TW>;
+  static constexpr int eslot = round128(G::ebx * S::BY * 4);
+  static constexpr int hslot = round128(G::hbx * S::HBY * 4);
+  static constexpr int cslot = CT ? round128(G::cbx * S::HBY * 2) : 0;
   static constexpr int e_off = 0;
   static constexpr int h_off = e_off + cES * 3 * eslot;
   static constexpr int c_off = h_off + cHS * 3 * hslot;      // [cHS][6][cslot]
   static constexpr int hs_off = c_off + cHS * 6 * cslot;
-  static constexpr int row_off = hs_off + round128(3 * cExt * 4);
-  static constexpr int raw_off = row_off + round128(2 * cRow * 4);     // [3][cRow][2] doubles
-  static constexpr int id_off = raw_off + round128(3 * cRow * 16);     // [3][threads] u64
+  static constexpr int row_off = hs_off + round128(3 * S::Ext * 4);
+  static constexpr int raw_off = row_off + round128(2 * S::Row * 4);   // [3][Row][2] doubles
+  static constexpr int id_off = raw_off + round128(3 * S::Row * 16);   // [3][threads] u64
   static constexpr int mat_off = id_off + round128(3 * cThreads * 8);
   static constexpr int bar_off = mat_off + round128(cMat * cMatW * 4);
   static constexpr int bytes = bar_off + (cES + cHS) * 8 + 128;
@@ -138,32 +161,34 @@ struct RowSrc {
   int fs, gs;
 };
 
+template <int TW>
 __device__ __forceinline__ RowSrc row_src(const FitParams<double>& p, int r, int i0, int j0) {
+  using S = CShape<TW>;
   const int Nx = p.Nx, Ny = p.Ny;
   RowSrc s{nullptr, nullptr, 0, 0};
-  if (r < R_HXB) {
-    const int j = j0 - 1 + (r - R_HXA);
-    if (r - R_HXA < 9 && j >= 0 && j < Ny) s = RowSrc{p.iAx + j, p.Ly + j, Ny, 0};
-  } else if (r < R_HYA) {
-    const int j = j0 - 1 + (r - R_HXB);
-    if (r - R_HXB < 9 && j >= 0 && j < Ny) s = RowSrc{p.iAx + j, p.Lz, Ny, 1};
-  } else if (r < R_HYB) {
-    const int i = i0 - 2 + (r - R_HYA);
-    if (r > R_HYA && i >= 0 && i < Nx) s = RowSrc{p.iAy + i, p.Lx + i, Nx, 0};
-  } else if (r < R_EXA) {
-    const int i = i0 - 2 + (r - R_HYB);
-    if (r > R_HYB && i >= 0 && i < Nx) s = RowSrc{p.iAy + i, p.Lz, Nx, 1};
-  } else if (r < R_EXB) {
-    const int j = j0 + (r - R_EXA);
+  if (r < S::R_HXB) {
+    const int j = j0 - 1 + (r - S::R_HXA);
+    if (r - S::R_HXA < S::TY + 1 && j >= 0 && j < Ny) s = RowSrc{p.iAx + j, p.Ly + j, Ny, 0};
+  } else if (r < S::R_HYA) {
+    const int j = j0 - 1 + (r - S::R_HXB);
+    if (r - S::R_HXB < S::TY + 1 && j >= 0 && j < Ny) s = RowSrc{p.iAx + j, p.Lz, Ny, 1};
+  } else if (r < S::R_HYB) {
+    const int i = i0 - 2 + (r - S::R_HYA);
+    if (r > S::R_HYA && i >= 0 && i < Nx) s = RowSrc{p.iAy + i, p.Lx + i, Nx, 0};
+  } else if (r < S::R_EXA) {
+    const int i = i0 - 2 + (r - S::R_HYB);
+    if (r > S::R_HYB && i >= 0 && i < Nx) s = RowSrc{p.iAy + i, p.Lz, Nx, 1};
+  } else if (r < S::R_EXB) {
+    const int j = j0 + (r - S::R_EXA);
     if (j < Ny) s = RowSrc{p.itAx + j, p.tLy + j, Ny, 0};
-  } else if (r < R_EYA) {
-    const int j = j0 + (r - R_EXB);
+  } else if (r < S::R_EYA) {
+    const int j = j0 + (r - S::R_EXB);
     if (j < Ny) s = RowSrc{p.itAx + j, p.tLz, Ny, 1};
-  } else if (r < R_EYB) {
-    const int i = i0 + (r - R_EYA);
+  } else if (r < S::R_EYB) {
+    const int i = i0 + (r - S::R_EYA);
     if (i < Nx) s = RowSrc{p.itAy + i, p.tLx + i, Nx, 0};
-  } else if (r < cRow) {
-    const int i = i0 + (r - R_EYB);
+  } else if (r < S::Row) {
+    const int i = i0 + (r - S::R_EYB);
     if (i < Nx) s = RowSrc{p.itAy + i, p.tLz, Nx, 1};
   }
   return s;
@@ -201,7 +226,7 @@ __device__ __forceinline__ float row_value(double dt, double f, double g) {
 // holds the compensation slots).  BATCH: the block runs further tiles after
 // this one, so the mbarriers are invalidated at the end.  Returns false when
 // a load wait ran out (the status word is then set).
-template <typename IdT, bool SIG, int MODE, int CTM, bool BATCH>
+template <typename IdT, bool SIG, int MODE, int CTM, bool BATCH, int TW = 64>
 __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const CompState& cs,
                                           const CompMaps& maps, long long step, int KC,
                                           unsigned bx, unsigned by, unsigned bz, bool ct_run,
@@ -210,17 +235,18 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
   constexpr bool ZFULL = MODE == 1;    // ... and every plane
   if (!BATCH) step = step_index(p, step);
   const bool CT = CTM == 2 ? ct_run : CTM == 1;
-  using Lay = CLayout<(MODE != 0), (CTM != 0)>;
-  using G = CGeom<(MODE != 0)>;
+  using S = CShape<TW>;
+  using Lay = CLayout<(MODE != 0), (CTM != 0), TW>;
+  using G = CGeom<(MODE != 0), TW>;
   constexpr int SE = Lay::eslot / 4, SH = Lay::hslot / 4, SC = Lay::cslot / 2;
   constexpr int EBX = G::ebx, XO = G::xo;
   unsigned char* sm = sm_raw + ((128 - (smem_u32(sm_raw) & 127)) & 127);
   float* Eb = reinterpret_cast<float*>(sm + Lay::e_off);
   float* Hb = reinterpret_cast<float*>(sm + Lay::h_off);
   uint16_t* Cb = reinterpret_cast<uint16_t*>(sm + Lay::c_off);   // [cHS][6][SC]
-  float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][cExt]
-  float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][cRow]
-  double* Rraw = reinterpret_cast<double*>(sm + Lay::raw_off); // [3][cRow][2] f, g
+  float* Hs = reinterpret_cast<float*>(sm + Lay::hs_off);     // [3][Ext]
+  float* Rw = reinterpret_cast<float*>(sm + Lay::row_off);    // [2][Row]
+  double* Rraw = reinterpret_cast<double*>(sm + Lay::raw_off); // [3][Row][2] f, g
   uint64_t* sidw = reinterpret_cast<uint64_t*>(sm + Lay::id_off);  // [3][threads] id words
   float* mt = reinterpret_cast<float*>(sm + Lay::mat_off);    // [n_mat][16]
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Lay::bar_off);
@@ -228,7 +254,7 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
   const int Nx = p.Nx, Ny = p.Ny;
   const long long N = p.N, NxNy = p.NxNy;
   const int Nz = p.Nz;
-  const int i0 = (FULL ? 0 : 2) + bx * cTX, j0 = (FULL ? 0 : 2) + by * cTY;
+  const int i0 = (FULL ? 0 : 2) + bx * S::TX, j0 = (FULL ? 0 : 2) + by * S::TY;
   const int k0 = (ZFULL ? 0 : 2) + bz * KC, k1 = min(k0 + KC, ZFULL ? Nz : Nz - 2);
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -236,8 +262,8 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
   // warp 9, which owns no item
   const bool prod = tid == cThreads - 1;
   const int pstart = k0 - 1;
-  const uint32_t e_bytes = 3u * EBX * cBY * 4u;
-  const uint32_t h_bytes = 3u * G::hbx * cHBY * 4u + (CT ? 6u * G::cbx * cHBY * 2u : 0u);
+  const uint32_t e_bytes = 3u * EBX * S::BY * 4u;
+  const uint32_t h_bytes = 3u * G::hbx * S::HBY * 4u + (CT ? 6u * G::cbx * S::HBY * 2u : 0u);
 
   if (prod) {
     for (int s = 0; s < cES + cHS; s++) mbar_init(&bar[s], 1);
@@ -276,9 +302,10 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
   }
 
   // role: 0 tile pair, 1 halo-row pair, 2 halo-column cell, 3 idle
-  const int role = warp < 8 ? 0 : (warp == 8 ? 1 : (lane < cTY + 1 ? 2 : 3));
+  const int role = warp < 8 ? 0
+                 : (warp == 8 ? (lane < S::PL ? 1 : 3) : (lane < S::TY + 1 ? 2 : 3));
   int ea, eb;
-  if (role == 0) { ea = 2 * lane + 1; eb = warp + 1; }
+  if (role == 0) { ea = 2 * (lane % S::PL) + 1; eb = warp * (32 / S::PL) + lane / S::PL + 1; }
   else if (role == 1) { ea = 2 * lane + 1; eb = 0; }
   else { ea = 0; eb = lane; }
   const int ci = i0 - 1 + ea, cj = j0 - 1 + eb;          // first cell of the item
@@ -295,7 +322,7 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
   const bool yf0 = cj == 0 || cj == Ny - 1, yf1 = cj + 1 >= Ny - 1;
   const bool nearface = hval && (xf0a || xf1a || (pair && (xf0b || xf1b)) || yf0 || yf1);
   const bool warp_face = FULL && __any_sync(0xffffffffu, nearface);
-  const int hi = eb * cEW + ea + 1;                       // Hs index
+  const int hi = eb * S::EW + ea + 1;                       // Hs index
   const int cix = eb * G::cbx + ea + G::cxo;              // compensation box index
   const long long nb = ci + (long long)cj * Nx;           // flat index at k = 0
   // the item holds a cell of the Ez capture window (plane-invariant test)
@@ -374,19 +401,19 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
   // The f, g inputs of factor-row entry tid of plane q go into ring slot
   // (q - pstart) % 3 by cp.async two planes ahead (one group per plane and
   // thread); the float row of plane q is formed at the end of plane q-1.
-  const RowSrc rsrc = row_src(p, tid < cRow ? tid : cRow, i0, j0);
+  const RowSrc rsrc = row_src<TW>(p, tid < S::Row ? tid : S::Row, i0, j0);
   // slot = (q - pstart) % 3, ida = the ids of the item at plane q
   auto stage_rows = [&](int q, int slot, const IdT* ida) {
     if (q < k1) {
-      if (tid < cRow) row_stage(rsrc, q, Nz, p.Lz, Rraw + (slot * cRow + tid) * 2);
+      if (tid < S::Row) row_stage(rsrc, q, Nz, p.Lz, Rraw + (slot * S::Row + tid) * 2);
       if (hval) stage_ids(q, ida, sidw + slot * cThreads + tid);
     }
     cp_async_commit();
   };
   auto form_row = [&](int q, int slot) {
-    if (tid < cRow) {
-      const double* v = Rraw + (slot * cRow + tid) * 2;
-      Rw[(q & 1) * cRow + tid] = row_value(p.dt, v[0], v[1]);
+    if (tid < S::Row) {
+      const double* v = Rraw + (slot * S::Row + tid) * 2;
+      Rw[(q & 1) * S::Row + tid] = row_value(p.dt, v[0], v[1]);
     }
   };
   stage_rows(pstart, 0, idp + (long long)pstart * NxNy);
@@ -437,7 +464,7 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
     const float* Ek1 = Eb + se1 * 3 * SE;
     const float* Hk = Hb + sh * 3 * SH;
     const uint16_t* Ck = Cb + sh * 6 * SC;
-    const float* R = Rw + (pl & 1) * cRow;
+    const float* R = Rw + (pl & 1) * S::Row;
     const long long n = nb + (long long)pl * NxNy;
 
     // plane face flags (MODE 1): at the plane and of the +z neighbour
@@ -449,9 +476,9 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
     float2 hxn = zero2, hyn = zero2;
     if (FULL && role < 3 && !hval) {
       if (pair) {
-        st2(Hs + hi, zero2); st2(Hs + cExt + hi, zero2); st2(Hs + 2 * cExt + hi, zero2);
+        st2(Hs + hi, zero2); st2(Hs + S::Ext + hi, zero2); st2(Hs + 2 * S::Ext + hi, zero2);
       } else {
-        Hs[hi] = 0.f; Hs[cExt + hi] = 0.f; Hs[2 * cExt + hi] = 0.f;
+        Hs[hi] = 0.f; Hs[S::Ext + hi] = 0.f; Hs[2 * S::Ext + hi] = 0.f;
       }
     }
     if (hval && (!prologue || role == 0) && !(ZFULL && pl < 0)) {
@@ -465,14 +492,14 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
         ex2 = ld2(Ek + bi + EBX); ez2 = ld2(Ek + 2 * SE + bi + EBX);
         ex3 = ld2(Ek1 + bi); ey3 = ld2(Ek1 + SE + bi);
         hx = ld2(Hk + hbi); hy = ld2(Hk + SH + hbi); hz = ld2(Hk + 2 * SH + hbi);
-        ya = ld2(R + R_HYA + ea + 1); yb = ld2(R + R_HYB + ea + 1);
+        ya = ld2(R + S::R_HYA + ea + 1); yb = ld2(R + S::R_HYB + ea + 1);
       } else {
         ex0 = bcast(Ek[bi]); ey0 = bcast(Ek[SE + bi]); ez0 = bcast(Ek[2 * SE + bi]);
         ey1 = bcast(Ek[SE + bi + 1]); ez1 = bcast(Ek[2 * SE + bi + 1]);
         ex2 = bcast(Ek[bi + EBX]); ez2 = bcast(Ek[2 * SE + bi + EBX]);
         ex3 = bcast(Ek1[bi]); ey3 = bcast(Ek1[SE + bi]);
         hx = bcast(Hk[hbi]); hy = bcast(Hk[SH + hbi]); hz = bcast(Hk[2 * SH + hbi]);
-        ya = bcast(R[R_HYA + ea + 1]); yb = bcast(R[R_HYB + ea + 1]);
+        ya = bcast(R[S::R_HYA + ea + 1]); yb = bcast(R[S::R_HYB + ea + 1]);
       }
       if (masked && !p.faces_clean) {
         // E column entries tangential to a face they lie on are masked
@@ -495,8 +522,8 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
       const float2 mux = make_float2(u0.x, u1.x), muy = make_float2(u0.y, u1.y),
                    muz = make_float2(u0.z, u1.z);
       // S_x = a (ey0 - ey3) + b (ez2 - ez0)   (a = dt iAx Ly imu_x, b = dt iAx Lz imu_x)
-      const float2 sx = fma2(mul2(mux, bcast(R[R_HXA + eb])), sub2(ey0, ey3),
-                             mul2(mul2(mux, bcast(R[R_HXB + eb])), sub2(ez2, ez0)));
+      const float2 sx = fma2(mul2(mux, bcast(R[S::R_HXA + eb])), sub2(ey0, ey3),
+                             mul2(mul2(mux, bcast(R[S::R_HXB + eb])), sub2(ez2, ez0)));
       // S_y = a (ex3 - ex0) + b (ez0 - ez1)   (a = dt iAy Lx imu_y, b = dt iAy Lz imu_y)
       const float2 sy = fma2(mul2(muy, ya), sub2(ex3, ex0), mul2(mul2(muy, yb), sub2(ez0, ez1)));
       // S_z = a (ex0 - ex2) + b (ey1 - ey0)   (a = dt iAz Lx imu_z, b = dt iAz Ly imu_z)
@@ -507,9 +534,9 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
       hy = cadd2(hy, hc[1], mul2(sy, m1v));
       hz = cadd2(hz, hc[2], mul2(sz, m1v));
       if (pair) {
-        st2(Hs + hi, hx); st2(Hs + cExt + hi, hy); st2(Hs + 2 * cExt + hi, hz);
+        st2(Hs + hi, hx); st2(Hs + S::Ext + hi, hy); st2(Hs + 2 * S::Ext + hi, hz);
       } else {
-        Hs[hi] = hx.x; Hs[cExt + hi] = hy.x; Hs[2 * cExt + hi] = hz.x;
+        Hs[hi] = hx.x; Hs[S::Ext + hi] = hy.x; Hs[2 * S::Ext + hi] = hz.x;
       }
       hxn = hx;
       hyn = hy;
@@ -529,10 +556,10 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
       const float* m0 = mt + id0 * cMatW;
       const float* m1 = mt + id1 * cMatW;
       const int b = eb - 1, a = ea - 1;
-      const float2 hx0 = ld2(Hs + hi), hy0 = ld2(Hs + cExt + hi), hz0 = ld2(Hs + 2 * cExt + hi);
-      const float2 hy1 = make_float2(Hs[cExt + hi - 1], hy0.x);
-      const float2 hz1 = make_float2(Hs[2 * cExt + hi - 1], hz0.x);
-      const float2 hx2 = ld2(Hs + hi - cEW), hz2 = ld2(Hs + 2 * cExt + hi - cEW);
+      const float2 hx0 = ld2(Hs + hi), hy0 = ld2(Hs + S::Ext + hi), hz0 = ld2(Hs + 2 * S::Ext + hi);
+      const float2 hy1 = make_float2(Hs[S::Ext + hi - 1], hy0.x);
+      const float2 hz1 = make_float2(Hs[2 * S::Ext + hi - 1], hz0.x);
+      const float2 hx2 = ld2(Hs + hi - S::EW), hz2 = ld2(Hs + 2 * S::Ext + hi - S::EW);
       const float4 w0 = *reinterpret_cast<const float4*>(m0 + 4);
       const float4 w1 = *reinterpret_cast<const float4*>(m1 + 4);
       const float2 iex = make_float2(w0.x, w1.x), iey = make_float2(w0.y, w1.y),
@@ -543,11 +570,11 @@ __device__ __forceinline__ bool comp_tile(const FitParams<double>& p, const Comp
                             make_float2(s0.z, s1.z)};
       // curl_x = c1 (hy3 - hy0) + c2 (hz0 - hz2)   (c1 = dt ieps_x itAx tLy, c2 = .. tLz)
       float2 cu[3];
-      cu[0] = fma2(mul2(iex, bcast(R[R_EXA + b])), sub2(hyp, hy0),
-                   mul2(mul2(iex, bcast(R[R_EXB + b])), sub2(hz0, hz2)));
+      cu[0] = fma2(mul2(iex, bcast(R[S::R_EXA + b])), sub2(hyp, hy0),
+                   mul2(mul2(iex, bcast(R[S::R_EXB + b])), sub2(hz0, hz2)));
       // curl_y = c1 (hx0 - hx3) + c2 (hz1 - hz0)   (c1 = dt ieps_y itAy tLx, c2 = .. tLz)
-      cu[1] = fma2(mul2(iey, ld2(R + R_EYA + a)), sub2(hx0, hxp),
-                   mul2(mul2(iey, ld2(R + R_EYB + a)), sub2(hz1, hz0)));
+      cu[1] = fma2(mul2(iey, ld2(R + S::R_EYA + a)), sub2(hx0, hxp),
+                   mul2(mul2(iey, ld2(R + S::R_EYB + a)), sub2(hz1, hz0)));
       // curl_z = c1 (hx2 - hx0) + c2 (hy0 - hy1)   (c1 = dt ieps_z itAz tLx, c2 = .. tLy)
       cu[2] = fma2(mul2(iez, eza), sub2(hx2, hx0), mul2(mul2(iez, ezb), sub2(hy0, hy1)));
       if (masked) {
