@@ -114,8 +114,9 @@ typedef struct wk_fit_desc {
   /* Kernel choice for wk_fit_step (WK_KERNEL_* below).
    * tile_planes (0 = automatic) sets the planes per block of the TMA kernel
    * and the planes per thread of the two-pass kernels.  tile_rows sets the
-   * tile shape of the WK_F32C TMA kernel and of the batched launches: 8
-   * for 64x8 tiles, 16 or 0 (the default) for 32x16 tiles.                 */
+   * tile shape of the TMA kernels and of the batched launches: 8 for 64x8
+   * tiles, 16 for 32x16 tiles, 0 for the faster on B200 (64x8 in FP64 and
+   * FP32, 32x16 in WK_F32C and the batched launches).                      */
   int kernel;
   int tile_rows, tile_planes;
   /* WK_F32C only: per-component compensation words of E and H (bf16 bit

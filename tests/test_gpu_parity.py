@@ -256,20 +256,22 @@ TMA_GRIDS = [((16, 12, 20), "float64"), ((24, 16, 30), "float64"), ((32, 20, 26)
              ((72, 18, 40), "float64")]
 
 
+@pytest.mark.parametrize("rows", [8, 16])
 @pytest.mark.parametrize("shape,dtype", TMA_GRIDS)
 @pytest.mark.parametrize("bcs", [(["pec"] * 3, ["pec"] * 3),
                                  (["periodic", "pec", "pml"], ["periodic", "pec", "pml"]),
                                  (["pec", "pec", "abc"], ["pec", "pec", "abc"]),
                                  (["pec", "electric", "periodic"], ["pml", "pec", "periodic"]),
                                  (["pec", "pec", "pec"], ["pec", "pec", "abc"])])
-def test_tma_kernel_exact_against_oracle(shape, dtype, bcs):
-    """TMA-staged fused kernel (interior) + shell: value-for-value equal to
-    the oracle after several steps from random fields (no exponential)."""
+def test_tma_kernel_exact_against_oracle(shape, dtype, bcs, rows):
+    """TMA-staged fused kernel (interior) + shell, on 64x8 (rows 8) and
+    32x16 tiles (rows 16): value-for-value equal to the oracle after
+    several steps from random fields (no exponential)."""
     c = dict(cases.STEP_CASES[2])     # conductive materials on the case boxes
     c.update(shape=shape, dtype=dtype, bc_low=bcs[0], bc_high=bcs[1], steps=5, n_pml=3)
     o = oracle_step_case(c)
     s = b200_step_case(c)
-    s.kernel, s.tile = "tma", (0, 0)
+    s.kernel, s.tile = "tma", (rows, 0)
     E0, H0 = cases.initial_fields(c, o.N)
     o.E[:], o.H[:] = E0, H0
     s.E.fromarray(E0)

@@ -233,7 +233,8 @@ cudaError_t launch_shell_pair(const FitParams<T>& p, long long step, cudaStream_
 template <typename T>
 bool tma_supported(const FitParams<T>& p);
 template <typename T>
-cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC);
+cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC,
+                       int rows);
 
 // Two steps per launch (fit_tma2.cu): k_tma2 covers grids whose faces are
 // all PEC-masked and clean, with J = 0 or sigma*E.

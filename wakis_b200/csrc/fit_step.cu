@@ -119,7 +119,7 @@ int run_fused(const wk_fit_desc* d, int n_steps, long long step0, cudaStream_t s
     }
     for (; s < n_steps; s++) {
       FitParams<T> p = make_params<T>(d, par);
-      cudaError_t e = launch_tma<T>(p, step0 + s, st, d->tile_planes);
+      cudaError_t e = launch_tma<T>(p, step0 + s, st, d->tile_planes, d->tile_rows);
       if (e != cudaSuccess) return wk_fail(-(int)e, "wk_fit_step: %s", cudaGetErrorString(e));
       par ^= 1;
     }

@@ -4,7 +4,8 @@
 // interior (2 <= i, j, k <= N-3, the two-cell shell in separate launches),
 // all of x and y for 2 <= k <= Nz-3 (x/y faces PEC-masked), or the whole grid
 // (every face PEC-masked).  Block (bx, by, bz) owns the tile
-// i in [i0, i0+64), j in [j0, j0+8) of planes [k0, k0+KC) and marches in z.
+// i in [i0, i0+TX), j in [j0, j0+TY) of planes [k0, k0+KC) and marches in z;
+// the tiles are 64x8 (the default) or 32x16 (wk_fit_desc.tile_rows = 16).
 // For plane k it needs E_old of planes k and k+1 on a box from (i0-2, j0-1)
 // (interior) or (i0-4, j0-1) (full-domain modes; x offsets stay 16-byte
 // aligned) and H_old of plane k on a box one row shorter.  An idle lane of
@@ -17,9 +18,10 @@
 // Per plane the block computes the new H on the tile plus its low halo row
 // and column (single-coefficient rows; the halo is recomputed so that no
 // block waits for another), a barrier, then the new E of the tile.  Each
-// thread owns the same cells in both phases (warps 0-7: row j0+w of the
-// tile, cells i0+lane and i0+32+lane; warp 8: the halo row; warp 9: the halo
-// column and the last cell of the halo row), so the new Hx, Hy of its tile
+// thread owns the same cells in both phases (warps 0-7, 64x8: row j0+w of
+// the tile, cells i0+lane and i0+32+lane; 32x16: rows j0+2w and j0+2w+1,
+// column i0+lane; warp 8: the halo row; warp 9: the halo column and the last
+// cell of the halo row), so the new Hx, Hy of its tile
 // cells stay in registers as H(k-1) of the next plane.  The per-plane metric
 // rows (iAx, iAy, itAx, itAy, Lz, tLz) go into a 3-slot ring by cp.async two
 // planes ahead, issued by warps 8 and 9 while the tile warps compute E; the
@@ -40,57 +42,74 @@
 
 namespace wk {
 
-constexpr int kTX = 64, kTY = 8;
-constexpr int kBX = kTX + 4, kBY = kTY + 2;          // E box
-constexpr int kHBY = kTY + 1;                        // H box rows
 constexpr int kES = 3, kHS = 2;                      // ring slots
 static_assert(kES == 3 && kHS == 2, "the step loop counts the ring slots for 3 E and 2 H slots");
 constexpr int kTmaThreads = 320;
-constexpr int kEW = kTX + 1;                         // ext tile row width
-constexpr int kExt = kEW * (kTY + 1);                // 585
-constexpr int kRow = 148;                            // per-plane metric values
 constexpr int kMatSmem = 32;                         // materials staged in smem
 
-// H box width: 66 doubles (528 B) or 68 floats (the inner box extent must
-// be a multiple of 16 bytes).
-template <typename T>
-constexpr int h_box_x() { return sizeof(T) == 8 ? kTX + 2 : kTX + 4; }
+// Tile shape: TW columns x 512/TW rows.  Each thread owns two cells: the
+// tile warps (0-7) a cell of tile row w and the cell 32 columns on (64x8),
+// or cells of tile rows 2w and 2w+1 in the same column (32x16); warp 8 and
+// warp 9 own the halo row and column.
+template <int TW>
+struct TShape {
+  static_assert(TW == 64 || TW == 32, "tile widths 64 and 32");
+  static constexpr int TX = TW, TY = 512 / TW;
+  static constexpr int BX = TX + 4, BY = TY + 2;     // interior E box, E box rows
+  static constexpr int HBY = TY + 1;                 // H box rows
+  static constexpr int EW = TX + 1;                  // ext tile row width
+  static constexpr int Ext = EW * (TY + 1);
+  // second cell of a thread: dx columns and dy rows on
+  static constexpr int DX = TW == 64 ? 32 : 0, DY = TW == 64 ? 0 : 1;
+  // per-plane metric row: [0, TY+1) iAx(j0-1..), [RY, RY+TX+1) iAy(i0-1..),
+  // [RTX, RTX+TY) itAx(j0..), [RTY, RTY+TX) itAy(i0..), RL Lz, RL+1 tLz
+  static constexpr int RY = TY + 1, RTX = RY + TX + 1, RTY = RTX + TY, RL = RTY + TX;
+  static constexpr int Row = RL + 2;
+  static constexpr int Lvals = EW + TY + 1 + TX + TY;   // Lx, Ly, tLx, tLy staged once
+  static_assert(Row <= 3 * 64 && Lvals <= kTmaThreads, "staging threads");
+};
+
+// H box width (interior variant): TX+2 doubles or TX+4 floats (the inner
+// box extent must be a multiple of 16 bytes).
+template <typename T, int TW>
+constexpr int h_box_x() { return sizeof(T) == 8 ? TW + 2 : TW + 4; }
 
 struct TmaMaps {
   CUtensorMap e[3];
   CUtensorMap h[3];
 };
 
-// Box geometry.  The interior variant loads E on x in [i0-2, i0+66) and H
-// on [i0-2, i0+64) (i0 = 2 + 64 bx); the full-domain variant (FULL, tiles
-// from i0 = 64 bx) starts both boxes at i0-4 so that the x offset stays
-// 16-byte aligned for float and double: E 72 wide, H 68 wide.
-template <typename T, bool FULL>
+// Box geometry.  The interior variant loads E on x in [i0-2, i0+TX+2) and
+// H on [i0-2, i0+TX) (i0 = 2 + TX bx); the full-domain variant (FULL, tiles
+// from i0 = TX bx) starts both boxes at i0-4 so that the x offset stays
+// 16-byte aligned for float and double: E TX+8 wide, H TX+4 wide.
+template <typename T, bool FULL, int TW = 64>
 struct TmaGeom {
-  static constexpr int ebx = FULL ? kTX + 8 : kBX;            // E box width
-  static constexpr int hbx = FULL ? kTX + 4 : h_box_x<T>();   // H box width
-  static constexpr int xo = FULL ? 3 : 1;                     // box x of ext column 0
-  static constexpr int xs_off = FULL ? 4 : 2;                 // box start = i0 - xs_off
+  using S = TShape<TW>;
+  static constexpr int ebx = FULL ? S::TX + 8 : S::BX;            // E box width
+  static constexpr int hbx = FULL ? S::TX + 4 : h_box_x<T, TW>();  // H box width
+  static constexpr int xo = FULL ? 3 : 1;                          // box x of ext column 0
+  static constexpr int xs_off = FULL ? 4 : 2;                      // box start = i0 - xs_off
 };
 
-template <typename T, bool FULL>
+template <typename T, bool FULL, int TW = 64>
 struct TmaLayout {
-  using G = TmaGeom<T, FULL>;
-  static constexpr int eslot = round128(G::ebx * kBY * (int)sizeof(T));        // per comp
-  static constexpr int hslot = round128(G::hbx * kHBY * (int)sizeof(T));
+  using S = TShape<TW>;
+  using G = TmaGeom<T, FULL, TW>;
+  static constexpr int eslot = round128(G::ebx * S::BY * (int)sizeof(T));        // per comp
+  static constexpr int hslot = round128(G::hbx * S::HBY * (int)sizeof(T));
   static constexpr int e_off = 0;
   static constexpr int h_off = e_off + kES * 3 * eslot;
   static constexpr int hs_off = h_off + kHS * 3 * hslot;
-  static constexpr int row_off = hs_off + round128(3 * kExt * (int)sizeof(T));
-  static constexpr int l_off = row_off + round128(3 * kRow * (int)sizeof(T));
-  static constexpr int mat_off = l_off + round128((kEW + kTY + 1 + kTX + kTY) * (int)sizeof(T));
+  static constexpr int row_off = hs_off + round128(3 * S::Ext * (int)sizeof(T));
+  static constexpr int l_off = row_off + round128(3 * S::Row * (int)sizeof(T));
+  static constexpr int mat_off = l_off + round128(S::Lvals * (int)sizeof(T));
   static constexpr int bar_off = mat_off + round128(9 * kMatSmem * (int)sizeof(T));
   static constexpr int bytes = bar_off + (kES + kHS) * 8 + 128;   // + base alignment
 };
 
 
-// Per-plane metric row of plane q: [0,9) iAx(j0-1..j0+7), [9,74) iAy(i0-1..i0+63),
-// [74,82) itAx(j0..j0+7), [82,146) itAy(i0..i0+63), 146 Lz, 147 tLz.
+// Per-plane metric row of plane q (TShape: RY, RTX, RTY, RL).
 // Entry r of plane q is a[q * stride] (RowEntry); entries outside the grid
 // (index < 0 or beyond the last cell, a == nullptr) and planes outside
 // [0, Nz) read as 0.
@@ -99,15 +118,16 @@ struct RowEntry {
   const T* a;
   int stride;
 };
-template <typename T>
+template <typename T, int TW>
 __device__ __forceinline__ RowEntry<T> row_entry(const FitParams<T>& p, int r, int i0, int j0) {
+  using S = TShape<TW>;
   int idx;
-  if (r < 9) { idx = j0 - 1 + r; if (idx < 0 || idx >= p.Ny) return {nullptr, 0}; return {p.iAx + idx, p.Ny}; }
-  if (r < 74) { idx = i0 - 10 + r; if (idx < 0 || idx >= p.Nx) return {nullptr, 0}; return {p.iAy + idx, p.Nx}; }
-  if (r < 82) { idx = j0 - 74 + r; if (idx < 0 || idx >= p.Ny) return {nullptr, 0}; return {p.itAx + idx, p.Ny}; }
-  if (r < 146) { idx = i0 - 82 + r; if (idx < 0 || idx >= p.Nx) return {nullptr, 0}; return {p.itAy + idx, p.Nx}; }
-  if (r == 146) return {p.Lz, 1};
-  if (r == 147) return {p.tLz, 1};
+  if (r < S::RY) { idx = j0 - 1 + r; if (idx < 0 || idx >= p.Ny) return {nullptr, 0}; return {p.iAx + idx, p.Ny}; }
+  if (r < S::RTX) { idx = i0 - 1 - S::RY + r; if (idx < 0 || idx >= p.Nx) return {nullptr, 0}; return {p.iAy + idx, p.Nx}; }
+  if (r < S::RTY) { idx = j0 - S::RTX + r; if (idx < 0 || idx >= p.Ny) return {nullptr, 0}; return {p.itAx + idx, p.Ny}; }
+  if (r < S::RL) { idx = i0 - S::RTY + r; if (idx < 0 || idx >= p.Nx) return {nullptr, 0}; return {p.itAy + idx, p.Nx}; }
+  if (r == S::RL) return {p.Lz, 1};
+  if (r == S::RL + 1) return {p.tLz, 1};
   return {nullptr, 0};
 }
 
@@ -128,14 +148,15 @@ __device__ __forceinline__ RowEntry<T> row_entry(const FitParams<T>& p, int r, i
 // 2 <= k <= Nz-3 (no z face is involved there), and the shell launches
 // cover only the planes k in {0, 1, Nz-2, Nz-1}.  Warps with no cell on or
 // next to a face take the unmasked rows.
-template <typename T, bool SM, int JM, int MODE, bool DESC>
+template <typename T, bool SM, int JM, int MODE, bool DESC, int TW>
 __global__ void __launch_bounds__(kTmaThreads, sizeof(T) == 8 ? 2 : 3)
 k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int KC) {
   constexpr bool FULL = MODE != 0;     // tiles cover x and y entirely
   constexpr bool ZFULL = MODE == 1;    // ... and every plane
   step = step_index(p, step);
-  using Lay = TmaLayout<T, (MODE != 0)>;
-  using G = TmaGeom<T, (MODE != 0)>;
+  using S = TShape<TW>;
+  using Lay = TmaLayout<T, (MODE != 0), TW>;
+  using G = TmaGeom<T, (MODE != 0), TW>;
   constexpr int HBX = G::hbx;
   constexpr int EBX = G::ebx;
   constexpr int XO = G::xo;
@@ -145,19 +166,19 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   unsigned char* sm = sm_raw + ((128 - (smem_u32(sm_raw) & 127)) & 127);
   T* Eb = reinterpret_cast<T*>(sm + Lay::e_off);     // [kES][3][SE]
   T* Hb = reinterpret_cast<T*>(sm + Lay::h_off);     // [kHS][3][SH]
-  T* Hs = reinterpret_cast<T*>(sm + Lay::hs_off);    // [3][kExt] new H of the plane
-  T* Rw = reinterpret_cast<T*>(sm + Lay::row_off);   // [3][kRow] per-plane metrics
-  T* sLx = reinterpret_cast<T*>(sm + Lay::l_off);    // Lx(i0-1..i0+63)
-  T* sLy = sLx + kEW;                                // Ly(j0-1..j0+7)
-  T* stLx = sLy + kTY + 1;                           // tLx(i0..i0+63)
-  T* stLy = stLx + kTX;                              // tLy(j0..j0+7)
+  T* Hs = reinterpret_cast<T*>(sm + Lay::hs_off);    // [3][Ext] new H of the plane
+  T* Rw = reinterpret_cast<T*>(sm + Lay::row_off);   // [3][Row] per-plane metrics
+  T* sLx = reinterpret_cast<T*>(sm + Lay::l_off);    // Lx(i0-1..i0+TX-1)
+  T* sLy = sLx + S::EW;                              // Ly(j0-1..j0+TY-1)
+  T* stLx = sLy + S::TY + 1;                         // tLx(i0..i0+TX-1)
+  T* stLy = stLx + S::TX;                            // tLy(j0..j0+TY-1)
   T* smat = reinterpret_cast<T*>(sm + Lay::mat_off);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + Lay::bar_off);  // E slots, then H slots
 
   const int Nx = p.Nx, Ny = p.Ny;
   const long long N = p.N, NxNy = p.NxNy;
   const int Nz = p.Nz;
-  const int i0 = (FULL ? 0 : 2) + blockIdx.x * kTX, j0 = (FULL ? 0 : 2) + blockIdx.y * kTY;
+  const int i0 = (FULL ? 0 : 2) + blockIdx.x * S::TX, j0 = (FULL ? 0 : 2) + blockIdx.y * S::TY;
   const int k0 = (ZFULL ? 0 : 2) + blockIdx.z * KC, k1 = min(k0 + KC, ZFULL ? Nz : Nz - 2);
   const int xs = i0 - G::xs_off, ys = j0 - 1;
   const int tid = threadIdx.x;
@@ -165,8 +186,8 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   // warp 9, which owns no cell
   const bool prod = tid == kTmaThreads - 1;
   const int pstart = k0 - 1;
-  const uint32_t e_bytes = (uint32_t)(3 * EBX * kBY * sizeof(T));
-  const uint32_t h_bytes = (uint32_t)(3 * HBX * kHBY * sizeof(T));
+  const uint32_t e_bytes = (uint32_t)(3 * EBX * S::BY * sizeof(T));
+  const uint32_t h_bytes = (uint32_t)(3 * HBX * S::HBY * sizeof(T));
 
   if (prod) {
     for (int s = 0; s < kES + kHS; s++) mbar_init(&bar[s], 1);
@@ -201,22 +222,27 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   }
 
   // owned cells, in ext-tile coordinates (ea, eb) with the origin at
-  // (i0-1, j0-1): warps 0-7 the tile cells (lane+1, w+1) and (lane+33, w+1);
-  // warp 8 the halo-row cells (lane, 0) and (lane+32, 0); warp 9 lanes 0-7
-  // the halo-column cells (0, lane+1) and lane 8 the halo-row cell (64, 0).
-  // The second cell of a thread is its first one 32 columns on.
+  // (i0-1, j0-1).  64x8: warps 0-7 the tile cells (lane+1, w+1) and
+  // (lane+33, w+1); warp 8 the halo-row cells (lane, 0) and (lane+32, 0).
+  // 32x16: warps 0-7 the tile cells (lane+1, 2w+1) and (lane+1, 2w+2); warp
+  // 8 the halo-row cell (lane, 0).  Warp 9: lanes 0..TY-1 the halo-column
+  // cells (0, lane+1) and lane TY the halo-row cell (TX, 0).  The second cell
+  // of a thread is its first one DX columns and DY rows on.
   const int warp = tid >> 5, lane = tid & 31;
   const bool tile = warp < 8;
-  const int ea0 = tile ? lane + 1 : (warp == 8 ? lane : (lane < 8 ? 0 : 64));
-  const int eb0 = tile ? warp + 1 : (warp == 8 ? 0 : (lane < 8 ? lane + 1 : 0));
-  const bool owns[2] = {warp < 9 || lane < 9, warp < 9};
-  const int ext0 = eb0 * kEW + ea0;
+  const int ea0 = tile ? lane + 1 : (warp == 8 ? lane : (lane < S::TY ? 0 : S::TX));
+  const int eb0 = tile ? (TW == 64 ? warp : 2 * warp) + 1
+                       : (warp == 8 ? 0 : (lane < S::TY ? lane + 1 : 0));
+  const bool owns[2] = {warp < 9 || lane < S::TY + 1, TW == 64 ? warp < 9 : warp < 8};
+  const int ext0 = eb0 * S::EW + ea0;
+  constexpr int dext = S::DX + S::DY * S::EW;         // ext offset of the second cell
+  const int dcell = S::DX + S::DY * Nx;               // flat offset of the second cell
   int ci[2], cj[2];
   bool hval[2], eval[2];
 #pragma unroll
   for (int r = 0; r < 2; r++) {
-    ci[r] = i0 - 1 + ea0 + 32 * r;
-    cj[r] = j0 - 1 + eb0;
+    ci[r] = i0 - 1 + ea0 + S::DX * r;
+    cj[r] = j0 - 1 + eb0 + S::DY * r;
     const bool own = owns[r];
     hval[r] = FULL ? (own && ci[r] >= 0 && ci[r] <= Nx - 1 && cj[r] >= 0 && cj[r] <= Ny - 1)
                    : (own && ci[r] <= Nx - 3 && cj[r] <= Ny - 3);
@@ -255,10 +281,13 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     iAz[r] = hval[r] ? p.iAz[m] : T(0);
     itAz[r] = eval[r] ? p.itAz[m] : T(0);
   }
-  if (tid < kEW) sLx[tid] = (i0 - 1 + tid >= 0 && i0 - 1 + tid < Nx) ? p.Lx[i0 - 1 + tid] : T(0);
-  else if (tid < kEW + kTY + 1) { const int j = j0 - 1 + tid - kEW; sLy[tid - kEW] = (j >= 0 && j < Ny) ? p.Ly[j] : T(0); }
-  else if (tid < kEW + kTY + 1 + kTX) { const int i = i0 + tid - kEW - kTY - 1; stLx[tid - kEW - kTY - 1] = i < Nx ? p.tLx[i] : T(0); }
-  else if (tid < kEW + kTY + 1 + kTX + kTY) { const int j = j0 + tid - kEW - kTY - 1 - kTX; stLy[tid - kEW - kTY - 1 - kTX] = j < Ny ? p.tLy[j] : T(0); }
+  {
+    constexpr int EW = S::EW, TX = S::TX, TY = S::TY;
+    if (tid < EW) sLx[tid] = (i0 - 1 + tid >= 0 && i0 - 1 + tid < Nx) ? p.Lx[i0 - 1 + tid] : T(0);
+    else if (tid < EW + TY + 1) { const int j = j0 - 1 + tid - EW; sLy[tid - EW] = (j >= 0 && j < Ny) ? p.Ly[j] : T(0); }
+    else if (tid < EW + TY + 1 + TX) { const int i = i0 + tid - EW - TY - 1; stLx[tid - EW - TY - 1] = i < Nx ? p.tLx[i] : T(0); }
+    else if (tid < EW + TY + 1 + TX + TY) { const int j = j0 + tid - EW - TY - 1 - TX; stLy[tid - EW - TY - 1 - TX] = j < Ny ? p.tLy[j] : T(0); }
+  }
   if (SM)
     for (int q = tid; q < 9 * p.n_mat; q += kTmaThreads) smat[q] = p.mat[q];
   const T* mat = SM ? smat : p.mat;
@@ -271,10 +300,10 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 #pragma unroll
       for (int u = 0; u < 3; u++) {
         const int r = tid - 256 + 64 * u;
-        if (r < kRow) {
-          const RowEntry<T> e = row_entry(p, r, i0, j0);
+        if (r < S::Row) {
+          const RowEntry<T> e = row_entry<T, TW>(p, r, i0, j0);
           const bool v = e.a != nullptr && q >= 0 && q < Nz;
-          cp_async<sizeof(T)>(Rw + slot * kRow + r, v ? e.a + (long long)q * e.stride : p.Lz, v);
+          cp_async<sizeof(T)>(Rw + slot * S::Row + r, v ? e.a + (long long)q * e.stride : p.Lz, v);
         }
       }
     }
@@ -288,7 +317,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
                              (ci[0] + (long long)cj[0] * Nx) * p.id_bytes;
   const long long id_plane = NxNy * p.id_bytes;
   auto id_at = [&](int r, int q) -> int {
-    const unsigned char* a = idp + (long long)q * id_plane + 32 * r * (SM ? 1 : p.id_bytes);
+    const unsigned char* a = idp + (long long)q * id_plane + dcell * r * (SM ? 1 : p.id_bytes);
     if (SM) return a[0];
     if (p.id_bytes == 1) return a[0];
     if (p.id_bytes == 2) return *reinterpret_cast<const uint16_t*>(a);
@@ -299,7 +328,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
   for (int r = 0; r < 2; r++) id[r] = (hval[r] && pstart >= 0) ? id_at(r, pstart) : 0;
   T hxp[2] = {T(0), T(0)}, hyp[2] = {T(0), T(0)};
   // per-plane cursors: the ids of plane pl+1, the outputs of cell 0 of
-  // plane pl (the second cell is 32 entries on); ring slots of E(pl), H(pl)
+  // plane pl (the second cell is dcell entries on); ring slots of E(pl), H(pl)
   // and of the metric row of pl, counted instead of taken modulo
   const unsigned char* idq = idp + (long long)(pstart + 1) * id_plane;
   const long long cn0 = ci[0] + (long long)cj[0] * Nx + (long long)pstart * NxNy;
@@ -330,7 +359,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
 #pragma unroll
       for (int r = 0; r < 2; r++) {
         if (!hval[r]) continue;
-        const unsigned char* a = idq + 32 * r * (SM ? 1 : p.id_bytes);
+        const unsigned char* a = idq + dcell * r * (SM ? 1 : p.id_bytes);
         if (SM || p.id_bytes == 1) idn[r] = a[0];
         else if (p.id_bytes == 2) idn[r] = *reinterpret_cast<const uint16_t*>(a);
         else idn[r] = (int)*reinterpret_cast<const uint32_t*>(a);
@@ -340,7 +369,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     const T* Ek = Eb + se * 3 * SE;
     const T* Ek1 = Eb + se1 * 3 * SE;
     const T* Hk = Hb + sh * 3 * SH;
-    const T* R = Rw + se * kRow;                     // row ring: also 3 slots
+    const T* R = Rw + se * S::Row;                   // row ring: also 3 slots
     const long long off = (long long)pl * NxNy;
     T* const hq1 = hq + N;
     T* const eq1 = eq + N;
@@ -356,19 +385,19 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     for (int r = 0; r < 2; r++) {
       hxn[r] = hyn[r] = T(0);
       const bool tile_cell = tile;
-      const int e = ext0 + 32 * r;
+      const int e = ext0 + dext * r;
       if (FULL && owns[r] && !hval[r]) {
         Hs[e] = T(0);
-        Hs[kExt + e] = T(0);
-        Hs[2 * kExt + e] = T(0);
+        Hs[S::Ext + e] = T(0);
+        Hs[2 * S::Ext + e] = T(0);
       }
       if (!hval[r] || (prologue && !tile_cell) || (ZFULL && pl < 0)) continue;
-      const int ea = ea0 + 32 * r, eb = eb0;
+      const int ea = ea0 + S::DX * r, eb = eb0 + S::DY * r;
       const int bi = eb * EBX + ea + XO;
       const int hb = eb * HBX + ea + XO;
       const T* m0 = mat + 9 * id[r];
       const T R0 = mul(R[eb], m0[3]);
-      const T R1 = mul(R[9 + ea], m0[4]);
+      const T R1 = mul(R[S::RY + ea], m0[4]);
       const T R2 = mul(iAz[r], m0[5]);
       T hx = Hk[hb], hy = Hk[SH + hb], hz = Hk[2 * SH + hb];
       T ex0 = Ek[bi], ey0 = Ek[SE + bi], ez0 = Ek[2 * SE + bi];
@@ -389,17 +418,17 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
         ex3 = (yf0[r] || zf1) ? z : ex3;
         ey3 = (xf0[r] || zf1) ? z : ey3;
       }
-      h_lean(p.dt, desc, R0, R1, R2, sLx[ea], sLy[eb], R[146], ex0, ey0, ez0, ey1, ez1, ex2,
+      h_lean(p.dt, desc, R0, R1, R2, sLx[ea], sLy[eb], R[S::RL], ex0, ey0, ez0, ey1, ez1, ex2,
              ez2, ex3, ey3, hx, hy, hz);
       Hs[e] = hx;
-      Hs[kExt + e] = hy;
-      Hs[2 * kExt + e] = hz;
+      Hs[S::Ext + e] = hy;
+      Hs[2 * S::Ext + e] = hz;
       hxn[r] = hx;
       hyn[r] = hy;
       if (!prologue && tile_cell) {
-        hq[32 * r] = hx;
-        hq1[32 * r] = hy;
-        hq1[N + 32 * r] = hz;
+        hq[dcell * r] = hx;
+        hq1[dcell * r] = hy;
+        hq1[N + dcell * r] = hz;
       }
     }
     __syncthreads();
@@ -408,21 +437,22 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
     // thread passed the top barrier of plane pl), stage the row of pl+2
     if (warp >= 8) stage_row(pl + 2, se == 0 ? kES - 1 : se - 1);
     if (!prologue) {
-      const T tLz = R[147];
+      const T tLz = R[S::RL + 1];
 #pragma unroll
       for (int r = 0; r < 2; r++) {
         if (!eval[r]) continue;
-        const int e = ext0 + 32 * r;
-        const int a = ea0 + 32 * r - 1, b = eb0 - 1;
+        const int e = ext0 + dext * r;
+        const int a = ea0 + S::DX * r - 1, b = eb0 + S::DY * r - 1;
         const int bi = (b + 1) * EBX + a + 1 + XO;
         const long long n = ci[r] + (long long)cj[r] * Nx + off;
         const T* m0 = mat + 9 * id[r];
-        const T R0 = mul(m0[0], R[74 + b]);
-        const T R1 = mul(m0[1], R[82 + a]);
+        const T R0 = mul(m0[0], R[S::RTX + b]);
+        const T R1 = mul(m0[1], R[S::RTY + a]);
         const T R2 = mul(m0[2], itAz[r]);
         T curl[3];
-        e_lean(R0, R1, R2, stLx[a], stLy[b], tLz, Hs[e], Hs[kExt + e], Hs[2 * kExt + e],
-               Hs[kExt + e - 1], Hs[2 * kExt + e - 1], Hs[e - kEW], Hs[2 * kExt + e - kEW],
+        e_lean(R0, R1, R2, stLx[a], stLy[b], tLz, Hs[e], Hs[S::Ext + e], Hs[2 * S::Ext + e],
+               Hs[S::Ext + e - 1], Hs[2 * S::Ext + e - 1], Hs[e - S::EW],
+               Hs[2 * S::Ext + e - S::EW],
                hxp[r], hyp[r], curl[0], curl[1], curl[2]);
         if (masked) {
           // E rows tangential to the face the cell lies on get no curl
@@ -443,7 +473,7 @@ k_tma(FitParams<T> p, const __grid_constant__ TmaMaps maps, long long step, int 
           if (JM == WK_J_ARRAY) jv = p.J[d * N + n];
           if (d == 2 && (cell_bits & (4 << r))) jv = j_in(p, d, cc, n, step, eold[d], sigma);
           const T enew = add(eold[d], mul(p.dt, sub(curl[d], mul(ieps, jv))));
-          (d == 0 ? eq : (d == 1 ? eq1 : eq1 + N))[32 * r] = enew;
+          (d == 0 ? eq : (d == 1 ? eq1 : eq1 + N))[dcell * r] = enew;
           if (JM == WK_J_ARRAY && p.use_cond) p.J[d * N + n] = mul(sigma, enew);
         }
       }
@@ -503,23 +533,23 @@ bool tma_supported(const FitParams<T>& p) {
 
 // Launch geometry cache per device: SM count and resident blocks per SM.
 struct TmaOcc { int sms = 0, per_sm = 0; bool attr = false; };
-static TmaOcc g_occ[2][2][3][3][2][64];
+static TmaOcc g_occ[2][2][3][3][2][2][64];
 
-template <typename T, bool SM, int JM, int MODE, bool DESC>
+template <typename T, bool SM, int JM, int MODE, bool DESC, int TW>
 static cudaError_t tma_occupancy(TmaOcc** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][MODE][DESC ? 1 : 0][dev];
+  TmaOcc& o = g_occ[sizeof(T) == 8 ? 0 : 1][SM ? 1 : 0][JM][MODE][DESC ? 1 : 0][TW == 32][dev];
   if (!o.attr) {
-    const int smem = TmaLayout<T, (MODE != 0)>::bytes;
-    e = cudaFuncSetAttribute(k_tma<T, SM, JM, MODE, DESC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem);
+    const int smem = TmaLayout<T, (MODE != 0), TW>::bytes;
+    e = cudaFuncSetAttribute(k_tma<T, SM, JM, MODE, DESC, TW>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&o.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, MODE, DESC>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.per_sm, k_tma<T, SM, JM, MODE, DESC, TW>,
                                                       kTmaThreads, smem);
     if (e != cudaSuccess) return e;
     if (o.per_sm < 1) o.per_sm = 1;
@@ -539,28 +569,30 @@ static int tma_mode(const FitParams<T>& p) {
   return (p.pec_face[4] == 0 && p.pec_face[5] == 0) ? 1 : 2;
 }
 
-template <typename T, bool SM, int JM, int MODE, bool DESC>
+template <typename T, bool SM, int JM, int MODE, bool DESC, int TW>
 static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cudaStream_t st,
                                       int KC) {
-  using G = TmaGeom<T, (MODE != 0)>;
+  using S = TShape<TW>;
+  using G = TmaGeom<T, (MODE != 0), TW>;
   TmaMaps maps;
   for (int d = 0; d < 3; d++) {
-    if (!encode_comp<T>(&maps.e[d], p.E_in + d * p.N, p.Nx, p.Ny, p.Nz, G::ebx, kBY) ||
-        !encode_comp<T>(&maps.h[d], p.H_in + d * p.N, p.Nx, p.Ny, p.Nz, G::hbx, kHBY))
+    if (!encode_comp<T>(&maps.e[d], p.E_in + d * p.N, p.Nx, p.Ny, p.Nz, G::ebx, S::BY) ||
+        !encode_comp<T>(&maps.h[d], p.H_in + d * p.N, p.Nx, p.Ny, p.Nz, G::hbx, S::HBY))
       return cudaErrorInvalidValue;
   }
   TmaOcc* occ = nullptr;
-  cudaError_t e = tma_occupancy<T, SM, JM, MODE, DESC>(&occ);
+  cudaError_t e = tma_occupancy<T, SM, JM, MODE, DESC, TW>(&occ);
   if (e != cudaSuccess) return e;
   const int span_x = MODE ? p.Nx : p.Nx - 4, span_y = MODE ? p.Ny : p.Ny - 4;
   const int planes = MODE == 1 ? p.Nz : p.Nz - 4;
-  const int gx = (span_x + kTX - 1) / kTX, gy = (span_y + kTY - 1) / kTY;
+  const int gx = (span_x + S::TX - 1) / S::TX, gy = (span_y + S::TY - 1) / S::TY;
   if (KC <= 0)
     KC = tma_auto_kc((long long)gx * gy, planes, (long long)occ->sms * occ->per_sm);
   const int gz = (planes + KC - 1) / KC;
   timer_begin(st);
-  k_tma<T, SM, JM, MODE, DESC><<<dim3(gx, gy, gz), kTmaThreads, TmaLayout<T, (MODE != 0)>::bytes,
-                           st>>>(p, maps, step, KC);
+  k_tma<T, SM, JM, MODE, DESC, TW><<<dim3(gx, gy, gz), kTmaThreads,
+                                     TmaLayout<T, (MODE != 0), TW>::bytes, st>>>(p, maps, step,
+                                                                                 KC);
   timer_end(st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -571,18 +603,27 @@ static cudaError_t launch_tma_variant(const FitParams<T>& p, long long step, cud
   return launch_shell_pair<T>(p, step, st, MODE == 2);
 }
 
-// One step with the TMA kernel in the mode the faces allow (see k_tma).
+// One step with the TMA kernel in the mode the faces allow (see k_tma), on
+// 64x8 tiles (rows 8 or 0, the faster on B200 at 256x256x512 in FP64 and
+// FP32) or 32x16 tiles (rows 16).
 template <typename T>
-cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC) {
+cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, int KC,
+                       int rows) {
   const bool sm_table = p.n_mat <= kMatSmem && p.id_bytes == 1;
   const int jm = p.j_mode == WK_J_SIGMA_E ? 1 : (p.j_mode == WK_J_ARRAY ? 2 : 0);
   const int mode = tma_mode(p);
   const bool desc = p.h_desc != 0;
+  const bool w32 = rows == 16;
+#define WK_TMA_WIDTH(SMV, JMV, MV, DV)                                                \
+  {                                                                                   \
+    if (w32) return launch_tma_variant<T, SMV, JMV, MV, DV, 32>(p, step, st, KC);     \
+    return launch_tma_variant<T, SMV, JMV, MV, DV, 64>(p, step, st, KC);              \
+  }
 #define WK_TMA_MODES(SMV, JMV, DV)                                                    \
   {                                                                                   \
-    if (mode == 1) return launch_tma_variant<T, SMV, JMV, 1, DV>(p, step, st, KC);    \
-    if (mode == 2) return launch_tma_variant<T, SMV, JMV, 2, DV>(p, step, st, KC);    \
-    return launch_tma_variant<T, SMV, JMV, 0, DV>(p, step, st, KC);                   \
+    if (mode == 1) WK_TMA_WIDTH(SMV, JMV, 1, DV)                                      \
+    if (mode == 2) WK_TMA_WIDTH(SMV, JMV, 2, DV)                                      \
+    WK_TMA_WIDTH(SMV, JMV, 0, DV)                                                     \
   }
 #define WK_TMA_CASE(SMV, JMV)                                                         \
   if (sm_table == SMV && jm == JMV) {                                                 \
@@ -593,6 +634,7 @@ cudaError_t launch_tma(const FitParams<T>& p, long long step, cudaStream_t st, i
   WK_TMA_CASE(false, 0) WK_TMA_CASE(false, 1) WK_TMA_CASE(false, 2)
 #undef WK_TMA_CASE
 #undef WK_TMA_MODES
+#undef WK_TMA_WIDTH
   return cudaErrorInvalidValue;
 }
 
@@ -607,7 +649,8 @@ template int tma_launches_per_step<double>(const FitParams<double>&);
 template int tma_launches_per_step<float>(const FitParams<float>&);
 template bool tma_supported<double>(const FitParams<double>&);
 template bool tma_supported<float>(const FitParams<float>&);
-template cudaError_t launch_tma<double>(const FitParams<double>&, long long, cudaStream_t, int);
-template cudaError_t launch_tma<float>(const FitParams<float>&, long long, cudaStream_t, int);
+template cudaError_t launch_tma<double>(const FitParams<double>&, long long, cudaStream_t, int,
+                                        int);
+template cudaError_t launch_tma<float>(const FitParams<float>&, long long, cudaStream_t, int, int);
 
 }  // namespace wk

@@ -192,8 +192,9 @@ class SolverFIT3D(RoutinesMixin):
         self._desc = d
         self.kernel = "auto"
         # (tile rows, planes per block), 0 = automatic: the rows pick the
-        # tile shape of the FP32-compensated TMA kernel and the batched
-        # launches (8: 64x8 tiles, 16 or 0: 32x16 tiles)
+        # tile shape of the TMA kernels and the batched launches (8: 64x8
+        # tiles, 16: 32x16 tiles, 0: 64x8 in FP64 and FP32, 32x16 with
+        # precision='fp32c')
         self.tile = (0, 0)
         # wk_fit_desc.steps_per_launch: 2 runs pairs of steps as one launch of
         # the temporal-blocking kernel where it applies, 1 one step per
