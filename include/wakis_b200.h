@@ -272,7 +272,9 @@ int wk_batch_run(const wk_batch_plan* plan, int n_steps, long long step0,
  *   wk_adj_grad: for each listed cell c = cells[q] (flat index < N),
  *                gI[q] += sum_comp lE1 inc[comp*ncell + q]     (inc: FP64,
  *                         dt (B0 H' - J) of the listed entries),
- *                gS[q] += -dt sum_comp ieps lE1 E0 smask   (when use_sigma)
+ *                gS[q] += -dt sum_comp ieps lE1 E0[comp*ncell + q] smask
+ *                         (when use_sigma; E0: dtype, the E of the listed
+ *                         entries, ncell per component like inc)
  *                (double accumulators, one entry per listed cell).
  * lH_in may equal lH_out and lE_in may equal lE_out.
  */

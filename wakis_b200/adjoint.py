@@ -180,7 +180,19 @@ class ImpedanceDesign:
         # formed as dt (B0 H' - J) instead of E' - E
         rows = np.concatenate([d * N + self.cells_np for d in range(3)])
         self.rows = torch.as_tensor(rows, device=self.dev)
-        self.Bd = _DevCSR(B0[rows, :], torch.float64, self.dev)
+        B0d = B0[rows, :].tocsr()
+        self.Bd = _DevCSR(B0d, torch.float64, self.dev)
+        # the same rows over only the H entries they read (for states whose
+        # H' is first converted to FP64: only those entries are gathered)
+        hcols = np.unique(B0d.indices)
+        self.hcols = torch.as_tensor(hcols.astype(np.int64), device=self.dev)
+        self.Bdc = _DevCSR(B0d[:, hcols], torch.float64, self.dev)
+        if self.comp:
+            # gather buffers of the design entries of the compensated state
+            self._gv = torch.empty(len(rows), dtype=s._E[0].dtype, device=self.dev)
+            self._gc = torch.empty(len(rows), dtype=s._Ec[0].dtype, device=self.dev)
+            self._hv = torch.empty(len(hcols), dtype=s._H[0].dtype, device=self.dev)
+            self._hc = torch.empty(len(hcols), dtype=s._Hc[0].dtype, device=self.dev)
         self.zd = torch.zeros(3 * nc, dtype=torch.float64, device=self.dev)
         ie, _, sg = s._dense_fields()
         self.ieps0 = ie.array.clone()
@@ -339,13 +351,29 @@ class ImpedanceDesign:
         vals = (qv * prof / bdx / bdy).astype(s.dtype).astype(np.float64)
         return torch.as_tensor(vals, device=self.dev)
 
-    def _values_into(self, out, which):
-        """E (which = 0) or H (1) of the live state into `out` (the state
-        values, or the FP64 sums v + c of the compensated state)."""
+    def _design_h_into(self, out):
+        """H of the live state at the entries the design rows of B0 read
+        (self.hcols) into `out` as FP64 (the values, or the sums v + c)."""
         st = self._live()
-        out.copy_(st[which])
         if self.comp:
-            out.add_(st[2 + which])
+            torch.index_select(st[1], 0, self.hcols, out=self._hv)
+            torch.index_select(st[3], 0, self.hcols, out=self._hc)
+            out.copy_(self._hv)
+            out.add_(self._hc)
+        else:
+            out.copy_(st[1].index_select(0, self.hcols))
+
+    def _design_e_into(self, out):
+        """E of the live state at the design entries (self.rows) into `out`
+        (3 x n_cells entries: the state values, or the FP64 sums v + c)."""
+        st = self._live()
+        if self.comp:
+            torch.index_select(st[0], 0, self.rows, out=self._gv)
+            torch.index_select(st[2], 0, self.rows, out=self._gc)
+            out.copy_(self._gv)
+            out.add_(self._gc)
+        else:
+            torch.index_select(st[0], 0, self.rows, out=out)
 
     def _segment(self, a, m, B, graph_descs=None):
         """Recompute steps a .. a+m-1 from the restored state and run their
@@ -360,7 +388,7 @@ class ImpedanceDesign:
         cond = bool(s.use_conductivity)
         bp = self._ws["beam_params"]
         Es, incs, J = B["Es"], B["incs"], B["J"]
-        self._values_into(Es[0], 0)
+        self._design_e_into(Es[0])
         par0 = s._par
         for q in range(m):
             n = a + q
@@ -372,19 +400,19 @@ class ImpedanceDesign:
                 _native.check(lib.wk_counter_add(ptr(B["ctr"]), 1, ctypes.c_void_p(st)),
                               "wk_counter_add")
                 s._par = par0 ^ ((q + 1) & 1)
-            self._values_into(Es[q + 1], 0)
+            self._design_e_into(Es[q + 1])
             # dt (B0 H' - J) at the design entries, FP64
             if B["Hd"] is None:
-                Hd = self._live()[1]
+                Hd, Bd = self._live()[1], self.Bd
             else:
-                Hd = B["Hd"]
-                self._values_into(Hd, 1)
+                Hd, Bd = B["Hd"], self.Bdc
+                self._design_h_into(Hd)
             _native.check(lib.wk_adj_e(
-                _native.WK_F64, ptr(self.Bd.rowptr), ptr(self.Bd.col), ptr(self.Bd.val),
-                self.Bd.n, ptr(Hd), ptr(self.zd), ptr(self.zd), ptr(incs[q]),
+                _native.WK_F64, ptr(Bd.rowptr), ptr(Bd.col), ptr(Bd.val),
+                Bd.n, ptr(Hd), ptr(self.zd), ptr(self.zd), ptr(incs[q]),
                 ctypes.c_void_p(st)), "wk_adj_e")
             if cond and n >= 1:
-                J.copy_(Es[q].index_select(0, self.rows))
+                J.copy_(Es[q])
                 J.mul_(self.sig_d)
                 if B["bJ"] is not None:
                     J.index_copy_(0, self.beam_rows, B["bJ"][q])
@@ -448,13 +476,14 @@ class ImpedanceDesign:
         vdt = torch.float64 if self.comp else self._live()[0].dtype
         beam_J = self._beam_rows_J(self._ws["beam_params"])
         B = {
-            "Es": torch.empty((K + 1, 3 * N), dtype=vdt, device=dev),
+            # E of the design entries after each step of the segment
+            "Es": torch.empty((K + 1, len(self.rows)), dtype=vdt, device=dev),
             "incs": torch.empty((K, len(self.zd)), dtype=torch.float64, device=dev),
-            # FP64 H' for the B0 rows: the live buffer itself only for a
-            # plain FP64 state
+            # FP64 H' for the B0 rows: the live buffer itself for a plain
+            # FP64 state, else the entries those rows read (hcols)
             "Hd": None if (not self.comp and vdt == torch.float64) else torch.empty(
-                3 * N, dtype=torch.float64, device=dev),
-            "E0": None if vdt == self.tdtype else torch.empty(3 * N, dtype=self.tdtype,
+                len(self.hcols), dtype=torch.float64, device=dev),
+            "E0": None if vdt == self.tdtype else torch.empty(len(self.rows), dtype=self.tdtype,
                                                               device=dev),
             "J": torch.empty_like(self.zd),
             "bJ": None if beam_J is None else torch.empty((K, beam_J.shape[1]),

@@ -13,7 +13,8 @@
 //   d/d ieps_c  += sum_comp lE' dt (B0 H' - J)             (wk_adj_grad)
 //   d/d sigma_c += -dt sum_comp ieps lE' E m,
 // the increment dt (B0 H' - J) of the design entries being formed in FP64
-// by the caller (no cancellation of E' - E in a float state).
+// by the caller (no cancellation of E' - E in a float state); E0 holds E of
+// the listed entries only (ncell per component, as the increments).
 // A^T and B0^T are CSR matrices assembled on the host from the same
 // coefficient tables the step kernels read (one thread per row; ~4 entries
 // per row), in the state dtype.
@@ -72,7 +73,7 @@ k_adj_grad(const long long* __restrict__ cells, long long ncell, long long N,
     const long long x = d * N + n;
     const double l = (double)lamE1[x];
     gi += l * inc[d * ncell + q];
-    if (use_sigma) gs -= dt * (double)ieps[x] * l * (double)E0[x] * (double)smask[x];
+    if (use_sigma) gs -= dt * (double)ieps[x] * l * (double)E0[d * ncell + q] * (double)smask[x];
   }
   gI[q] += gi;
   gS[q] += gs;
