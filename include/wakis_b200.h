@@ -116,7 +116,8 @@ typedef struct wk_fit_desc {
    * and the planes per thread of the two-pass kernels.  tile_rows sets the
    * tile shape of the TMA kernels and of the batched launches: 8 for 64x8
    * tiles, 16 for 32x16 tiles, 0 for the faster on B200 (64x8 in FP64 and
-   * FP32, 32x16 in WK_F32C and the batched launches).                      */
+   * FP32; in WK_F32C 32x16 on planes of 256x256 cells or more, else 64x8;
+   * 32x16 in the batched launches).                                        */
   int kernel;
   int tile_rows, tile_planes;
   /* WK_F32C only: per-component compensation words of E and H (bf16 bit

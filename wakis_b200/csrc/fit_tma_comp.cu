@@ -74,9 +74,13 @@ cudaError_t launch_tma_comp(const wk_fit_desc* d, const FitParams<double>& p, in
   // compensation words by TMA: 16-byte row pitch and component bases
   const bool ct = p.Nx % 8 == 0 && ((uintptr_t)cs.Hc_in % 16) == 0 &&
                   ((uintptr_t)cs.Ec_in % 16) == 0;
-  // tile shape: 64x8 with tile_rows == 8, else 32x16 (the faster on B200:
-  // less halo work per tile, the same rows for every cell)
-  const bool w32 = d->tile_rows != 8;
+  // tile shape: 32x16 with tile_rows == 16, 64x8 with 8; by default 32x16
+  // on planes of 256x256 cells or more (less halo work per tile; the same
+  // rows for every cell) and 64x8 below.  Measured on B200 (Gcell-steps/s,
+  // 64x8 / 32x16): 128x128x256 47.7 / 45.2, 256x256x512 58.5 / 59.7,
+  // 448x448x896 63.7 / 63.8.
+  const bool w32 = d->tile_rows == 16 ||
+                   (d->tile_rows != 8 && (long long)p.Nx * p.Ny >= 256LL * 256);
   const CompDims cd = w32 ? comp_dims<32>(full, ct) : comp_dims<64>(full, ct);
   for (int c = 0; c < 3; c++) {
     if (!encode_3d(&maps.e[c], cs.E_in + c * p.N, 4, p.Nx, p.Ny, p.Nz, cd.ebx, cd.by) ||

@@ -193,8 +193,9 @@ class SolverFIT3D(RoutinesMixin):
         self.kernel = "auto"
         # (tile rows, planes per block), 0 = automatic: the rows pick the
         # tile shape of the TMA kernels and the batched launches (8: 64x8
-        # tiles, 16: 32x16 tiles, 0: 64x8 in FP64 and FP32, 32x16 with
-        # precision='fp32c')
+        # tiles, 16: 32x16 tiles, 0: 64x8 in FP64 and FP32; with
+        # precision='fp32c' 32x16 on planes of 256x256 cells or more and in
+        # the batched launches, else 64x8)
         self.tile = (0, 0)
         # wk_fit_desc.steps_per_launch: 2 runs pairs of steps as one launch of
         # the temporal-blocking kernel where it applies, 1 one step per
