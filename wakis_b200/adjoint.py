@@ -187,11 +187,12 @@ class ImpedanceDesign:
         hcols = np.unique(B0d.indices)
         self.hcols = torch.as_tensor(hcols.astype(np.int64), device=self.dev)
         self.Bdc = _DevCSR(B0d[:, hcols], torch.float64, self.dev)
+        # gather buffers of the design entries (E) and of the H entries the
+        # design rows read, in the state types
+        self._hv = torch.empty(len(hcols), dtype=s._H[0].dtype, device=self.dev)
         if self.comp:
-            # gather buffers of the design entries of the compensated state
             self._gv = torch.empty(len(rows), dtype=s._E[0].dtype, device=self.dev)
             self._gc = torch.empty(len(rows), dtype=s._Ec[0].dtype, device=self.dev)
-            self._hv = torch.empty(len(hcols), dtype=s._H[0].dtype, device=self.dev)
             self._hc = torch.empty(len(hcols), dtype=s._Hc[0].dtype, device=self.dev)
         self.zd = torch.zeros(3 * nc, dtype=torch.float64, device=self.dev)
         ie, _, sg = s._dense_fields()
@@ -361,7 +362,8 @@ class ImpedanceDesign:
             out.copy_(self._hv)
             out.add_(self._hc)
         else:
-            out.copy_(st[1].index_select(0, self.hcols))
+            torch.index_select(st[1], 0, self.hcols, out=self._hv)
+            out.copy_(self._hv)
 
     def _design_e_into(self, out):
         """E of the live state at the design entries (self.rows) into `out`
