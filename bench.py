@@ -500,7 +500,8 @@ def run_adjoint(args):
                          "design cells (upstream's clamp), fixed for every evaluation",
             "fd": "FP64 forward runs, Richardson-extrapolated central differences"}
     for name, r in runs.items():
-        line[name] = {"loss": r["L"], "grad_rel_err_max": max(errs[name]),
+        line[name] = {"loss": r["L"],
+                      "grad_rel_err_max": max(errs[name]) if errs[name] else None,
                       "grad_rel_err": errs[name], "forward_s": r["forward_s"],
                       "backward_s": r["backward_s"], "setup_s": r["setup_s"],
                       "forward_gcell_steps_per_s": N * nsteps / r["forward_s"] / 1e9,
