@@ -24,6 +24,7 @@
 #include "abi_internal.h"
 #include "fit_common.cuh"
 #include "fit_kernels.cuh"
+#include "tma_util.cuh"
 
 using namespace wk;
 
@@ -236,30 +237,39 @@ __device__ __forceinline__ bool adj_src(int i, int j, int q, int Nx, int Ny, int
   return c.k >= 0 && c.k < Nz;
 }
 
-// factor and adjoint value of the three components of one entry (0 where
-// adj_src gives no cell)
-template <typename L>
-struct AdjRaw {
-  L f[3], v[3];
-};
+// Raw inputs of the entries of one plane (the factor and adjoint value of
+// the three components) are staged in shared memory by cp.async two planes
+// ahead, in a 3-slot ring [slot][value][entry]: values f0 f1 f2 v0 v1 v2;
+// entry tid is the thread's own cell, kATh + tid its halo entry.  Each
+// thread stages and reads only its own entries.
+constexpr int kAStage = kATh + kAHalo;             // staged entries per plane
+constexpr int kASlots = 3;
 
+// stage the entry (i, j) of plane q into dst[0 .. 5 kAStage) (zero-filled
+// where adj_src gives no cell)
 template <int DIR, typename L>
-__device__ __forceinline__ void adj_raw(const L* fac, const L* lam, int i, int j, int q, int Nx,
-                                        int Ny, int Nz, long long N, AdjRaw<L>& r) {
+__device__ __forceinline__ void adj_stage(const L* fac, const L* lam, int i, int j, int q, int Nx,
+                                          int Ny, int Nz, long long N, L* dst) {
   Cell c;
   const bool v = adj_src<DIR>(i, j, q, Nx, Ny, Nz, c);
   const long long n = v ? c.i + (long long)c.j * Nx + (long long)c.k * Nx * (long long)Ny : 0;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    r.f[d] = v ? fac[d * N + n] : L(0);
-    r.v[d] = v ? lam[d * N + n] : L(0);
+    cp_async<sizeof(L)>(dst + d * kAStage, v ? fac + d * N + n : fac, v);
+    cp_async<sizeof(L)>(dst + (3 + d) * kAStage, v ? lam + d * N + n : lam, v);
   }
 }
 
+// products of a staged entry into the plane slot (entry e)
 template <typename L>
-__device__ __forceinline__ void adj_put(const AdjRaw<L>& r, L* slot, int e) {
+__device__ __forceinline__ void adj_put(const L* src, L* slot, int e) {
 #pragma unroll
-  for (int d = 0; d < 3; d++) slot[d * kAEnt + e] = mul(r.f[d], r.v[d]);
+  for (int d = 0; d < 3; d++) slot[d * kAEnt + e] = mul(src[d * kAStage], src[(3 + d) * kAStage]);
+}
+
+template <typename L>
+constexpr int adj_tile_smem() {
+  return (kASlots * 3 * kAEnt + kASlots * 6 * kAStage) * (int)sizeof(L);
 }
 
 // DIR > 0: xout = xin + dt tL pmc (sum of u), lam = lamE (wk_adj_h_fit);
@@ -268,7 +278,9 @@ template <typename T, typename L, int DIR>
 __global__ void __launch_bounds__(kATh, 3)
 k_adj_tile(FitParams<T> p, const L* __restrict__ fac, const L* __restrict__ lam, const L* xin,
            const L* __restrict__ decay, L* xout, int KC) {
-  __shared__ L S[3][3 * kAEnt];                    // [slot][comp][entry]
+  extern __shared__ __align__(16) unsigned char adj_sm[];
+  L* S = reinterpret_cast<L*>(adj_sm);             // [kASlots][3][kAEnt] products
+  L* R = S + kASlots * 3 * kAEnt;                  // [kASlots][6][kAStage] staged inputs
   constexpr int o = DIR > 0 ? 0 : 1;               // entry of tile cell (0, 0)
   const int Nx = p.Nx, Ny = p.Ny, Nz = p.Nz;
   const long long N = p.N;
@@ -284,23 +296,33 @@ k_adj_tile(FitParams<T> p, const L* __restrict__ fac, const L* __restrict__ lam,
   const int ha = tid < kAY ? (DIR > 0 ? kAX : -1) : tid - kAY;
   const int hb = tid < kAY ? tid : (DIR > 0 ? kAY : -1);
   const int he = (hb + o) * kAW + ha + o;
-  // plane q written at iteration it: p0 + 1 + it (u(k+1) or w(k)); slot 0
-  // holds plane p0 (u(k0) or w(k0-1))
+  // plane p0 + t is staged as group t into ring slot t % 3 (t = 0 .. n,
+  // n = k1 - k0); its products go into plane slot t % 3 at iteration t - 1
+  // (slot 0 before the march): u(k0 + t) or w(k0 - 1 + t)
   const int p0 = DIR > 0 ? k0 : k0 - 1;
-  AdjRaw<L> r1, r2;
-  adj_raw<DIR>(fac, lam, i, j, p0, Nx, Ny, Nz, N, r2);
-  adj_put(r2, S[0], e0);
-  if (halo) {
-    AdjRaw<L> h;
-    adj_raw<DIR>(fac, lam, i0 + ha, j0 + hb, p0, Nx, Ny, Nz, N, h);
-    adj_put(h, S[0], he);
-  }
-  adj_raw<DIR>(fac, lam, i, j, p0 + 1, Nx, Ny, Nz, N, r1);
-  int sa = 0;                                      // slot of plane p0 + it
+  const int n = k1 - k0;
+  auto stage = [&](int t) {
+    if (t <= n) {
+      L* dst = R + (t % kASlots) * 6 * kAStage;
+      adj_stage<DIR>(fac, lam, i, j, p0 + t, Nx, Ny, Nz, N, dst + tid);
+      if (halo) adj_stage<DIR>(fac, lam, i0 + ha, j0 + hb, p0 + t, Nx, Ny, Nz, N, dst + kATh + tid);
+    }
+    cp_async_commit();   // one group per plane (empty past the last one)
+  };
+  auto put = [&](int t, L* slot) {
+    const L* src = R + (t % kASlots) * 6 * kAStage;
+    adj_put(src + tid, slot, e0);
+    if (halo) adj_put(src + kATh + tid, slot, he);
+  };
+  stage(0);
+  stage(1);
+  stage(2);
+  cp_async_wait<2>();                              // group 0 (this thread's entries)
+  put(0, S);
+  int sa = 0;                                      // plane slot of plane p0 + it
   for (int k = k0; k < k1; k++) {
-    const int sb = sa == 2 ? 0 : sa + 1;           // slot of plane p0 + it + 1
-    const int q = p0 + 1 + (k - k0);
-    if (k + 1 < k1) adj_raw<DIR>(fac, lam, i, j, q + 1, Nx, Ny, Nz, N, r2);
+    const int it = k - k0;
+    const int sb = sa == 2 ? 0 : sa + 1;           // plane slot of plane p0 + it + 1
     const long long m = i + (long long)j * Nx + (long long)k * p.NxNy;
     L xi[3], dc[3];
 #pragma unroll
@@ -308,17 +330,16 @@ k_adj_tile(FitParams<T> p, const L* __restrict__ fac, const L* __restrict__ lam,
       xi[e] = own ? xin[e * N + m] : L(0);
       dc[e] = (DIR < 0 && own && decay) ? decay[e * N + m] : L(1);
     }
-    adj_put(r1, S[sb], e0);
-    if (halo) {
-      AdjRaw<L> h;
-      adj_raw<DIR>(fac, lam, i0 + ha, j0 + hb, q, Nx, Ny, Nz, N, h);
-      adj_put(h, S[sb], he);
-    }
+    cp_async_wait<1>();                            // group it + 1
+    put(it + 1, S + sb * 3 * kAEnt);
+    // the ring slot of group it was read at iteration it - 1, before the
+    // barrier that ended it: stage group it + 3 there
+    stage(it + 3);
     __syncthreads();
     if (own) {
       if (DIR > 0) {
-        const L* uc = S[sa];                       // u(k)
-        const L* un = S[sb];                       // u(k+1)
+        const L* uc = S + sa * 3 * kAEnt;          // u(k)
+        const L* un = S + sb * 3 * kAEnt;          // u(k+1)
         const L u0 = uc[e0], u1 = uc[kAEnt + e0], u2 = uc[2 * kAEnt + e0];
         const L u0y = uc[e0 + kAW], u2y = uc[2 * kAEnt + e0 + kAW];
         const L u1x = uc[kAEnt + e0 + 1], u2x = uc[2 * kAEnt + e0 + 1];
@@ -329,8 +350,8 @@ k_adj_tile(FitParams<T> p, const L* __restrict__ fac, const L* __restrict__ lam,
         for (int e = 0; e < 3; e++)
           xout[e * N + m] = add(xi[e], mul(mul(dt, (L)coltL(p, e, i, j, k)), acc[e]));
       } else {
-        const L* wc = S[sb];                       // w(k)
-        const L* wp = S[sa];                       // w(k-1)
+        const L* wc = S + sb * 3 * kAEnt;          // w(k)
+        const L* wp = S + sa * 3 * kAEnt;          // w(k-1)
         const L w0 = wc[e0], w1 = wc[kAEnt + e0], w2 = wc[2 * kAEnt + e0];
         const L w0y = wc[e0 - kAW], w2y = wc[2 * kAEnt + e0 - kAW];
         const L w1x = wc[kAEnt + e0 - 1], w2x = wc[2 * kAEnt + e0 - 1];
@@ -341,9 +362,9 @@ k_adj_tile(FitParams<T> p, const L* __restrict__ fac, const L* __restrict__ lam,
           xout[e * N + m] = sub(mul(dc[e], xi[e]), mul((L)colL(p, e, i, j, k), acc[e]));
       }
     }
-    r1 = r2;
     sa = sb;
   }
+  cp_async_wait<0>();                              // no copy outlives the block
 }
 
 int check_common(int dtype, const void* a, const void* b, long long n, const char* where) {
@@ -437,8 +458,9 @@ dim3 adj_tile_grid(const wk_fit_desc* d, int* KC) {
 }
 
 template <typename T, typename L>
-void adj_fit_run(const wk_fit_desc* d, const FitParams<T>& p, int which, const void* fac,
-                 const void* a, const void* b, const void* decay, void* out, cudaStream_t st) {
+cudaError_t adj_fit_run(const wk_fit_desc* d, const FitParams<T>& p, int which, const void* fac,
+                        const void* a, const void* b, const void* decay, void* out,
+                        cudaStream_t st) {
   const long long N = (long long)d->Nx * d->Ny * d->Nz;
   if (d->kernel == WK_KERNEL_CELL || !fac) {
     if (which == 0)
@@ -446,27 +468,45 @@ void adj_fit_run(const wk_fit_desc* d, const FitParams<T>& p, int which, const v
     else
       k_adj_e_fit<T, L><<<blocks(N), kAdjThreads, 0, st>>>(p, (const L*)a, (const L*)b,
                                                              (const L*)decay, (L*)out);
-    return;
+    return cudaSuccess;
   }
   int KC;
   const dim3 grid = adj_tile_grid(d, &KC);
+  constexpr int smem = adj_tile_smem<L>();
+  // the dynamic shared memory above 48 KB, once per kernel and device
+  static bool attr[2][64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[which][dev]) {
+    e = which == 0
+        ? cudaFuncSetAttribute(k_adj_tile<T, L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem)
+        : cudaFuncSetAttribute(k_adj_tile<T, L, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem);
+    if (e != cudaSuccess) return e;
+    attr[which][dev] = true;
+  }
   if (which == 0)
-    k_adj_tile<T, L, 1><<<grid, kATh, 0, st>>>(p, (const L*)fac, (const L*)a, (const L*)b,
-                                               nullptr, (L*)out, KC);
+    k_adj_tile<T, L, 1><<<grid, kATh, smem, st>>>(p, (const L*)fac, (const L*)a, (const L*)b,
+                                                  nullptr, (L*)out, KC);
   else
-    k_adj_tile<T, L, -1><<<grid, kATh, 0, st>>>(p, (const L*)fac, (const L*)a, (const L*)b,
-                                                (const L*)decay, (L*)out, KC);
+    k_adj_tile<T, L, -1><<<grid, kATh, smem, st>>>(p, (const L*)fac, (const L*)a, (const L*)b,
+                                                   (const L*)decay, (L*)out, KC);
+  return cudaSuccess;
 }
 
 template <typename L>
 int adj_fit_launch(const wk_fit_desc* d, int which, const void* fac, const void* a,
                    const void* b, const void* decay, void* out, cudaStream_t st) {
   const bool coef64 = d->dtype == WK_F64 || d->dtype == WK_F32C;
-  if (coef64)
-    adj_fit_run<double, L>(d, make_params<double>(d, d->par), which, fac, a, b, decay, out, st);
-  else
-    adj_fit_run<float, L>(d, make_params<float>(d, d->par), which, fac, a, b, decay, out, st);
-  return WK_OK;
+  const cudaError_t e =
+      coef64 ? adj_fit_run<double, L>(d, make_params<double>(d, d->par), which, fac, a, b,
+                                      decay, out, st)
+             : adj_fit_run<float, L>(d, make_params<float>(d, d->par), which, fac, a, b, decay,
+                                     out, st);
+  return e == cudaSuccess ? WK_OK : -(int)e;
 }
 
 int adj_fit(const wk_fit_desc* d, int dtype, int which, const void* fac, const void* a,
@@ -478,8 +518,9 @@ int adj_fit(const wk_fit_desc* d, int dtype, int which, const void* fac, const v
   if ((long long)d->Nx * d->Ny * d->Nz >= (1LL << 31))
     return wk_fail(WK_E_SHAPE, "%s: more than 2^31 cells", where);
   cudaStream_t st = (cudaStream_t)stream;
-  if (dtype == WK_F64) adj_fit_launch<double>(d, which, fac, a, b, decay, out, st);
-  else adj_fit_launch<float>(d, which, fac, a, b, decay, out, st);
+  rc = dtype == WK_F64 ? adj_fit_launch<double>(d, which, fac, a, b, decay, out, st)
+                       : adj_fit_launch<float>(d, which, fac, a, b, decay, out, st);
+  if (rc) return wk_fail(rc, "%s: %s", where, cudaGetErrorString((cudaError_t)-rc));
   return wk_check_launch(where);
 }
 
