@@ -35,7 +35,7 @@ from . import geometry
 
 KC_CANDIDATES = (0, 4, 8, 16, 32)
 # planes per work item tried by the autotuner of the batched launches
-BATCH_KC_CANDIDATES = (16, 32, 48, 64, 96)
+BATCH_KC_CANDIDATES = (16, 32, 48, 64, 96, 128, 192)
 # tile-shape policies of the batched launches: every instance on 64x8 or
 # 32x16 tiles, or each on the shape whose tiles leave fewer lanes idle
 TILE_POLICIES = ("64x8", "fill", "32x16")
